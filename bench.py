@@ -1,0 +1,387 @@
+#!/usr/bin/env python
+"""Benchmark of the happyray hot path on B200: per-frame grid rebuild + traversal.
+
+Default workload (the configuration the headline metric is quoted on):
+  c2: two-level grid over 1,048,576 seeded triangles (64 clusters of level-4 icospheres +
+      ground plane), top density 1/16, leaf density 2; 1920x1080 primary rays + 8 cosine AO
+      rays per hit, AO radius 0.1 x bounds diagonal, PCG32 per pixel.
+A step is one frame: device key-frame interpolation + bounds, two-level grid rebuild,
+primary + AO traversal.  value = rays traced / step time (Mrays/s), whole job over all GPUs.
+Other workloads: c1 (uniform grid, 129x129 heightfield, 256x256 primary rays) and c3
+(2,097,152 triangles, 16 curl-noise key frames, rebuild per frame, 1280x720 path tracing).
+
+Multi-GPU (torchrun): independent replicas, one per GPU (the path has no exchange step).
+`--impl reference` times the CPU restatement of the reference's build + traversal
+(oracle/, all host threads) on the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import signal
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "Mrays/s (AO, PT) and grid rebuild ms per frame; p50/p99 request latency"
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def workload(name: str):
+    from happyray_b200 import scenes as S
+    if name == "c1":
+        v, f = S.heightfield(129, 0)
+        return dict(name="c1_uniform_primary_heightfield_256", v=v, f=f, kind=0, exact=True, ug=5.0,
+                    cam=S.camera_c1((256, 256)), mode=0, frames=None)
+    if name == "c2":
+        v, f = S.clusters(1_048_576, seed=0)
+        return dict(name="c2_two_level_ao_1M_1080p", v=v, f=f, kind=1, top=0.0625, leaf=2.0,
+                    cam=S.camera_at_bounds(v, (1920, 1080)), mode=3, ao=8, frames=None)
+    if name == "c3":
+        v, f = S.clusters(2_097_152, seed=0)
+        frames = S.curl_keyframes(v, 16, amp=0.02, octaves=4, seed=0)
+        return dict(name="c3_two_level_keyframe_pt_2M_720p", v=v, f=f, kind=1, top=0.0625, leaf=2.0,
+                    cam=S.camera_at_bounds(v, (1280, 720)), mode=1, bounces=4, frames=frames)
+    raise SystemExit(f"unknown config {name}")
+
+
+def algorithmic_build_bytes(gi, nv, ntri, lerp=True):
+    """Bytes read + written once by each stage (per-unit figures of the build roofline):
+    uniform 40V + 2M + 36P + 8C, two-level 104V + 48N + 52 P_top + 44 C_top + 36 P_leaf + 8 C_leaf,
+    M = 12N + 16V; the 40V interpolation term is kept since every step interpolates."""
+    if gi["kind"] == 0:
+        M = 12 * ntri + 16 * nv
+        return (40 * nv if lerp else 0) + 2 * M + 36 * gi["num_pairs"] + 8 * gi["num_cells"]
+    return (104 * nv + 48 * ntri + 52 * gi["num_top_pairs"] + 44 * gi["num_cells"] + 36 * gi["num_pairs"]
+            + 8 * gi["num_leaves"] - (0 if lerp else 40 * nv))
+
+
+def trace_bytes(rays, cells, tests):
+    """Algorithmic traversal bytes: per ray 28 B ray + 16 B hit, 8 B per cell or leaf visited,
+    52 B per triangle test (4 B reference + 12 B indices + 36 B vertices)."""
+    return 44 * rays + 8 * cells + 52 * tests
+
+
+class ClockSampler:
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        out = ROOT / "gpurun_out"
+        out.mkdir(exist_ok=True)
+        self.path = out / f"clocks_gpu{self.index}.csv"
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.send_signal(signal.SIGTERM)
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.fh.close()
+
+    def summary(self):
+        if not self.path or not self.path.exists():
+            return None
+        rows = [r.split(",") for r in self.path.read_text().strip().splitlines() if r.count(",") >= 8]
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if "Active" in r[5 + i] and "Not" not in r[5 + i]})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    if ws <= 1:
+        return 0, 1, 0
+    import torch.distributed as dist
+    from datetime import timedelta
+    rank = int(os.environ["RANK"])
+    local = int(os.environ.get("LOCAL_RANK", rank))
+    import torch
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    return rank, ws, local
+
+
+def cpu_baseline(W, kind_budget_s=25.0):
+    """The oracle (CPU restatement of the reference's build and traversal) on a bounded
+    sample of the workload, all host threads: full build + a strided pixel sample, scaled."""
+    import oracle as O
+    v, f = W["v"], W["f"]
+    frames = W["frames"]
+    src = frames[0] if frames is not None else v
+    t0 = time.perf_counter()
+    v4, bmin, bmax = O.lerp_bounds(src, frames[1] if frames is not None else src, 0.5 if frames is not None else 1.0)
+    if W["kind"] == 0:
+        b = O.build_ug(v4, f, bmin, bmax, W["ug"], W["exact"])
+    else:
+        b = O.build_tl(v4, f, bmin, bmax, W["top"], W["leaf"])
+    t_build = time.perf_counter() - t0
+    cam = W["cam"]
+    oc = O.camera(cam["position"], cam["orientation"], cam["up"], cam["fov"], cam["res_x"], cam["res_y"])
+    npx = cam["res_x"] * cam["res_y"]
+    stride = 1 if W["mode"] != 1 else 2
+    t1 = time.perf_counter()
+    if W["mode"] == 3:
+        _, rays = O.render_ao(b, oc, W["ao"], float(np.float32(0.1) * b.diag()), 0x853c49e6748fea9b, pixel_stride=stride)
+    elif W["mode"] == 1:
+        _, rays = O.render_pt(b, oc, O.make_light(), W["bounces"], 0.7, float(np.float32(1e-4) * b.diag()),
+                              0x853c49e6748fea9b, pixel_stride=stride)
+    else:
+        org, d = O.primary_rays(oc)
+        O.trace(b, org[::stride], d[::stride])
+        rays = org[::stride].shape[0]
+    t_trace = time.perf_counter() - t1
+    sampled = len(range(0, npx, stride))
+    scale = npx / sampled
+    est = t_build + t_trace * scale
+    return {"value": rays * scale / est / 1e6, "unit": "Mrays/s", "cores": O.num_threads(), "kind": "port",
+            "sample": f"full build ({t_build * 1e3:.0f} ms) + every {stride}th pixel ({sampled} px, "
+                      f"{rays} rays, {t_trace * 1e3:.0f} ms) scaled to the full frame",
+            "build_ms": t_build * 1e3}
+
+
+def run_reference(args, W, rank, ws):
+    if rank != 0:
+        return
+    import oracle as O
+    for _ in range(args.warmup):
+        cpu_baseline(W)
+    vals, builds = [], []
+    t0 = time.perf_counter()
+    res = None
+    for _ in range(args.steps):
+        res = cpu_baseline(W)
+        vals.append(res["value"])
+        builds.append(res["build_ms"])
+    wall = time.perf_counter() - t0
+    value = statistics.median(vals)
+    line = {"metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": wall * 1e3 / max(1, args.steps), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+            "config": {"workload": W["name"], "triangles": int(W["f"].shape[0])}, "impl": "reference",
+            "build_ms_per_frame": statistics.median(builds),
+            "cpu_baseline": {"value": value, "unit": "Mrays/s", "cores": O.num_threads(), "kind": "port",
+                             "sample": res["sample"]},
+            "e2e": {"value": value, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    rank, ws, local = dist_setup() if os.environ.get("WORLD_SIZE") else (0, 1, 0)
+
+    W = workload(args.config)
+    if args.impl == "reference":
+        run_reference(args, W, rank, ws)
+        return
+
+    import torch
+    from happyray_b200 import Engine
+    dev = local
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream(device=dev)
+    eng = Engine(dev, stream=stream.cuda_stream)
+    v, f, cam = W["v"], W["f"], W["cam"]
+    frames = W["frames"]
+    if frames is None:
+        frames = v[None]
+    eng.set_keyframes(frames, f)
+    if W["kind"] == 0:
+        eng.set_uniform_density(W["ug"])
+    else:
+        eng.setGridDensities(W["top"], W["leaf"])
+    eng.setCamera(cam["position"], cam["orientation"], cam["up"], cam["fov"], cam["res_x"], cam["res_y"])
+    if W["mode"] == 3:
+        eng.set_integrator(ao_samples=W["ao"], ao_radius=-0.1)
+    elif W["mode"] == 1:
+        eng.set_integrator(pt_bounces=W["bounces"], albedo=0.7)
+        eng.setLights((0.4, 0.4, 1.0), (0.2, 0.0, 0.0), (0.0, 0.2, 0.0), 20.0)
+    npx = cam["res_x"] * cam["res_y"]
+    d_fb = torch.zeros(npx * 3, dtype=torch.float32, device=f"cuda:{dev}")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{dev}")
+    K = frames.shape[0]
+    times = [16.0 * k / 120.0 for k in range(120)] if K > 1 else [0.0]
+
+    def frame_time(i):
+        t = times[i % len(times)]
+        return t if K > 1 else 0.0
+
+    def step(i, evs=None):
+        eng.set_frame_time(frame_time(i), 0.0)
+        if evs:
+            evs[0].record(stream)
+        eng.build(W["kind"], W.get("exact", True))
+        if evs:
+            evs[1].record(stream)
+        eng.render_device(d_fb, 0, W["mode"])
+        if evs:
+            evs[2].record(stream)
+
+    # algorithmic figures from an instrumented frame (not timed)
+    eng.set_stats(True)
+    eng.counters(reset=True)
+    step(0)
+    eng.sync()
+    st = eng.counters(reset=True)
+    eng.set_stats(False)
+    gi = eng.grid_info()
+    rays_per_step = st["rays"]
+    b_trace = trace_bytes(st["rays"], st["cells"], st["tests"])
+    b_build = algorithmic_build_bytes(gi, v.shape[0], f.shape[0], lerp=True)
+
+    for i in range(args.warmup):
+        step(i)
+    eng.sync()
+    torch.cuda.synchronize()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    l0 = eng.counters()["launches"]
+    with ClockSampler(dev) as clk:
+        torch.cuda.synchronize()
+        for i in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()   # L2 flush between timed steps (256 MiB > 126 MB L2), outside the events
+            step(args.warmup + i, evs[i])
+        eng.sync()
+        torch.cuda.synchronize()
+    launches = eng.counters()["launches"] - l0
+    build_ms = [e[0].elapsed_time(e[1]) for e in evs]
+    trace_ms = [e[1].elapsed_time(e[2]) for e in evs]
+    step_ms = [b + t for b, t in zip(build_ms, trace_ms)]
+    total_ms = sum(step_ms)
+    if ws > 1:
+        import torch.distributed as dist
+        tt = torch.tensor([total_ms], dtype=torch.float64, device=f"cuda:{dev}")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        total_ms = float(tt.item())
+    value = ws * rays_per_step * args.steps / (total_ms * 1e-3) / 1e6
+
+    # end to end through the public API: pinned host inputs, upload + build + render + readback
+    e2e = None
+    if not args.no_e2e:
+        hv = torch.from_numpy(np.ascontiguousarray(frames[0])).pin_memory().numpy()
+        hf = torch.from_numpy(f.view(np.int32)).pin_memory().numpy().view(np.uint32)
+        hfb = torch.zeros((npx, 3), dtype=torch.float32).pin_memory().numpy()
+        e_ms = []
+        for i in range(args.warmup + args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            eng.upload(hv, hv, hf, 1.0)
+            eng.build(W["kind"], W.get("exact", True))
+            eng.renderFrame(hfb, 0, W["mode"])
+            b.record(stream)
+            b.synchronize()
+            if i >= args.warmup:
+                e_ms.append(a.elapsed_time(b))
+        et = sum(e_ms)
+        if ws > 1:
+            import torch.distributed as dist
+            tt = torch.tensor([et], dtype=torch.float64, device=f"cuda:{dev}")
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            et = float(tt.item())
+        e2e = {"value": ws * rays_per_step * args.steps / (et * 1e-3) / 1e6, "unit": "Mrays/s",
+               "h2d_bytes_per_step": int(2 * hv.nbytes + hf.nbytes), "d2h_bytes_per_step": int(hfb.nbytes),
+               "ms_per_step": et / args.steps}
+
+    if rank != 0:
+        eng.cleanup()
+        if ws > 1:
+            import torch.distributed as dist
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+    peak, peak_kind = peaks()
+    kern = {0: "k_render_primary", 1: "k_render_pt", 3: "k_render_ao"}[W["mode"]]
+    tr_med = statistics.median(trace_ms)
+    achieved = b_trace / (tr_med * 1e-3) / 1e9
+    traffic = None
+    prof = ROOT / "profiles" / f"{kern}__{W['name']}.md"
+    if prof.exists():
+        for line in prof.read_text().splitlines():
+            if line.startswith("dram_bytes_per_launch:"):
+                traffic = float(line.split(":")[1])
+    bmed = statistics.median(build_ms)
+    line = {
+        "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene generators, no dataset)",
+        "config": {"workload": W["name"], "triangles": int(f.shape[0]), "vertices": int(v.shape[0]),
+                   "resolution": [cam["res_x"], cam["res_y"]], "grid": "two-level" if W["kind"] else "uniform",
+                   "densities": [W.get("top", W.get("ug")), W.get("leaf")], "l2": "flushed between steps (256 MiB write)",
+                   "parallelism": f"replicas x{ws}"},
+        "rays_per_step": rays_per_step, "build_ms_per_frame": bmed, "trace_ms_per_frame": tr_med,
+        "trace_mrays_s": rays_per_step / (tr_med * 1e-3) / 1e6,
+        "grid": {k: gi[k] for k in ("res", "num_cells", "num_leaves", "num_pairs", "num_top_pairs")},
+        "roofline": {"bound": "hbm", "kernel": kern, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
+                     "algorithmic_bytes_per_launch": b_trace},
+        "build_roofline": {"bound": "hbm", "achieved": b_build / (bmed * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                           "frac": b_build / (bmed * 1e-3) / 1e9 / peak, "algorithmic_bytes": b_build},
+        "gpu_launches": launches,
+        "e2e": e2e,
+    }
+    clk_s = clk.summary()
+    if clk_s:
+        line["clocks"] = clk_s
+    if not args.no_cpu and ws == 1:
+        try:
+            line["cpu_baseline"] = cpu_baseline(W)
+            line["cpu_baseline"].pop("build_ms", None)
+        except Exception as ex:   # the CPU leg is a reported baseline only
+            line["cpu_baseline"] = {"error": str(ex)}
+    print(json.dumps(line), flush=True)
+    eng.cleanup()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,99 @@
+"""ctypes binding of libhappyray_b200.so (C-ABI in include/happyray.h).
+
+The product path always runs the CUDA library: if the shared object is missing or
+cannot be loaded, every call raises HRError -- there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import threading
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "libhappyray_b200.so"
+
+HR_OK = 0
+STATUS = {0: "HR_OK", 1: "HR_ERR_INVALID_ARG", 2: "HR_ERR_OUT_OF_MEMORY", 3: "HR_ERR_CAPACITY_RETRY",
+          4: "HR_ERR_DEVICE", 5: "HR_ERR_TIMEOUT", 6: "HR_ERR_NOT_READY"}
+
+GRID_UNIFORM, GRID_TWO_LEVEL = 0, 1
+RENDER_PRIMARY, RENDER_PATH, RENDER_PATH_SINGLE_KERNEL, RENDER_AO = 0, 1, 2, 3
+
+
+class HRError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+class GridInfo(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("res", C.c_int32 * 3), ("bounds_min", C.c_float * 3),
+                ("bounds_max", C.c_float * 3), ("cell_size", C.c_float * 3), ("cell_size_rcp", C.c_float * 3),
+                ("num_cells", C.c_uint32), ("num_leaves", C.c_uint32), ("num_pairs", C.c_uint32),
+                ("num_top_pairs", C.c_uint32)]
+
+
+# every exported symbol with (restype, argtypes); the CPU tests check the .so exports them all
+P = C.c_void_p
+SIGNATURES = {
+    "hr_create": (C.c_int, [C.POINTER(P), C.c_int32, P]),
+    "hr_destroy": (None, [P]),
+    "hr_last_error": (C.c_char_p, [P]),
+    "hr_upload": (C.c_int, [P, P, P, C.c_uint32, P, C.c_uint32, C.c_float]),
+    "hr_set_keyframes": (C.c_int, [P, P, C.c_uint32, C.c_uint32, P, C.c_uint32]),
+    "hr_set_frame_time": (C.c_int, [P, C.c_float, C.c_float]),
+    "hr_set_grid_densities": (C.c_int, [P, C.c_float, C.c_float]),
+    "hr_set_uniform_density": (C.c_int, [P, C.c_float]),
+    "hr_build": (C.c_int, [P, C.c_int32, C.c_int32]),
+    "hr_grid_get_info": (C.c_int, [P, C.POINTER(GridInfo)]),
+    "hr_grid_download": (C.c_int, [P, P, P, P]),
+    "hr_set_timing": (C.c_int, [P, C.c_int32]),
+    "hr_get_stage_times": (C.c_int32, [P, P, C.c_int32]),
+    "hr_download_vertices": (C.c_int, [P, P]),
+    "hr_set_camera": (C.c_int, [P, P, P, P, C.c_float, C.c_int32, C.c_int32]),
+    "hr_set_light": (C.c_int, [P, P, P, P, C.c_float]),
+    "hr_set_integrator": (C.c_int, [P, C.c_int32, C.c_float, C.c_int32, C.c_float, C.c_uint64]),
+    "hr_render": (C.c_int, [P, C.c_int32, C.c_int32, P]),
+    "hr_render_device": (C.c_int, [P, C.c_int32, C.c_int32, P]),
+    "hr_trace_rays": (C.c_int, [P, P, P, C.c_uint32, P, P, P, P]),
+    "hr_trace_rays_device": (C.c_int, [P, P, P, C.c_uint32, P, P, P, P]),
+    "hr_trace_primary_device": (C.c_int, [P, P, P, P, P, P]),
+    "hr_occluded_device": (C.c_int, [P, P, P, P, C.c_uint32, P]),
+    "hr_get_ray_count": (C.c_int, [P, C.POINTER(C.c_uint64), C.c_int32]),
+    "hr_set_stats": (C.c_int, [P, C.c_int32]),
+    "hr_get_counters": (C.c_int, [P, C.POINTER(C.c_uint64), C.c_int32]),
+    "hr_sync": (C.c_int, [P]),
+    "hr_bounds_diagonal": (C.c_float, [P]),
+    "hr_exclusive_scan_device": (C.c_int, [P, P, C.c_uint32]),
+    "hr_radix_sort_pairs_device": (C.c_int, [P, P, P, C.c_uint32, C.c_int32]),
+}
+
+_lock = threading.Lock()
+_lib = None
+
+
+def load(path: Path | None = None):
+    """Load the CUDA library (raises HRError if it is missing: no fallback)."""
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        p = Path(path) if path else LIB_PATH
+        if not p.exists():
+            raise HRError(4, f"{p} is missing; build it with happyray_b200.build.build()")
+        L = C.CDLL(str(p))
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+        return L
+
+
+def check(ctx, status: int, what: str = ""):
+    if status != HR_OK:
+        msg = ""
+        if ctx:
+            m = load().hr_last_error(ctx)
+            msg = m.decode() if m else ""
+        raise HRError(status, f"{what}: {msg}" if what else msg)

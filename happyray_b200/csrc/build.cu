@@ -1,0 +1,573 @@
+// build.cu -- per-frame construction of uniform and two-level grids on the device.
+//
+// Reference path (javorkk/happyray):
+//   keyframe lerp + bounds     src/Application/WFObjectUploader.h:82-114 (host loop there;
+//                              fused into the first device pass here)
+//   resolution                 src/RT/Algorithm/UGridSortBuilder.h:78-92, TLGridSortBuilder.h:80-92
+//   pair count                 src/RT/Algorithm/UniformGridBuildKernels.h:40-105
+//   pair scatter               UniformGridBuildKernels.h:180-252, exact SAT .cu:224-383
+//   radix sort                 src/Utils/Sort.cu:31-53
+//   cell ranges                UniformGridBuildKernels.h:384-487
+//   leaf cells / leaf pairs    src/RT/Algorithm/TLGridBuildKernels.h:45-147, 304-409, 536-663, 750-834
+//
+// Differences in structure (results are identical to the reference's, canonicalised to
+// ascending triangle id inside every cell):
+//   * each triangle's pairs are written at its own exclusive-scan offset (block sums +
+//     in-block scan) instead of a shared-memory atomicAdd slot, so the stable sort
+//     yields ascending triangle ids per cell without any extra pass;
+//   * all sizes (bounds, resolution, pair counts, leaf counts) stay in a device-side
+//     descriptor; the whole build is enqueued without a host round trip and capacity
+//     overflow is reported by flag;
+//   * leaf-level pairs are never globally sorted: their keys are already grouped by top
+//     cell (leaf ranges are allocated in top-cell order), so one CTA per top cell counts,
+//     scans, scatters and orders its own leaves, which is the same permutation the global
+//     stable sort of TLGridSortBuilder.h:375-380 produces.
+#include "hr_internal.h"
+#include "hr_block.cuh"
+
+#include <cmath>
+#include <cstdio>
+
+namespace hr {
+
+int scan_block_sums(hr_ctx* c, uint32_t* sums, uint32_t n, uint32_t* d_total, uint32_t* ovf,
+                    uint32_t cap, uint32_t ovf_bit, uint32_t* d_req, cudaStream_t s);
+
+namespace {
+
+constexpr int kBT = 256;   // build block size
+
+__device__ __forceinline__ float pow_third(float x) { return (float)pow((double)x, (double)0.3333333f); }
+
+__global__ void k_desc_init(GridDesc* d, int32_t kind, uint32_t ntri, const uint32_t* bad_index_count) {
+    d->bmin_enc[0] = d->bmin_enc[1] = d->bmin_enc[2] = fenc(FLT_MAX);
+    d->bmax_enc[0] = d->bmax_enc[1] = d->bmax_enc[2] = fenc(-FLT_MAX);
+    d->ncells = d->npairs = d->ntop_pairs = d->nleaves = 0u;
+    d->overflow = 0u;
+    d->error = *bad_index_count != 0u ? 1u : 0u;   // set by the index check of the last upload
+    d->kind = kind;
+    d->ntri = ntri;
+}
+
+__device__ __forceinline__ void reduce_bounds(f3 lo, f3 hi, GridDesc* d) {
+    __shared__ float s[6][kBT / 32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        lo.x = hmin(lo.x, __shfl_xor_sync(kFullMask, lo.x, o));
+        lo.y = hmin(lo.y, __shfl_xor_sync(kFullMask, lo.y, o));
+        lo.z = hmin(lo.z, __shfl_xor_sync(kFullMask, lo.z, o));
+        hi.x = hmax(hi.x, __shfl_xor_sync(kFullMask, hi.x, o));
+        hi.y = hmax(hi.y, __shfl_xor_sync(kFullMask, hi.y, o));
+        hi.z = hmax(hi.z, __shfl_xor_sync(kFullMask, hi.z, o));
+    }
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) { s[0][w] = lo.x; s[1][w] = lo.y; s[2][w] = lo.z; s[3][w] = hi.x; s[4][w] = hi.y; s[5][w] = hi.z; }
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        float v = s[threadIdx.x][0];
+        for (int i = 1; i < kBT / 32; ++i) v = threadIdx.x < 3 ? hmin(v, s[threadIdx.x][i]) : hmax(v, s[threadIdx.x][i]);
+        if (threadIdx.x < 3) atomicMin(&d->bmin_enc[threadIdx.x], fenc(v));
+        else atomicMax(&d->bmax_enc[threadIdx.x - 3], fenc(v));
+    }
+}
+
+// a1: fused keyframe interpolation + bounds (WFObjectUploader.h:82-110).  coeff applies
+// to frame b: v = a * (1 - c) + b * c.  With a == nullptr the vertices are only reduced.
+__global__ __launch_bounds__(kBT) void k_lerp_bounds(const float4* __restrict__ a, const float4* __restrict__ b,
+                                                     float coeff, float4* __restrict__ out, uint32_t nv, GridDesc* d) {
+    f3 lo = mk(FLT_MAX, FLT_MAX, FLT_MAX), hi = mk(-FLT_MAX, -FLT_MAX, -FLT_MAX);
+    const float w1 = 1.0f - coeff;
+    for (uint32_t i = blockIdx.x * kBT + threadIdx.x; i < nv; i += gridDim.x * kBT) {
+        f3 p;
+        if (a) {
+            float4 qa = __ldg(a + i), qb = __ldg(b + i);
+            p.x = qa.x * w1 + qb.x * coeff;
+            p.y = qa.y * w1 + qb.y * coeff;
+            p.z = qa.z * w1 + qb.z * coeff;
+            out[i] = make_float4(p.x, p.y, p.z, 0.0f);
+        } else {
+            float4 q = __ldg(out + i);
+            p = mk(q.x, q.y, q.z);
+        }
+        lo = vmin(p, lo);
+        hi = vmax(p, hi);
+    }
+    reduce_bounds(lo, hi, d);
+}
+
+// a2: padded bounds and resolution, single thread (WFObjectUploader.h:112-114,
+// UGridSortBuilder.h:78-92, UGridMemoryManager.cu:338-345, UGridMemoryManager.h:93-101)
+__global__ void k_grid_setup(GridDesc* d, float density, uint32_t cap_cells) {
+    f3 lo = mk(fdec(d->bmin_enc[0]), fdec(d->bmin_enc[1]), fdec(d->bmin_enc[2]));
+    f3 hi = mk(fdec(d->bmax_enc[0]), fdec(d->bmax_enc[1]), fdec(d->bmax_enc[2]));
+    f3 dd = sub(hi, lo);
+    float diag = sqrtf(dot(dd, dd));
+    float pad = 0.001f * diag;
+    d->bmin[0] = lo.x - pad; d->bmin[1] = lo.y - pad; d->bmin[2] = lo.z - pad;
+    d->bmax[0] = hi.x + pad; d->bmax[1] = hi.y + pad; d->bmax[2] = hi.z + pad;
+    f3 e = mk(d->bmax[0] - d->bmin[0], d->bmax[1] - d->bmin[1], d->bmax[2] - d->bmin[2]);
+    float vol = e.x * e.y * e.z;
+    float m = pow_third(density * (float)d->ntri / vol);
+    e = mulf(e, m);
+    int32_t r[3] = {f2i(e.x), f2i(e.y), f2i(e.z)};
+    if (r[0] <= 0 || r[1] <= 0 || r[2] <= 0) r[0] = r[1] = r[2] = 32;
+    for (int k = 0; k < 3; ++k) {
+        d->res[k] = r[k];
+        float dk = d->bmax[k] - d->bmin[k];
+        d->cs[k] = dk / (float)r[k];
+        d->rcp[k] = (float)r[k] / dk;
+    }
+    const uint64_t nc = (uint64_t)r[0] * (uint64_t)r[1] * (uint64_t)r[2];
+    if (nc >= (uint64_t)cap_cells) {
+        // publish zero cells so later stages do nothing; the host regrows from req_cells
+        d->overflow |= kOvfCells;
+        d->req_cells = nc > 0xfffffff0ull ? 0xfffffff0u : (uint32_t)nc;
+        d->ncells = 0u;
+    } else {
+        d->ncells = (uint32_t)nc;
+    }
+}
+
+struct DescRegs {
+    f3 bmin, cs;
+    float rcp[3];
+    int32_t res[3];
+    uint32_t ncells;
+};
+__device__ __forceinline__ DescRegs load_desc(const GridDesc* d) {
+    DescRegs r;
+    r.bmin = mk(d->bmin[0], d->bmin[1], d->bmin[2]);
+    r.cs = mk(d->cs[0], d->cs[1], d->cs[2]);
+    for (int k = 0; k < 3; ++k) { r.rcp[k] = d->rcp[k]; r.res[k] = d->res[k]; }
+    r.ncells = d->ncells;
+    return r;
+}
+
+// a3: pair count, one triangle per thread; block sums for the scan (UniformGridBuildKernels.h:40-105)
+__global__ __launch_bounds__(kBT) void k_count_pairs(const float4* __restrict__ v, const uint32_t* __restrict__ idx,
+                                                     uint32_t ntri, const GridDesc* d, uint32_t* block_sums) {
+    if (d->overflow | d->error) {
+        if (threadIdx.x == 0) block_sums[blockIdx.x] = 0u;
+        return;
+    }
+    const DescRegs g = load_desc(d);
+    const uint32_t t = blockIdx.x * kBT + threadIdx.x;
+    uint32_t n = 0;
+    if (t < ntri) {
+        f3 p[3], lo, hi;
+        CRange r;
+        tri_load(v, idx, t, p);
+        tri_bbox(p, &lo, &hi);
+        n = cell_range(lo, hi, g.bmin, g.rcp, g.res, &r);
+    }
+    uint32_t tot;
+    block_excl_scan<uint32_t, kBT>(n, &tot);
+    if (threadIdx.x == 0) block_sums[blockIdx.x] = tot;
+}
+
+// exact triangle/box test, UniformGridBuildKernels.cu:8-48, 299-366
+__device__ __forceinline__ bool axis_test(float a, float b, float fa, float fb, float v0a, float v0b,
+                                          float v1a, float v1b, float ha, float hb) {
+    float p0 = a * v0a + b * v0b;
+    float p1 = a * v1a + b * v1b;
+    float mn = hmin(p0, p1), mx = hmax(p0, p1);
+    float rad = fa * ha + fb * hb;
+    return !(mn > rad + kEps || mx + kEps < -rad);
+}
+__device__ __forceinline__ bool sat_overlap(f3 nrm, f3 c, const f3* tv, f3 h) {
+    f3 v0 = sub(tv[0], c), v1 = sub(tv[1], c), v2 = sub(tv[2], c);
+    f3 e0 = sub(v1, v0), e1 = sub(v2, v1), e2 = sub(v0, v2);
+    bool pass = true;
+    f3 mn, mx;
+    mn.x = (nrm.x > 0.0f) ? -h.x : h.x;
+    mn.y = (nrm.y > 0.0f) ? -h.y : h.y;
+    mn.z = (nrm.z > 0.0f) ? -h.z : h.z;
+    mx = mk(-mn.x, -mn.y, -mn.z);
+    mx = sub(mx, v0);
+    mn = sub(mn, v0);
+    pass = pass && dot(nrm, mn) <= 0.0f && dot(nrm, mx) > 0.0f;
+    f3 fe = mk(fabsf(e0.x), fabsf(e0.y), fabsf(e0.z));
+    pass = pass && axis_test(e0.z, -e0.y, fe.z, fe.y, v0.y, v0.z, v2.y, v2.z, h.y, h.z);
+    pass = pass && axis_test(-e0.z, e0.x, fe.z, fe.x, v0.x, v0.z, v2.x, v2.z, h.x, h.z);
+    pass = pass && axis_test(e0.y, -e0.x, fe.y, fe.x, v1.x, v1.y, v2.x, v2.y, h.x, h.y);
+    fe = mk(fabsf(e1.x), fabsf(e1.y), fabsf(e1.z));
+    pass = pass && axis_test(e1.z, -e1.y, fe.z, fe.y, v0.y, v0.z, v2.y, v2.z, h.y, h.z);
+    pass = pass && axis_test(-e1.z, e1.x, fe.z, fe.x, v0.x, v0.z, v2.x, v2.z, h.x, h.z);
+    pass = pass && axis_test(e1.y, -e1.x, fe.y, fe.x, v0.x, v0.y, v1.x, v1.y, h.x, h.y);
+    fe = mk(fabsf(e2.x), fabsf(e2.y), fabsf(e2.z));
+    pass = pass && axis_test(e2.z, -e2.y, fe.z, fe.y, v0.y, v0.z, v1.y, v1.z, h.y, h.z);
+    pass = pass && axis_test(-e2.z, e2.x, fe.z, fe.x, v0.x, v0.z, v1.x, v1.z, h.x, h.z);
+    pass = pass && axis_test(e2.y, -e2.x, fe.y, fe.x, v1.x, v1.y, v2.x, v2.y, h.x, h.y);
+    return pass;
+}
+
+// a5: pair scatter at the triangle's exclusive-scan offset.  Keys are x + y*rx + z*rx*ry;
+// with EXACT a cell rejected by the SAT test gets key = ncells (sorted last, skipped).
+template <bool EXACT>
+__global__ __launch_bounds__(kBT) void k_write_pairs(const float4* __restrict__ v, const uint32_t* __restrict__ idx,
+                                                     uint32_t ntri, const GridDesc* d, const uint32_t* block_sums,
+                                                     uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+    if (d->overflow | d->error) return;
+    const DescRegs g = load_desc(d);
+    const uint32_t t = blockIdx.x * kBT + threadIdx.x;
+    uint32_t n = 0;
+    f3 p[3], lo, hi;
+    CRange r;
+    if (t < ntri) {
+        tri_load(v, idx, t, p);
+        tri_bbox(p, &lo, &hi);
+        n = cell_range(lo, hi, g.bmin, g.rcp, g.res, &r);
+    }
+    uint32_t tot;
+    uint32_t slot = block_excl_scan<uint32_t, kBT>(n, &tot) + block_sums[blockIdx.x];
+    if (n == 0) return;
+    const uint32_t rx = (uint32_t)g.res[0], rxy = (uint32_t)g.res[0] * (uint32_t)g.res[1];
+    if (!EXACT) {
+        for (int32_t z = r.lo[2]; z < r.hi[2]; ++z)
+            for (int32_t y = r.lo[1]; y < r.hi[1]; ++y)
+                for (int32_t x = r.lo[0]; x < r.hi[0]; ++x, ++slot) {
+                    keys[slot] = (uint32_t)x + (uint32_t)y * rx + (uint32_t)z * rxy;
+                    vals[slot] = t;
+                }
+        return;
+    }
+    const f3 nrm = normalize(cross(sub(p[1], p[0]), sub(p[2], p[0])));
+    const f3 h = mulf(g.cs, 0.505f);
+    f3 mc = mk((float)r.lo[0], (float)r.lo[1], (float)r.lo[2]);
+    mc = mk(mc.x * g.cs.x, mc.y * g.cs.y, mc.z * g.cs.z);
+    mc = add(add(mc, g.bmin), h);
+    f3 c;
+    c.z = mc.z - g.cs.z;
+    for (int32_t z = r.lo[2]; z < r.hi[2]; ++z) {
+        c.z += g.cs.z;
+        c.y = mc.y - g.cs.y;
+        for (int32_t y = r.lo[1]; y < r.hi[1]; ++y) {
+            c.y += g.cs.y;
+            c.x = mc.x - g.cs.x;
+            for (int32_t x = r.lo[0]; x < r.hi[0]; ++x, ++slot) {
+                c.x += g.cs.x;
+                keys[slot] = sat_overlap(nrm, c, p, h) ? (uint32_t)x + (uint32_t)y * rx + (uint32_t)z * rxy
+                                                       : g.ncells;
+                vals[slot] = t;
+            }
+        }
+    }
+}
+
+__global__ void k_fill_u2(uint2* a, const uint32_t* d_count, uint2 val) {
+    const uint32_t n = *d_count;   // 0 after a cell overflow
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) a[i] = val;
+}
+
+// a7: cell ranges from sorted keys (UniformGridBuildKernels.h:384-487); keys >= ncells skipped
+__global__ void k_cell_ranges(const uint32_t* __restrict__ keys, const uint32_t* d_count, const GridDesc* d,
+                              uint2* cells) {
+    if (d->overflow | d->error) return;
+    const uint32_t n = *d_count, C = d->ncells;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t k = keys[i];
+        if (k >= C) continue;
+        if (i == 0 || keys[i - 1] != k) cells[k].x = i;
+        if (i + 1 == n || keys[i + 1] != k) cells[k].y = i + 1;
+    }
+}
+
+// a8 / a10: leaf resolution and leaf pair count, one warp per top cell
+// (TLGridBuildKernels.h:45-122 countLeafLevelCells, 304-409 countLeafLevelPairs)
+struct LeafGeom { uint32_t res[3]; bool leaf; };
+__device__ __forceinline__ LeafGeom leaf_geom(const DescRegs& g, uint32_t refs, float leaf_density) {
+    LeafGeom lg;
+    float vol = g.cs.x * g.cs.y * g.cs.z;
+    float m = pow_third(leaf_density * (float)refs / vol);
+    lg.leaf = refs <= kLeafRefsMax;
+    float r0 = hmin(255.0f, hmax(1.0f, g.cs.x * m));
+    float r1 = hmin(255.0f, hmax(1.0f, g.cs.y * m));
+    float r2 = hmin(255.0f, hmax(1.0f, g.cs.z * m));
+    lg.res[0] = lg.leaf ? 1u : (uint32_t)r0;
+    lg.res[1] = lg.leaf ? 1u : (uint32_t)r1;
+    lg.res[2] = lg.leaf ? 1u : (uint32_t)r2;
+    return lg;
+}
+__device__ __forceinline__ uint32_t leaf_range(const DescRegs& g, const uint32_t* lres, uint32_t c, f3 lo, f3 hi,
+                                               CRange* r) {
+    const uint32_t rx = (uint32_t)g.res[0], rxy = (uint32_t)g.res[0] * (uint32_t)g.res[1];
+    const uint32_t cc[3] = {c % rx, (c % rxy) / rx, c / rxy};
+    f3 org;
+    org.x = (float)cc[0] * g.cs.x + g.bmin.x;
+    org.y = (float)cc[1] * g.cs.y + g.bmin.y;
+    org.z = (float)cc[2] * g.cs.z + g.bmin.z;
+    float srcp[3] = {(float)lres[0] / g.cs.x, (float)lres[1] / g.cs.y, (float)lres[2] / g.cs.z};
+    int32_t ires[3] = {(int32_t)lres[0], (int32_t)lres[1], (int32_t)lres[2]};
+    return cell_range(lo, hi, org, srcp, ires, r);
+}
+
+__global__ __launch_bounds__(kBT) void k_tl_leaf_count(const uint2* __restrict__ top_ranges,
+                                                       const uint32_t* __restrict__ top_refs,
+                                                       const float4* __restrict__ v, const uint32_t* __restrict__ idx,
+                                                       const GridDesc* d, float leaf_density, uint2* leaf_cnt,
+                                                       uint2* top_cells) {
+    if (d->overflow | d->error) return;
+    const DescRegs g = load_desc(d);
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t nw = gridDim.x * (kBT / 32);
+    for (uint32_t c = blockIdx.x * (kBT / 32) + (threadIdx.x >> 5); c < g.ncells; c += nw) {
+        const uint2 rg = top_ranges[c];
+        const uint32_t refs = rg.y - rg.x;
+        const LeafGeom lg = leaf_geom(g, refs, leaf_density);
+        uint32_t cnt = 0;
+        for (uint32_t i = rg.x + lane; i < rg.y; i += 32) {
+            f3 p[3], lo, hi;
+            CRange r;
+            tri_load(v, idx, __ldg(top_refs + i), p);
+            tri_bbox(p, &lo, &hi);
+            cnt += leaf_range(g, lg.res, c, lo, hi, &r);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(kFullMask, cnt, o);
+        if (lane == 0) {
+            uint32_t y = (lg.res[0] & 0xFFu) | ((lg.res[1] & 0xFFu) << 8) | ((lg.res[2] & 0xFFu) << 16);
+            if (lg.leaf) y |= kLeafMask;
+            if (refs != 0) y |= kNotEmptyMask;
+            leaf_cnt[c] = make_uint2(lg.res[0] * lg.res[1] * lg.res[2], cnt);
+            top_cells[c].y = y;
+        }
+    }
+}
+
+__global__ void k_check_caps(GridDesc* d, uint32_t cap_leaves, uint32_t cap_leaf_pairs) {
+    if (d->overflow | d->error) return;   // leaf totals are meaningless after an earlier overflow
+    if (d->nleaves > cap_leaves) d->overflow |= kOvfLeaves;
+    if (d->npairs > cap_leaf_pairs) d->overflow |= kOvfLeafPairs;
+}
+
+constexpr int kLT = 128;   // leaf-build block size
+
+// a11-a13: per top cell leaf ranges and ordered leaf primitive lists
+// (TLGridBuildKernels.h:536-663 + TLGridSortBuilder.h:375-380 + TLGridBuildKernels.h:750-834).
+// leaf_cnt holds the exclusive scans: x = first leaf, y = first leaf pair.
+__global__ __launch_bounds__(kLT) void k_tl_leaf_build(const uint2* __restrict__ top_ranges,
+                                                       const uint32_t* __restrict__ top_refs,
+                                                       const float4* __restrict__ v, const uint32_t* __restrict__ idx,
+                                                       const GridDesc* d, const uint2* __restrict__ leaf_cnt,
+                                                       uint2* top_cells, uint2* leaves, uint32_t* prims) {
+    if (d->overflow | d->error) return;
+    const DescRegs g = load_desc(d);
+    for (uint32_t c = blockIdx.x; c < g.ncells; c += gridDim.x) {
+        const uint2 rg = top_ranges[c];
+        const uint2 beg = leaf_cnt[c];
+        const uint32_t y = top_cells[c].y;
+        const uint32_t lres[3] = {y & 0xFFu, (y >> 8) & 0xFFu, (y >> 16) & 0xFFu};
+        const uint32_t nl = lres[0] * lres[1] * lres[2];
+        const uint32_t lb = beg.x, rb = beg.y;
+        if (threadIdx.x == 0) top_cells[c].x = lb;
+        if (rg.x == rg.y) {
+            if (threadIdx.x == 0) leaves[lb] = make_uint2(0u, 0u);
+            continue;
+        }
+        for (uint32_t i = threadIdx.x; i < nl; i += kLT) leaves[lb + i] = make_uint2(0u, 0u);
+        __syncthreads();
+        for (uint32_t i = rg.x + threadIdx.x; i < rg.y; i += kLT) {
+            f3 p[3], lo, hi;
+            CRange r;
+            tri_load(v, idx, __ldg(top_refs + i), p);
+            tri_bbox(p, &lo, &hi);
+            leaf_range(g, lres, c, lo, hi, &r);
+            for (int32_t z = r.lo[2]; z < r.hi[2]; ++z)
+                for (int32_t yy = r.lo[1]; yy < r.hi[1]; ++yy)
+                    for (int32_t x = r.lo[0]; x < r.hi[0]; ++x)
+                        atomicAdd(&leaves[lb + (uint32_t)x + (uint32_t)yy * lres[0] + (uint32_t)z * lres[0] * lres[1]].y, 1u);
+        }
+        __syncthreads();
+        uint32_t carry = 0;
+        for (uint32_t base = 0; base < nl; base += kLT) {
+            const uint32_t i = base + threadIdx.x;
+            const uint32_t cnt = i < nl ? __ldcg(&leaves[lb + i].y) : 0u;
+            uint32_t tot;
+            const uint32_t ex = block_excl_scan<uint32_t, kLT>(cnt, &tot);
+            if (i < nl) leaves[lb + i].x = rb + carry + ex;
+            carry += tot;
+        }
+        __syncthreads();
+        for (uint32_t i = rg.x + threadIdx.x; i < rg.y; i += kLT) {
+            f3 p[3], lo, hi;
+            CRange r;
+            const uint32_t tri = __ldg(top_refs + i);
+            tri_load(v, idx, tri, p);
+            tri_bbox(p, &lo, &hi);
+            leaf_range(g, lres, c, lo, hi, &r);
+            for (int32_t z = r.lo[2]; z < r.hi[2]; ++z)
+                for (int32_t yy = r.lo[1]; yy < r.hi[1]; ++yy)
+                    for (int32_t x = r.lo[0]; x < r.hi[0]; ++x) {
+                        uint32_t slot = atomicAdd(&leaves[lb + (uint32_t)x + (uint32_t)yy * lres[0] + (uint32_t)z * lres[0] * lres[1]].x, 1u);
+                        prims[slot] = tri;
+                    }
+        }
+        __syncthreads();
+        for (uint32_t i = threadIdx.x; i < nl; i += kLT) {
+            const uint2 lv = __ldcg(&leaves[lb + i]);
+            if (lv.y == 0) {   // empty leaf: {0, 0} as after the reference's memset
+                leaves[lb + i] = make_uint2(0u, 0u);
+                continue;
+            }
+            const uint32_t end = lv.x, start = end - lv.y;
+            // canonical order inside a leaf: ascending triangle id (insertion sort, short lists)
+            for (uint32_t a = start + 1; a < end; ++a) {
+                const uint32_t key = __ldcg(prims + a);
+                uint32_t b = a;
+                uint32_t prev;
+                while (b > start && (prev = __ldcg(prims + b - 1)) > key) { prims[b] = prev; --b; }
+                prims[b] = key;
+            }
+            leaves[lb + i] = make_uint2(start, end);
+        }
+        __syncthreads();
+    }
+}
+
+int key_bits_for(size_t max_key) {
+    int b = 1;
+    while (b < 32 && ((size_t)1 << b) <= max_key) ++b;
+    return b;
+}
+
+int radix_passes(int key_bits) { return (key_bits + 7) / 8; }
+
+}  // namespace
+
+// Host orchestration of one build.  Returns HR status code (0 = ok).
+static int build_once(hr_ctx* c, int32_t kind, int32_t exact, uint32_t* ovf_out) {
+    cudaStream_t s = c->stream;
+    GridBuffers& B = c->g;
+    const uint32_t ntri = c->ntri;
+    const float dens = kind == kUniform ? c->ug_density : c->top_density;
+    // capacity of the cell array is a bound (prod res <= density * N), not a guess
+    const size_t cells_bound = (size_t)(std::floor((double)dens * (double)ntri * 1.01)) + 32768u + 64u;
+    if (B.cap_cells < cells_bound) B.cap_cells = cells_bound;
+    if (B.cap_pairs == 0) B.cap_pairs = (size_t)ntri * (kind == kUniform ? 6u : 3u) + 4096u;
+    if (kind == kTwoLevel) {
+        if (B.cap_leaf_pairs == 0) B.cap_leaf_pairs = (size_t)ntri * 4u + 4096u;
+        if (B.cap_leaves == 0) B.cap_leaves = (size_t)(c->leaf_density * 2.0f * (float)B.cap_pairs) + B.cap_cells;
+    }
+    const size_t cap_pairs = B.cap_pairs;   // uniform pairs, or top-level pairs for two-level
+    const uint32_t nblocks = (ntri + kBT - 1) / kBT;
+    const int key_bits = key_bits_for(B.cap_cells);
+    const int passes = radix_passes(key_bits);
+    int rc;
+    if ((rc = ensure(c, B.desc, sizeof(GridDesc)))) return rc;
+    if ((rc = ensure(c, B.cells, sizeof(uint2) * B.cap_cells))) return rc;
+    if ((rc = ensure(c, B.keys_a, sizeof(uint32_t) * cap_pairs))) return rc;
+    if ((rc = ensure(c, B.vals_a, sizeof(uint32_t) * cap_pairs))) return rc;
+    if ((rc = ensure(c, B.keys_b, sizeof(uint32_t) * cap_pairs))) return rc;
+    if ((rc = ensure(c, B.vals_b, sizeof(uint32_t) * cap_pairs))) return rc;
+    if ((rc = ensure(c, B.block_sums, sizeof(uint32_t) * (nblocks + 1)))) return rc;
+    if ((rc = ensure(c, B.tile_hist, sizeof(uint32_t) * radix_tile_hist_words(cap_pairs, key_bits)))) return rc;
+    if ((rc = ensure(c, B.row_total, sizeof(uint32_t) * 256))) return rc;
+    if (kind == kUniform) {
+        if ((rc = ensure(c, B.prims, sizeof(uint32_t) * cap_pairs))) return rc;
+    } else {
+        if ((rc = ensure(c, B.top_ranges, sizeof(uint2) * B.cap_cells))) return rc;
+        if ((rc = ensure(c, B.top_refs, sizeof(uint32_t) * cap_pairs))) return rc;
+        if ((rc = ensure(c, B.leaf_cnt, sizeof(uint2) * B.cap_cells))) return rc;
+        if ((rc = ensure(c, B.scan_partials, sizeof(uint2) * scan_partials_words(B.cap_cells)))) return rc;
+        if ((rc = ensure(c, B.leaves, sizeof(uint2) * B.cap_leaves))) return rc;
+        if ((rc = ensure(c, B.prims, sizeof(uint32_t) * B.cap_leaf_pairs))) return rc;
+    }
+    GridDesc* d = B.desc.as<GridDesc>();
+    int ev = 0;
+    auto mark = [&]() { if (c->timing && ev < 16) cudaEventRecord(c->ev[ev++], s); };
+    mark();
+    // launches of this function (radix sort and scans count their own)
+    c->launches += 3 + (nblocks > 0 ? 3 : 0) + 2 + (kind == kTwoLevel ? 3 : 0);
+    k_desc_init<<<1, 1, 0, s>>>(d, kind, ntri, c->counters.as<uint32_t>() + 2);
+    const int gridv = std::max(1, std::min((int)((c->nverts + kBT - 1) / kBT), c->num_sms * 8));
+    if (c->lerp_pending) {
+        const float4* kf = c->keyframes.as<float4>();
+        k_lerp_bounds<<<gridv, kBT, 0, s>>>(kf + (size_t)c->frame_a * c->nverts, kf + (size_t)c->frame_b * c->nverts,
+                                            c->frame_coeff, c->verts.as<float4>(), c->nverts, d);
+    } else {
+        k_lerp_bounds<<<gridv, kBT, 0, s>>>(nullptr, nullptr, 0.0f, c->verts.as<float4>(), c->nverts, d);
+    }
+    k_grid_setup<<<1, 1, 0, s>>>(d, dens, (uint32_t)std::min(B.cap_cells, (size_t)0xffffffffu));
+    mark();
+    const float4* v = c->verts.as<float4>();
+    const uint32_t* ix = c->idx.as<uint32_t>();
+    uint32_t* bsum = B.block_sums.as<uint32_t>();
+    uint32_t* d_np = kind == kUniform ? &d->npairs : &d->ntop_pairs;
+    if (nblocks > 0) {
+        k_count_pairs<<<nblocks, kBT, 0, s>>>(v, ix, ntri, d, bsum);
+        if ((rc = scan_block_sums(c, bsum, nblocks, d_np, &d->overflow, (uint32_t)std::min(cap_pairs, (size_t)0xffffffffu),
+                                  kind == kUniform ? kOvfPairs : kOvfTopPairs, &d->req_pairs, s)))
+            return rc;
+        if (kind == kUniform && exact)
+            k_write_pairs<true><<<nblocks, kBT, 0, s>>>(v, ix, ntri, d, bsum, B.keys_a.as<uint32_t>(), B.vals_a.as<uint32_t>());
+        else
+            k_write_pairs<false><<<nblocks, kBT, 0, s>>>(v, ix, ntri, d, bsum, B.keys_a.as<uint32_t>(), B.vals_a.as<uint32_t>());
+    }
+    mark();
+    uint32_t* sorted_keys = (passes % 2 == 1) ? B.keys_b.as<uint32_t>() : B.keys_a.as<uint32_t>();
+    uint32_t* sorted_vals = kind == kUniform ? B.prims.as<uint32_t>() : B.top_refs.as<uint32_t>();
+    if ((rc = radix_sort_pairs(c, B.keys_a.as<uint32_t>(), B.vals_a.as<uint32_t>(), B.keys_b.as<uint32_t>(),
+                               B.vals_b.as<uint32_t>(), sorted_keys, sorted_vals, d_np, cap_pairs, key_bits,
+                               B.tile_hist.as<uint32_t>(), B.row_total.as<uint32_t>(), s)))
+        return rc;
+    mark();
+    uint2* ranges = kind == kUniform ? B.cells.as<uint2>() : B.top_ranges.as<uint2>();
+    const int gcells = std::max(1, std::min((int)((B.cap_cells + 255) / 256), c->num_sms * 16));
+    k_fill_u2<<<gcells, 256, 0, s>>>(ranges, &d->ncells, make_uint2(0u, 0u));
+    const int gpairs = std::max(1, std::min((int)((cap_pairs + 255) / 256), c->num_sms * 16));
+    k_cell_ranges<<<gpairs, 256, 0, s>>>(sorted_keys, d_np, d, ranges);
+    mark();
+    if (kind == kTwoLevel) {
+        const int gw = std::max(1, std::min((int)((B.cap_cells + 7) / 8), c->num_sms * 16));
+        k_tl_leaf_count<<<gw, kBT, 0, s>>>(ranges, B.top_refs.as<uint32_t>(), v, ix, d, c->leaf_density,
+                                          B.leaf_cnt.as<uint2>(), B.cells.as<uint2>());
+        if ((rc = exclusive_scan_u32x2(c, B.leaf_cnt.as<uint2>(), &d->ncells, B.cap_cells, &d->nleaves, &d->npairs,
+                                       B.scan_partials.as<uint2>(), s)))
+            return rc;
+        k_check_caps<<<1, 1, 0, s>>>(d, (uint32_t)std::min(B.cap_leaves, (size_t)0xffffffffu),
+                                     (uint32_t)std::min(B.cap_leaf_pairs, (size_t)0xffffffffu));
+        mark();
+        const int gl = std::max(1, std::min((int)B.cap_cells, c->num_sms * 16));
+        k_tl_leaf_build<<<gl, kLT, 0, s>>>(ranges, B.top_refs.as<uint32_t>(), v, ix, d, B.leaf_cnt.as<uint2>(),
+                                          B.cells.as<uint2>(), B.leaves.as<uint2>(), B.prims.as<uint32_t>());
+        mark();
+    }
+    c->nstages = ev;
+    if ((rc = cuda_check(c, cudaGetLastError(), "build launch"))) return rc;
+    if ((rc = cuda_check(c, cudaMemcpyAsync(&c->host_desc, d, sizeof(GridDesc), cudaMemcpyDeviceToHost, s),
+                         "descriptor download")))
+        return rc;
+    if ((rc = cuda_check(c, cudaStreamSynchronize(s), "build"))) return rc;
+    if (c->timing)
+        for (int i = 0; i + 1 < ev; ++i) cudaEventElapsedTime(&c->stage_ms[i], c->ev[i], c->ev[i + 1]);
+    if (c->host_desc.error) return set_error(c, 1, "triangle index out of range of the uploaded vertices");
+    *ovf_out = c->host_desc.overflow;
+    return 0;
+}
+
+int build_grid(hr_ctx* c, int32_t kind, int32_t exact) {
+    GridBuffers& B = c->g;
+    if (c->built_kind != kind) {
+        B.cap_pairs = 0; B.cap_leaf_pairs = 0; B.cap_leaves = 0;
+    }
+    for (int attempt = 0; attempt < 6; ++attempt) {
+        uint32_t ovf = 0;
+        int rc = build_once(c, kind, exact, &ovf);
+        if (rc) return rc;
+        const GridDesc& hd = c->host_desc;
+        if (ovf == 0) {
+            c->built_kind = kind;
+            c->built = true;
+            c->lerp_pending = false;
+            return 0;
+        }
+        // grow what overflowed from the exact sizes the device computed, and rebuild
+        if (ovf & kOvfCells) B.cap_cells = (size_t)hd.req_cells + 64u;
+        if (ovf & (kOvfPairs | kOvfTopPairs)) B.cap_pairs = (size_t)(hd.req_pairs * 1.25) + 4096u;
+        if (ovf & kOvfLeaves) B.cap_leaves = (size_t)(hd.nleaves * 1.25) + 4096u;
+        if (ovf & kOvfLeafPairs) B.cap_leaf_pairs = (size_t)(hd.npairs * 1.25) + 4096u;
+    }
+    return set_error(c, 3, "grid build: capacity did not converge");
+}
+
+}  // namespace hr

@@ -1,0 +1,138 @@
+// hr_internal.h -- host-side context and launcher declarations of libhappyray_b200.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstddef>
+#include <string>
+
+#include "hr_common.cuh"
+
+namespace hr {
+
+// Grow-only device allocation (MemoryManager.h:104-119 semantics: never shrinks).
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    template <class T> T* as() const { return static_cast<T*>(p); }
+};
+
+struct Camera {
+    float pos[3], top_left[3], step_x[3], step_y[3];
+    int32_t w = 0, h = 0;
+};
+
+struct Light {
+    float corner[3] = {0.4f, 0.4f, 1.0f};
+    float e1[3] = {0.2f, 0.0f, 0.0f};
+    float e2[3] = {0.0f, 0.2f, 0.0f};
+    float emission = 20.0f;
+};
+
+struct IntegratorParams {
+    int32_t ao_samples = 8;
+    float ao_radius_frac = 0.1f;   // AO radius as a fraction of the bounds diagonal
+    float ao_radius_abs = 0.0f;    // > 0 overrides the fraction
+    int32_t pt_bounces = 4;
+    float albedo = 0.7f;
+    float ray_eps_frac = 1e-4f;    // PT ray offset as a fraction of the bounds diagonal
+    uint64_t seed = 0x853c49e6748fea9bULL;
+};
+
+// Scratch and result buffers of one acceleration structure.
+struct GridBuffers {
+    DevBuf desc;          // GridDesc
+    DevBuf cells;         // uint2 per cell (uniform) or packed top cell (two-level)
+    DevBuf leaves;        // uint2 per leaf (two-level)
+    DevBuf prims;         // uint32 per pair
+    DevBuf keys_a, vals_a, keys_b, vals_b;   // pair ping-pong
+    DevBuf block_sums;    // per-block counts of the pair-count pass
+    DevBuf tile_hist;     // radix tile histograms
+    DevBuf row_total;     // radix digit totals
+    DevBuf top_ranges;    // two-level: uint2 per top cell
+    DevBuf top_refs;      // two-level: sorted top-level values
+    DevBuf leaf_cnt;      // two-level: uint2 (leaf cells, leaf pairs) per top cell, scanned in place
+    DevBuf scan_partials; // generic scan partial sums
+    size_t cap_cells = 0, cap_pairs = 0, cap_top_pairs = 0, cap_leaves = 0, cap_leaf_pairs = 0;
+};
+
+struct Stats {
+    uint64_t rays = 0;
+};
+
+}  // namespace hr
+
+struct hr_ctx {
+    int device = 0;
+    int num_sms = 148;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    std::string err;
+
+    // mesh
+    uint32_t ntri = 0, nverts = 0, nkeyframes = 0;
+    hr::DevBuf verts;      // float4 current frame
+    hr::DevBuf idx;        // uint32 x3
+    hr::DevBuf keyframes;  // float4 x nverts x nkeyframes
+    hr::DevBuf staging;    // float4 staging of host keyframes on upload
+    int32_t frame_a = 0, frame_b = 0;
+    float frame_coeff = 1.0f;
+    bool have_frame = false;     // a frame (static or lerp request) is set
+    bool lerp_pending = false;   // the next build interpolates resident keyframes
+
+    // grid
+    float top_density = 0.0625f, leaf_density = 2.0f, ug_density = 5.0f;
+    int32_t built_kind = -1;
+    bool built = false;
+    hr::GridBuffers g;
+    hr::GridDesc host_desc{};    // last downloaded descriptor
+    hr::DevBuf counters;         // uint64 ray counters
+    uint64_t launches = 0;       // kernels enqueued by this context (host-side count)
+    bool collect_stats = false;  // render kernels accumulate cells visited / triangle tests
+    cudaEvent_t ev[16] = {};
+    bool timing = false;
+    float stage_ms[16] = {};
+    int nstages = 0;
+
+    // camera / integrators
+    hr::Camera cam;
+    bool have_camera = false;
+    hr::Light light;
+    hr::IntegratorParams ip;
+    hr::DevBuf fb;               // float3 framebuffer (device)
+    hr::DevBuf out_id, out_t, out_u, out_v, ray_in;  // ray-query staging
+    void* pinned = nullptr;      // pinned host staging
+    size_t pinned_bytes = 0;
+};
+
+namespace hr {
+
+// status helpers (capi.cu)
+int set_error(hr_ctx* c, int code, const char* fmt, ...);
+int cuda_check(hr_ctx* c, cudaError_t e, const char* what);
+int ensure(hr_ctx* c, DevBuf& b, size_t bytes);
+
+// build.cu
+int build_grid(hr_ctx* c, int32_t kind, int32_t exact);
+
+// sort.cu
+int radix_sort_pairs(hr_ctx* c, const uint32_t* keys_in, const uint32_t* vals_in,
+                     uint32_t* keys_tmp, uint32_t* vals_tmp, uint32_t* keys_out, uint32_t* vals_out,
+                     const uint32_t* d_count, size_t cap_count, int key_bits,
+                     uint32_t* tile_hist, uint32_t* row_total, cudaStream_t s);
+size_t radix_tile_hist_words(size_t cap_count, int key_bits);
+int exclusive_scan_u32(hr_ctx* c, uint32_t* data, const uint32_t* d_count, size_t cap_count,
+                       uint32_t* d_total, uint32_t* partials, cudaStream_t s);
+int exclusive_scan_u32x2(hr_ctx* c, uint2* data, const uint32_t* d_count, size_t cap_count,
+                         uint32_t* d_total_x, uint32_t* d_total_y, uint2* partials, cudaStream_t s);
+size_t scan_partials_words(size_t cap_count);
+
+// trace.cu
+int launch_trace_rays(hr_ctx* c, const float* org, const float* dir, uint32_t n, int32_t* id,
+                      float* t, float* u, float* v, uint32_t* stats);
+int launch_trace_primary(hr_ctx* c, int32_t* id, float* t, float* u, float* v, uint32_t* stats);
+int launch_render(hr_ctx* c, int32_t mode, int32_t image_id, float* d_fb);
+int launch_occluded(hr_ctx* c, const float* org, const float* dir, const float* tmax, uint32_t n,
+                    uint8_t* occluded);
+
+}  // namespace hr

@@ -1,0 +1,288 @@
+"""GPU parity: the CUDA library (through the C-ABI) against the CPU oracle on the same
+inputs.  Integer results (cells, leaves, primitive lists, hit ids) and the float results
+(t, u, v, AO / PT pixels) are compared bit-exact: both sides evaluate the same binary32
+expressions in the same order without FMA contraction.  t/u/v are additionally held to
+1e-5 relative against the FP64 brute-force oracle (see test_oracle.compare_fp64)."""
+import numpy as np
+import pytest
+
+from happyray_b200 import GRID_TWO_LEVEL, GRID_UNIFORM, RENDER_AO, RENDER_PATH, RENDER_PRIMARY
+from happyray_b200 import scenes as S
+
+pytestmark = pytest.mark.gpu
+
+
+def oracle_build(O, v, f, kind, exact=True, ug=5.0, top=0.0625, leaf=2.0):
+    v4, bmin, bmax = O.lerp_bounds(v, v, 1.0)
+    if kind == GRID_UNIFORM:
+        return O.build_ug(v4, f, bmin, bmax, ug, exact)
+    return O.build_tl(v4, f, bmin, bmax, top, leaf)
+
+
+def gpu_build(e, v, f, kind, exact=True, ug=5.0, top=0.0625, leaf=2.0, coeff=1.0, v2=None):
+    e.upload(v, v if v2 is None else v2, f, coeff)
+    e.set_uniform_density(ug)
+    e.setGridDensities(top, leaf)
+    e.build(kind, exact)
+    return e.grid_download()
+
+
+def assert_same_grid(gpu, orc):
+    gi, cells, leaves, prims = gpu
+    g = orc.grid
+    assert gi["res"] == tuple(g.res)
+    assert np.array_equal(gi["bounds_min"], np.array(g.bmin, np.float32))
+    assert np.array_equal(gi["bounds_max"], np.array(g.bmax, np.float32))
+    assert np.array_equal(gi["cell_size"], np.array(g.cs, np.float32))
+    assert np.array_equal(gi["cell_size_rcp"], np.array(g.rcp, np.float32))
+    assert gi["num_cells"] == g.ncells
+    assert gi["num_pairs"] == orc.npairs
+    assert np.array_equal(cells, orc.cells)
+    if orc.leaves is not None:
+        assert gi["num_top_pairs"] == orc.ntop_pairs
+        assert np.array_equal(leaves, orc.leaves)
+    assert np.array_equal(prims, orc.prims)
+
+
+def ocam(O, cam):
+    return O.camera(cam["position"], cam["orientation"], cam["up"], cam["fov"], cam["res_x"], cam["res_y"])
+
+
+def set_cam(e, cam):
+    e.setCamera(cam["position"], cam["orientation"], cam["up"], cam["fov"], cam["res_x"], cam["res_y"])
+
+
+@pytest.mark.parametrize("exact", [True, False])
+def test_build_uniform_c1(engine, oracle, c1_scene, exact):
+    v, f = c1_scene
+    assert_same_grid(gpu_build(engine, v, f, GRID_UNIFORM, exact), oracle_build(oracle, v, f, GRID_UNIFORM, exact))
+
+
+def test_build_two_level_c1(engine, oracle, c1_scene):
+    v, f = c1_scene
+    assert_same_grid(gpu_build(engine, v, f, GRID_TWO_LEVEL), oracle_build(oracle, v, f, GRID_TWO_LEVEL))
+
+
+@pytest.mark.parametrize("dens", [(0.0625, 2.0), (1.2, 2.2), (1 / 32, 8.0), (0.25, 1.0)])
+def test_build_two_level_clusters(engine, oracle, small_clusters, dens):
+    v, f = small_clusters
+    assert_same_grid(gpu_build(engine, v, f, GRID_TWO_LEVEL, top=dens[0], leaf=dens[1]),
+                     oracle_build(oracle, v, f, GRID_TWO_LEVEL, top=dens[0], leaf=dens[1]))
+
+
+def test_build_uniform_clusters(engine, oracle, small_clusters):
+    v, f = small_clusters
+    assert_same_grid(gpu_build(engine, v, f, GRID_UNIFORM, True), oracle_build(oracle, v, f, GRID_UNIFORM, True))
+
+
+def test_keyframe_lerp_and_rebuild(engine, oracle, small_clusters):
+    """Resident key frames, frame-time selection (AnimationManager.hpp:68-97) and the fused
+    device interpolation give the oracle's vertices and grid at every frame time."""
+    v, f = small_clusters
+    frames = S.curl_keyframes(v, 6, seed=4)
+    engine.set_keyframes(frames, f)
+    engine.setGridDensities(0.0625, 2.0)
+    for tt, step in [(0.0, 0.0), (2.75, 0.0), (5.5, 0.0), (1.25, 1.0)]:
+        engine.set_frame_time(tt, step)
+        engine.build(GRID_TWO_LEVEL)
+        k = int(tt)
+        nxt = (k + 1 + int(step)) % frames.shape[0]
+        c = np.float32(tt) - np.float32(k)
+        v4, bmin, bmax = oracle.lerp_bounds(frames[k], frames[nxt], float(c))
+        assert np.array_equal(engine.vertices(v.shape[0]), v4)
+        b = oracle.build_tl(v4, f, bmin, bmax, 0.0625, 2.0)
+        assert_same_grid(engine.grid_download(), b)
+
+
+def test_upload_coefficient(engine, oracle, small_clusters):
+    v, f = small_clusters
+    v2 = (v + np.random.default_rng(3).normal(0, 0.005, v.shape)).astype(np.float32)
+    gpu = gpu_build(engine, v, f, GRID_UNIFORM, True, coeff=0.3, v2=v2)
+    v4, bmin, bmax = oracle.lerp_bounds(v, v2, 0.3)
+    assert np.array_equal(engine.vertices(v.shape[0]), v4)
+    assert_same_grid(gpu, oracle.build_ug(v4, f, bmin, bmax, 5.0, True))
+
+
+@pytest.mark.parametrize("kind", [GRID_UNIFORM, GRID_TWO_LEVEL])
+def test_trace_primary_bitexact_c1(engine, oracle, c1_scene, kind):
+    import torch
+    v, f = c1_scene
+    gpu_build(engine, v, f, kind)
+    b = oracle_build(oracle, v, f, kind)
+    cam = S.camera_c1()
+    set_cam(engine, cam)
+    n = 256 * 256
+    out = [torch.empty(n, dtype=dt, device="cuda") for dt in (torch.int32, torch.float32, torch.float32, torch.float32)]
+    st = torch.empty(2 * n, dtype=torch.int32, device="cuda")
+    torch.cuda.synchronize()
+    engine.trace_primary_device(*out, st)
+    engine.sync()
+    hid, t, u, vv, ost = oracle.trace_primary(b, ocam(oracle, cam), stats=True)
+    assert np.array_equal(out[0].cpu().numpy(), hid)
+    assert np.array_equal(out[1].cpu().numpy(), t)
+    assert np.array_equal(out[2].cpu().numpy(), u)
+    assert np.array_equal(out[3].cpu().numpy(), vv)
+    assert np.array_equal(st.cpu().numpy().view(np.uint32).reshape(-1, 2), ost)
+    assert (hid >= 0).sum() > 10000
+
+
+@pytest.mark.parametrize("kind", [GRID_UNIFORM, GRID_TWO_LEVEL])
+def test_trace_rays_host_api(engine, oracle, small_clusters, kind):
+    v, f = small_clusters
+    gpu_build(engine, v, f, kind)
+    b = oracle_build(oracle, v, f, kind)
+    rng = np.random.default_rng(11)
+    n = 40000
+    org = rng.uniform(-0.2, 1.2, (n, 3)).astype(np.float32)
+    d = rng.normal(size=(n, 3)).astype(np.float32)
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    d[:50, 1:] = 0.0     # axis-parallel rays (infinite reciprocals)
+    d[:50, 0] = 1.0
+    got = engine.trace_rays(org, d)
+    want = oracle.trace(b, org, d)
+    for g_, w_ in zip(got, want):
+        assert np.array_equal(g_, w_)
+    from test_oracle import compare_fp64
+    sel = slice(0, 3000)
+    frac, nhit = compare_fp64(oracle, b.v4, f, org[sel], d[sel], got[0][sel], got[1][sel], got[2][sel], got[3][sel])
+    assert frac > 0.98
+
+
+def test_occluded_matches_oracle(engine, oracle, small_clusters):
+    import torch
+    v, f = small_clusters
+    gpu_build(engine, v, f, GRID_TWO_LEVEL)
+    b = oracle_build(oracle, v, f, GRID_TWO_LEVEL)
+    rng = np.random.default_rng(12)
+    n = 30000
+    org = rng.uniform(0, 1, (n, 3)).astype(np.float32)
+    d = rng.normal(size=(n, 3)).astype(np.float32)
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    tmax = rng.uniform(0.01, 0.5, n).astype(np.float32)
+    want = oracle.occluded(b, org, d, tmax)
+    to = lambda a: torch.from_numpy(a).cuda()
+    occ = torch.empty(n, dtype=torch.uint8, device="cuda")
+    torch.cuda.synchronize()
+    engine.occluded_device(to(org), to(d), to(tmax), n, occ)
+    engine.sync()
+    assert np.array_equal(occ.cpu().numpy(), want)
+    assert 0 < want.sum() < n
+
+
+def test_render_ao_bitexact(engine, oracle, small_clusters):
+    v, f = small_clusters
+    gpu_build(engine, v, f, GRID_TWO_LEVEL)
+    b = oracle_build(oracle, v, f, GRID_TWO_LEVEL)
+    cam = S.camera_at_bounds(v, (160, 120))
+    set_cam(engine, cam)
+    alpha = float(np.float32(0.1) * b.diag())
+    seed = 1234567
+    engine.set_integrator(ao_samples=8, ao_radius=alpha, seed=seed)
+    engine.ray_count(reset=True)
+    fb = engine.renderFrame(None, 0, RENDER_AO)
+    rays = engine.ray_count(reset=True)
+    img, orays = oracle.render_ao(b, ocam(oracle, cam), 8, alpha, seed)
+    assert np.array_equal(fb[:, 0], img) and np.array_equal(fb[:, 1], img) and np.array_equal(fb[:, 2], img)
+    assert rays == orays
+    # progressive blend of a second image (AOIntegrator.h:168-175)
+    fb2 = engine.renderFrame(fb.copy(), 1, RENDER_AO)
+    img2, _ = oracle.render_ao(b, ocam(oracle, cam), 8, alpha, seed, image_id=1, fb=img.copy())
+    assert np.array_equal(fb2[:, 0], img2)
+
+
+def test_render_pt_bitexact(engine, oracle, small_clusters):
+    v, f = small_clusters
+    gpu_build(engine, v, f, GRID_TWO_LEVEL)
+    b = oracle_build(oracle, v, f, GRID_TWO_LEVEL)
+    cam = S.camera_at_bounds(v, (128, 96))
+    set_cam(engine, cam)
+    seed = 99
+    engine.set_integrator(pt_bounces=4, albedo=0.7, seed=seed)
+    engine.setLights((0.4, 0.4, 1.0), (0.2, 0, 0), (0, 0.2, 0), 20.0)
+    engine.ray_count(reset=True)
+    fb = engine.renderFrame(None, 0, RENDER_PATH)
+    rays = engine.ray_count(reset=True)
+    eps = float(np.float32(1e-4) * b.diag())
+    img, orays = oracle.render_pt(b, ocam(oracle, cam), oracle.make_light(), 4, 0.7, eps, seed)
+    assert np.array_equal(fb[:, 0], img)
+    assert rays == orays
+    assert img.max() > 0
+
+
+def test_render_primary_mode0(engine, oracle, c1_scene):
+    v, f = c1_scene
+    gpu_build(engine, v, f, GRID_UNIFORM)
+    cam = S.camera_c1((64, 64))
+    set_cam(engine, cam)
+    fb = engine.renderFrame(None, 0, RENDER_PRIMARY)
+    b = oracle_build(oracle, v, f, GRID_UNIFORM)
+    hid, t, u, vv = oracle.trace_primary(b, ocam(oracle, cam))
+    miss = hid < 0
+    assert np.allclose(fb[miss], [0.15, 0.2, 0.3])
+    hit = ~miss
+    # barycentric false colour: (w0, w1, w2) * |cos|
+    s = fb[hit].sum(1)
+    assert np.all(s <= 1.0 + 1e-6) and np.all(s >= 0)
+    assert np.allclose(fb[hit, 1] / np.maximum(s, 1e-12), u[hit] / np.maximum(u[hit] + vv[hit] + (1 - u[hit] - vv[hit]), 1e-12), atol=1e-4)
+
+
+def test_radix_sort_and_scan_device(engine):
+    import torch
+    rng = np.random.default_rng(7)
+    for n, bits in [(1, 1), (1000, 5), (123457, 17), (2_000_001, 24), (70000, 32)]:
+        keys = rng.integers(0, 2 ** bits, n, dtype=np.uint64).astype(np.uint32)
+        vals = np.arange(n, dtype=np.uint32)
+        tk = torch.from_numpy(keys.view(np.int32)).cuda()
+        tv = torch.from_numpy(vals.view(np.int32)).cuda()
+        torch.cuda.synchronize()
+        engine.radix_sort_pairs_device(tk, tv, n, bits)
+        order = np.argsort(keys, kind="stable")
+        assert np.array_equal(tk.cpu().numpy().view(np.uint32), keys[order])
+        assert np.array_equal(tv.cpu().numpy().view(np.uint32), vals[order])
+    for n in [1, 2047, 2048, 2049, 1_000_003]:
+        x = rng.integers(0, 100, n).astype(np.uint32)
+        tx = torch.from_numpy(x.view(np.int32)).cuda()
+        torch.cuda.synchronize()
+        engine.exclusive_scan_device(tx, n)
+        want = np.concatenate([[0], np.cumsum(x, dtype=np.uint64)[:-1]]).astype(np.uint32)
+        assert np.array_equal(tx.cpu().numpy().view(np.uint32), want)
+
+
+def test_edge_cases(engine, oracle):
+    # single triangle
+    v = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0]], np.float32)
+    f = np.array([[0, 1, 2]], np.uint32)
+    for kind in (GRID_UNIFORM, GRID_TWO_LEVEL):
+        gpu = gpu_build(engine, v, f, kind)
+        assert_same_grid(gpu, oracle_build(oracle, v, f, kind))
+        hid, t, u, vv = engine.trace_rays(np.array([[0.25, 0.25, 1.0]], np.float32), np.array([[0, 0, -1.0]], np.float32))
+        assert hid[0] == 0 and abs(t[0] - 1) < 1e-6
+    # a few huge overlapping triangles: pair counts far above the initial capacity estimate,
+    # the build regrows from the device-computed totals and rebuilds
+    rng = np.random.default_rng(3)
+    v = rng.uniform(0, 1, (300, 3)).astype(np.float32)
+    f = rng.integers(0, 300, (100, 3)).astype(np.uint32)
+    for kind in (GRID_UNIFORM, GRID_TWO_LEVEL):
+        gpu = gpu_build(engine, v, f, kind)
+        b = oracle_build(oracle, v, f, kind)
+        assert b.npairs > 6 * 100
+        assert_same_grid(gpu, b)
+    # degenerate triangles only
+    v = np.array([[0, 0, 0], [1, 1, 1], [2, 2, 2]], np.float32)
+    f = np.array([[0, 1, 2], [0, 0, 0]], np.uint32)
+    gpu = gpu_build(engine, v, f, GRID_UNIFORM)
+    assert_same_grid(gpu, oracle_build(oracle, v, f, GRID_UNIFORM))
+    hid, *_ = engine.trace_rays(np.array([[0.5, 0.5, 3.0]], np.float32), np.array([[0, 0, -1.0]], np.float32))
+    assert hid[0] == -1
+
+
+def test_empty_mesh(engine):
+    from happyray_b200 import HRError
+    v = np.zeros((3, 3), np.float32)
+    f = np.zeros((0, 3), np.uint32)
+    engine.upload(v, v, f, 1.0)
+    engine.build(GRID_TWO_LEVEL)
+    hid, t, *_ = engine.trace_rays(np.zeros((2, 3), np.float32), np.array([[0, 0, 1.0], [1, 0, 0]], np.float32))
+    assert np.all(hid == -1)
+    with pytest.raises(HRError):
+        engine.build(7)
