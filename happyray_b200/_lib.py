@@ -66,6 +66,7 @@ SIGNATURES = {
     "hr_bounds_diagonal": (C.c_float, [P]),
     "hr_exclusive_scan_device": (C.c_int, [P, P, C.c_uint32]),
     "hr_radix_sort_pairs_device": (C.c_int, [P, P, P, C.c_uint32, C.c_int32]),
+    "hr_radix_sort_pairs_noalloc": (C.c_int, [P, P, P, C.c_uint32, C.c_int32]),
 }
 
 _lock = threading.Lock()

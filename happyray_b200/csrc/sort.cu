@@ -340,4 +340,32 @@ int radix_sort_pairs(hr_ctx* c, const uint32_t* keys_in, const uint32_t* vals_in
     return cuda_check(c, cudaGetLastError(), "radix_sort_pairs");
 }
 
+// Same pass sequence as radix_sort_pairs, without a context (no status text, no launch
+// count); used by the allocation-free entry point.
+cudaError_t radix_sort_pairs_raw(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_tmp,
+                                 uint32_t* vals_tmp, uint32_t* keys_out, uint32_t* vals_out,
+                                 const uint32_t* d_count, size_t cap_count, int key_bits, uint32_t* tile_hist,
+                                 uint32_t* row_total, cudaStream_t s) {
+    int passes, db;
+    radix_plan(key_bits, &passes, &db);
+    const uint32_t mask = (1u << db) - 1u;
+    const uint32_t ntiles = (uint32_t)((cap_count + kTile - 1) / kTile);
+    if (ntiles == 0) return cudaSuccess;
+    const uint32_t* src_k = keys_in;
+    const uint32_t* src_v = vals_in;
+    for (int p = 0; p < passes; ++p) {
+        const bool last = p == passes - 1;
+        uint32_t* dk = last ? keys_out : ((p % 2 == 0) ? keys_tmp : const_cast<uint32_t*>(keys_in));
+        uint32_t* dv = last ? vals_out : ((p % 2 == 0) ? vals_tmp : const_cast<uint32_t*>(vals_in));
+        const int shift = p * db;
+        k_radix_upsweep<<<ntiles, kThreads, 0, s>>>(src_k, d_count, shift, mask, tile_hist, ntiles);
+        k_radix_scan<<<mask + 1, 1024, 0, s>>>(tile_hist, ntiles, row_total);
+        k_radix_downsweep<<<ntiles, kThreads, 0, s>>>(src_k, src_v, dk, dv, d_count, shift, mask, tile_hist,
+                                                      ntiles, row_total);
+        src_k = dk;
+        src_v = dv;
+    }
+    return cudaGetLastError();
+}
+
 }  // namespace hr

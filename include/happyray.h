@@ -148,6 +148,23 @@ hr_status hr_exclusive_scan_device(hr_ctx *ctx, uint32_t *d_data, uint32_t n);
 hr_status hr_radix_sort_pairs_device(hr_ctx *ctx, uint32_t *d_keys, uint32_t *d_values,
                                      uint32_t n, int32_t key_bits);
 
+/* Largest n accepted by hr_radix_sort_pairs_noalloc. */
+#define HR_NOALLOC_MAX_PAIRS (1u << 20)
+/* The same stable radix sort as hr_radix_sort_pairs_device, for callers that must not
+ * allocate device memory: a renderer or serving process that reserves its whole HBM
+ * budget up front cannot call cudaMalloc inside its frame / request loop, where an
+ * allocation may stall the device or fail under memory pressure.  No counterpart in
+ * the reference (its RadixSort allocates through CUB's caching allocator).
+ * Needs no context and allocates nothing: the scratch is a static per-GPU array of about
+ * 8.5 MiB, held by every GPU that loads the library until the process exits.  Sorts
+ * d_keys / d_values (device pointers of the current device) in place on `stream`
+ * (cudaStream_t, NULL = default stream).  Returns HR_ERR_INVALID_ARG if n exceeds
+ * HR_NOALLOC_MAX_PAIRS or key_bits is outside 1..32.  The first call on a device looks up
+ * the scratch address; make it before any stream capture.  All calls share the one
+ * scratch array: calls that overlap on the GPU race, so serialise them. */
+hr_status hr_radix_sort_pairs_noalloc(void *stream, uint32_t *d_keys, uint32_t *d_values,
+                                      uint32_t n, int32_t key_bits);
+
 #ifdef __cplusplus
 }
 #endif
