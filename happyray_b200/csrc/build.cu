@@ -254,16 +254,18 @@ __global__ __launch_bounds__(kBT) void k_write_pairs(const float4* __restrict__ 
     }
 }
 
-__global__ void k_fill_u2(uint2* a, const uint32_t* d_count, uint2 val) {
-    const uint32_t n = *d_count;   // 0 after a cell overflow
+__global__ void k_fill_u2(uint2* a, const uint32_t* d_count, const GridDesc* d, uint2 val) {
+    if (d->overflow | d->error) return;   // counts may exceed the buffers after an overflow
+    const uint32_t n = *d_count;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) a[i] = val;
 }
 
-// a7: cell ranges from sorted keys (UniformGridBuildKernels.h:384-487); keys >= ncells skipped
-__global__ void k_cell_ranges(const uint32_t* __restrict__ keys, const uint32_t* d_count, const GridDesc* d,
-                              uint2* cells) {
+// a7 / a13: cell (or leaf) ranges from sorted keys (UniformGridBuildKernels.h:384-487,
+// TLGridBuildKernels.h:750-834); keys >= *d_ncells (rejected exact-insertion pairs) are skipped
+__global__ void k_cell_ranges(const uint32_t* __restrict__ keys, const uint32_t* d_count, const uint32_t* d_ncells,
+                              const GridDesc* d, uint2* cells) {
     if (d->overflow | d->error) return;
-    const uint32_t n = *d_count, C = d->ncells;
+    const uint32_t n = *d_count, C = *d_ncells;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const uint32_t k = keys[i];
         if (k >= C) continue;
@@ -272,8 +274,7 @@ __global__ void k_cell_ranges(const uint32_t* __restrict__ keys, const uint32_t*
     }
 }
 
-// a8 / a10: leaf resolution and leaf pair count, one warp per top cell
-// (TLGridBuildKernels.h:45-122 countLeafLevelCells, 304-409 countLeafLevelPairs)
+// a8: leaf resolution of a top cell (TLGridBuildKernels.h:55-87)
 struct LeafGeom { uint32_t res[3]; bool leaf; };
 __device__ __forceinline__ LeafGeom leaf_geom(const DescRegs& g, uint32_t refs, float leaf_density) {
     LeafGeom lg;
@@ -288,6 +289,8 @@ __device__ __forceinline__ LeafGeom leaf_geom(const DescRegs& g, uint32_t refs, 
     lg.res[2] = lg.leaf ? 1u : (uint32_t)r2;
     return lg;
 }
+
+// sub-cell range of a triangle inside top cell c (TLGridBuildKernels.h:338-377)
 __device__ __forceinline__ uint32_t leaf_range(const DescRegs& g, const uint32_t* lres, uint32_t c, f3 lo, f3 hi,
                                                CRange* r) {
     const uint32_t rx = (uint32_t)g.res[0], rxy = (uint32_t)g.res[0] * (uint32_t)g.res[1];
@@ -301,127 +304,101 @@ __device__ __forceinline__ uint32_t leaf_range(const DescRegs& g, const uint32_t
     return cell_range(lo, hi, org, srcp, ires, r);
 }
 
-__global__ __launch_bounds__(kBT) void k_tl_leaf_count(const uint2* __restrict__ top_ranges,
-                                                       const uint32_t* __restrict__ top_refs,
-                                                       const float4* __restrict__ v, const uint32_t* __restrict__ idx,
-                                                       const GridDesc* d, float leaf_density, uint2* leaf_cnt,
-                                                       uint2* top_cells) {
+// a8: per top cell: leaf resolution, flags, leaf-cell count (countLeafLevelCells,
+// TLGridBuildKernels.h:45-122); packed y of TwoLevelGridCell (TwoLevelGrid.h:38-161)
+__global__ void k_tl_cells(const uint2* __restrict__ top_ranges, const GridDesc* d, float leaf_density,
+                           uint32_t* __restrict__ leaf_cnt, uint2* __restrict__ top_cells) {
     if (d->overflow | d->error) return;
     const DescRegs g = load_desc(d);
-    const uint32_t lane = threadIdx.x & 31;
-    const uint32_t nw = gridDim.x * (kBT / 32);
-    for (uint32_t c = blockIdx.x * (kBT / 32) + (threadIdx.x >> 5); c < g.ncells; c += nw) {
+    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < g.ncells; c += gridDim.x * blockDim.x) {
         const uint2 rg = top_ranges[c];
         const uint32_t refs = rg.y - rg.x;
         const LeafGeom lg = leaf_geom(g, refs, leaf_density);
-        uint32_t cnt = 0;
-        for (uint32_t i = rg.x + lane; i < rg.y; i += 32) {
-            f3 p[3], lo, hi;
-            CRange r;
-            tri_load(v, idx, __ldg(top_refs + i), p);
-            tri_bbox(p, &lo, &hi);
-            cnt += leaf_range(g, lg.res, c, lo, hi, &r);
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(kFullMask, cnt, o);
-        if (lane == 0) {
-            uint32_t y = (lg.res[0] & 0xFFu) | ((lg.res[1] & 0xFFu) << 8) | ((lg.res[2] & 0xFFu) << 16);
-            if (lg.leaf) y |= kLeafMask;
-            if (refs != 0) y |= kNotEmptyMask;
-            leaf_cnt[c] = make_uint2(lg.res[0] * lg.res[1] * lg.res[2], cnt);
-            top_cells[c].y = y;
-        }
+        uint32_t y = (lg.res[0] & 0xFFu) | ((lg.res[1] & 0xFFu) << 8) | ((lg.res[2] & 0xFFu) << 16);
+        if (lg.leaf) y |= kLeafMask;
+        if (refs != 0) y |= kNotEmptyMask;
+        top_cells[c].y = y;
+        leaf_cnt[c] = lg.res[0] * lg.res[1] * lg.res[2];
     }
 }
 
-__global__ void k_check_caps(GridDesc* d, uint32_t cap_leaves, uint32_t cap_leaf_pairs) {
-    if (d->overflow | d->error) return;   // leaf totals are meaningless after an earlier overflow
+__global__ void k_check_leaves(GridDesc* d, uint32_t cap_leaves) {
+    if (d->overflow | d->error) return;   // the leaf total is meaningless after an earlier overflow
     if (d->nleaves > cap_leaves) d->overflow |= kOvfLeaves;
-    if (d->npairs > cap_leaf_pairs) d->overflow |= kOvfLeafPairs;
 }
 
-constexpr int kLT = 128;   // leaf-build block size
+// a9: first leaf of every top cell (prepareTopLevelCellRanges, TLGridBuildKernels.h:130-147)
+__global__ void k_tl_cell_begin(const uint32_t* __restrict__ leaf_begin, const GridDesc* d, uint2* top_cells) {
+    if (d->overflow | d->error) return;
+    const uint32_t C = d->ncells;
+    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < C; c += gridDim.x * blockDim.x)
+        top_cells[c].x = leaf_begin[c];
+}
 
-// a11-a13: per top cell leaf ranges and ordered leaf primitive lists
-// (TLGridBuildKernels.h:536-663 + TLGridSortBuilder.h:375-380 + TLGridBuildKernels.h:750-834).
-// leaf_cnt holds the exclusive scans: x = first leaf, y = first leaf pair.
-__global__ __launch_bounds__(kLT) void k_tl_leaf_build(const uint2* __restrict__ top_ranges,
-                                                       const uint32_t* __restrict__ top_refs,
-                                                       const float4* __restrict__ v, const uint32_t* __restrict__ idx,
-                                                       const GridDesc* d, const uint2* __restrict__ leaf_cnt,
-                                                       uint2* top_cells, uint2* leaves, uint32_t* prims) {
+// sub-cell range of top-level reference i: its top cell (sorted key), triangle, cell sub-grid
+__device__ __forceinline__ uint32_t ref_leaf_range(const DescRegs& g, const uint32_t* __restrict__ top_keys,
+                                                   const uint32_t* __restrict__ top_refs,
+                                                   const float4* __restrict__ v, const uint32_t* __restrict__ idx,
+                                                   const uint2* __restrict__ top_cells, uint32_t i, uint32_t* cell,
+                                                   uint32_t* tri, uint32_t* lres, CRange* r) {
+    *cell = __ldg(top_keys + i);
+    *tri = __ldg(top_refs + i);
+    const uint32_t y = top_cells[*cell].y;
+    lres[0] = y & 0xFFu; lres[1] = (y >> 8) & 0xFFu; lres[2] = (y >> 16) & 0xFFu;
+    f3 p[3], lo, hi;
+    tri_load(v, idx, *tri, p);
+    tri_bbox(p, &lo, &hi);
+    return leaf_range(g, lres, *cell, lo, hi, r);
+}
+
+// a10: leaf pair count per top-level reference, block sums (countLeafLevelPairs,
+// TLGridBuildKernels.h:304-409)
+__global__ __launch_bounds__(kBT) void k_leaf_count_pairs(const uint32_t* __restrict__ top_keys,
+                                                          const uint32_t* __restrict__ top_refs,
+                                                          const float4* __restrict__ v, const uint32_t* __restrict__ idx,
+                                                          const GridDesc* d, const uint2* __restrict__ top_cells,
+                                                          uint32_t* block_sums) {
+    if (d->overflow | d->error) {
+        if (threadIdx.x == 0) block_sums[blockIdx.x] = 0u;
+        return;
+    }
+    const DescRegs g = load_desc(d);
+    const uint32_t i = blockIdx.x * kBT + threadIdx.x;
+    uint32_t n = 0;
+    if (i < d->ntop_pairs) {
+        uint32_t cell, tri, lres[3];
+        CRange r;
+        n = ref_leaf_range(g, top_keys, top_refs, v, idx, top_cells, i, &cell, &tri, lres, &r);
+    }
+    uint32_t tot;
+    block_excl_scan<uint32_t, kBT>(n, &tot);
+    if (threadIdx.x == 0) block_sums[blockIdx.x] = tot;
+}
+
+// a11: leaf pairs in reference order at each reference's scan offset; key = first leaf of
+// the top cell + local sub-cell index (writeLeafLevelKeysAndValues, TLGridBuildKernels.h:536-663)
+__global__ __launch_bounds__(kBT) void k_leaf_write_pairs(const uint32_t* __restrict__ top_keys,
+                                                          const uint32_t* __restrict__ top_refs,
+                                                          const float4* __restrict__ v, const uint32_t* __restrict__ idx,
+                                                          const GridDesc* d, const uint2* __restrict__ top_cells,
+                                                          const uint32_t* block_sums, uint32_t* __restrict__ keys,
+                                                          uint32_t* __restrict__ vals) {
     if (d->overflow | d->error) return;
     const DescRegs g = load_desc(d);
-    for (uint32_t c = blockIdx.x; c < g.ncells; c += gridDim.x) {
-        const uint2 rg = top_ranges[c];
-        const uint2 beg = leaf_cnt[c];
-        const uint32_t y = top_cells[c].y;
-        const uint32_t lres[3] = {y & 0xFFu, (y >> 8) & 0xFFu, (y >> 16) & 0xFFu};
-        const uint32_t nl = lres[0] * lres[1] * lres[2];
-        const uint32_t lb = beg.x, rb = beg.y;
-        if (threadIdx.x == 0) top_cells[c].x = lb;
-        if (rg.x == rg.y) {
-            if (threadIdx.x == 0) leaves[lb] = make_uint2(0u, 0u);
-            continue;
-        }
-        for (uint32_t i = threadIdx.x; i < nl; i += kLT) leaves[lb + i] = make_uint2(0u, 0u);
-        __syncthreads();
-        for (uint32_t i = rg.x + threadIdx.x; i < rg.y; i += kLT) {
-            f3 p[3], lo, hi;
-            CRange r;
-            tri_load(v, idx, __ldg(top_refs + i), p);
-            tri_bbox(p, &lo, &hi);
-            leaf_range(g, lres, c, lo, hi, &r);
-            for (int32_t z = r.lo[2]; z < r.hi[2]; ++z)
-                for (int32_t yy = r.lo[1]; yy < r.hi[1]; ++yy)
-                    for (int32_t x = r.lo[0]; x < r.hi[0]; ++x)
-                        atomicAdd(&leaves[lb + (uint32_t)x + (uint32_t)yy * lres[0] + (uint32_t)z * lres[0] * lres[1]].y, 1u);
-        }
-        __syncthreads();
-        uint32_t carry = 0;
-        for (uint32_t base = 0; base < nl; base += kLT) {
-            const uint32_t i = base + threadIdx.x;
-            const uint32_t cnt = i < nl ? __ldcg(&leaves[lb + i].y) : 0u;
-            uint32_t tot;
-            const uint32_t ex = block_excl_scan<uint32_t, kLT>(cnt, &tot);
-            if (i < nl) leaves[lb + i].x = rb + carry + ex;
-            carry += tot;
-        }
-        __syncthreads();
-        for (uint32_t i = rg.x + threadIdx.x; i < rg.y; i += kLT) {
-            f3 p[3], lo, hi;
-            CRange r;
-            const uint32_t tri = __ldg(top_refs + i);
-            tri_load(v, idx, tri, p);
-            tri_bbox(p, &lo, &hi);
-            leaf_range(g, lres, c, lo, hi, &r);
-            for (int32_t z = r.lo[2]; z < r.hi[2]; ++z)
-                for (int32_t yy = r.lo[1]; yy < r.hi[1]; ++yy)
-                    for (int32_t x = r.lo[0]; x < r.hi[0]; ++x) {
-                        uint32_t slot = atomicAdd(&leaves[lb + (uint32_t)x + (uint32_t)yy * lres[0] + (uint32_t)z * lres[0] * lres[1]].x, 1u);
-                        prims[slot] = tri;
-                    }
-        }
-        __syncthreads();
-        for (uint32_t i = threadIdx.x; i < nl; i += kLT) {
-            const uint2 lv = __ldcg(&leaves[lb + i]);
-            if (lv.y == 0) {   // empty leaf: {0, 0} as after the reference's memset
-                leaves[lb + i] = make_uint2(0u, 0u);
-                continue;
+    const uint32_t i = blockIdx.x * kBT + threadIdx.x;
+    uint32_t n = 0, cell = 0, tri = 0, lres[3] = {1u, 1u, 1u};
+    CRange r;
+    if (i < d->ntop_pairs) n = ref_leaf_range(g, top_keys, top_refs, v, idx, top_cells, i, &cell, &tri, lres, &r);
+    uint32_t tot;
+    uint32_t slot = block_excl_scan<uint32_t, kBT>(n, &tot) + block_sums[blockIdx.x];
+    if (n == 0) return;
+    const uint32_t base = top_cells[cell].x;
+    for (int32_t z = r.lo[2]; z < r.hi[2]; ++z)
+        for (int32_t yy = r.lo[1]; yy < r.hi[1]; ++yy)
+            for (int32_t x = r.lo[0]; x < r.hi[0]; ++x, ++slot) {
+                keys[slot] = base + (uint32_t)x + (uint32_t)yy * lres[0] + (uint32_t)z * lres[0] * lres[1];
+                vals[slot] = tri;
             }
-            const uint32_t end = lv.x, start = end - lv.y;
-            // canonical order inside a leaf: ascending triangle id (insertion sort, short lists)
-            for (uint32_t a = start + 1; a < end; ++a) {
-                const uint32_t key = __ldcg(prims + a);
-                uint32_t b = a;
-                uint32_t prev;
-                while (b > start && (prev = __ldcg(prims + b - 1)) > key) { prims[b] = prev; --b; }
-                prims[b] = key;
-            }
-            leaves[lb + i] = make_uint2(start, end);
-        }
-        __syncthreads();
-    }
 }
 
 int key_bits_for(size_t max_key) {
@@ -452,6 +429,11 @@ static int build_once(hr_ctx* c, int32_t kind, int32_t exact, uint32_t* ovf_out)
     const uint32_t nblocks = (ntri + kBT - 1) / kBT;
     const int key_bits = key_bits_for(B.cap_cells);
     const int passes = radix_passes(key_bits);
+    const int leaf_bits = key_bits_for(B.cap_leaves);
+    const int leaf_passes = radix_passes(leaf_bits);
+    const uint32_t nref_blocks = (uint32_t)((cap_pairs + kBT - 1) / kBT);   // per top-level reference
+    size_t hist_words = radix_tile_hist_words(cap_pairs, key_bits);
+    if (kind == kTwoLevel) hist_words = std::max(hist_words, radix_tile_hist_words(B.cap_leaf_pairs, leaf_bits));
     int rc;
     if ((rc = ensure(c, B.desc, sizeof(GridDesc)))) return rc;
     if ((rc = ensure(c, B.cells, sizeof(uint2) * B.cap_cells))) return rc;
@@ -459,17 +441,21 @@ static int build_once(hr_ctx* c, int32_t kind, int32_t exact, uint32_t* ovf_out)
     if ((rc = ensure(c, B.vals_a, sizeof(uint32_t) * cap_pairs))) return rc;
     if ((rc = ensure(c, B.keys_b, sizeof(uint32_t) * cap_pairs))) return rc;
     if ((rc = ensure(c, B.vals_b, sizeof(uint32_t) * cap_pairs))) return rc;
-    if ((rc = ensure(c, B.block_sums, sizeof(uint32_t) * (nblocks + 1)))) return rc;
-    if ((rc = ensure(c, B.tile_hist, sizeof(uint32_t) * radix_tile_hist_words(cap_pairs, key_bits)))) return rc;
+    if ((rc = ensure(c, B.block_sums, sizeof(uint32_t) * (std::max(nblocks, nref_blocks) + 1)))) return rc;
+    if ((rc = ensure(c, B.tile_hist, sizeof(uint32_t) * hist_words))) return rc;
     if ((rc = ensure(c, B.row_total, sizeof(uint32_t) * 256))) return rc;
     if (kind == kUniform) {
         if ((rc = ensure(c, B.prims, sizeof(uint32_t) * cap_pairs))) return rc;
     } else {
         if ((rc = ensure(c, B.top_ranges, sizeof(uint2) * B.cap_cells))) return rc;
         if ((rc = ensure(c, B.top_refs, sizeof(uint32_t) * cap_pairs))) return rc;
-        if ((rc = ensure(c, B.leaf_cnt, sizeof(uint2) * B.cap_cells))) return rc;
-        if ((rc = ensure(c, B.scan_partials, sizeof(uint2) * scan_partials_words(B.cap_cells)))) return rc;
+        if ((rc = ensure(c, B.leaf_cnt, sizeof(uint32_t) * B.cap_cells))) return rc;
+        if ((rc = ensure(c, B.scan_partials, sizeof(uint32_t) * (scan_partials_words(B.cap_cells) + 2)))) return rc;
         if ((rc = ensure(c, B.leaves, sizeof(uint2) * B.cap_leaves))) return rc;
+        if ((rc = ensure(c, B.lkeys_a, sizeof(uint32_t) * B.cap_leaf_pairs))) return rc;
+        if ((rc = ensure(c, B.lvals_a, sizeof(uint32_t) * B.cap_leaf_pairs))) return rc;
+        if ((rc = ensure(c, B.lkeys_b, sizeof(uint32_t) * B.cap_leaf_pairs))) return rc;
+        if ((rc = ensure(c, B.lvals_b, sizeof(uint32_t) * B.cap_leaf_pairs))) return rc;
         if ((rc = ensure(c, B.prims, sizeof(uint32_t) * B.cap_leaf_pairs))) return rc;
     }
     GridDesc* d = B.desc.as<GridDesc>();
@@ -477,7 +463,7 @@ static int build_once(hr_ctx* c, int32_t kind, int32_t exact, uint32_t* ovf_out)
     auto mark = [&]() { if (c->timing && ev < 16) cudaEventRecord(c->ev[ev++], s); };
     mark();
     // launches of this function (radix sort and scans count their own)
-    c->launches += 3 + (nblocks > 0 ? 3 : 0) + 2 + (kind == kTwoLevel ? 3 : 0);
+    c->launches += 3 + (nblocks > 0 ? 3 : 0) + 2 + (kind == kTwoLevel ? 9 : 0);
     k_desc_init<<<1, 1, 0, s>>>(d, kind, ntri, c->counters.as<uint32_t>() + 2);
     const int gridv = std::max(1, std::min((int)((c->nverts + kBT - 1) / kBT), c->num_sms * 8));
     if (c->lerp_pending) {
@@ -513,23 +499,42 @@ static int build_once(hr_ctx* c, int32_t kind, int32_t exact, uint32_t* ovf_out)
     mark();
     uint2* ranges = kind == kUniform ? B.cells.as<uint2>() : B.top_ranges.as<uint2>();
     const int gcells = std::max(1, std::min((int)((B.cap_cells + 255) / 256), c->num_sms * 16));
-    k_fill_u2<<<gcells, 256, 0, s>>>(ranges, &d->ncells, make_uint2(0u, 0u));
+    k_fill_u2<<<gcells, 256, 0, s>>>(ranges, &d->ncells, d, make_uint2(0u, 0u));
     const int gpairs = std::max(1, std::min((int)((cap_pairs + 255) / 256), c->num_sms * 16));
-    k_cell_ranges<<<gpairs, 256, 0, s>>>(sorted_keys, d_np, d, ranges);
+    k_cell_ranges<<<gpairs, 256, 0, s>>>(sorted_keys, d_np, &d->ncells, d, ranges);
     mark();
     if (kind == kTwoLevel) {
-        const int gw = std::max(1, std::min((int)((B.cap_cells + 7) / 8), c->num_sms * 16));
-        k_tl_leaf_count<<<gw, kBT, 0, s>>>(ranges, B.top_refs.as<uint32_t>(), v, ix, d, c->leaf_density,
-                                          B.leaf_cnt.as<uint2>(), B.cells.as<uint2>());
-        if ((rc = exclusive_scan_u32x2(c, B.leaf_cnt.as<uint2>(), &d->ncells, B.cap_cells, &d->nleaves, &d->npairs,
-                                       B.scan_partials.as<uint2>(), s)))
+        // leaf level, TLGridSortBuilder.h:256-410: leaf cells per top cell, scan, leaf pairs
+        // per reference in reference order, stable sort by leaf, leaf ranges
+        k_tl_cells<<<gcells, 256, 0, s>>>(ranges, d, c->leaf_density, B.leaf_cnt.as<uint32_t>(), B.cells.as<uint2>());
+        uint32_t* sp = B.scan_partials.as<uint32_t>();
+        if ((rc = exclusive_scan_u32(c, B.leaf_cnt.as<uint32_t>(), &d->ncells, B.cap_cells, &d->nleaves, sp, s)))
             return rc;
-        k_check_caps<<<1, 1, 0, s>>>(d, (uint32_t)std::min(B.cap_leaves, (size_t)0xffffffffu),
-                                     (uint32_t)std::min(B.cap_leaf_pairs, (size_t)0xffffffffu));
+        k_check_leaves<<<1, 1, 0, s>>>(d, (uint32_t)std::min(B.cap_leaves, (size_t)0xffffffffu));
+        k_tl_cell_begin<<<gcells, 256, 0, s>>>(B.leaf_cnt.as<uint32_t>(), d, B.cells.as<uint2>());
         mark();
-        const int gl = std::max(1, std::min((int)B.cap_cells, c->num_sms * 16));
-        k_tl_leaf_build<<<gl, kLT, 0, s>>>(ranges, B.top_refs.as<uint32_t>(), v, ix, d, B.leaf_cnt.as<uint2>(),
-                                          B.cells.as<uint2>(), B.leaves.as<uint2>(), B.prims.as<uint32_t>());
+        uint32_t* lsum = B.block_sums.as<uint32_t>();
+        k_leaf_count_pairs<<<nref_blocks, kBT, 0, s>>>(sorted_keys, B.top_refs.as<uint32_t>(), v, ix, d,
+                                                       B.cells.as<uint2>(), lsum);
+        if ((rc = scan_block_sums(c, lsum, nref_blocks, &d->npairs, &d->overflow,
+                                  (uint32_t)std::min(B.cap_leaf_pairs, (size_t)0xffffffffu), kOvfLeafPairs,
+                                  &d->req_leaf_pairs, s)))
+            return rc;
+        k_leaf_write_pairs<<<nref_blocks, kBT, 0, s>>>(sorted_keys, B.top_refs.as<uint32_t>(), v, ix, d,
+                                                       B.cells.as<uint2>(), lsum, B.lkeys_a.as<uint32_t>(),
+                                                       B.lvals_a.as<uint32_t>());
+        mark();
+        uint32_t* leaf_keys = (leaf_passes % 2 == 1) ? B.lkeys_b.as<uint32_t>() : B.lkeys_a.as<uint32_t>();
+        if ((rc = radix_sort_pairs(c, B.lkeys_a.as<uint32_t>(), B.lvals_a.as<uint32_t>(), B.lkeys_b.as<uint32_t>(),
+                                   B.lvals_b.as<uint32_t>(), leaf_keys, B.prims.as<uint32_t>(), &d->npairs,
+                                   B.cap_leaf_pairs, leaf_bits, B.tile_hist.as<uint32_t>(),
+                                   B.row_total.as<uint32_t>(), s)))
+            return rc;
+        mark();
+        const int gleaves = std::max(1, std::min((int)((B.cap_leaves + 255) / 256), c->num_sms * 16));
+        k_fill_u2<<<gleaves, 256, 0, s>>>(B.leaves.as<uint2>(), &d->nleaves, d, make_uint2(0u, 0u));
+        const int glp = std::max(1, std::min((int)((B.cap_leaf_pairs + 255) / 256), c->num_sms * 16));
+        k_cell_ranges<<<glp, 256, 0, s>>>(leaf_keys, &d->npairs, &d->nleaves, d, B.leaves.as<uint2>());
         mark();
     }
     c->nstages = ev;
@@ -565,7 +570,7 @@ int build_grid(hr_ctx* c, int32_t kind, int32_t exact) {
         if (ovf & kOvfCells) B.cap_cells = (size_t)hd.req_cells + 64u;
         if (ovf & (kOvfPairs | kOvfTopPairs)) B.cap_pairs = (size_t)(hd.req_pairs * 1.25) + 4096u;
         if (ovf & kOvfLeaves) B.cap_leaves = (size_t)(hd.nleaves * 1.25) + 4096u;
-        if (ovf & kOvfLeafPairs) B.cap_leaf_pairs = (size_t)(hd.npairs * 1.25) + 4096u;
+        if (ovf & kOvfLeafPairs) B.cap_leaf_pairs = (size_t)(hd.req_leaf_pairs * 1.25) + 4096u;
     }
     return set_error(c, 3, "grid build: capacity did not converge");
 }

@@ -43,7 +43,8 @@ struct GridDesc {
     int32_t bmin_enc[3], bmax_enc[3];  // ordered-int encoded running bounds
     uint32_t req_cells;   // cells needed when kOvfCells is set (ncells is then 0)
     uint32_t req_pairs;   // pairs needed when kOvfPairs / kOvfTopPairs is set (count is then 0)
-    uint32_t pad[2];
+    uint32_t req_leaf_pairs;   // leaf pairs needed when kOvfLeafPairs is set (count is then 0)
+    uint32_t pad1;
 };
 
 __host__ __device__ __forceinline__ float hmin(float a, float b) { return (a != a) ? b : ((b < a) ? b : a); }

@@ -51,7 +51,8 @@ struct GridBuffers {
     DevBuf row_total;     // radix digit totals
     DevBuf top_ranges;    // two-level: uint2 per top cell
     DevBuf top_refs;      // two-level: sorted top-level values
-    DevBuf leaf_cnt;      // two-level: uint2 (leaf cells, leaf pairs) per top cell, scanned in place
+    DevBuf leaf_cnt;      // two-level: leaf cells per top cell, scanned in place to the first leaf
+    DevBuf lkeys_a, lvals_a, lkeys_b, lvals_b;   // two-level: leaf pair ping-pong
     DevBuf scan_partials; // generic scan partial sums
     size_t cap_cells = 0, cap_pairs = 0, cap_top_pairs = 0, cap_leaves = 0, cap_leaf_pairs = 0;
 };
