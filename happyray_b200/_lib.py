@@ -62,6 +62,7 @@ SIGNATURES = {
     "hr_get_ray_count": (C.c_int, [P, C.POINTER(C.c_uint64), C.c_int32]),
     "hr_set_stats": (C.c_int, [P, C.c_int32]),
     "hr_get_counters": (C.c_int, [P, C.POINTER(C.c_uint64), C.c_int32]),
+    "hr_get_render_times": (C.c_int32, [P, P, C.c_int32]),
     "hr_sync": (C.c_int, [P]),
     "hr_bounds_diagonal": (C.c_float, [P]),
     "hr_exclusive_scan_device": (C.c_int, [P, P, C.c_uint32]),

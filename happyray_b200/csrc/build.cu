@@ -18,10 +18,10 @@
 //   * all sizes (bounds, resolution, pair counts, leaf counts) stay in a device-side
 //     descriptor; the whole build is enqueued without a host round trip and capacity
 //     overflow is reported by flag;
-//   * leaf-level pairs are never globally sorted: their keys are already grouped by top
-//     cell (leaf ranges are allocated in top-cell order), so one CTA per top cell counts,
-//     scans, scatters and orders its own leaves, which is the same permutation the global
-//     stable sort of TLGridSortBuilder.h:375-380 produces.
+//   * leaf-level pairs are likewise written at per-reference scan offsets in top-level
+//     reference order, so the stable leaf sort gives ascending triangle ids per leaf;
+//   * the pair-count pass also writes a per-triangle vertex array (3 float4) that the
+//     later passes and the traversal read with one contiguous load per triangle.
 #include "hr_internal.h"
 #include "hr_block.cuh"
 
@@ -143,9 +143,12 @@ __device__ __forceinline__ DescRegs load_desc(const GridDesc* d) {
     return r;
 }
 
-// a3: pair count, one triangle per thread; block sums for the scan (UniformGridBuildKernels.h:40-105)
+// a3: pair count, one triangle per thread; block sums for the scan (UniformGridBuildKernels.h:40-105).
+// Also writes the per-triangle vertex array (3 float4) that the later build passes and the
+// traversal read instead of gathering through the index buffer.
 __global__ __launch_bounds__(kBT) void k_count_pairs(const float4* __restrict__ v, const uint32_t* __restrict__ idx,
-                                                     uint32_t ntri, const GridDesc* d, uint32_t* block_sums) {
+                                                     uint32_t ntri, const GridDesc* d, uint32_t* block_sums,
+                                                     float4* __restrict__ tris) {
     if (d->overflow | d->error) {
         if (threadIdx.x == 0) block_sums[blockIdx.x] = 0u;
         return;
@@ -157,6 +160,10 @@ __global__ __launch_bounds__(kBT) void k_count_pairs(const float4* __restrict__ 
         f3 p[3], lo, hi;
         CRange r;
         tri_load(v, idx, t, p);
+        float4* q = tris + 3 * (size_t)t;
+        q[0] = make_float4(p[0].x, p[0].y, p[0].z, 0.0f);
+        q[1] = make_float4(p[1].x, p[1].y, p[1].z, 0.0f);
+        q[2] = make_float4(p[2].x, p[2].y, p[2].z, 0.0f);
         tri_bbox(p, &lo, &hi);
         n = cell_range(lo, hi, g.bmin, g.rcp, g.res, &r);
     }
@@ -204,9 +211,9 @@ __device__ __forceinline__ bool sat_overlap(f3 nrm, f3 c, const f3* tv, f3 h) {
 // a5: pair scatter at the triangle's exclusive-scan offset.  Keys are x + y*rx + z*rx*ry;
 // with EXACT a cell rejected by the SAT test gets key = ncells (sorted last, skipped).
 template <bool EXACT>
-__global__ __launch_bounds__(kBT) void k_write_pairs(const float4* __restrict__ v, const uint32_t* __restrict__ idx,
-                                                     uint32_t ntri, const GridDesc* d, const uint32_t* block_sums,
-                                                     uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+__global__ __launch_bounds__(kBT) void k_write_pairs(const float4* __restrict__ tris, uint32_t ntri, const GridDesc* d,
+                                                     const uint32_t* block_sums, uint32_t* __restrict__ keys,
+                                                     uint32_t* __restrict__ vals) {
     if (d->overflow | d->error) return;
     const DescRegs g = load_desc(d);
     const uint32_t t = blockIdx.x * kBT + threadIdx.x;
@@ -214,7 +221,7 @@ __global__ __launch_bounds__(kBT) void k_write_pairs(const float4* __restrict__ 
     f3 p[3], lo, hi;
     CRange r;
     if (t < ntri) {
-        tri_load(v, idx, t, p);
+        tri_fetch(tris, t, p);
         tri_bbox(p, &lo, &hi);
         n = cell_range(lo, hi, g.bmin, g.rcp, g.res, &r);
     }
@@ -338,7 +345,7 @@ __global__ void k_tl_cell_begin(const uint32_t* __restrict__ leaf_begin, const G
 // sub-cell range of top-level reference i: its top cell (sorted key), triangle, cell sub-grid
 __device__ __forceinline__ uint32_t ref_leaf_range(const DescRegs& g, const uint32_t* __restrict__ top_keys,
                                                    const uint32_t* __restrict__ top_refs,
-                                                   const float4* __restrict__ v, const uint32_t* __restrict__ idx,
+                                                   const float4* __restrict__ tris,
                                                    const uint2* __restrict__ top_cells, uint32_t i, uint32_t* cell,
                                                    uint32_t* tri, uint32_t* lres, CRange* r) {
     *cell = __ldg(top_keys + i);
@@ -346,7 +353,7 @@ __device__ __forceinline__ uint32_t ref_leaf_range(const DescRegs& g, const uint
     const uint32_t y = top_cells[*cell].y;
     lres[0] = y & 0xFFu; lres[1] = (y >> 8) & 0xFFu; lres[2] = (y >> 16) & 0xFFu;
     f3 p[3], lo, hi;
-    tri_load(v, idx, *tri, p);
+    tri_fetch(tris, *tri, p);
     tri_bbox(p, &lo, &hi);
     return leaf_range(g, lres, *cell, lo, hi, r);
 }
@@ -355,7 +362,7 @@ __device__ __forceinline__ uint32_t ref_leaf_range(const DescRegs& g, const uint
 // TLGridBuildKernels.h:304-409)
 __global__ __launch_bounds__(kBT) void k_leaf_count_pairs(const uint32_t* __restrict__ top_keys,
                                                           const uint32_t* __restrict__ top_refs,
-                                                          const float4* __restrict__ v, const uint32_t* __restrict__ idx,
+                                                          const float4* __restrict__ tris,
                                                           const GridDesc* d, const uint2* __restrict__ top_cells,
                                                           uint32_t* block_sums) {
     if (d->overflow | d->error) {
@@ -368,7 +375,7 @@ __global__ __launch_bounds__(kBT) void k_leaf_count_pairs(const uint32_t* __rest
     if (i < d->ntop_pairs) {
         uint32_t cell, tri, lres[3];
         CRange r;
-        n = ref_leaf_range(g, top_keys, top_refs, v, idx, top_cells, i, &cell, &tri, lres, &r);
+        n = ref_leaf_range(g, top_keys, top_refs, tris, top_cells, i, &cell, &tri, lres, &r);
     }
     uint32_t tot;
     block_excl_scan<uint32_t, kBT>(n, &tot);
@@ -379,7 +386,7 @@ __global__ __launch_bounds__(kBT) void k_leaf_count_pairs(const uint32_t* __rest
 // the top cell + local sub-cell index (writeLeafLevelKeysAndValues, TLGridBuildKernels.h:536-663)
 __global__ __launch_bounds__(kBT) void k_leaf_write_pairs(const uint32_t* __restrict__ top_keys,
                                                           const uint32_t* __restrict__ top_refs,
-                                                          const float4* __restrict__ v, const uint32_t* __restrict__ idx,
+                                                          const float4* __restrict__ tris,
                                                           const GridDesc* d, const uint2* __restrict__ top_cells,
                                                           const uint32_t* block_sums, uint32_t* __restrict__ keys,
                                                           uint32_t* __restrict__ vals) {
@@ -388,7 +395,7 @@ __global__ __launch_bounds__(kBT) void k_leaf_write_pairs(const uint32_t* __rest
     const uint32_t i = blockIdx.x * kBT + threadIdx.x;
     uint32_t n = 0, cell = 0, tri = 0, lres[3] = {1u, 1u, 1u};
     CRange r;
-    if (i < d->ntop_pairs) n = ref_leaf_range(g, top_keys, top_refs, v, idx, top_cells, i, &cell, &tri, lres, &r);
+    if (i < d->ntop_pairs) n = ref_leaf_range(g, top_keys, top_refs, tris, top_cells, i, &cell, &tri, lres, &r);
     uint32_t tot;
     uint32_t slot = block_excl_scan<uint32_t, kBT>(n, &tot) + block_sums[blockIdx.x];
     if (n == 0) return;
@@ -436,6 +443,7 @@ static int build_once(hr_ctx* c, int32_t kind, int32_t exact, uint32_t* ovf_out)
     if (kind == kTwoLevel) hist_words = std::max(hist_words, radix_tile_hist_words(B.cap_leaf_pairs, leaf_bits));
     int rc;
     if ((rc = ensure(c, B.desc, sizeof(GridDesc)))) return rc;
+    if ((rc = ensure(c, c->tris, sizeof(float4) * 3 * (size_t)ntri))) return rc;
     if ((rc = ensure(c, B.cells, sizeof(uint2) * B.cap_cells))) return rc;
     if ((rc = ensure(c, B.keys_a, sizeof(uint32_t) * cap_pairs))) return rc;
     if ((rc = ensure(c, B.vals_a, sizeof(uint32_t) * cap_pairs))) return rc;
@@ -480,14 +488,14 @@ static int build_once(hr_ctx* c, int32_t kind, int32_t exact, uint32_t* ovf_out)
     uint32_t* bsum = B.block_sums.as<uint32_t>();
     uint32_t* d_np = kind == kUniform ? &d->npairs : &d->ntop_pairs;
     if (nblocks > 0) {
-        k_count_pairs<<<nblocks, kBT, 0, s>>>(v, ix, ntri, d, bsum);
+        k_count_pairs<<<nblocks, kBT, 0, s>>>(v, ix, ntri, d, bsum, c->tris.as<float4>());
         if ((rc = scan_block_sums(c, bsum, nblocks, d_np, &d->overflow, (uint32_t)std::min(cap_pairs, (size_t)0xffffffffu),
                                   kind == kUniform ? kOvfPairs : kOvfTopPairs, &d->req_pairs, s)))
             return rc;
         if (kind == kUniform && exact)
-            k_write_pairs<true><<<nblocks, kBT, 0, s>>>(v, ix, ntri, d, bsum, B.keys_a.as<uint32_t>(), B.vals_a.as<uint32_t>());
+            k_write_pairs<true><<<nblocks, kBT, 0, s>>>(c->tris.as<float4>(), ntri, d, bsum, B.keys_a.as<uint32_t>(), B.vals_a.as<uint32_t>());
         else
-            k_write_pairs<false><<<nblocks, kBT, 0, s>>>(v, ix, ntri, d, bsum, B.keys_a.as<uint32_t>(), B.vals_a.as<uint32_t>());
+            k_write_pairs<false><<<nblocks, kBT, 0, s>>>(c->tris.as<float4>(), ntri, d, bsum, B.keys_a.as<uint32_t>(), B.vals_a.as<uint32_t>());
     }
     mark();
     uint32_t* sorted_keys = (passes % 2 == 1) ? B.keys_b.as<uint32_t>() : B.keys_a.as<uint32_t>();
@@ -514,13 +522,13 @@ static int build_once(hr_ctx* c, int32_t kind, int32_t exact, uint32_t* ovf_out)
         k_tl_cell_begin<<<gcells, 256, 0, s>>>(B.leaf_cnt.as<uint32_t>(), d, B.cells.as<uint2>());
         mark();
         uint32_t* lsum = B.block_sums.as<uint32_t>();
-        k_leaf_count_pairs<<<nref_blocks, kBT, 0, s>>>(sorted_keys, B.top_refs.as<uint32_t>(), v, ix, d,
+        k_leaf_count_pairs<<<nref_blocks, kBT, 0, s>>>(sorted_keys, B.top_refs.as<uint32_t>(), c->tris.as<float4>(), d,
                                                        B.cells.as<uint2>(), lsum);
         if ((rc = scan_block_sums(c, lsum, nref_blocks, &d->npairs, &d->overflow,
                                   (uint32_t)std::min(B.cap_leaf_pairs, (size_t)0xffffffffu), kOvfLeafPairs,
                                   &d->req_leaf_pairs, s)))
             return rc;
-        k_leaf_write_pairs<<<nref_blocks, kBT, 0, s>>>(sorted_keys, B.top_refs.as<uint32_t>(), v, ix, d,
+        k_leaf_write_pairs<<<nref_blocks, kBT, 0, s>>>(sorted_keys, B.top_refs.as<uint32_t>(), c->tris.as<float4>(), d,
                                                        B.cells.as<uint2>(), lsum, B.lkeys_a.as<uint32_t>(),
                                                        B.lvals_a.as<uint32_t>());
         mark();

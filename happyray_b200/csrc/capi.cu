@@ -188,6 +188,7 @@ hr_status hr_create(hr_ctx** out, int32_t device, void* stream) {
         c->own_stream = true;
     }
     for (auto& e : c->ev) cudaEventCreate(&e);
+    for (auto& e : c->rev) cudaEventCreate(&e);
     if (ensure(c, c->counters, 64)) { hr_destroy(c); return HR_ERR_OUT_OF_MEMORY; }
     cudaMemsetAsync(c->counters.p, 0, 64, c->stream);
     *out = c;
@@ -198,14 +199,16 @@ void hr_destroy(hr_ctx* c) {
     if (!c) return;
     DeviceGuard dg(c->device);
     cudaStreamSynchronize(c->stream);
-    DevBuf* bufs[] = {&c->verts, &c->idx, &c->keyframes, &c->staging, &c->counters, &c->fb, &c->out_id,
+    DevBuf* bufs[] = {&c->verts, &c->idx, &c->tris, &c->keyframes, &c->staging, &c->counters, &c->fb, &c->out_id,
                       &c->out_t, &c->out_u, &c->out_v, &c->ray_in, &c->g.desc, &c->g.cells, &c->g.leaves,
                       &c->g.prims, &c->g.keys_a, &c->g.vals_a, &c->g.keys_b, &c->g.vals_b, &c->g.block_sums,
                       &c->g.tile_hist, &c->g.row_total, &c->g.top_ranges, &c->g.top_refs, &c->g.leaf_cnt,
-                      &c->g.lkeys_a, &c->g.lvals_a, &c->g.lkeys_b, &c->g.lvals_b, &c->g.scan_partials};
+                      &c->g.lkeys_a, &c->g.lvals_a, &c->g.lkeys_b, &c->g.lvals_b, &c->g.scan_partials,
+                      &c->hit_t, &c->hit_tri, &c->unocc, &c->queue};
     for (DevBuf* b : bufs) free_buf(c, *b);
     cudaStreamSynchronize(c->stream);
     for (auto& e : c->ev) if (e) cudaEventDestroy(e);
+    for (auto& e : c->rev) if (e) cudaEventDestroy(e);
     if (c->pinned) cudaFreeHost(c->pinned);
     if (c->own_stream) cudaStreamDestroy(c->stream);
     delete c;
@@ -468,14 +471,28 @@ hr_status hr_occluded_device(hr_ctx* c, const float* org, const float* dir, cons
     return (hr_status)launch_occluded(c, org, dir, tmax, n, occ);
 }
 
+// device counter words: [0] rays, [2] cells, [3] tests of the primary pass; [4] rays,
+// [5] cells, [6] tests of the secondary pass; [1] index check; [7] AO queue length
+static int read_counters(hr_ctx* c, uint64_t w[8], int32_t reset) {
+    int rc;
+    if ((rc = cuda_check(c, cudaMemcpyAsync(w, c->counters.p, 64, cudaMemcpyDeviceToHost, c->stream), "counters")))
+        return rc;
+    if (reset) {
+        // word 1 holds the index-check result of the last upload and is kept
+        cudaMemsetAsync(c->counters.p, 0, 8, c->stream);
+        cudaMemsetAsync(c->counters.as<uint64_t>() + 2, 0, 40, c->stream);
+    }
+    return cuda_check(c, cudaStreamSynchronize(c->stream), "counters");
+}
+
 hr_status hr_get_ray_count(hr_ctx* c, uint64_t* rays, int32_t reset) {
     if (bad(c) || !rays) return HR_ERR_INVALID_ARG;
     DeviceGuard dg(c->device);
+    uint64_t w[8];
     int rc;
-    if ((rc = cuda_check(c, cudaMemcpyAsync(rays, c->counters.p, 8, cudaMemcpyDeviceToHost, c->stream), "counter")))
-        return (hr_status)rc;
-    if (reset) cudaMemsetAsync(c->counters.p, 0, 8, c->stream);
-    return (hr_status)cuda_check(c, cudaStreamSynchronize(c->stream), "get_ray_count");
+    if ((rc = read_counters(c, w, reset))) return (hr_status)rc;
+    *rays = w[0] + w[4];
+    return HR_OK;
 }
 
 hr_status hr_set_stats(hr_ctx* c, int32_t enable) {
@@ -484,24 +501,33 @@ hr_status hr_set_stats(hr_ctx* c, int32_t enable) {
     return HR_OK;
 }
 
-hr_status hr_get_counters(hr_ctx* c, uint64_t out[4], int32_t reset) {
+hr_status hr_get_counters(hr_ctx* c, uint64_t out[8], int32_t reset) {
     if (bad(c) || !out) return HR_ERR_INVALID_ARG;
     DeviceGuard dg(c->device);
-    uint64_t w[4];
+    uint64_t w[8];
     int rc;
-    if ((rc = cuda_check(c, cudaMemcpyAsync(w, c->counters.p, sizeof(w), cudaMemcpyDeviceToHost, c->stream), "counters")))
-        return (hr_status)rc;
-    if (reset) {
-        // word 1 holds the index-check result of the last upload and is kept
-        cudaMemsetAsync(c->counters.p, 0, 8, c->stream);
-        cudaMemsetAsync(c->counters.as<uint64_t>() + 2, 0, 16, c->stream);
-    }
-    if ((rc = cuda_check(c, cudaStreamSynchronize(c->stream), "get_counters"))) return (hr_status)rc;
-    out[0] = w[0];
-    out[1] = w[2];
-    out[2] = w[3];
+    if ((rc = read_counters(c, w, reset))) return (hr_status)rc;
+    out[0] = w[0] + w[4];
+    out[1] = w[2] + w[5];
+    out[2] = w[3] + w[6];
     out[3] = c->launches;
+    out[4] = w[4];
+    out[5] = w[5];
+    out[6] = w[6];
+    out[7] = 0;
     return HR_OK;
+}
+
+int32_t hr_get_render_times(hr_ctx* c, float* ms, int32_t max_kernels) {
+    if (bad(c) || !ms || !c->timing) return 0;
+    DeviceGuard dg(c->device);
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) return 0;
+    int32_t n = c->nrender_ev > 0 ? c->nrender_ev - 1 : 0;
+    if (n > max_kernels) n = max_kernels;
+    for (int32_t i = 0; i < n; ++i) {
+        if (cudaEventElapsedTime(&ms[i], c->rev[i], c->rev[i + 1]) != cudaSuccess) return 0;
+    }
+    return n;
 }
 
 hr_status hr_sync(hr_ctx* c) {

@@ -91,6 +91,14 @@ __device__ __forceinline__ void tri_load(const float4* __restrict__ v, const uin
     uint32_t i0 = __ldg(idx + 3 * (size_t)t), i1 = __ldg(idx + 3 * (size_t)t + 1), i2 = __ldg(idx + 3 * (size_t)t + 2);
     p[0] = ldv(v, i0); p[1] = ldv(v, i1); p[2] = ldv(v, i2);
 }
+// Triangle vertices from the per-triangle array (3 float4 per triangle, written by the
+// pair-count pass of every build): one contiguous 48-byte load instead of three
+// index-dependent vertex gathers.
+__device__ __forceinline__ void tri_fetch(const float4* __restrict__ tris, uint32_t t, f3* p) {
+    const float4* q = tris + 3 * (size_t)t;
+    const float4 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2);
+    p[0] = mk(a.x, a.y, a.z); p[1] = mk(b.x, b.y, b.z); p[2] = mk(c.x, c.y, c.z);
+}
 __device__ __forceinline__ void tri_bbox(const f3* p, f3* lo, f3* hi) {
     f3 a = mk(FLT_MAX, FLT_MAX, FLT_MAX), b = mk(-FLT_MAX, -FLT_MAX, -FLT_MAX);
 #pragma unroll

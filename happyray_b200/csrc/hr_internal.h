@@ -74,6 +74,7 @@ struct hr_ctx {
     uint32_t ntri = 0, nverts = 0, nkeyframes = 0;
     hr::DevBuf verts;      // float4 current frame
     hr::DevBuf idx;        // uint32 x3
+    hr::DevBuf tris;       // float4 x3 per triangle: the current frame's vertices, written by each build
     hr::DevBuf keyframes;  // float4 x nverts x nkeyframes
     hr::DevBuf staging;    // float4 staging of host keyframes on upload
     int32_t frame_a = 0, frame_b = 0;
@@ -102,6 +103,9 @@ struct hr_ctx {
     hr::IntegratorParams ip;
     hr::DevBuf fb;               // float3 framebuffer (device)
     hr::DevBuf out_id, out_t, out_u, out_v, ray_in;  // ray-query staging
+    hr::DevBuf hit_t, hit_tri, unocc, queue;          // AO wavefront: per-pixel hits, hit-pixel queue
+    cudaEvent_t rev[8] = {};     // render kernel boundaries (timing mode)
+    int nrender_ev = 0;
     void* pinned = nullptr;      // pinned host staging
     size_t pinned_bytes = 0;
 };

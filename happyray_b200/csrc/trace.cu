@@ -16,6 +16,14 @@
 //     points use the direction itself instead of re-deriving it with __fdividef;
 //   * primary ray directions are normalised, so t is a distance;
 //   * no fast-math: IEEE division / square root, no FMA contraction.
+//
+// Execution model: the traversal is warp-synchronous.  Every lane advances its own DDA
+// to its next non-empty cell or leaf, then the warp tests the triangle lists together:
+// a lane with a short list tests it alone; a long list (more than kCoopMin triangles,
+// e.g. a whole small sphere inside one leaf) is tested by all 32 lanes, strided, and
+// reduced by (smallest t, then smallest list position), which is exactly the
+// first-tested-wins rule of the sequential intersector.  Traversal functions must
+// therefore be called by all lanes of a warp; lanes without a ray pass active = false.
 #include "hr_internal.h"
 #include "hr_block.cuh"
 
@@ -23,9 +31,10 @@ namespace hr {
 
 namespace {
 
+constexpr uint32_t kCoopMin = 8;   // longer triangle lists are intersected by the whole warp
+
 struct Scene {
-    const float4* __restrict__ v;
-    const uint32_t* __restrict__ idx;
+    const float4* __restrict__ tris;   // 3 float4 per triangle (current frame)
     const uint2* __restrict__ cells;
     const uint2* __restrict__ leaves;
     const uint32_t* __restrict__ prims;
@@ -55,24 +64,33 @@ struct Hit {
     bool hit;
 };
 
-// a16: Moller-Trumbore over prims[b, e); first-tested wins ties (strict <)
+// a16: Moller-Trumbore of one triangle (RayTriangleIntersector.h:52-90); returns the hit
+// test with strict t < tbest
+__device__ __forceinline__ bool mt_test(const Scene& s, uint32_t tri, f3 o, f3 d, float tbest, float* ot, float* ou,
+                                        float* ov) {
+    f3 p[3];
+    tri_fetch(s.tris, tri, p);
+    const f3 e1 = sub(p[1], p[0]), e2 = sub(p[2], p[0]);
+    const f3 pv = cross(d, e2);
+    const float det = dot(e1, pv);
+    const float inv = 1.0f / det;
+    const f3 sv = sub(o, p[0]);
+    const float u = dot(sv, pv) * inv;
+    const f3 q = cross(sv, e1);
+    const float v = dot(q, d) * inv;
+    const float t = dot(e2, q) * inv;
+    *ot = t; *ou = u; *ov = v;
+    return u >= 0.0f && v >= 0.0f && u + v <= 1.0f && t > kIsectEps && t < tbest;
+}
+
+// prims[b, e) tested in order by one lane; first-tested wins ties (strict <)
 template <bool ANY, bool STATS>
 __device__ __forceinline__ bool isect_range(const Scene& s, f3 o, f3 d, uint32_t b, uint32_t e, Hit& h) {
     for (uint32_t it = b; it < e; ++it) {
         const uint32_t tri = __ldg(s.prims + it);
-        f3 p[3];
-        tri_load(s.v, s.idx, tri, p);
-        const f3 e1 = sub(p[1], p[0]), e2 = sub(p[2], p[0]);
-        const f3 pv = cross(d, e2);
-        const float det = dot(e1, pv);
-        const float inv = 1.0f / det;
-        const f3 sv = sub(o, p[0]);
-        const float u = dot(sv, pv) * inv;
-        const f3 q = cross(sv, e1);
-        const float v = dot(q, d) * inv;
-        const float t = dot(e2, q) * inv;
+        float t, u, v;
         if (STATS) h.tests++;
-        if (u >= 0.0f && v >= 0.0f && u + v <= 1.0f && t > kIsectEps && t < h.t) {
+        if (mt_test(s, tri, o, d, h.t, &t, &u, &v)) {
             h.t = t; h.u = u; h.v = v; h.tri = tri; h.hit = true;
             if (ANY) return true;
         }
@@ -80,7 +98,86 @@ __device__ __forceinline__ bool isect_range(const Scene& s, f3 o, f3 d, uint32_t
     return false;
 }
 
+__device__ __forceinline__ float shfl(float x, int src) { return __shfl_sync(kFullMask, x, src); }
+__device__ __forceinline__ uint32_t shfl(uint32_t x, int src) { return __shfl_sync(kFullMask, x, src); }
+
+// Warp-wide test of every lane's list prims[b, e).  Must be called by all 32 lanes.
+// Returns true on the lanes whose any-hit query is answered (ANY) by this test.
+template <bool ANY, bool STATS>
+__device__ __forceinline__ bool test_lists(const Scene& s, f3 o, f3 d, uint32_t b, uint32_t e, Hit& h) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t n = e - b;
+    const bool coop = n > kCoopMin;
+    bool done = false;
+    if (!coop && n) done = isect_range<ANY, STATS>(s, o, d, b, e, h);
+    uint32_t m = __ballot_sync(kFullMask, coop);
+    while (m) {
+        const int src = __ffs(m) - 1;
+        m &= m - 1;
+        const f3 so = mk(shfl(o.x, src), shfl(o.y, src), shfl(o.z, src));
+        const f3 sd = mk(shfl(d.x, src), shfl(d.y, src), shfl(d.z, src));
+        const uint32_t sb = shfl(b, src), se = shfl(e, src);
+        float bt = shfl(h.t, src), bu = 0.0f, bv = 0.0f;
+        uint32_t bit = 0xffffffffu;
+        uint32_t tested = 0;
+        for (uint32_t base = sb; base < se; base += 32u) {
+            const uint32_t it = base + lane;
+            if (it < se) {
+                float t, u, v;
+                if (mt_test(s, __ldg(s.prims + it), so, sd, bt, &t, &u, &v)) { bt = t; bu = u; bv = v; bit = it; }
+            }
+            tested += min(32u, se - base);
+            if (ANY && __any_sync(kFullMask, bit != 0xffffffffu)) break;
+        }
+        // (smallest t, smallest position) over the warp = the sequential first-tested-wins hit
+        float rt = bt;
+        uint32_t rit = bit;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            const float ot = __shfl_xor_sync(kFullMask, rt, off);
+            const uint32_t oit = __shfl_xor_sync(kFullMask, rit, off);
+            if (ot < rt || (ot == rt && oit < rit)) { rt = ot; rit = oit; }
+        }
+        const uint32_t own = __ballot_sync(kFullMask, bit == rit && rit != 0xffffffffu);
+        if (rit != 0xffffffffu) {
+            const int w = __ffs(own) - 1;
+            const float wu = shfl(bu, w), wv = shfl(bv, w);
+            if ((int)lane == src) {
+                h.t = rt; h.u = wu; h.v = wv; h.tri = __ldg(s.prims + rit); h.hit = true;
+                if (ANY) done = true;
+            }
+        }
+        if (STATS && (int)lane == src) h.tests += tested;
+    }
+    return done;
+}
+
 __device__ __forceinline__ int min_dim(float a, float b, float c) { return a < b ? (a < c ? 0 : 2) : (b < c ? 1 : 2); }
+
+// One DDA step along the axis of the smallest tmax.  The state arrays are only indexed
+// with constants (one branch per axis, as TLGridTraverser.h:226-290 writes it out), so
+// they stay in registers.  Returns tmax of the axis before the step in *t_before and
+// whether the new cell index is inside [0, res).
+__device__ __forceinline__ bool dda_step(float* tmax, int32_t* cell, const float* rcp, const float* cs,
+                                         const int32_t* res, float* t_before) {
+    const int k = min_dim(tmax[0], tmax[1], tmax[2]);
+    if (k == 0) {
+        *t_before = tmax[0];
+        cell[0] += rcp[0] > 0.0f ? 1 : -1;
+        tmax[0] += cs[0] * fabsf(rcp[0]);
+        return cell[0] < res[0] && cell[0] > -1;
+    } else if (k == 1) {
+        *t_before = tmax[1];
+        cell[1] += rcp[1] > 0.0f ? 1 : -1;
+        tmax[1] += cs[1] * fabsf(rcp[1]);
+        return cell[1] < res[1] && cell[1] > -1;
+    } else {
+        *t_before = tmax[2];
+        cell[2] += rcp[2] > 0.0f ? 1 : -1;
+        tmax[2] += cs[2] * fabsf(rcp[2]);
+        return cell[2] < res[2] && cell[2] > -1;
+    }
+}
 
 __device__ __forceinline__ bool clip(const G& g, f3 o, const float* rcp, float* t0, float* t1) {
     float tn[3], tf[3];
@@ -95,115 +192,166 @@ __device__ __forceinline__ bool clip(const G& g, f3 o, const float* rcp, float* 
     return *t1 > *t0 && *t1 >= 0.0f;
 }
 
-// a14: uniform grid DDA (UGridTraverser.h:76-172)
+// a14: uniform grid DDA (UGridTraverser.h:76-172), warp-synchronous
 template <bool ANY, bool STATS>
-__device__ void trace_ug(const Scene& s, const G& g, f3 o, f3 d, Hit& h) {
-    float rcp[3] = {1.0f / d.x, 1.0f / d.y, 1.0f / d.z};
-    float t0, t1;
-    if (!clip(g, o, rcp, &t0, &t1)) return;
-    f3 ep = o;
-    if (t0 >= 0.0f) {
-        const float te = t0 + kEps;
-        ep = mk(o.x + te * d.x, o.y + te * d.y, o.z + te * d.z);
-    }
-    float tmax[3];
-    int32_t cell[3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        float cf = floorf((comp(ep, k) - g.bmin[k]) * g.rcp[k]);
-        cf = hmin((float)g.res[k] - 1.0f, hmax(cf, 0.0f));
-        const float stp = rcp[k] > 0.0f ? 1.0f : 0.0f;
-        tmax[k] = ((cf + stp) * g.cs[k] + g.bmin[k] - comp(o, k)) * rcp[k];
-        cell[k] = f2i(cf);
-    }
-    bool active = cell[0] < g.res[0] && cell[0] > -1 && cell[1] < g.res[1] && cell[1] > -1 &&
-                  cell[2] < g.res[2] && cell[2] > -1;
-    const uint32_t rx = (uint32_t)g.res[0], rxy = (uint32_t)g.res[0] * (uint32_t)g.res[1];
-    while (active) {
-        const uint32_t c = (uint32_t)cell[0] + (uint32_t)cell[1] * rx + (uint32_t)cell[2] * rxy;
-        const uint2 cr = __ldg(s.cells + c);
-        if (STATS) h.cells++;
-        if (isect_range<ANY, STATS>(s, o, d, cr.x, cr.y, h)) return;
-        const int k = min_dim(tmax[0], tmax[1], tmax[2]);
-        active = h.t > tmax[k];
-        cell[k] += rcp[k] > 0.0f ? 1 : -1;
-        tmax[k] += g.cs[k] * fabsf(rcp[k]);
-        active = active && cell[k] < g.res[k] && cell[k] > -1;
-    }
-}
-
-// a15: two-level DDA (TLGridTraverser.h:79-349)
-template <bool ANY, bool STATS>
-__device__ void trace_tl(const Scene& s, const G& g, f3 o, f3 d, Hit& h) {
-    float rcp[3] = {1.0f / d.x, 1.0f / d.y, 1.0f / d.z};
-    float t0, t1;
-    if (!clip(g, o, rcp, &t0, &t1)) return;
-    float tentry = hmax(0.0f, t0);
-    const f3 ep = mk(o.x + tentry * d.x, o.y + tentry * d.y, o.z + tentry * d.z);
-    float tmax[3];
-    int32_t cell[3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        float cf = floorf((comp(ep, k) - g.bmin[k]) * g.rcp[k]);
-        cf = hmin((float)g.res[k] - 1.0f, hmax(cf, 0.0f));
-        const float stp = rcp[k] > 0.0f ? 1.0f : 0.0f;
-        tmax[k] = ((cf + stp) * g.cs[k] + g.bmin[k] - comp(o, k)) * rcp[k];
-        cell[k] = f2i(cf);
-    }
-    bool active = cell[0] < g.res[0] && cell[0] > -1 && cell[1] < g.res[1] && cell[1] > -1 &&
-                  cell[2] < g.res[2] && cell[2] > -1;
-    const uint32_t rx = (uint32_t)g.res[0], rxy = (uint32_t)g.res[0] * (uint32_t)g.res[1];
-    while (active) {
-        const uint32_t c = (uint32_t)cell[0] + (uint32_t)cell[1] * rx + (uint32_t)cell[2] * rxy;
-        const uint2 tc = __ldg(s.cells + c);
-        if (STATS) h.cells++;
-        if (tc.y & kNotEmptyMask) {
-            const uint32_t lres[3] = {tc.y & 0xFFu, (tc.y >> 8) & 0xFFu, (tc.y >> 16) & 0xFFu};
-            const f3 e2 = mk(o.x + tentry * d.x, o.y + tentry * d.y, o.z + tentry * d.z);
-            float scs[3], tm2[3];
-            int32_t c2[3];
+__device__ void trace_ug(const Scene& s, const G& g, f3 o, f3 d, Hit& h, bool active) {
+    float rcp[3] = {0.0f, 0.0f, 0.0f}, tmax[3] = {0.0f, 0.0f, 0.0f};
+    int32_t cell[3] = {0, 0, 0};
+    if (active) {
+        rcp[0] = 1.0f / d.x; rcp[1] = 1.0f / d.y; rcp[2] = 1.0f / d.z;
+        float t0, t1;
+        active = clip(g, o, rcp, &t0, &t1);
+        if (active) {
+            f3 ep = o;
+            if (t0 >= 0.0f) {
+                const float te = t0 + kEps;
+                ep = mk(o.x + te * d.x, o.y + te * d.y, o.z + te * d.z);
+            }
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
-                const float cres = (float)lres[k];
-                const float srcp = g.rcp[k] * cres;
-                const float mb = (float)cell[k] * g.cs[k] + g.bmin[k];
-                float cf = floorf((comp(e2, k) - mb) * srcp);
-                scs[k] = 1.0f / srcp;
-                cf = hmin(cres - 1.0f, hmax(cf, 0.0f));
+                float cf = floorf((comp(ep, k) - g.bmin[k]) * g.rcp[k]);
+                cf = hmin((float)g.res[k] - 1.0f, hmax(cf, 0.0f));
                 const float stp = rcp[k] > 0.0f ? 1.0f : 0.0f;
-                tm2[k] = ((cf + stp) * scs[k] + mb - comp(o, k)) * rcp[k];
-                c2[k] = f2i(cf);
+                tmax[k] = ((cf + stp) * g.cs[k] + g.bmin[k] - comp(o, k)) * rcp[k];
+                cell[k] = f2i(cf);
             }
-            bool inner = true;
-            while (inner) {
-                const uint32_t li = tc.x + (uint32_t)c2[0] + lres[0] * (uint32_t)c2[1] + lres[0] * lres[1] * (uint32_t)c2[2];
-                const uint2 lr = __ldg(s.leaves + li);
-                if (STATS) h.cells++;
-                if (isect_range<ANY, STATS>(s, o, d, lr.x, lr.y, h)) return;
-                const int k = min_dim(tm2[0], tm2[1], tm2[2]);
-                if (h.t < tm2[k]) { inner = false; active = false; }
-                c2[k] += rcp[k] > 0.0f ? 1 : -1;
-                tm2[k] += scs[k] * fabsf(rcp[k]);
-                inner = inner && c2[k] != (int32_t)lres[k] && c2[k] != -1;
-            }
+            active = cell[0] < g.res[0] && cell[0] > -1 && cell[1] < g.res[1] && cell[1] > -1 &&
+                     cell[2] < g.res[2] && cell[2] > -1;
         }
+    }
+    const uint32_t rx = (uint32_t)g.res[0], rxy = (uint32_t)g.res[0] * (uint32_t)g.res[1];
+    while (__any_sync(kFullMask, active)) {
+        uint32_t b = 0, e = 0;
         if (active) {
-            const int k = min_dim(tmax[0], tmax[1], tmax[2]);
-            active = h.t > tmax[k];
-            tentry = tmax[k];
-            cell[k] += rcp[k] > 0.0f ? 1 : -1;
-            tmax[k] += g.cs[k] * fabsf(rcp[k]);
-            active = active && cell[k] != g.res[k] && cell[k] != -1;
+            const uint2 cr = __ldg(s.cells + ((uint32_t)cell[0] + (uint32_t)cell[1] * rx + (uint32_t)cell[2] * rxy));
+            b = cr.x; e = cr.y;
+            if (STATS) h.cells++;
+        }
+        const bool done = test_lists<ANY, STATS>(s, o, d, b, e, h);
+        if (active) {
+            if (done) {
+                active = false;
+            } else {
+                float tk;
+                const bool inside = dda_step(tmax, cell, rcp, g.cs, g.res, &tk);
+                active = h.t > tk && inside;
+            }
         }
     }
 }
 
+// Two-level DDA state of one lane (TLGridTraverser.h:79-349).
+struct TL {
+    float rcp[3], tmax[3], tentry;
+    int32_t cell[3];
+    uint32_t lbase, lres[3];   // current top cell: first leaf, sub-grid resolution
+    float scs[3], tm2[3];
+    int32_t c2[3];
+};
+
+// Enter the sub-grid of the current top cell at tentry (TLGridTraverser.h:145-197).
+__device__ __forceinline__ void tl_enter(TL& q, const G& g, f3 o, f3 d, uint2 tc) {
+    q.lbase = tc.x;
+    q.lres[0] = tc.y & 0xFFu; q.lres[1] = (tc.y >> 8) & 0xFFu; q.lres[2] = (tc.y >> 16) & 0xFFu;
+    const f3 e2 = mk(o.x + q.tentry * d.x, o.y + q.tentry * d.y, o.z + q.tentry * d.z);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float cres = (float)q.lres[k];
+        const float srcp = g.rcp[k] * cres;
+        const float mb = (float)q.cell[k] * g.cs[k] + g.bmin[k];
+        float cf = floorf((comp(e2, k) - mb) * srcp);
+        q.scs[k] = 1.0f / srcp;
+        cf = hmin(cres - 1.0f, hmax(cf, 0.0f));
+        const float stp = q.rcp[k] > 0.0f ? 1.0f : 0.0f;
+        q.tm2[k] = ((cf + stp) * q.scs[k] + mb - comp(o, k)) * q.rcp[k];
+        q.c2[k] = f2i(cf);
+    }
+}
+
+// Outer step (TLGridTraverser.h:296-348): returns false when the ray is done.
+__device__ __forceinline__ bool tl_outer_step(TL& q, const G& g, const Hit& h) {
+    float tk;
+    const bool inside = dda_step(q.tmax, q.cell, q.rcp, g.cs, g.res, &tk);
+    q.tentry = tk;
+    return h.t > tk && inside;
+}
+
+// From the current top cell, walk to the first non-empty one and enter it; false if the
+// ray leaves the grid (or is done) first.
+template <bool STATS>
+__device__ __forceinline__ bool tl_seek(TL& q, const Scene& s, const G& g, f3 o, f3 d, Hit& h) {
+    const uint32_t rx = (uint32_t)g.res[0], rxy = (uint32_t)g.res[0] * (uint32_t)g.res[1];
+    while (true) {
+        const uint2 tc = __ldg(s.cells + ((uint32_t)q.cell[0] + (uint32_t)q.cell[1] * rx + (uint32_t)q.cell[2] * rxy));
+        if (STATS) h.cells++;
+        if (tc.y & kNotEmptyMask) {
+            tl_enter(q, g, o, d, tc);
+            return true;
+        }
+        if (!tl_outer_step(q, g, h)) return false;
+    }
+}
+
+// a15: two-level DDA, warp-synchronous
 template <bool ANY, bool STATS>
-__device__ __forceinline__ void trace_one(const Scene& s, const G& g, f3 o, f3 d, float tmax, Hit& h) {
+__device__ void trace_tl(const Scene& s, const G& g, f3 o, f3 d, Hit& h, bool active) {
+    TL q;
+    if (active) {
+        q.rcp[0] = 1.0f / d.x; q.rcp[1] = 1.0f / d.y; q.rcp[2] = 1.0f / d.z;
+        float t0, t1;
+        active = clip(g, o, q.rcp, &t0, &t1);
+        if (active) {
+            q.tentry = hmax(0.0f, t0);
+            const f3 ep = mk(o.x + q.tentry * d.x, o.y + q.tentry * d.y, o.z + q.tentry * d.z);
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                float cf = floorf((comp(ep, k) - g.bmin[k]) * g.rcp[k]);
+                cf = hmin((float)g.res[k] - 1.0f, hmax(cf, 0.0f));
+                const float stp = q.rcp[k] > 0.0f ? 1.0f : 0.0f;
+                q.tmax[k] = ((cf + stp) * g.cs[k] + g.bmin[k] - comp(o, k)) * q.rcp[k];
+                q.cell[k] = f2i(cf);
+            }
+            active = q.cell[0] < g.res[0] && q.cell[0] > -1 && q.cell[1] < g.res[1] && q.cell[1] > -1 &&
+                     q.cell[2] < g.res[2] && q.cell[2] > -1;
+            if (active) active = tl_seek<STATS>(q, s, g, o, d, h);
+        }
+    }
+    while (__any_sync(kFullMask, active)) {
+        uint32_t b = 0, e = 0;
+        if (active) {
+            const uint2 lr = __ldg(s.leaves + (q.lbase + (uint32_t)q.c2[0] + q.lres[0] * (uint32_t)q.c2[1] +
+                                               q.lres[0] * q.lres[1] * (uint32_t)q.c2[2]));
+            b = lr.x; e = lr.y;
+            if (STATS) h.cells++;
+        }
+        const bool done = test_lists<ANY, STATS>(s, o, d, b, e, h);
+        if (active) {
+            if (done) {
+                active = false;
+            } else {
+                // inner step (TLGridTraverser.h:225-290): stop when the hit lies before the
+                // leaf's exit, else step; leaving the sub-grid continues in the top grid
+                const int32_t lres[3] = {(int32_t)q.lres[0], (int32_t)q.lres[1], (int32_t)q.lres[2]};
+                float tk;
+                const bool inside = dda_step(q.tm2, q.c2, q.rcp, q.scs, lres, &tk);
+                if (h.t < tk) {
+                    active = false;
+                } else if (!inside) {
+                    active = tl_outer_step(q, g, h);
+                    if (active) active = tl_seek<STATS>(q, s, g, o, d, h);
+                }
+            }
+        }
+    }
+}
+
+// Closest hit (ANY = false) or any hit within (1e-4, tmax).  Warp-synchronous.
+template <bool ANY, bool STATS>
+__device__ __forceinline__ void trace_one(const Scene& s, const G& g, f3 o, f3 d, float tmax, Hit& h, bool active) {
     h.t = tmax; h.u = 0.0f; h.v = 0.0f; h.tri = 0; h.hit = false; h.cells = 0; h.tests = 0;
     if (s.ntri == 0) return;
-    if (s.kind == kUniform) trace_ug<ANY, STATS>(s, g, o, d, h);
-    else trace_tl<ANY, STATS>(s, g, o, d, h);
+    if (s.kind == kUniform) trace_ug<ANY, STATS>(s, g, o, d, h, active);
+    else trace_tl<ANY, STATS>(s, g, o, d, h, active);
 }
 
 struct Cam {
@@ -224,7 +372,7 @@ __device__ __forceinline__ f3 primary_dir(const Cam& c, uint32_t pix) {
 
 __device__ __forceinline__ f3 face_normal(const Scene& s, uint32_t tri, f3 d) {
     f3 p[3];
-    tri_load(s.v, s.idx, tri, p);
+    tri_fetch(s.tris, tri, p);
     f3 n = normalize(cross(sub(p[1], p[0]), sub(p[2], p[0])));
     if (dot(n, d) > 0.0f) n = mk(-n.x, -n.y, -n.z);
     return n;
@@ -238,58 +386,24 @@ __device__ __forceinline__ float blend(float old, float val, int32_t image_id) {
 
 constexpr int kTT = 128;
 
-template <bool STATS>
-__global__ __launch_bounds__(kTT) void k_trace_rays(Scene s, const float* __restrict__ org, const float* __restrict__ dir,
-                                                    uint32_t n, int32_t* __restrict__ oid, float* __restrict__ ot,
-                                                    float* __restrict__ ou, float* __restrict__ ov,
-                                                    uint32_t* __restrict__ stats) {
-    const G g = load_g(s.desc);
-    for (uint32_t i = blockIdx.x * kTT + threadIdx.x; i < n; i += gridDim.x * kTT) {
-        const f3 o = mk(__ldg(org + 3 * (size_t)i), __ldg(org + 3 * (size_t)i + 1), __ldg(org + 3 * (size_t)i + 2));
-        const f3 d = mk(__ldg(dir + 3 * (size_t)i), __ldg(dir + 3 * (size_t)i + 1), __ldg(dir + 3 * (size_t)i + 2));
-        Hit h;
-        trace_one<false, STATS>(s, g, o, d, FLT_MAX, h);
-        oid[i] = h.hit ? (int32_t)h.tri : -1;
-        ot[i] = h.hit ? h.t : FLT_MAX;
-        ou[i] = h.u;
-        ov[i] = h.v;
-        if (STATS) { stats[2 * (size_t)i] = h.cells; stats[2 * (size_t)i + 1] = h.tests; }
-    }
+// Camera rays are issued in warp-sized 8x4 pixel tiles: the 32 rays of a warp start from
+// the same point into a small solid angle and walk nearly the same cells.
+__device__ __forceinline__ uint32_t tile_slots(const Cam& c) {
+    return (((uint32_t)c.w + 7u) / 8u) * (((uint32_t)c.h + 3u) / 4u) * 32u;
+}
+__device__ __forceinline__ bool tile_pixel(const Cam& c, uint32_t slot, uint32_t* pix) {
+    const uint32_t tile = slot >> 5, lane = slot & 31u;
+    const uint32_t tx = ((uint32_t)c.w + 7u) / 8u;
+    const uint32_t x = (tile % tx) * 8u + (lane & 7u), y = (tile / tx) * 4u + (lane >> 3);
+    *pix = y * (uint32_t)c.w + x;
+    return x < (uint32_t)c.w && y < (uint32_t)c.h;
 }
 
+// Device counters (uint64 words): [0] rays, [2] cells, [3] triangle tests of the primary
+// pass; [4] rays, [5] cells, [6] tests of the secondary pass (AO samples, shadow rays);
+// word 1 holds the index check of the last upload, word 7 the AO hit-pixel queue length.
 template <bool STATS>
-__global__ __launch_bounds__(kTT) void k_trace_primary(Scene s, Cam cam, int32_t* __restrict__ oid,
-                                                       float* __restrict__ ot, float* __restrict__ ou,
-                                                       float* __restrict__ ov, uint32_t* __restrict__ stats) {
-    const G g = load_g(s.desc);
-    const uint32_t n = (uint32_t)cam.w * (uint32_t)cam.h;
-    const f3 o = mk(cam.pos[0], cam.pos[1], cam.pos[2]);
-    for (uint32_t i = blockIdx.x * kTT + threadIdx.x; i < n; i += gridDim.x * kTT) {
-        Hit h;
-        trace_one<false, STATS>(s, g, o, primary_dir(cam, i), FLT_MAX, h);
-        oid[i] = h.hit ? (int32_t)h.tri : -1;
-        ot[i] = h.hit ? h.t : FLT_MAX;
-        ou[i] = h.u;
-        ov[i] = h.v;
-        if (STATS) { stats[2 * (size_t)i] = h.cells; stats[2 * (size_t)i + 1] = h.tests; }
-    }
-}
-
-__global__ __launch_bounds__(kTT) void k_occluded(Scene s, const float* __restrict__ org, const float* __restrict__ dir,
-                                                  const float* __restrict__ tmax, uint32_t n, uint8_t* __restrict__ occ) {
-    const G g = load_g(s.desc);
-    for (uint32_t i = blockIdx.x * kTT + threadIdx.x; i < n; i += gridDim.x * kTT) {
-        const f3 o = mk(org[3 * (size_t)i], org[3 * (size_t)i + 1], org[3 * (size_t)i + 2]);
-        const f3 d = mk(dir[3 * (size_t)i], dir[3 * (size_t)i + 1], dir[3 * (size_t)i + 2]);
-        Hit h;
-        trace_one<true, false>(s, g, o, d, tmax[i], h);
-        occ[i] = h.hit ? 1 : 0;
-    }
-}
-
-// warp-aggregated counters: [0] rays traced, [2] cells visited, [3] triangle tests
-template <bool STATS>
-__device__ __forceinline__ void add_rays(unsigned long long* counter, uint32_t rays, uint32_t cells = 0,
+__device__ __forceinline__ void add_rays(unsigned long long* counter, bool secondary, uint32_t rays, uint32_t cells = 0,
                                          uint32_t tests = 0) {
     unsigned long long r = rays, c = cells, t = tests;
     for (int o = 16; o > 0; o >>= 1) {
@@ -300,11 +414,82 @@ __device__ __forceinline__ void add_rays(unsigned long long* counter, uint32_t r
         }
     }
     if ((threadIdx.x & 31) == 0 && counter) {
-        atomicAdd(counter, r);
+        unsigned long long* base = counter + (secondary ? 4 : 0);
+        if (r) atomicAdd(base, r);
         if (STATS) {
-            atomicAdd(counter + 2, c);
-            atomicAdd(counter + 3, t);
+            atomicAdd(secondary ? counter + 5 : counter + 2, c);
+            atomicAdd(secondary ? counter + 6 : counter + 3, t);
         }
+    }
+}
+
+// warp-uniform bound of a 1-D grid-stride loop over n items
+__device__ __forceinline__ uint32_t round32(uint32_t n) { return (n + 31u) & ~31u; }
+
+template <bool STATS>
+__global__ __launch_bounds__(kTT) void k_trace_rays(Scene s, const float* __restrict__ org, const float* __restrict__ dir,
+                                                    uint32_t n, int32_t* __restrict__ oid, float* __restrict__ ot,
+                                                    float* __restrict__ ou, float* __restrict__ ov,
+                                                    uint32_t* __restrict__ stats) {
+    const G g = load_g(s.desc);
+    const uint32_t nl = round32(n);
+    for (uint32_t i = blockIdx.x * kTT + threadIdx.x; i < nl; i += gridDim.x * kTT) {
+        const bool valid = i < n;
+        f3 o = mk(0.0f, 0.0f, 0.0f), d = mk(1.0f, 0.0f, 0.0f);
+        if (valid) {
+            o = mk(__ldg(org + 3 * (size_t)i), __ldg(org + 3 * (size_t)i + 1), __ldg(org + 3 * (size_t)i + 2));
+            d = mk(__ldg(dir + 3 * (size_t)i), __ldg(dir + 3 * (size_t)i + 1), __ldg(dir + 3 * (size_t)i + 2));
+        }
+        Hit h;
+        trace_one<false, STATS>(s, g, o, d, FLT_MAX, h, valid);
+        if (valid) {
+            oid[i] = h.hit ? (int32_t)h.tri : -1;
+            ot[i] = h.hit ? h.t : FLT_MAX;
+            ou[i] = h.u;
+            ov[i] = h.v;
+            if (STATS) { stats[2 * (size_t)i] = h.cells; stats[2 * (size_t)i + 1] = h.tests; }
+        }
+    }
+}
+
+template <bool STATS>
+__global__ __launch_bounds__(kTT) void k_trace_primary(Scene s, Cam cam, int32_t* __restrict__ oid,
+                                                       float* __restrict__ ot, float* __restrict__ ou,
+                                                       float* __restrict__ ov, uint32_t* __restrict__ stats) {
+    const G g = load_g(s.desc);
+    const uint32_t slots = tile_slots(cam);
+    const f3 o = mk(cam.pos[0], cam.pos[1], cam.pos[2]);
+    for (uint32_t slot = blockIdx.x * kTT + threadIdx.x; slot < slots; slot += gridDim.x * kTT) {
+        uint32_t i;
+        const bool valid = tile_pixel(cam, slot, &i);
+        Hit h;
+        trace_one<false, STATS>(s, g, o, valid ? primary_dir(cam, i) : mk(1.0f, 0.0f, 0.0f), FLT_MAX, h, valid);
+        if (valid) {
+            oid[i] = h.hit ? (int32_t)h.tri : -1;
+            ot[i] = h.hit ? h.t : FLT_MAX;
+            ou[i] = h.u;
+            ov[i] = h.v;
+            if (STATS) { stats[2 * (size_t)i] = h.cells; stats[2 * (size_t)i + 1] = h.tests; }
+        }
+    }
+}
+
+__global__ __launch_bounds__(kTT) void k_occluded(Scene s, const float* __restrict__ org, const float* __restrict__ dir,
+                                                  const float* __restrict__ tmax, uint32_t n, uint8_t* __restrict__ occ) {
+    const G g = load_g(s.desc);
+    const uint32_t nl = round32(n);
+    for (uint32_t i = blockIdx.x * kTT + threadIdx.x; i < nl; i += gridDim.x * kTT) {
+        const bool valid = i < n;
+        f3 o = mk(0.0f, 0.0f, 0.0f), d = mk(1.0f, 0.0f, 0.0f);
+        float tm = 0.0f;
+        if (valid) {
+            o = mk(org[3 * (size_t)i], org[3 * (size_t)i + 1], org[3 * (size_t)i + 2]);
+            d = mk(dir[3 * (size_t)i], dir[3 * (size_t)i + 1], dir[3 * (size_t)i + 2]);
+            tm = tmax[i];
+        }
+        Hit h;
+        trace_one<true, false>(s, g, o, d, tm, h, valid);
+        if (valid) occ[i] = h.hit ? 1 : 0;
     }
 }
 
@@ -313,18 +498,15 @@ template <bool STATS>
 __global__ __launch_bounds__(kTT) void k_render_primary(Scene s, Cam cam, int32_t image_id, float* __restrict__ fb,
                                                         unsigned long long* counter) {
     const G g = load_g(s.desc);
-    const uint32_t n = (uint32_t)cam.w * (uint32_t)cam.h;
+    const uint32_t slots = tile_slots(cam);
     const f3 o = mk(cam.pos[0], cam.pos[1], cam.pos[2]);
-    const uint32_t nn = (n + kTT - 1) / kTT * kTT;
-    for (uint32_t i = blockIdx.x * kTT + threadIdx.x; i < nn; i += gridDim.x * kTT) {
-        uint32_t rays = 0, ncell = 0, ntest = 0;
-        if (i < n) {
-            const f3 d = primary_dir(cam, i);
-            Hit h;
-            trace_one<false, STATS>(s, g, o, d, FLT_MAX, h);
-            rays = 1;
-            ncell = h.cells;
-            ntest = h.tests;
+    for (uint32_t slot = blockIdx.x * kTT + threadIdx.x; slot < slots; slot += gridDim.x * kTT) {
+        uint32_t i;
+        const bool valid = tile_pixel(cam, slot, &i);
+        const f3 d = valid ? primary_dir(cam, i) : mk(1.0f, 0.0f, 0.0f);
+        Hit h;
+        trace_one<false, STATS>(s, g, o, d, FLT_MAX, h, valid);
+        if (valid) {
             float r = 0.15f, gg = 0.2f, b = 0.3f;
             if (h.hit) {
                 const f3 nrm = face_normal(s, h.tri, d);
@@ -335,16 +517,62 @@ __global__ __launch_bounds__(kTT) void k_render_primary(Scene s, Cam cam, int32_
             fb[3 * (size_t)i + 1] = blend(fb[3 * (size_t)i + 1], gg, image_id);
             fb[3 * (size_t)i + 2] = blend(fb[3 * (size_t)i + 2], b, image_id);
         }
-        add_rays<STATS>(counter, rays, ncell, ntest);
+        add_rays<STATS>(counter, false, valid ? 1u : 0u, h.cells, h.tests);
     }
 }
 
-// mode 3: ambient occlusion (AOIntegrator.h:234-351, RayGenerators.h:286-342), with the
-// configured sample count, radius alpha and a PCG32 stream per (image, pixel, seed)
+// mode 3, ambient occlusion (AOIntegrator.h:234-351: primary trace, AO rays, shading), as
+// a wavefront of three kernels:
+//   k_ao_primary  camera rays in pixel tiles; misses are shaded at once, hit pixels are
+//                 appended (warp-aggregated) to a queue with their t and triangle;
+//   k_ao_samples  one thread per (hit pixel, sample): AO ray generation as
+//                 RayGenerators.h:286-342 with the configured radius and PCG32 stream of
+//                 the pixel (sample k uses draws 2k and 2k+1), any-hit traversal, and the
+//                 unoccluded count of the pixel (match_any-aggregated atomics);
+//   k_ao_finish   visibility = unoccluded / samples, progressive blend (AOIntegrator.h:168-175).
 template <bool STATS>
-__global__ __launch_bounds__(kTT) void k_render_ao(Scene s, Cam cam, int32_t spp, float alpha_frac, float alpha_abs,
-                                                   uint64_t seed, int32_t image_id, float* __restrict__ fb,
-                                                   unsigned long long* counter) {
+__global__ __launch_bounds__(kTT) void k_ao_primary(Scene s, Cam cam, int32_t image_id, float* __restrict__ fb,
+                                                    float* __restrict__ hit_t, uint32_t* __restrict__ hit_tri,
+                                                    uint32_t* __restrict__ unocc, uint32_t* __restrict__ queue,
+                                                    uint32_t* qcount, unsigned long long* counter) {
+    const G g = load_g(s.desc);
+    const uint32_t slots = tile_slots(cam);
+    const f3 o = mk(cam.pos[0], cam.pos[1], cam.pos[2]);
+    const uint32_t lane = threadIdx.x & 31u, lt = (1u << lane) - 1u;
+    for (uint32_t slot = blockIdx.x * kTT + threadIdx.x; slot < slots; slot += gridDim.x * kTT) {
+        uint32_t pix;
+        const bool valid = tile_pixel(cam, slot, &pix);
+        Hit h;
+        trace_one<false, STATS>(s, g, o, valid ? primary_dir(cam, pix) : mk(1.0f, 0.0f, 0.0f), FLT_MAX, h, valid);
+        const bool hit = valid && h.hit;
+        if (hit) {
+            hit_t[pix] = h.t;
+            hit_tri[pix] = h.tri;
+            unocc[pix] = 0u;
+        } else if (valid) {
+            const float val = blend(fb[3 * (size_t)pix], 1.0f, image_id);
+            fb[3 * (size_t)pix] = val;
+            fb[3 * (size_t)pix + 1] = val;
+            fb[3 * (size_t)pix + 2] = val;
+        }
+        const uint32_t m = __ballot_sync(kFullMask, hit);
+        if (m) {
+            const int leader = __ffs(m) - 1;
+            uint32_t base = 0;
+            if ((int)lane == leader) base = atomicAdd(qcount, (uint32_t)__popc(m));
+            base = __shfl_sync(kFullMask, base, leader);
+            if (hit) queue[base + __popc(m & lt)] = pix;
+        }
+        add_rays<STATS>(counter, false, valid ? 1u : 0u, h.cells, h.tests);
+    }
+}
+
+template <bool STATS>
+__global__ __launch_bounds__(kTT) void k_ao_samples(Scene s, Cam cam, int32_t spp, float alpha_frac, float alpha_abs,
+                                                    uint64_t seed, int32_t image_id, const float* __restrict__ hit_t,
+                                                    const uint32_t* __restrict__ hit_tri,
+                                                    const uint32_t* __restrict__ queue, const uint32_t* qcount,
+                                                    uint32_t* __restrict__ unocc, unsigned long long* counter) {
     const G g = load_g(s.desc);
     float alpha = alpha_abs;
     if (!(alpha > 0.0f)) {
@@ -352,44 +580,47 @@ __global__ __launch_bounds__(kTT) void k_render_ao(Scene s, Cam cam, int32_t spp
         alpha = alpha_frac * sqrtf(dot(dd, dd));
     }
     const float off = 0.01f * alpha;
-    const uint32_t n = (uint32_t)cam.w * (uint32_t)cam.h;
     const f3 o = mk(cam.pos[0], cam.pos[1], cam.pos[2]);
-    const uint32_t nn = (n + kTT - 1) / kTT * kTT;
-    for (uint32_t pix = blockIdx.x * kTT + threadIdx.x; pix < nn; pix += gridDim.x * kTT) {
-        uint32_t rays = 0, ncell = 0, ntest = 0;
-        if (pix < n) {
+    const uint32_t nitems = *qcount * (uint32_t)spp;
+    const uint32_t nloop = round32(nitems);
+    for (uint32_t item = blockIdx.x * kTT + threadIdx.x; item < nloop; item += gridDim.x * kTT) {
+        const bool valid = item < nitems;
+        uint32_t pix = 0xffffffffu;
+        f3 ao = mk(0.0f, 0.0f, 0.0f), w = mk(1.0f, 0.0f, 0.0f);
+        if (valid) {
+            const uint32_t q = item / (uint32_t)spp, k = item % (uint32_t)spp;
+            pix = queue[q];
             const f3 d = primary_dir(cam, pix);
-            Hit h;
-            trace_one<false, STATS>(s, g, o, d, FLT_MAX, h);
-            rays = 1;
-            ncell = h.cells;
-            ntest = h.tests;
-            float vis = 1.0f;
-            if (h.hit) {
-                const f3 p = mk(o.x + h.t * d.x, o.y + h.t * d.y, o.z + h.t * d.z);
-                const f3 nrm = face_normal(s, h.tri, d);
-                Pcg32 rng;
-                pcg_seed(rng, ((uint64_t)(uint32_t)image_id << 32) | pix, seed);
-                int32_t unocc = 0;
-                for (int32_t k = 0; k < spp; ++k) {
-                    const float u1 = pcg_float(rng), u2 = pcg_float(rng);
-                    const f3 w = cosine_dir(nrm, u1, u2);
-                    const f3 ao = mk(p.x + off * w.x, p.y + off * w.y, p.z + off * w.z);
-                    Hit hs;
-                    trace_one<true, STATS>(s, g, ao, w, alpha, hs);
-                    unocc += hs.hit ? 0 : 1;
-                    ncell += hs.cells;
-                    ntest += hs.tests;
-                }
-                rays += (uint32_t)spp;
-                vis = (float)unocc / (float)spp;
-            }
-            const float val = blend(fb[3 * (size_t)pix], vis, image_id);
-            fb[3 * (size_t)pix] = val;
-            fb[3 * (size_t)pix + 1] = val;
-            fb[3 * (size_t)pix + 2] = val;
+            const float t = hit_t[pix];
+            const f3 p = mk(o.x + t * d.x, o.y + t * d.y, o.z + t * d.z);
+            const f3 nrm = face_normal(s, hit_tri[pix], d);
+            Pcg32 rng;
+            pcg_seed(rng, ((uint64_t)(uint32_t)image_id << 32) | pix, seed);
+            for (uint32_t j = 0; j < 2u * k; ++j) pcg_next(rng);
+            const float u1 = pcg_float(rng), u2 = pcg_float(rng);
+            w = cosine_dir(nrm, u1, u2);
+            ao = mk(p.x + off * w.x, p.y + off * w.y, p.z + off * w.z);
         }
-        add_rays<STATS>(counter, rays, ncell, ntest);
+        Hit hs;
+        trace_one<true, STATS>(s, g, ao, w, alpha, hs, valid);
+        const bool free = valid && !hs.hit;
+        const uint32_t peers = __match_any_sync(kFullMask, pix);
+        const uint32_t nfree = __popc(__ballot_sync(kFullMask, free) & peers);
+        if (valid && nfree && (int)(threadIdx.x & 31u) == __ffs(peers) - 1) atomicAdd(unocc + pix, nfree);
+        add_rays<STATS>(counter, true, valid ? 1u : 0u, hs.cells, hs.tests);
+    }
+}
+
+__global__ void k_ao_finish(const uint32_t* __restrict__ queue, const uint32_t* qcount, const uint32_t* __restrict__ unocc,
+                            int32_t spp, int32_t image_id, float* __restrict__ fb) {
+    const uint32_t n = *qcount;
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        const uint32_t pix = queue[q];
+        const float vis = (float)unocc[pix] / (float)spp;
+        const float val = blend(fb[3 * (size_t)pix], vis, image_id);
+        fb[3 * (size_t)pix] = val;
+        fb[3 * (size_t)pix + 1] = val;
+        fb[3 * (size_t)pix + 2] = val;
     }
 }
 
@@ -398,7 +629,9 @@ struct LightP {
     float emission;
 };
 
-// mode 1/2: path tracing with next-event estimation (PathTracer.h:41-372 structure)
+// mode 1/2: path tracing with next-event estimation (PathTracer.h:41-372 structure).  The
+// bounce loop runs the same number of iterations on every lane (finished paths pass
+// active = false), so the warp-synchronous traversal can be called inside it.
 template <bool STATS>
 __global__ __launch_bounds__(kTT) void k_render_pt(Scene s, Cam cam, LightP l, int32_t bounces, float albedo,
                                                    float eps_frac, uint64_t seed, int32_t image_id,
@@ -410,19 +643,23 @@ __global__ __launch_bounds__(kTT) void k_render_pt(Scene s, Cam cam, LightP l, i
     const f3 lcr = cross(le1, le2);
     const float larea = sqrtf(dot(lcr, lcr));
     const float a_pi = albedo * 0.318309886f;
-    const uint32_t n = (uint32_t)cam.w * (uint32_t)cam.h;
-    const uint32_t nn = (n + kTT - 1) / kTT * kTT;
-    for (uint32_t pix = blockIdx.x * kTT + threadIdx.x; pix < nn; pix += gridDim.x * kTT) {
-        uint32_t rays = 0, ncell = 0, ntest = 0;
-        if (pix < n) {
-            Pcg32 rng;
-            pcg_seed(rng, ((uint64_t)(uint32_t)image_id << 32) | pix, seed);
-            f3 o = mk(cam.pos[0], cam.pos[1], cam.pos[2]);
-            f3 d = primary_dir(cam, pix);
-            float L = 0.0f, beta = 1.0f;
-            for (int32_t bounce = 0; bounce < bounces; ++bounce) {
-                Hit h;
-                trace_one<false, STATS>(s, g, o, d, FLT_MAX, h);
+    const uint32_t slots = tile_slots(cam);
+    for (uint32_t slot = blockIdx.x * kTT + threadIdx.x; slot < slots; slot += gridDim.x * kTT) {
+        uint32_t pix, rays = 0, ncell = 0, ntest = 0, srays = 0, scell = 0, stest = 0;
+        const bool valid = tile_pixel(cam, slot, &pix);
+        bool alive = valid;
+        Pcg32 rng;
+        pcg_seed(rng, ((uint64_t)(uint32_t)image_id << 32) | (valid ? pix : 0u), seed);
+        f3 o = mk(cam.pos[0], cam.pos[1], cam.pos[2]);
+        f3 d = valid ? primary_dir(cam, pix) : mk(1.0f, 0.0f, 0.0f);
+        float L = 0.0f, beta = 1.0f;
+        for (int32_t bounce = 0; bounce < bounces; ++bounce) {
+            Hit h;
+            trace_one<false, STATS>(s, g, o, d, FLT_MAX, h, alive);
+            bool shadow = false;
+            f3 p = mk(0.0f, 0.0f, 0.0f), nrm = mk(0.0f, 0.0f, 1.0f), wi = mk(0.0f, 0.0f, 1.0f), so = p;
+            float dist = 0.0f, dist2 = 1.0f, cos_s = 0.0f, cos_l = 0.0f;
+            if (alive) {
                 rays += 1;
                 ncell += h.cells;
                 ntest += h.tests;
@@ -432,27 +669,33 @@ __global__ __launch_bounds__(kTT) void k_render_pt(Scene s, Cam cam, LightP l, i
                     const float fx = (px - lc.x) / le1.x, fy = (py - lc.y) / le2.y;
                     if (tl > kIsectEps && tl < h.t && fx >= 0.0f && fx <= 1.0f && fy >= 0.0f && fy <= 1.0f) {
                         L = L + l.emission;
-                        break;
+                        alive = false;
                     }
                 }
-                if (!h.hit) break;
-                const f3 p = mk(o.x + h.t * d.x, o.y + h.t * d.y, o.z + h.t * d.z);
-                const f3 nrm = face_normal(s, h.tri, d);
-                const float u1 = pcg_float(rng), u2 = pcg_float(rng);
-                const f3 lp = mk(lc.x + u1 * le1.x + u2 * le2.x, lc.y + u1 * le1.y + u2 * le2.y,
-                                 lc.z + u1 * le1.z + u2 * le2.z);
-                f3 wi = sub(lp, p);
-                const float dist2 = dot(wi, wi);
-                const float dist = sqrtf(dist2);
-                wi = mulf(wi, 1.0f / dist);
-                const float cos_s = dot(nrm, wi), cos_l = wi.z;
-                if (cos_s > 0.0f && cos_l > 0.0f) {
-                    const f3 so = mk(p.x + ray_eps * wi.x, p.y + ray_eps * wi.y, p.z + ray_eps * wi.z);
-                    Hit hs;
-                    trace_one<true, STATS>(s, g, so, wi, dist - ray_eps, hs);
-                    rays += 1;
-                    ncell += hs.cells;
-                    ntest += hs.tests;
+                if (alive && !h.hit) alive = false;
+                if (alive) {
+                    p = mk(o.x + h.t * d.x, o.y + h.t * d.y, o.z + h.t * d.z);
+                    nrm = face_normal(s, h.tri, d);
+                    const float u1 = pcg_float(rng), u2 = pcg_float(rng);
+                    const f3 lp = mk(lc.x + u1 * le1.x + u2 * le2.x, lc.y + u1 * le1.y + u2 * le2.y,
+                                     lc.z + u1 * le1.z + u2 * le2.z);
+                    wi = sub(lp, p);
+                    dist2 = dot(wi, wi);
+                    dist = sqrtf(dist2);
+                    wi = mulf(wi, 1.0f / dist);
+                    cos_s = dot(nrm, wi);
+                    cos_l = wi.z;
+                    shadow = cos_s > 0.0f && cos_l > 0.0f;
+                    so = mk(p.x + ray_eps * wi.x, p.y + ray_eps * wi.y, p.z + ray_eps * wi.z);
+                }
+            }
+            Hit hs;
+            trace_one<true, STATS>(s, g, so, wi, dist - ray_eps, hs, shadow);
+            if (alive) {
+                if (shadow) {
+                    srays += 1;
+                    scell += hs.cells;
+                    stest += hs.tests;
                     if (!hs.hit) L = L + beta * a_pi * l.emission * cos_s * cos_l * larea / dist2;
                 }
                 beta = beta * albedo;
@@ -460,19 +703,21 @@ __global__ __launch_bounds__(kTT) void k_render_pt(Scene s, Cam cam, LightP l, i
                 d = cosine_dir(nrm, u3, u4);
                 o = mk(p.x + ray_eps * d.x, p.y + ray_eps * d.y, p.z + ray_eps * d.z);
             }
+        }
+        if (valid) {
             const float val = blend(fb[3 * (size_t)pix], L, image_id);
             fb[3 * (size_t)pix] = val;
             fb[3 * (size_t)pix + 1] = val;
             fb[3 * (size_t)pix + 2] = val;
         }
-        add_rays<STATS>(counter, rays, ncell, ntest);
+        add_rays<STATS>(counter, false, rays, ncell, ntest);
+        add_rays<STATS>(counter, true, srays, scell, stest);
     }
 }
 
 Scene make_scene(hr_ctx* c) {
     Scene s;
-    s.v = c->verts.as<float4>();
-    s.idx = c->idx.as<uint32_t>();
+    s.tris = c->tris.as<float4>();
     s.cells = c->g.cells.as<uint2>();
     s.leaves = c->g.leaves.as<uint2>();
     s.prims = c->g.prims.as<uint32_t>();
@@ -498,6 +743,10 @@ int grid_for(const hr_ctx* c, uint32_t n) {
     return (int)(b < 1 ? 1 : (b > cap ? cap : b));
 }
 
+uint32_t slots_for(const hr_ctx* c) {
+    return (((uint32_t)c->cam.w + 7u) / 8u) * (((uint32_t)c->cam.h + 3u) / 4u) * 32u;
+}
+
 }  // namespace
 
 int launch_trace_rays(hr_ctx* c, const float* org, const float* dir, uint32_t n, int32_t* id, float* t, float* u,
@@ -516,8 +765,9 @@ int launch_trace_primary(hr_ctx* c, int32_t* id, float* t, float* u, float* v, u
     const uint32_t n = (uint32_t)k.w * (uint32_t)k.h;
     if (n == 0) return 0;
     c->launches += 1;
-    if (stats) k_trace_primary<true><<<grid_for(c, n), kTT, 0, c->stream>>>(s, k, id, t, u, v, stats);
-    else k_trace_primary<false><<<grid_for(c, n), kTT, 0, c->stream>>>(s, k, id, t, u, v, nullptr);
+    const int gb = grid_for(c, slots_for(c));
+    if (stats) k_trace_primary<true><<<gb, kTT, 0, c->stream>>>(s, k, id, t, u, v, stats);
+    else k_trace_primary<false><<<gb, kTT, 0, c->stream>>>(s, k, id, t, u, v, nullptr);
     return cuda_check(c, cudaGetLastError(), "trace_primary launch");
 }
 
@@ -534,35 +784,70 @@ int launch_render(hr_ctx* c, int32_t mode, int32_t image_id, float* d_fb) {
     const uint32_t n = (uint32_t)k.w * (uint32_t)k.h;
     if (n == 0) return 0;
     unsigned long long* ctr = c->counters.as<unsigned long long>();
-    const int gb = grid_for(c, n);
-    c->launches += 1;
+    const int gb = grid_for(c, slots_for(c));
     const bool st = c->collect_stats;
+    cudaStream_t strm = c->stream;
+    auto mark = [&](int i) { if (c->timing && i < 8) cudaEventRecord(c->rev[i], strm); };
+    c->nrender_ev = 0;
     switch (mode) {
     case 0:
-        if (st) k_render_primary<true><<<gb, kTT, 0, c->stream>>>(s, k, image_id, d_fb, ctr);
-        else k_render_primary<false><<<gb, kTT, 0, c->stream>>>(s, k, image_id, d_fb, ctr);
+        c->launches += 1;
+        mark(0);
+        if (st) k_render_primary<true><<<gb, kTT, 0, strm>>>(s, k, image_id, d_fb, ctr);
+        else k_render_primary<false><<<gb, kTT, 0, strm>>>(s, k, image_id, d_fb, ctr);
+        mark(1);
+        c->nrender_ev = 2;
         break;
     case 1:
     case 2: {
         LightP l;
         for (int i = 0; i < 3; ++i) { l.c[i] = c->light.corner[i]; l.e1[i] = c->light.e1[i]; l.e2[i] = c->light.e2[i]; }
         l.emission = c->light.emission;
+        c->launches += 1;
+        mark(0);
         if (st)
-            k_render_pt<true><<<gb, kTT, 0, c->stream>>>(s, k, l, c->ip.pt_bounces, c->ip.albedo, c->ip.ray_eps_frac,
-                                                         c->ip.seed, image_id, d_fb, ctr);
+            k_render_pt<true><<<gb, kTT, 0, strm>>>(s, k, l, c->ip.pt_bounces, c->ip.albedo, c->ip.ray_eps_frac,
+                                                    c->ip.seed, image_id, d_fb, ctr);
         else
-            k_render_pt<false><<<gb, kTT, 0, c->stream>>>(s, k, l, c->ip.pt_bounces, c->ip.albedo, c->ip.ray_eps_frac,
-                                                          c->ip.seed, image_id, d_fb, ctr);
+            k_render_pt<false><<<gb, kTT, 0, strm>>>(s, k, l, c->ip.pt_bounces, c->ip.albedo, c->ip.ray_eps_frac,
+                                                     c->ip.seed, image_id, d_fb, ctr);
+        mark(1);
+        c->nrender_ev = 2;
         break;
     }
-    case 3:
+    case 3: {
+        int rc;
+        if ((rc = ensure(c, c->hit_t, sizeof(float) * n)) || (rc = ensure(c, c->hit_tri, sizeof(uint32_t) * n)) ||
+            (rc = ensure(c, c->unocc, sizeof(uint32_t) * n)) || (rc = ensure(c, c->queue, sizeof(uint32_t) * n)))
+            return rc;
+        uint32_t* qcount = reinterpret_cast<uint32_t*>(ctr + 7);
+        if ((rc = cuda_check(c, cudaMemsetAsync(qcount, 0, sizeof(uint32_t), strm), "queue reset"))) return rc;
+        const int spp = c->ip.ao_samples;
+        c->launches += 3;
+        mark(0);
         if (st)
-            k_render_ao<true><<<gb, kTT, 0, c->stream>>>(s, k, c->ip.ao_samples, c->ip.ao_radius_frac,
-                                                         c->ip.ao_radius_abs, c->ip.seed, image_id, d_fb, ctr);
+            k_ao_primary<true><<<gb, kTT, 0, strm>>>(s, k, image_id, d_fb, c->hit_t.as<float>(), c->hit_tri.as<uint32_t>(),
+                                                     c->unocc.as<uint32_t>(), c->queue.as<uint32_t>(), qcount, ctr);
         else
-            k_render_ao<false><<<gb, kTT, 0, c->stream>>>(s, k, c->ip.ao_samples, c->ip.ao_radius_frac,
-                                                          c->ip.ao_radius_abs, c->ip.seed, image_id, d_fb, ctr);
+            k_ao_primary<false><<<gb, kTT, 0, strm>>>(s, k, image_id, d_fb, c->hit_t.as<float>(), c->hit_tri.as<uint32_t>(),
+                                                      c->unocc.as<uint32_t>(), c->queue.as<uint32_t>(), qcount, ctr);
+        mark(1);
+        const int gs = c->num_sms * 16;
+        if (st)
+            k_ao_samples<true><<<gs, kTT, 0, strm>>>(s, k, spp, c->ip.ao_radius_frac, c->ip.ao_radius_abs, c->ip.seed,
+                                                     image_id, c->hit_t.as<float>(), c->hit_tri.as<uint32_t>(),
+                                                     c->queue.as<uint32_t>(), qcount, c->unocc.as<uint32_t>(), ctr);
+        else
+            k_ao_samples<false><<<gs, kTT, 0, strm>>>(s, k, spp, c->ip.ao_radius_frac, c->ip.ao_radius_abs, c->ip.seed,
+                                                      image_id, c->hit_t.as<float>(), c->hit_tri.as<uint32_t>(),
+                                                      c->queue.as<uint32_t>(), qcount, c->unocc.as<uint32_t>(), ctr);
+        mark(2);
+        k_ao_finish<<<c->num_sms * 4, 256, 0, strm>>>(c->queue.as<uint32_t>(), qcount, c->unocc.as<uint32_t>(), spp,
+                                                      image_id, d_fb);
+        mark(3);
+        c->nrender_ev = 4;
         break;
+    }
     default:
         return set_error(c, 1, "render: unknown mode %d", mode);
     }

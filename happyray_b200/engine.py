@@ -193,9 +193,15 @@ class Engine:
         self._chk(self.L.hr_set_stats(self.ctx, int(on)), "hr_set_stats")
 
     def counters(self, reset: bool = False) -> dict:
-        w = (C.c_uint64 * 4)()
+        w = (C.c_uint64 * 8)()
         self._chk(self.L.hr_get_counters(self.ctx, w, int(reset)), "hr_get_counters")
-        return {"rays": int(w[0]), "cells": int(w[1]), "tests": int(w[2]), "launches": int(w[3])}
+        return {"rays": int(w[0]), "cells": int(w[1]), "tests": int(w[2]), "launches": int(w[3]),
+                "rays2": int(w[4]), "cells2": int(w[5]), "tests2": int(w[6])}
+
+    def render_times(self):
+        buf = (C.c_float * 8)()
+        n = self.L.hr_get_render_times(self.ctx, buf, 8)
+        return [float(buf[i]) for i in range(n)]
 
     def sync(self):
         self._chk(self.L.hr_sync(self.ctx), "hr_sync")

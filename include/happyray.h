@@ -134,9 +134,15 @@ hr_status hr_get_ray_count(hr_ctx *ctx, uint64_t *rays, int32_t reset);
 /* Traversal statistics of the render calls (the reference's debug counters have no
  * equivalent; these size the algorithmic bytes of a frame): with enable != 0 the
  * render kernels also count grid cells visited and triangle tests.  out[0] rays,
- * out[1] cells visited, out[2] triangle tests, out[3] kernels launched by the context. */
+ * out[1] cells visited, out[2] triangle tests, out[3] kernels launched by the context;
+ * out[4..6] the rays / cells / tests of the secondary pass alone (AO samples, shadow
+ * rays); out[7] reserved. */
 hr_status hr_set_stats(hr_ctx *ctx, int32_t enable);
-hr_status hr_get_counters(hr_ctx *ctx, uint64_t out[4], int32_t reset);
+hr_status hr_get_counters(hr_ctx *ctx, uint64_t out[8], int32_t reset);
+/* With timing enabled (hr_set_timing): device time in ms of each kernel of the last
+ * render call, in launch order (AO: primary pass, AO samples, shading).  Returns the
+ * number of kernels written. */
+int32_t hr_get_render_times(hr_ctx *ctx, float *ms, int32_t max_kernels);
 hr_status hr_sync(hr_ctx *ctx);
 /* RTEngine::getBoundingBoxDiagonalLength (RTEngine.h:64, RTEngine.cu:190-193) */
 float hr_bounds_diagonal(hr_ctx *ctx);
