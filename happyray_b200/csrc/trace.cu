@@ -427,7 +427,7 @@ __device__ __forceinline__ void add_rays(unsigned long long* counter, bool secon
 __device__ __forceinline__ uint32_t round32(uint32_t n) { return (n + 31u) & ~31u; }
 
 template <bool STATS>
-__global__ __launch_bounds__(kTT) void k_trace_rays(Scene s, const float* __restrict__ org, const float* __restrict__ dir,
+__global__ __launch_bounds__(kTT, 8) void k_trace_rays(Scene s, const float* __restrict__ org, const float* __restrict__ dir,
                                                     uint32_t n, int32_t* __restrict__ oid, float* __restrict__ ot,
                                                     float* __restrict__ ou, float* __restrict__ ov,
                                                     uint32_t* __restrict__ stats) {
@@ -453,7 +453,7 @@ __global__ __launch_bounds__(kTT) void k_trace_rays(Scene s, const float* __rest
 }
 
 template <bool STATS>
-__global__ __launch_bounds__(kTT) void k_trace_primary(Scene s, Cam cam, int32_t* __restrict__ oid,
+__global__ __launch_bounds__(kTT, 8) void k_trace_primary(Scene s, Cam cam, int32_t* __restrict__ oid,
                                                        float* __restrict__ ot, float* __restrict__ ou,
                                                        float* __restrict__ ov, uint32_t* __restrict__ stats) {
     const G g = load_g(s.desc);
@@ -474,7 +474,7 @@ __global__ __launch_bounds__(kTT) void k_trace_primary(Scene s, Cam cam, int32_t
     }
 }
 
-__global__ __launch_bounds__(kTT) void k_occluded(Scene s, const float* __restrict__ org, const float* __restrict__ dir,
+__global__ __launch_bounds__(kTT, 8) void k_occluded(Scene s, const float* __restrict__ org, const float* __restrict__ dir,
                                                   const float* __restrict__ tmax, uint32_t n, uint8_t* __restrict__ occ) {
     const G g = load_g(s.desc);
     const uint32_t nl = round32(n);
@@ -495,7 +495,7 @@ __global__ __launch_bounds__(kTT) void k_occluded(Scene s, const float* __restri
 
 // mode 0: primary rays with barycentric false colour (SimpleIntegrator.h:41-126)
 template <bool STATS>
-__global__ __launch_bounds__(kTT) void k_render_primary(Scene s, Cam cam, int32_t image_id, float* __restrict__ fb,
+__global__ __launch_bounds__(kTT, 8) void k_render_primary(Scene s, Cam cam, int32_t image_id, float* __restrict__ fb,
                                                         unsigned long long* counter) {
     const G g = load_g(s.desc);
     const uint32_t slots = tile_slots(cam);
@@ -531,7 +531,7 @@ __global__ __launch_bounds__(kTT) void k_render_primary(Scene s, Cam cam, int32_
 //                 unoccluded count of the pixel (match_any-aggregated atomics);
 //   k_ao_finish   visibility = unoccluded / samples, progressive blend (AOIntegrator.h:168-175).
 template <bool STATS>
-__global__ __launch_bounds__(kTT) void k_ao_primary(Scene s, Cam cam, int32_t image_id, float* __restrict__ fb,
+__global__ __launch_bounds__(kTT, 8) void k_ao_primary(Scene s, Cam cam, int32_t image_id, float* __restrict__ fb,
                                                     float* __restrict__ hit_t, uint32_t* __restrict__ hit_tri,
                                                     uint32_t* __restrict__ unocc, uint32_t* __restrict__ queue,
                                                     uint32_t* qcount, unsigned long long* counter) {
@@ -568,7 +568,7 @@ __global__ __launch_bounds__(kTT) void k_ao_primary(Scene s, Cam cam, int32_t im
 }
 
 template <bool STATS>
-__global__ __launch_bounds__(kTT) void k_ao_samples(Scene s, Cam cam, int32_t spp, float alpha_frac, float alpha_abs,
+__global__ __launch_bounds__(kTT, 8) void k_ao_samples(Scene s, Cam cam, int32_t spp, float alpha_frac, float alpha_abs,
                                                     uint64_t seed, int32_t image_id, const float* __restrict__ hit_t,
                                                     const uint32_t* __restrict__ hit_tri,
                                                     const uint32_t* __restrict__ queue, const uint32_t* qcount,
@@ -633,7 +633,7 @@ struct LightP {
 // bounce loop runs the same number of iterations on every lane (finished paths pass
 // active = false), so the warp-synchronous traversal can be called inside it.
 template <bool STATS>
-__global__ __launch_bounds__(kTT) void k_render_pt(Scene s, Cam cam, LightP l, int32_t bounces, float albedo,
+__global__ __launch_bounds__(kTT, 8) void k_render_pt(Scene s, Cam cam, LightP l, int32_t bounces, float albedo,
                                                    float eps_frac, uint64_t seed, int32_t image_id,
                                                    float* __restrict__ fb, unsigned long long* counter) {
     const G g = load_g(s.desc);
