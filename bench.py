@@ -7,8 +7,10 @@ Default workload (the configuration the headline metric is quoted on):
       rays per hit, AO radius 0.1 x bounds diagonal, PCG32 per pixel.
 A step is one frame: device key-frame interpolation + bounds, two-level grid rebuild,
 primary + AO traversal.  value = rays traced / step time (Mrays/s), whole job over all GPUs.
-Other workloads: c1 (uniform grid, 129x129 heightfield, 256x256 primary rays) and c3
-(2,097,152 triangles, 16 curl-noise key frames, rebuild per frame, 1280x720 path tracing).
+Other workloads: c1 (uniform grid, 129x129 heightfield, 256x256 primary rays), c3
+(2,097,152 triangles, 16 curl-noise key frames, rebuild per frame, 1280x720 path tracing)
+and c4 (256 scenes of 1k-500k triangles batched: one segmented build + one persistent
+render launch in a CUDA graph, against the per-scene path on the same scenes).
 
 Multi-GPU (torchrun): independent replicas, one per GPU (the path has no exchange step).
 `--impl reference` times the CPU restatement of the reference's build + traversal
@@ -200,17 +202,240 @@ def run_reference(args, W, rank, ws):
     print(json.dumps(line), flush=True)
 
 
+DEFAULT_SEED = 0x853c49e6748fea9b
+
+
+def batch_workload(n: int = 256, seed: int = 0):
+    """Batched workload: n scenes, triangles log-uniform in [1k, 500k], heightfield or
+    cluster scene (coin flip), square images log-uniform in [64^2, 512^2] pixels, primary
+    rays + 4 AO rays per hit."""
+    from happyray_b200 import scenes as S
+    from happyray_b200.batch import SceneSpec
+    raw = S.batch_scenes(n, seed)
+    specs = [SceneSpec(r["v"], r["f"], r["cam"]["position"], r["cam"]["orientation"], r["cam"]["up"],
+                       r["cam"]["fov"], r["cam"]["res_x"], r["cam"]["res_y"], ao_samples=4) for r in raw]
+    return dict(name=f"c4_batched_{n}_scenes_primary_ao4", specs=specs)
+
+
+def cpu_baseline_batch(specs, top=0.0625, leaf=2.0, budget_s=20.0):
+    """The oracle on whole scenes of the batch, in order, until the time budget: full
+    two-level build + AO render (4 samples) of each, all host threads."""
+    import oracle as O
+    rays_tot, t_tot, ns = 0, 0.0, 0
+    for sp in specs:
+        t0 = time.perf_counter()
+        v4, bmin, bmax = O.lerp_bounds(sp.vertices, sp.vertices, 1.0)
+        b = O.build_tl(v4, sp.faces, bmin, bmax, top, leaf)
+        oc = O.camera(sp.position, sp.orientation, sp.up, sp.fov, sp.width, sp.height)
+        _, rays = O.render_ao(b, oc, sp.ao_samples, float(np.float32(0.1) * b.diag()), DEFAULT_SEED)
+        t_tot += time.perf_counter() - t0
+        rays_tot += rays
+        ns += 1
+        if t_tot > budget_s:
+            break
+    return {"value": rays_tot / t_tot / 1e6, "unit": "Mrays/s", "cores": O.num_threads(), "kind": "port",
+            "sample": f"first {ns} of {len(specs)} scenes, each a full build + AO render ({rays_tot} rays, "
+                      f"{t_tot:.1f} s)"}
+
+
+def run_batched(args, rank, ws, local):
+    """c4: the batched form (one segmented build + one persistent render launch for all
+    scenes, CUDA graph) against the plain per-scene path (one hr_ctx per scene, build +
+    render each) on the same scenes, densities and samples."""
+    W = batch_workload()
+    specs = W["specs"]
+    if args.impl == "reference":
+        if rank == 0:
+            cb = cpu_baseline_batch(specs)
+            v = cb["value"]
+            print(json.dumps({"metric": METRIC, "value": v, "unit": "Mrays/s", "n_gpus": 1, "steps": args.steps,
+                              "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+                              "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+                              "config": {"workload": W["name"]}, "impl": "reference", "cpu_baseline": cb,
+                              "e2e": {"value": v, "unit": "Mrays/s", "h2d_bytes_per_step": 0,
+                                      "d2h_bytes_per_step": 0}}), flush=True)
+        return
+    import torch
+    from happyray_b200 import GRID_TWO_LEVEL, RENDER_AO, Engine
+    from happyray_b200.batch import Batch
+    dev = local
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream(device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{dev}")
+    b = Batch(dev, stream=stream.cuda_stream)
+    b.set_scenes(specs)
+    b.set_integrator(0.1, DEFAULT_SEED)
+    t0 = time.perf_counter()
+    tuning = b.autotune(reps=2) if not args.no_tune else None
+    tune_s = time.perf_counter() - t0
+    top = tuning["top_density"] if tuning else 0.0625
+    leaf = tuning["leaf_density"] if tuning else 2.0
+    b.run(0)
+    b.counters(reset=True)
+    b.run(0)
+    rays_per_step = b.counters(reset=True)[0]
+    for _ in range(args.warmup):
+        b.run(0)
+    torch.cuda.synchronize()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    l0 = b.counters()[1]
+    step_ms, build_ms, render_ms = [], [], []
+    with ClockSampler(dev) as clk:
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()   # L2 flush between timed steps, outside the step's events
+            b.run(0)
+            tb, tr, tt = b.times()
+            build_ms.append(tb)
+            render_ms.append(tr)
+            step_ms.append(tt)
+        torch.cuda.synchronize()
+    launches = b.counters()[1] - l0
+    total_ms = sum(step_ms)
+    if ws > 1:
+        import torch.distributed as dist
+        tt = torch.tensor([total_ms], dtype=torch.float64, device=f"cuda:{dev}")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        total_ms = float(tt.item())
+    value = ws * rays_per_step * args.steps / (total_ms * 1e-3) / 1e6
+
+    # end to end through the public API: new vertex positions of every scene from pinned
+    # host memory, build + render, every image back to pinned host memory
+    e2e = None
+    if not args.no_e2e:
+        allv = np.concatenate([np.asarray(s.vertices, np.float32).reshape(-1, 3) for s in specs])
+        hv = torch.from_numpy(allv).pin_memory().numpy()
+        npx = sum(s.width * s.height for s in specs)
+        himg = torch.zeros(npx * 3, dtype=torch.float32).pin_memory().numpy()
+        e_ms = []
+        for i in range(args.warmup + args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+            a, z = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            b.set_vertices(hv)
+            b.run(0)
+            b.download_images(himg)
+            z.record(stream)
+            z.synchronize()
+            if i >= args.warmup:
+                e_ms.append(a.elapsed_time(z))
+        et = sum(e_ms)
+        e2e = {"value": ws * rays_per_step * args.steps / (et * 1e-3) / 1e6, "unit": "Mrays/s",
+               "h2d_bytes_per_step": int(hv.nbytes), "d2h_bytes_per_step": int(himg.nbytes),
+               "ms_per_step": et / args.steps}
+
+    # the plain per-scene path on the same scenes: one context per scene, all on one
+    # stream, each step a build + render of every scene
+    engines, fbs = [], []
+    for sp in specs:
+        e = Engine(dev, stream=stream.cuda_stream)
+        e.upload(sp.vertices, sp.vertices, sp.faces, 1.0)
+        e.setGridDensities(top, leaf)
+        e.setCamera(sp.position, sp.orientation, sp.up, sp.fov, sp.width, sp.height)
+        e.set_integrator(ao_samples=sp.ao_samples, ao_radius=-0.1, seed=DEFAULT_SEED)
+        engines.append(e)
+        fbs.append(torch.zeros(sp.width * sp.height * 3, dtype=torch.float32, device=f"cuda:{dev}"))
+
+    def plain_step():
+        for e, fb in zip(engines, fbs):
+            e.build(GRID_TWO_LEVEL)
+            e.render_device(fb, 0, RENDER_AO)
+
+    # one instrumented pass: ray counts must match the batch; cells / tests size the
+    # algorithmic traversal bytes, the grids the algorithmic build bytes
+    for e in engines:
+        e.set_stats(True)
+        e.counters(reset=True)
+    plain_step()
+    torch.cuda.synchronize()
+    st = [e.counters(reset=True) for e in engines]
+    plain_rays = sum(s["rays"] for s in st)
+    b_trace = sum(trace_bytes(s["rays"], s["cells"], s["tests"]) for s in st)
+    b_build = 0
+    for e, sp in zip(engines, specs):
+        e.set_stats(False)
+        b_build += algorithmic_build_bytes(e.grid_info(), sp.vertices.shape[0], sp.faces.shape[0], lerp=False)
+    plain_ms = []
+    for i in range(args.warmup + max(1, args.steps // 4)):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        a, z = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        plain_step()
+        z.record(stream)
+        z.synchronize()
+        if i >= args.warmup:
+            plain_ms.append(a.elapsed_time(z))
+    for e in engines:
+        e.cleanup()
+    plain_value = plain_rays / (statistics.median(plain_ms) * 1e-3) / 1e6
+
+    if rank != 0:
+        b.close()
+        if ws > 1:
+            import torch.distributed as dist
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+    peak, peak_kind = peaks()
+    rmed, bmed = statistics.median(render_ms), statistics.median(build_ms)
+    ntri = sum(s.faces.shape[0] for s in specs)
+    line = {
+        "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene generators, no dataset)",
+        "config": {"workload": W["name"], "scenes": len(specs), "triangles": int(ntri),
+                   "pixels": int(sum(s.width * s.height for s in specs)), "ao_samples": 4,
+                   "densities": [top, leaf], "block_threads": tuning["block_threads"] if tuning else 256,
+                   "tile_width": tuning["tile_width"] if tuning else 8, "cuda_graph": True,
+                   "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{ws}"},
+        "rays_per_step": rays_per_step, "build_ms_per_step": bmed, "render_ms_per_step": rmed,
+        "plain_path": {"value": plain_value, "unit": "Mrays/s", "ms_per_step": statistics.median(plain_ms),
+                       "rays_per_step": plain_rays, "note": "one hr_ctx per scene: build + render each, one stream"},
+        "speedup_vs_plain": value / plain_value,
+        "autotune": dict(tuning, seconds=tune_s) if tuning else None,
+        "roofline": {"bound": "hbm", "kernel": "k_trace_jobs", "achieved": b_trace / (rmed * 1e-3) / 1e9,
+                     "peak": peak, "unit": "GB/s", "frac": b_trace / (rmed * 1e-3) / 1e9 / peak, "traffic": None,
+                     "peak_source": peak_kind, "algorithmic_bytes_per_launch": b_trace, "kernel_ms": rmed},
+        "build_roofline": {"bound": "hbm", "achieved": b_build / (bmed * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                           "frac": b_build / (bmed * 1e-3) / 1e9 / peak, "algorithmic_bytes": b_build},
+        "gpu_launches": launches,
+        "e2e": e2e,
+    }
+    clk_s = clk.summary()
+    if clk_s:
+        line["clocks"] = clk_s
+    if not args.no_cpu and ws == 1:
+        try:
+            line["cpu_baseline"] = cpu_baseline_batch(specs, top, leaf)
+        except Exception as ex:   # the CPU leg is a reported baseline only
+            line["cpu_baseline"] = {"error": str(ex)}
+    print(json.dumps(line), flush=True)
+    b.close()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3"])
+    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3", "c4"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-tune", action="store_true", help="c4: skip the autotuner (densities 1/16, 2)")
     args = ap.parse_args()
     rank, ws, local = dist_setup() if os.environ.get("WORLD_SIZE") else (0, 1, 0)
+    if args.config == "c4":
+        run_batched(args, rank, ws, local)
+        return
 
     W = workload(args.config)
     if args.impl == "reference":

@@ -68,7 +68,40 @@ SIGNATURES = {
     "hr_exclusive_scan_device": (C.c_int, [P, P, C.c_uint32]),
     "hr_radix_sort_pairs_device": (C.c_int, [P, P, P, C.c_uint32, C.c_int32]),
     "hr_radix_sort_pairs_noalloc": (C.c_int, [P, P, P, C.c_uint32, C.c_int32]),
+    # batched scenes
+    "hr_batch_create": (C.c_int, [C.POINTER(P), C.c_int32, P]),
+    "hr_batch_destroy": (None, [P]),
+    "hr_batch_last_error": (C.c_char_p, [P]),
+    "hr_batch_set_scenes": (C.c_int, [P, P, C.c_uint32]),
+    "hr_batch_set_densities": (C.c_int, [P, C.c_uint32, C.c_float, C.c_float]),
+    "hr_batch_set_launch": (C.c_int, [P, C.c_int32, C.c_int32]),
+    "hr_batch_set_integrator": (C.c_int, [P, C.c_float, C.c_uint64]),
+    "hr_batch_set_graph": (C.c_int, [P, C.c_int32]),
+    "hr_batch_set_vertices": (C.c_int, [P, P, C.c_uint32]),
+    "hr_batch_run": (C.c_int, [P, C.c_int32]),
+    "hr_batch_get_times": (C.c_int, [P, P, P, P]),
+    "hr_batch_get_counters": (C.c_int, [P, P, C.c_int32]),
+    "hr_batch_get_image": (C.c_int, [P, C.c_uint32, P]),
+    "hr_batch_image_device": (C.c_int, [P, C.c_uint32, P]),
+    "hr_batch_download_images": (C.c_int, [P, P, C.c_uint64]),
+    "hr_batch_grid_info": (C.c_int, [P, C.c_uint32, C.POINTER(GridInfo)]),
+    "hr_batch_grid_download": (C.c_int, [P, C.c_uint32, P, P, P]),
+    "hr_batch_autotune": (C.c_int, [P, C.c_int32, P]),
 }
+
+
+class BatchScene(C.Structure):
+    """hr_batch_scene"""
+    _fields_ = [("vertices_xyz", P), ("num_vertices", C.c_uint32), ("indices", P), ("num_triangles", C.c_uint32),
+                ("cam_position", C.c_float * 3), ("cam_orientation", C.c_float * 3), ("cam_up", C.c_float * 3),
+                ("cam_fov_deg", C.c_float), ("width", C.c_int32), ("height", C.c_int32), ("ao_samples", C.c_int32),
+                ("top_density", C.c_float), ("leaf_density", C.c_float)]
+
+
+class BatchTuning(C.Structure):
+    """hr_batch_tuning"""
+    _fields_ = [("top_density", C.c_float), ("leaf_density", C.c_float), ("block_threads", C.c_int32),
+                ("tile_width", C.c_int32), ("ms_per_step", C.c_float), ("trials", C.c_int32)]
 
 _lock = threading.Lock()
 _lib = None

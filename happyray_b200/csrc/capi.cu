@@ -52,14 +52,6 @@ int ensure(hr_ctx* c, DevBuf& b, size_t bytes) {
     return 0;
 }
 
-namespace {
-
-void free_buf(hr_ctx* c, DevBuf& b) {
-    if (b.p) cudaFreeAsync(b.p, c->stream);
-    b.p = nullptr;
-    b.bytes = 0;
-}
-
 // Camera::init (Camera.h:40-64), evaluated on the host in binary32
 void camera_init(Camera* c, const float pos[3], const float fwd[3], const float up[3], float fov, int w, int h) {
     auto norm = [](float v[3]) {
@@ -93,16 +85,27 @@ void camera_init(Camera* c, const float pos[3], const float fwd[3], const float 
     c->h = h;
 }
 
+namespace {
+
+void free_buf(hr_ctx* c, DevBuf& b) {
+    if (b.p) cudaFreeAsync(b.p, c->stream);
+    b.p = nullptr;
+    b.bytes = 0;
+}
+
 __global__ void k_expand_xyz(const float* __restrict__ xyz, float4* __restrict__ out, size_t n) {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
         out[i] = make_float4(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2], 0.0f);
 }
 
-struct DeviceGuard {
-    explicit DeviceGuard(int dev) { cudaGetDevice(&prev); if (prev != dev) cudaSetDevice(dev); }
-    ~DeviceGuard() { int cur; cudaGetDevice(&cur); if (cur != prev) cudaSetDevice(prev); }
-    int prev = 0;
-};
+}  // namespace
+
+void expand_xyz(const float* xyz, float4* out, size_t n, int grid, cudaStream_t s) {
+    k_expand_xyz<<<grid, 256, 0, s>>>(xyz, out, n);
+}
+
+namespace {
+
 
 int ensure_pinned(hr_ctx* c, size_t bytes) {
     if (c->pinned_bytes >= bytes) return 0;

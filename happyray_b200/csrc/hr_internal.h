@@ -116,6 +116,17 @@ namespace hr {
 int set_error(hr_ctx* c, int code, const char* fmt, ...);
 int cuda_check(hr_ctx* c, cudaError_t e, const char* what);
 int ensure(hr_ctx* c, DevBuf& b, size_t bytes);
+// xyz (3 floats per vertex, device) -> float4 with w = 0
+void expand_xyz(const float* xyz, float4* out, size_t n, int grid, cudaStream_t s);
+// Camera::init (Camera.h:40-64) in binary32 on the host
+void camera_init(Camera* c, const float pos[3], const float fwd[3], const float up[3], float fov, int w, int h);
+
+// makes `dev` current for the lifetime of the guard
+struct DeviceGuard {
+    explicit DeviceGuard(int dev) { cudaGetDevice(&prev); if (prev != dev) cudaSetDevice(dev); }
+    ~DeviceGuard() { int cur; cudaGetDevice(&cur); if (cur != prev) cudaSetDevice(prev); }
+    int prev = 0;
+};
 
 // build.cu
 int build_grid(hr_ctx* c, int32_t kind, int32_t exact);
@@ -131,6 +142,10 @@ int exclusive_scan_u32(hr_ctx* c, uint32_t* data, const uint32_t* d_count, size_
 int exclusive_scan_u32x2(hr_ctx* c, uint2* data, const uint32_t* d_count, size_t cap_count,
                          uint32_t* d_total_x, uint32_t* d_total_y, uint2* partials, cudaStream_t s);
 size_t scan_partials_words(size_t cap_count);
+// Exclusive scan of per-block counts in place; the total goes to *d_total, or, when it
+// exceeds cap, ovf_bit is set in *ovf, the total to *d_req and *d_total becomes 0.
+int scan_block_sums(hr_ctx* c, uint32_t* sums, uint32_t n, uint32_t* d_total, uint32_t* ovf,
+                    uint32_t cap, uint32_t ovf_bit, uint32_t* d_req, cudaStream_t s);
 
 // trace.cu
 int launch_trace_rays(hr_ctx* c, const float* org, const float* dir, uint32_t n, int32_t* id,

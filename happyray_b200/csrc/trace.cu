@@ -17,414 +17,12 @@
 //   * primary ray directions are normalised, so t is a distance;
 //   * no fast-math: IEEE division / square root, no FMA contraction.
 //
-// Execution model: the traversal is warp-synchronous.  Every lane advances its own DDA
-// to its next non-empty cell or leaf, then the warp tests the triangle lists together:
-// a lane with a short list tests it alone; a long list (more than kCoopMin triangles,
-// e.g. a whole small sphere inside one leaf) is tested by all 32 lanes, strided, and
-// reduced by (smallest t, then smallest list position), which is exactly the
-// first-tested-wins rule of the sequential intersector.  Traversal functions must
-// therefore be called by all lanes of a warp; lanes without a ray pass active = false.
-#include "hr_internal.h"
-#include "hr_block.cuh"
+// The traversal itself (warp-synchronous DDA + intersection) lives in traverse.cuh.
+#include "traverse.cuh"
 
 namespace hr {
 
 namespace {
-
-constexpr uint32_t kCoopMin = 8;   // longer triangle lists are intersected by the whole warp
-
-struct Scene {
-    const float4* __restrict__ tris;   // 3 float4 per triangle (current frame)
-    const uint2* __restrict__ cells;
-    const uint2* __restrict__ leaves;
-    const uint32_t* __restrict__ prims;
-    const GridDesc* desc;
-    uint32_t ntri;
-    int32_t kind;
-};
-
-struct G {
-    float bmin[3], bmax[3], cs[3], rcp[3];
-    int32_t res[3];
-};
-__device__ __forceinline__ G load_g(const GridDesc* d) {
-    G g;
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        g.bmin[k] = __ldg(&d->bmin[k]); g.bmax[k] = __ldg(&d->bmax[k]);
-        g.cs[k] = __ldg(&d->cs[k]); g.rcp[k] = __ldg(&d->rcp[k]); g.res[k] = __ldg(&d->res[k]);
-    }
-    return g;
-}
-
-struct Hit {
-    float t, u, v;
-    uint32_t tri;
-    uint32_t cells, tests;
-    bool hit;
-};
-
-// a16: Moller-Trumbore of one triangle (RayTriangleIntersector.h:52-90); returns the hit
-// test with strict t < tbest
-__device__ __forceinline__ bool mt_test(const Scene& s, uint32_t tri, f3 o, f3 d, float tbest, float* ot, float* ou,
-                                        float* ov) {
-    f3 p[3];
-    tri_fetch(s.tris, tri, p);
-    const f3 e1 = sub(p[1], p[0]), e2 = sub(p[2], p[0]);
-    const f3 pv = cross(d, e2);
-    const float det = dot(e1, pv);
-    const float inv = 1.0f / det;
-    const f3 sv = sub(o, p[0]);
-    const float u = dot(sv, pv) * inv;
-    const f3 q = cross(sv, e1);
-    const float v = dot(q, d) * inv;
-    const float t = dot(e2, q) * inv;
-    *ot = t; *ou = u; *ov = v;
-    return u >= 0.0f && v >= 0.0f && u + v <= 1.0f && t > kIsectEps && t < tbest;
-}
-
-// prims[b, e) tested in order by one lane; first-tested wins ties (strict <)
-template <bool ANY, bool STATS>
-__device__ __forceinline__ bool isect_range(const Scene& s, f3 o, f3 d, uint32_t b, uint32_t e, Hit& h) {
-    for (uint32_t it = b; it < e; ++it) {
-        const uint32_t tri = __ldg(s.prims + it);
-        float t, u, v;
-        if (STATS) h.tests++;
-        if (mt_test(s, tri, o, d, h.t, &t, &u, &v)) {
-            h.t = t; h.u = u; h.v = v; h.tri = tri; h.hit = true;
-            if (ANY) return true;
-        }
-    }
-    return false;
-}
-
-__device__ __forceinline__ float shfl(float x, int src) { return __shfl_sync(kFullMask, x, src); }
-__device__ __forceinline__ uint32_t shfl(uint32_t x, int src) { return __shfl_sync(kFullMask, x, src); }
-
-// Warp-wide test of every lane's list prims[b, e).  Must be called by all 32 lanes.
-// Returns true on the lanes whose any-hit query is answered (ANY) by this test.
-template <bool ANY, bool STATS>
-__device__ __forceinline__ bool test_lists(const Scene& s, f3 o, f3 d, uint32_t b, uint32_t e, Hit& h) {
-    const uint32_t lane = threadIdx.x & 31u;
-    const uint32_t n = e - b;
-    const bool coop = n > kCoopMin;
-    bool done = false;
-    if (!coop && n) done = isect_range<ANY, STATS>(s, o, d, b, e, h);
-    uint32_t m = __ballot_sync(kFullMask, coop);
-    while (m) {
-        const int src = __ffs(m) - 1;
-        m &= m - 1;
-        const f3 so = mk(shfl(o.x, src), shfl(o.y, src), shfl(o.z, src));
-        const f3 sd = mk(shfl(d.x, src), shfl(d.y, src), shfl(d.z, src));
-        const uint32_t sb = shfl(b, src), se = shfl(e, src);
-        float bt = shfl(h.t, src), bu = 0.0f, bv = 0.0f;
-        uint32_t bit = 0xffffffffu;
-        uint32_t tested = 0;
-        for (uint32_t base = sb; base < se; base += 32u) {
-            const uint32_t it = base + lane;
-            if (it < se) {
-                float t, u, v;
-                if (mt_test(s, __ldg(s.prims + it), so, sd, bt, &t, &u, &v)) { bt = t; bu = u; bv = v; bit = it; }
-            }
-            tested += min(32u, se - base);
-            if (ANY && __any_sync(kFullMask, bit != 0xffffffffu)) break;
-        }
-        // (smallest t, smallest position) over the warp = the sequential first-tested-wins hit
-        float rt = bt;
-        uint32_t rit = bit;
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) {
-            const float ot = __shfl_xor_sync(kFullMask, rt, off);
-            const uint32_t oit = __shfl_xor_sync(kFullMask, rit, off);
-            if (ot < rt || (ot == rt && oit < rit)) { rt = ot; rit = oit; }
-        }
-        const uint32_t own = __ballot_sync(kFullMask, bit == rit && rit != 0xffffffffu);
-        if (rit != 0xffffffffu) {
-            const int w = __ffs(own) - 1;
-            const float wu = shfl(bu, w), wv = shfl(bv, w);
-            if ((int)lane == src) {
-                h.t = rt; h.u = wu; h.v = wv; h.tri = __ldg(s.prims + rit); h.hit = true;
-                if (ANY) done = true;
-            }
-        }
-        if (STATS && (int)lane == src) h.tests += tested;
-    }
-    return done;
-}
-
-__device__ __forceinline__ int min_dim(float a, float b, float c) { return a < b ? (a < c ? 0 : 2) : (b < c ? 1 : 2); }
-
-// One DDA step along the axis of the smallest tmax.  The state arrays are only indexed
-// with constants (one branch per axis, as TLGridTraverser.h:226-290 writes it out), so
-// they stay in registers.  Returns tmax of the axis before the step in *t_before and
-// whether the new cell index is inside [0, res).
-__device__ __forceinline__ bool dda_step(float* tmax, int32_t* cell, const float* rcp, const float* cs,
-                                         const int32_t* res, float* t_before) {
-    const int k = min_dim(tmax[0], tmax[1], tmax[2]);
-    if (k == 0) {
-        *t_before = tmax[0];
-        cell[0] += rcp[0] > 0.0f ? 1 : -1;
-        tmax[0] += cs[0] * fabsf(rcp[0]);
-        return cell[0] < res[0] && cell[0] > -1;
-    } else if (k == 1) {
-        *t_before = tmax[1];
-        cell[1] += rcp[1] > 0.0f ? 1 : -1;
-        tmax[1] += cs[1] * fabsf(rcp[1]);
-        return cell[1] < res[1] && cell[1] > -1;
-    } else {
-        *t_before = tmax[2];
-        cell[2] += rcp[2] > 0.0f ? 1 : -1;
-        tmax[2] += cs[2] * fabsf(rcp[2]);
-        return cell[2] < res[2] && cell[2] > -1;
-    }
-}
-
-__device__ __forceinline__ bool clip(const G& g, f3 o, const float* rcp, float* t0, float* t1) {
-    float tn[3], tf[3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        float a = (g.bmin[k] - comp(o, k)) * rcp[k];
-        float b = (g.bmax[k] - comp(o, k)) * rcp[k];
-        tn[k] = hmin(a, b); tf[k] = hmax(a, b);
-    }
-    *t0 = hmax(hmax(tn[0], tn[1]), tn[2]);
-    *t1 = hmin(hmin(tf[0], tf[1]), tf[2]);
-    return *t1 > *t0 && *t1 >= 0.0f;
-}
-
-// a14: uniform grid DDA (UGridTraverser.h:76-172), warp-synchronous
-template <bool ANY, bool STATS>
-__device__ void trace_ug(const Scene& s, const G& g, f3 o, f3 d, Hit& h, bool active) {
-    float rcp[3] = {0.0f, 0.0f, 0.0f}, tmax[3] = {0.0f, 0.0f, 0.0f};
-    int32_t cell[3] = {0, 0, 0};
-    if (active) {
-        rcp[0] = 1.0f / d.x; rcp[1] = 1.0f / d.y; rcp[2] = 1.0f / d.z;
-        float t0, t1;
-        active = clip(g, o, rcp, &t0, &t1);
-        if (active) {
-            f3 ep = o;
-            if (t0 >= 0.0f) {
-                const float te = t0 + kEps;
-                ep = mk(o.x + te * d.x, o.y + te * d.y, o.z + te * d.z);
-            }
-#pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                float cf = floorf((comp(ep, k) - g.bmin[k]) * g.rcp[k]);
-                cf = hmin((float)g.res[k] - 1.0f, hmax(cf, 0.0f));
-                const float stp = rcp[k] > 0.0f ? 1.0f : 0.0f;
-                tmax[k] = ((cf + stp) * g.cs[k] + g.bmin[k] - comp(o, k)) * rcp[k];
-                cell[k] = f2i(cf);
-            }
-            active = cell[0] < g.res[0] && cell[0] > -1 && cell[1] < g.res[1] && cell[1] > -1 &&
-                     cell[2] < g.res[2] && cell[2] > -1;
-        }
-    }
-    const uint32_t rx = (uint32_t)g.res[0], rxy = (uint32_t)g.res[0] * (uint32_t)g.res[1];
-    while (__any_sync(kFullMask, active)) {
-        uint32_t b = 0, e = 0;
-        if (active) {
-            const uint2 cr = __ldg(s.cells + ((uint32_t)cell[0] + (uint32_t)cell[1] * rx + (uint32_t)cell[2] * rxy));
-            b = cr.x; e = cr.y;
-            if (STATS) h.cells++;
-        }
-        const bool done = test_lists<ANY, STATS>(s, o, d, b, e, h);
-        if (active) {
-            if (done) {
-                active = false;
-            } else {
-                float tk;
-                const bool inside = dda_step(tmax, cell, rcp, g.cs, g.res, &tk);
-                active = h.t > tk && inside;
-            }
-        }
-    }
-}
-
-// Two-level DDA state of one lane (TLGridTraverser.h:79-349).
-struct TL {
-    float rcp[3], tmax[3], tentry;
-    int32_t cell[3];
-    uint32_t lbase, lres[3];   // current top cell: first leaf, sub-grid resolution
-    float scs[3], tm2[3];
-    int32_t c2[3];
-};
-
-// Enter the sub-grid of the current top cell at tentry (TLGridTraverser.h:145-197).
-__device__ __forceinline__ void tl_enter(TL& q, const G& g, f3 o, f3 d, uint2 tc) {
-    q.lbase = tc.x;
-    q.lres[0] = tc.y & 0xFFu; q.lres[1] = (tc.y >> 8) & 0xFFu; q.lres[2] = (tc.y >> 16) & 0xFFu;
-    const f3 e2 = mk(o.x + q.tentry * d.x, o.y + q.tentry * d.y, o.z + q.tentry * d.z);
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        const float cres = (float)q.lres[k];
-        const float srcp = g.rcp[k] * cres;
-        const float mb = (float)q.cell[k] * g.cs[k] + g.bmin[k];
-        float cf = floorf((comp(e2, k) - mb) * srcp);
-        q.scs[k] = 1.0f / srcp;
-        cf = hmin(cres - 1.0f, hmax(cf, 0.0f));
-        const float stp = q.rcp[k] > 0.0f ? 1.0f : 0.0f;
-        q.tm2[k] = ((cf + stp) * q.scs[k] + mb - comp(o, k)) * q.rcp[k];
-        q.c2[k] = f2i(cf);
-    }
-}
-
-// Outer step (TLGridTraverser.h:296-348): returns false when the ray is done.
-__device__ __forceinline__ bool tl_outer_step(TL& q, const G& g, const Hit& h) {
-    float tk;
-    const bool inside = dda_step(q.tmax, q.cell, q.rcp, g.cs, g.res, &tk);
-    q.tentry = tk;
-    return h.t > tk && inside;
-}
-
-// From the current top cell, walk to the first non-empty one and enter it; false if the
-// ray leaves the grid (or is done) first.
-template <bool STATS>
-__device__ __forceinline__ bool tl_seek(TL& q, const Scene& s, const G& g, f3 o, f3 d, Hit& h) {
-    const uint32_t rx = (uint32_t)g.res[0], rxy = (uint32_t)g.res[0] * (uint32_t)g.res[1];
-    while (true) {
-        const uint2 tc = __ldg(s.cells + ((uint32_t)q.cell[0] + (uint32_t)q.cell[1] * rx + (uint32_t)q.cell[2] * rxy));
-        if (STATS) h.cells++;
-        if (tc.y & kNotEmptyMask) {
-            tl_enter(q, g, o, d, tc);
-            return true;
-        }
-        if (!tl_outer_step(q, g, h)) return false;
-    }
-}
-
-// a15: two-level DDA, warp-synchronous
-template <bool ANY, bool STATS>
-__device__ void trace_tl(const Scene& s, const G& g, f3 o, f3 d, Hit& h, bool active) {
-    TL q;
-    if (active) {
-        q.rcp[0] = 1.0f / d.x; q.rcp[1] = 1.0f / d.y; q.rcp[2] = 1.0f / d.z;
-        float t0, t1;
-        active = clip(g, o, q.rcp, &t0, &t1);
-        if (active) {
-            q.tentry = hmax(0.0f, t0);
-            const f3 ep = mk(o.x + q.tentry * d.x, o.y + q.tentry * d.y, o.z + q.tentry * d.z);
-#pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                float cf = floorf((comp(ep, k) - g.bmin[k]) * g.rcp[k]);
-                cf = hmin((float)g.res[k] - 1.0f, hmax(cf, 0.0f));
-                const float stp = q.rcp[k] > 0.0f ? 1.0f : 0.0f;
-                q.tmax[k] = ((cf + stp) * g.cs[k] + g.bmin[k] - comp(o, k)) * q.rcp[k];
-                q.cell[k] = f2i(cf);
-            }
-            active = q.cell[0] < g.res[0] && q.cell[0] > -1 && q.cell[1] < g.res[1] && q.cell[1] > -1 &&
-                     q.cell[2] < g.res[2] && q.cell[2] > -1;
-            if (active) active = tl_seek<STATS>(q, s, g, o, d, h);
-        }
-    }
-    while (__any_sync(kFullMask, active)) {
-        uint32_t b = 0, e = 0;
-        if (active) {
-            const uint2 lr = __ldg(s.leaves + (q.lbase + (uint32_t)q.c2[0] + q.lres[0] * (uint32_t)q.c2[1] +
-                                               q.lres[0] * q.lres[1] * (uint32_t)q.c2[2]));
-            b = lr.x; e = lr.y;
-            if (STATS) h.cells++;
-        }
-        const bool done = test_lists<ANY, STATS>(s, o, d, b, e, h);
-        if (active) {
-            if (done) {
-                active = false;
-            } else {
-                // inner step (TLGridTraverser.h:225-290): stop when the hit lies before the
-                // leaf's exit, else step; leaving the sub-grid continues in the top grid
-                const int32_t lres[3] = {(int32_t)q.lres[0], (int32_t)q.lres[1], (int32_t)q.lres[2]};
-                float tk;
-                const bool inside = dda_step(q.tm2, q.c2, q.rcp, q.scs, lres, &tk);
-                if (h.t < tk) {
-                    active = false;
-                } else if (!inside) {
-                    active = tl_outer_step(q, g, h);
-                    if (active) active = tl_seek<STATS>(q, s, g, o, d, h);
-                }
-            }
-        }
-    }
-}
-
-// Closest hit (ANY = false) or any hit within (1e-4, tmax).  Warp-synchronous.
-template <bool ANY, bool STATS>
-__device__ __forceinline__ void trace_one(const Scene& s, const G& g, f3 o, f3 d, float tmax, Hit& h, bool active) {
-    h.t = tmax; h.u = 0.0f; h.v = 0.0f; h.tri = 0; h.hit = false; h.cells = 0; h.tests = 0;
-    if (s.ntri == 0) return;
-    if (s.kind == kUniform) trace_ug<ANY, STATS>(s, g, o, d, h, active);
-    else trace_tl<ANY, STATS>(s, g, o, d, h, active);
-}
-
-struct Cam {
-    float pos[3], tl[3], sx[3], sy[3];
-    int32_t w, h;
-};
-
-// pixel-centre ray, normalised (Camera.h:66-69 getDirection)
-__device__ __forceinline__ f3 primary_dir(const Cam& c, uint32_t pix) {
-    const float px = (float)(pix % (uint32_t)c.w) + 0.5f;
-    const float py = (float)(pix / (uint32_t)c.w) + 0.5f;
-    f3 d;
-    d.x = c.tl[0] + px * c.sx[0] + py * c.sy[0];
-    d.y = c.tl[1] + px * c.sx[1] + py * c.sy[1];
-    d.z = c.tl[2] + px * c.sx[2] + py * c.sy[2];
-    return normalize(d);
-}
-
-__device__ __forceinline__ f3 face_normal(const Scene& s, uint32_t tri, f3 d) {
-    f3 p[3];
-    tri_fetch(s.tris, tri, p);
-    f3 n = normalize(cross(sub(p[1], p[0]), sub(p[2], p[0])));
-    if (dot(n, d) > 0.0f) n = mk(-n.x, -n.y, -n.z);
-    return n;
-}
-
-__device__ __forceinline__ float blend(float old, float val, int32_t image_id) {
-    const float nw = 1.0f / (float)(image_id + 1);
-    const float ow = 1.0f - nw;
-    return old * ow + val * nw;   // AOIntegrator.h:168-175 progressive average
-}
-
-constexpr int kTT = 128;
-
-// Camera rays are issued in warp-sized 8x4 pixel tiles: the 32 rays of a warp start from
-// the same point into a small solid angle and walk nearly the same cells.
-__device__ __forceinline__ uint32_t tile_slots(const Cam& c) {
-    return (((uint32_t)c.w + 7u) / 8u) * (((uint32_t)c.h + 3u) / 4u) * 32u;
-}
-__device__ __forceinline__ bool tile_pixel(const Cam& c, uint32_t slot, uint32_t* pix) {
-    const uint32_t tile = slot >> 5, lane = slot & 31u;
-    const uint32_t tx = ((uint32_t)c.w + 7u) / 8u;
-    const uint32_t x = (tile % tx) * 8u + (lane & 7u), y = (tile / tx) * 4u + (lane >> 3);
-    *pix = y * (uint32_t)c.w + x;
-    return x < (uint32_t)c.w && y < (uint32_t)c.h;
-}
-
-// Device counters (uint64 words): [0] rays, [2] cells, [3] triangle tests of the primary
-// pass; [4] rays, [5] cells, [6] tests of the secondary pass (AO samples, shadow rays);
-// word 1 holds the index check of the last upload, word 7 the AO hit-pixel queue length.
-template <bool STATS>
-__device__ __forceinline__ void add_rays(unsigned long long* counter, bool secondary, uint32_t rays, uint32_t cells = 0,
-                                         uint32_t tests = 0) {
-    unsigned long long r = rays, c = cells, t = tests;
-    for (int o = 16; o > 0; o >>= 1) {
-        r += __shfl_xor_sync(kFullMask, r, o);
-        if (STATS) {
-            c += __shfl_xor_sync(kFullMask, c, o);
-            t += __shfl_xor_sync(kFullMask, t, o);
-        }
-    }
-    if ((threadIdx.x & 31) == 0 && counter) {
-        unsigned long long* base = counter + (secondary ? 4 : 0);
-        if (r) atomicAdd(base, r);
-        if (STATS) {
-            atomicAdd(secondary ? counter + 5 : counter + 2, c);
-            atomicAdd(secondary ? counter + 6 : counter + 3, t);
-        }
-    }
-}
-
-// warp-uniform bound of a 1-D grid-stride loop over n items
-__device__ __forceinline__ uint32_t round32(uint32_t n) { return (n + 31u) & ~31u; }
 
 template <bool STATS>
 __global__ __launch_bounds__(kTT, 8) void k_trace_rays(Scene s, const float* __restrict__ org, const float* __restrict__ dir,
@@ -623,11 +221,6 @@ __global__ void k_ao_finish(const uint32_t* __restrict__ queue, const uint32_t* 
         fb[3 * (size_t)pix + 2] = val;
     }
 }
-
-struct LightP {
-    float c[3], e1[3], e2[3];
-    float emission;
-};
 
 // mode 1/2: path tracing with next-event estimation (PathTracer.h:41-372 structure).  The
 // bounce loop runs the same number of iterations on every lane (finished paths pass

@@ -159,3 +159,32 @@ def config_scene(name: str, seed: int = 0):
     if name == "c3":
         return clusters(2_097_152, seed)
     raise ValueError(name)
+
+
+def heightfield_tris(n_tris: int, seed: int = 0):
+    """Heightfield of the config-1 kind with exactly n_tris triangles: the smallest
+    square grid holding them, its last triangles dropped."""
+    n = max(2, int(math.ceil(math.sqrt(n_tris / 2.0))) + 1)
+    v, f = heightfield(n, seed)
+    return v, np.ascontiguousarray(f[:n_tris])
+
+
+def batch_scenes(n_scenes: int = 256, seed: int = 0, tri_range=(1_000, 500_000), px_range=(64 * 64, 512 * 512)):
+    """Batched-workload scenes: triangle counts log-uniform in tri_range, each a heightfield
+    or a cluster scene (coin flip), a square image whose pixel count is log-uniform in
+    px_range, camera as camera_at_bounds.  Returns dicts with v, f, cam."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n_scenes):
+        nt = int(round(math.exp(rng.uniform(math.log(tri_range[0]), math.log(tri_range[1])))))
+        npx = math.exp(rng.uniform(math.log(px_range[0]), math.log(px_range[1])))
+        side = max(8, int(round(math.sqrt(npx))))
+        sseed = int(rng.integers(0, 2**31 - 1))
+        if rng.random() < 0.5:
+            v, f = heightfield_tris(nt, sseed)
+            kind = "heightfield"
+        else:
+            v, f = clusters(max(nt, 3), sseed)
+            kind = "clusters"
+        out.append(dict(v=v, f=f, cam=camera_at_bounds(v, (side, side)), kind=kind))
+    return out

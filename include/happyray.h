@@ -171,6 +171,79 @@ hr_status hr_radix_sort_pairs_device(hr_ctx *ctx, uint32_t *d_keys, uint32_t *d_
 hr_status hr_radix_sort_pairs_noalloc(void *stream, uint32_t *d_keys, uint32_t *d_values,
                                       uint32_t n, int32_t key_bits);
 
+/* ---------------------------------------------------------------------------------
+ * Batched scenes.  No counterpart in the reference, whose RTEngine holds one scene in
+ * static globals (RTEngine.cu:91-181); it is the per-scene path above run for many
+ * independent scenes at once.  All scenes of a batch get a two-level grid
+ * (TLGridSortBuilder.h:66-452) built by ONE segmented pipeline whose launch count does
+ * not depend on the number of scenes, and are rendered by ONE persistent traversal
+ * launch; the whole step is captured in a CUDA graph and replayed.  Each scene's grid
+ * and image are bit-identical to what the per-scene path gives for the same scene,
+ * densities, camera, samples and seed.
+ */
+typedef struct hr_batch hr_batch;
+
+typedef struct hr_batch_scene {
+    const float *vertices_xyz;      /* host, 3 floats per vertex */
+    uint32_t num_vertices;
+    const uint32_t *indices;        /* host, 3 scene-local vertex indices per triangle */
+    uint32_t num_triangles;         /* >= 1 */
+    float cam_position[3], cam_orientation[3], cam_up[3];
+    float cam_fov_deg;
+    int32_t width, height;
+    int32_t ao_samples;             /* 0: primary rays only (HR_RENDER_PRIMARY shading);
+                                       > 0: HR_RENDER_AO with this many samples per hit */
+    float top_density, leaf_density;  /* <= 0: the batch defaults (1/16, 2) */
+} hr_batch_scene;
+
+typedef struct hr_batch_tuning {
+    float top_density, leaf_density;  /* applied to every scene */
+    int32_t block_threads;            /* persistent traversal block size: 64, 128 or 256 */
+    int32_t tile_width;               /* pixel tile of one warp: tile_width x (32 / tile_width) */
+    float ms_per_step;                /* measured build + render time of the batch */
+    int32_t trials;                   /* configurations timed */
+} hr_batch_tuning;
+
+hr_status hr_batch_create(hr_batch **out, int32_t device, void *stream);
+void hr_batch_destroy(hr_batch *batch);
+const char *hr_batch_last_error(const hr_batch *batch);
+/* Copies the scenes' meshes and cameras to the device (replacing any previous set). */
+hr_status hr_batch_set_scenes(hr_batch *batch, const hr_batch_scene *scenes, uint32_t num_scenes);
+/* Grid densities of one scene (scene < num_scenes) or of all (scene = UINT32_MAX). */
+hr_status hr_batch_set_densities(hr_batch *batch, uint32_t scene, float top_density, float leaf_density);
+/* Launch shape of the persistent traversal: block_threads in {32, 64, ..., 256}, tile_width
+ * in {1, 2, 4, 8, 16, 32}. */
+hr_status hr_batch_set_launch(hr_batch *batch, int32_t block_threads, int32_t tile_width);
+/* AO radius as a fraction of each scene's bounds diagonal, and the PCG32 sequence seed. */
+hr_status hr_batch_set_integrator(hr_batch *batch, float ao_radius_fraction, uint64_t seed);
+/* use_graph != 0 (default): a step is one replay of a captured CUDA graph. */
+hr_status hr_batch_set_graph(hr_batch *batch, int32_t use_graph);
+/* New vertex positions for every scene, same meshes (host, 3 floats per vertex, scenes
+ * concatenated in order; num_vertices = the batch total).  The next step uses them. */
+hr_status hr_batch_set_vertices(hr_batch *batch, const float *vertices_xyz, uint32_t num_vertices);
+/* One step: rebuild every scene's grid and render every scene into its framebuffer
+ * (progressive blend with weight 1 / (image_id + 1), as hr_render).  Synchronous. */
+hr_status hr_batch_run(hr_batch *batch, int32_t image_id);
+/* Device time of the last step: build, render (ms; -1 when not measured) and total. */
+hr_status hr_batch_get_times(hr_batch *batch, float *build_ms, float *render_ms, float *total_ms);
+/* out[0] rays, out[1] kernels launched, out[2] scenes, out[3] pixels, out[4] secondary
+ * rays, out[5..7] reserved; reset != 0 zeroes the ray counts. */
+hr_status hr_batch_get_counters(hr_batch *batch, uint64_t out[8], int32_t reset);
+/* The framebuffer (float RGB per pixel) of one scene: host copy, or its device address. */
+hr_status hr_batch_get_image(hr_batch *batch, uint32_t scene, float *rgb);
+hr_status hr_batch_image_device(hr_batch *batch, uint32_t scene, float **d_rgb);
+/* Every scene's framebuffer, scenes concatenated in order (num_floats = 3 x total pixels). */
+hr_status hr_batch_download_images(hr_batch *batch, float *rgb, uint64_t num_floats);
+/* One scene's grid, in the per-scene layout of hr_grid_get_info / hr_grid_download
+ * (scene-local cell, leaf, pair and triangle indices). */
+hr_status hr_batch_grid_info(hr_batch *batch, uint32_t scene, hr_grid_info *info);
+hr_status hr_batch_grid_download(hr_batch *batch, uint32_t scene, uint32_t *cells, uint32_t *leaves,
+                                 uint32_t *prims);
+/* Autotuner: times top x leaf densities {1/32, 1/16, 1/8, 1/4} x {1, 2, 4, 8}, then
+ * block_threads {64, 128, 256} x tile_width {4, 8, 16} at the best densities, each on
+ * `reps` graph replays of the current batch; applies and returns the fastest. */
+hr_status hr_batch_autotune(hr_batch *batch, int32_t reps, hr_batch_tuning *best);
+
 #ifdef __cplusplus
 }
 #endif
