@@ -8,9 +8,11 @@ Default workload (the configuration the headline metric is quoted on):
 A step is one frame: device key-frame interpolation + bounds, two-level grid rebuild,
 primary + AO traversal.  value = rays traced / step time (Mrays/s), whole job over all GPUs.
 Other workloads: c1 (uniform grid, 129x129 heightfield, 256x256 primary rays), c3
-(2,097,152 triangles, 16 curl-noise key frames, rebuild per frame, 1280x720 path tracing)
-and c4 (256 scenes of 1k-500k triangles batched: one segmented build + one persistent
-render launch in a CUDA graph, against the per-scene path on the same scenes).
+(2,097,152 triangles, 16 curl-noise key frames, rebuild per frame, 1280x720 path tracing),
+c4 (256 scenes of 1k-500k triangles batched: one segmented build + one persistent
+render launch in a CUDA graph, against the per-scene path on the same scenes) and c5
+(64 resident animated scenes served under Poisson arrivals, continuous batching against
+the serial per-scene path; p50/p99 latency).
 
 Multi-GPU (torchrun): independent replicas, one per GPU (the path has no exchange step).
 `--impl reference` times the CPU restatement of the reference's build + traversal
@@ -20,6 +22,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import signal
 import statistics
@@ -421,13 +424,132 @@ def run_batched(args, rank, ws, local):
         dist.destroy_process_group()
 
 
+def served_requests(pool, n, rate, seed=0):
+    """Poisson arrivals at `rate` req/s; each request draws a scene, a frame time U[0,1) of
+    the animation (snapped to its 120 evenly spaced frame times), a square image whose
+    pixel count is log-uniform in [128^2, 1024^2], spp in {1, 4, 16} and AO or 4-bounce PT."""
+    from happyray_b200 import scenes as S
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate, n))
+    reqs = []
+    for i in range(n):
+        sc = int(rng.integers(0, len(pool)))
+        kf = pool[sc][0]
+        K = kf.shape[0]
+        frame = int(rng.uniform(0.0, 1.0) * 120)
+        side = int(round(math.sqrt(math.exp(rng.uniform(math.log(128 * 128), math.log(1024 * 1024))))))
+        spp = int(rng.choice([1, 4, 16]))
+        pt = bool(rng.random() < 0.5)
+        reqs.append(dict(at=float(t[i]), scene=sc, ft=K * frame / 120.0, side=side, spp=spp, pt=pt,
+                         cam=S.camera_at_bounds(kf[0], (side, side))))
+    return reqs
+
+
+def serve_run(pool, reqs, mode, budget, seed=DEFAULT_SEED):
+    """Replays the arrival schedule against one server; returns latency and throughput."""
+    import torch
+    from happyray_b200 import RENDER_AO, RENDER_PATH
+    from happyray_b200.server import Server
+    srv = Server(0, budget, mode)
+    t0 = time.perf_counter()
+    for kf, f in pool:
+        srv.add_scene(kf, f)
+    load_s = time.perf_counter() - t0
+    # pinned result buffers (one allocation), so result copies overlap the next wave
+    sizes = [r["side"] * r["side"] * 3 for r in reqs]
+    offs = np.concatenate([[0], np.cumsum(sizes)])
+    host = torch.empty(int(offs[-1]), dtype=torch.float32).pin_memory().numpy()
+    # warm-up (not measured): one small request per integrator
+    for r in reqs[:4]:
+        cam = dict(r["cam"], res_x=32, res_y=32)
+        srv.submit_render(r["scene"], r["ft"], RENDER_PATH if r["pt"] else RENDER_AO, 1, cam, seed).wait()
+    s0 = srv.stats()
+    pend = []
+    start = time.perf_counter()
+    for i, r in enumerate(reqs):
+        while True:   # open-loop arrivals
+            dt = start + r["at"] - time.perf_counter()
+            if dt <= 0:
+                break
+            time.sleep(dt if dt > 2e-3 else 0)
+        out = host[offs[i]:offs[i + 1]].reshape(-1, 3)
+        pend.append(srv.submit_render(r["scene"], r["ft"], RENDER_PATH if r["pt"] else RENDER_AO, r["spp"],
+                                      r["cam"], seed, out=out))
+    for p in pend:
+        p.wait()
+    s1 = srv.stats()
+    infos = [p.info() for p in pend]
+    srv.close()
+    lat = np.array([(i["done_ns"] - i["submit_ns"]) * 1e-6 for i in infos])
+    span_s = (max(i["done_ns"] for i in infos) - min(i["submit_ns"] for i in infos)) * 1e-9
+    rays = s1["rays"] - s0["rays"]
+    return {"mrays_s": rays / span_s / 1e6, "rays": int(rays), "span_s": span_s,
+            "completed_per_s": len(reqs) / span_s, "p50_ms": float(np.percentile(lat, 50)),
+            "p99_ms": float(np.percentile(lat, 99)), "mean_ms": float(lat.mean()),
+            "waves": int(s1["waves"] - s0["waves"]), "rebuilds": int(s1["rebuilds"] - s0["rebuilds"]),
+            "failed": int(s1["failed"] - s0["failed"]), "peak_inflight_bytes": int(s1["peak_inflight_bytes"]),
+            "resident_bytes": int(s1["resident_bytes"]), "launches": int(s1["launches"] - s0["launches"]),
+            "scene_load_s": load_s}
+
+
+def run_served(args, rank, ws, local):
+    """c5: served rendering (continuous batching over resident animated scenes) against
+    the serial per-scene path, on one replayed Poisson arrival schedule."""
+    import torch
+    from happyray_b200 import scenes as S
+    from happyray_b200.server import BATCHED, SERIAL
+    n_req = args.requests
+    name = f"c5_served_64_scenes_{n_req}_requests_2000rps"
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps({"impl": "reference", "unavailable": "the served workload has no CPU form in the "
+                              "reference (no server); the CPU baseline of the same integrators is the c2/c3 lines"}),
+                  flush=True)
+        return
+    torch.cuda.set_device(local)
+    t0 = time.perf_counter()
+    pool = S.served_scenes(64, 0, device=f"cuda:{local}")
+    gen_s = time.perf_counter() - t0
+    reqs = served_requests(pool, n_req, 2000.0)
+    budget = 120 << 30
+    with ClockSampler(local) as clk:
+        served = serve_run(pool, reqs, BATCHED, budget)
+        serial = serve_run(pool, reqs, SERIAL, budget)
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": served["mrays_s"], "unit": "Mrays/s", "n_gpus": ws, "steps": n_req,
+        "warmup": 4, "ms_per_step": served["mean_ms"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene generators, no dataset)",
+        "config": {"workload": name, "scenes": len(pool), "triangles": int(sum(f.shape[0] for _, f in pool)),
+                   "keyframes": 16, "arrivals": "Poisson 2000 req/s, open loop", "requests": n_req,
+                   "frame_times": "U[0,1) snapped to 120 per cycle", "resolution": "log-uniform 128^2..1024^2",
+                   "spp": [1, 4, 16], "integrators": ["AO", "PT 4 bounces"], "hbm_budget_gb": 120,
+                   "parallelism": f"replicas x{ws}"},
+        "served": served, "serial_path": serial, "speedup_vs_serial": served["mrays_s"] / serial["mrays_s"],
+        "p50_ms": served["p50_ms"], "p99_ms": served["p99_ms"],
+        "timing": "wall clock from each request's submission to its completion (results in pinned host memory); "
+                  "throughput = rays / (last completion - first submission)",
+        "scene_generation_s": gen_s,
+        "gpu_launches": served["launches"],
+        "e2e": {"value": served["mrays_s"], "unit": "Mrays/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": int(sum(r["side"] ** 2 * 12 for r in reqs) / n_req),
+                "note": "every request is end to end: submission to result in host memory"},
+    }
+    clk_s = clk.summary()
+    if clk_s:
+        line["clocks"] = clk_s
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3", "c4"])
+    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3", "c4", "c5"])
+    ap.add_argument("--requests", type=int, default=1000, help="c5: requests replayed per mode")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="c4: skip the autotuner (densities 1/16, 2)")
@@ -435,6 +557,9 @@ def main():
     rank, ws, local = dist_setup() if os.environ.get("WORLD_SIZE") else (0, 1, 0)
     if args.config == "c4":
         run_batched(args, rank, ws, local)
+        return
+    if args.config == "c5":
+        run_served(args, rank, ws, local)
         return
 
     W = workload(args.config)

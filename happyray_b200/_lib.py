@@ -87,6 +87,17 @@ SIGNATURES = {
     "hr_batch_grid_info": (C.c_int, [P, C.c_uint32, C.POINTER(GridInfo)]),
     "hr_batch_grid_download": (C.c_int, [P, C.c_uint32, P, P, P]),
     "hr_batch_autotune": (C.c_int, [P, C.c_int32, P]),
+    # served rendering
+    "hr_server_create": (C.c_int, [C.POINTER(P), C.c_int32, C.c_uint64, C.c_int32]),
+    "hr_server_destroy": (None, [P]),
+    "hr_server_last_error": (C.c_char_p, [P]),
+    "hr_server_add_scene": (C.c_int, [P, P, C.c_uint32, C.c_uint32, P, C.c_uint32, C.c_float, C.c_float,
+                                      C.POINTER(C.c_uint32)]),
+    "hr_server_submit": (C.c_int, [P, P, C.POINTER(C.c_uint64)]),
+    "hr_server_wait": (C.c_int, [P, C.c_uint64, C.c_int32]),
+    "hr_server_drain": (C.c_int, [P, C.c_int32]),
+    "hr_server_request_info": (C.c_int, [P, C.c_uint64, P]),
+    "hr_server_get_stats": (C.c_int, [P, P]),
 }
 
 
@@ -102,6 +113,29 @@ class BatchTuning(C.Structure):
     """hr_batch_tuning"""
     _fields_ = [("top_density", C.c_float), ("leaf_density", C.c_float), ("block_threads", C.c_int32),
                 ("tile_width", C.c_int32), ("ms_per_step", C.c_float), ("trials", C.c_int32)]
+
+
+class Request(C.Structure):
+    """hr_request"""
+    _fields_ = [("scene", C.c_uint32), ("frame_time", C.c_float), ("kind", C.c_int32), ("mode", C.c_int32),
+                ("spp", C.c_int32), ("cam_position", C.c_float * 3), ("cam_orientation", C.c_float * 3),
+                ("cam_up", C.c_float * 3), ("cam_fov_deg", C.c_float), ("width", C.c_int32), ("height", C.c_int32),
+                ("seed", C.c_uint64), ("out_rgb", P), ("ray_org", P), ("ray_dir", P), ("num_rays", C.c_uint32),
+                ("out_id", P), ("out_t", P), ("out_u", P), ("out_v", P)]
+
+
+class RequestInfo(C.Structure):
+    """hr_request_info"""
+    _fields_ = [("status", C.c_int32), ("wave", C.c_uint32), ("submit_ns", C.c_uint64), ("admit_ns", C.c_uint64),
+                ("done_ns", C.c_uint64)]
+
+
+class ServerStats(C.Structure):
+    """hr_server_stats"""
+    _fields_ = [("completed", C.c_uint64), ("failed", C.c_uint64), ("waves", C.c_uint64), ("rebuilds", C.c_uint64),
+                ("rays", C.c_uint64), ("resident_bytes", C.c_uint64), ("peak_inflight_bytes", C.c_uint64),
+                ("launches", C.c_uint64)]
+
 
 _lock = threading.Lock()
 _lib = None

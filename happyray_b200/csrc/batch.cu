@@ -42,17 +42,6 @@ struct BScene {
 
 namespace {
 
-// largest s in [0, n) with off[s] <= x, for ascending off with off[0] = 0
-__device__ __forceinline__ uint32_t find_segment(const uint32_t* __restrict__ off, uint32_t n, uint32_t x) {
-    uint32_t lo = 0, hi = n;
-    while (hi - lo > 1u) {
-        const uint32_t mid = (lo + hi) >> 1;
-        if (__ldg(off + mid) <= x) lo = mid;
-        else hi = mid;
-    }
-    return lo;
-}
-
 // ---------------------------------------------------------------------------------
 // segmented build.  Blocks of the per-triangle (per-vertex) passes never straddle two
 // scenes: chunk b covers kBT triangles (vertices) of scene chunk[b].x from chunk[b].y.
@@ -287,208 +276,6 @@ __global__ __launch_bounds__(kBT) void kb_leaf_write_pairs(const uint32_t* __res
             }
 }
 
-// ---------------------------------------------------------------------------------
-// persistent rendering of many jobs
-
-// One render job: a grid, a camera, an integrator and an output image.  Grids built in
-// one batch share arrays; cells_offset then points at the device-computed first top cell
-// of the job's scene.
-struct Job {
-    const float4* tris;
-    const uint2* cells;
-    const uint2* leaves;
-    const uint32_t* prims;
-    const GridDesc* desc;
-    const uint32_t* cells_offset;   // nullable
-    float* fb;                      // float RGB per pixel of this job's image
-    Cam cam;
-    uint32_t ntri;
-    int32_t kind;                   // kTwoLevel
-    int32_t mode;                   // HR_RENDER_PRIMARY or HR_RENDER_AO
-    int32_t spp;
-    int32_t image_id;
-    float alpha_frac, alpha_abs;
-    int32_t pad;
-    uint64_t seed;
-};
-
-// trace_one for two-level grids only (every batch grid is two-level)
-template <bool ANY, bool STATS>
-__device__ __forceinline__ void trace_tl_job(const Scene& s, const G& g, f3 o, f3 d, float tmax, Hit& h, bool active) {
-    h.t = tmax; h.u = 0.0f; h.v = 0.0f; h.tri = 0; h.hit = false; h.cells = 0; h.tests = 0;
-    trace_tl<ANY, STATS>(s, g, o, d, h, active);
-}
-
-constexpr int kJobTT = 256;   // largest block of the persistent kernel
-#ifndef HR_JOB_MIN_BLOCKS
-#define HR_JOB_MIN_BLOCKS 3    // blocks of kJobTT per SM the register budget must allow (3: 80 registers)
-#endif
-
-// position of the q-th (0-based) set bit of m; m has more than q set bits
-__device__ __forceinline__ uint32_t nth_set_bit(uint32_t m, uint32_t q) {
-    uint32_t pos = 0;
-#pragma unroll
-    for (uint32_t step = 16; step > 0; step >>= 1) {
-        const uint32_t c = __popc(m & ((1u << step) - 1u));
-        if (q >= c) { q -= c; m >>= step; pos += step; }
-    }
-    return pos;
-}
-
-// Per-warp state of the tile being rendered, in shared memory: the job's scene and grid
-// parameters (which the per-scene kernels get from their launch parameters) and the hit
-// points of the tile's camera rays, which the AO rounds read by lane.
-struct TileCtx {
-    Scene s;
-    G g;
-    Cam cam;
-    float* fb;
-    uint64_t seed;
-    float alpha, off;
-    uint32_t spp;
-    int32_t image_id, mode;
-    float px[32], py[32], pz[32], nx[32], ny[32], nz[32];
-    uint32_t pix[32];
-};
-
-// Persistent traversal over the 32-pixel tiles of all jobs.  A warp takes a tile from
-// the work counter, traces its camera rays (closest hit), then either shades them
-// (primary mode, as k_render_primary) or traces the AO samples of its hit pixels in
-// rounds of 32: item i of a round is sample (i mod spp) of the (i / spp)-th hit pixel.
-// The sample's PCG32 stream, direction, origin and radius are those of k_ao_samples,
-// and the unoccluded count of each pixel is summed from the round ballots in the
-// owning lane's register.
-template <bool STATS>
-__global__ __launch_bounds__(kJobTT, HR_JOB_MIN_BLOCKS) void k_trace_jobs(const Job* __restrict__ jobs,
-                                                        const uint32_t* __restrict__ tile_off, uint32_t njobs,
-                                                        uint32_t* work, int32_t tile_w,
-                                                        unsigned long long* counter) {
-    __shared__ TileCtx s_tile[kJobTT / 32];
-    TileCtx& T = s_tile[threadIdx.x >> 5];
-    const uint32_t lane = threadIdx.x & 31u;
-    const uint32_t ntiles = __ldg(tile_off + njobs);
-    const uint32_t tw = (uint32_t)tile_w, th = 32u / tw;
-    while (true) {
-        uint32_t tile = 0;
-        if (lane == 0) tile = atomicAdd(work, 1u);
-        tile = __shfl_sync(kFullMask, tile, 0);
-        if (tile >= ntiles) break;
-        const uint32_t j = find_segment(tile_off, njobs, tile);
-        if (lane == 0) {
-            const Job* J = jobs + j;
-            T.s.tris = J->tris;
-            T.s.cells = J->cells + (J->cells_offset ? __ldg(J->cells_offset) : 0u);
-            T.s.leaves = J->leaves;
-            T.s.prims = J->prims;
-            T.s.desc = J->desc;
-            T.s.ntri = J->ntri;
-            T.s.kind = J->kind;
-            T.g = load_g(J->desc);
-            T.cam = J->cam;
-            T.fb = J->fb;
-            T.seed = J->seed;
-            T.spp = (uint32_t)J->spp;
-            T.image_id = J->image_id;
-            T.mode = J->mode;
-            float alpha = J->alpha_abs;
-            if (!(alpha > 0.0f)) {
-                const f3 dd = mk(T.g.bmax[0] - T.g.bmin[0], T.g.bmax[1] - T.g.bmin[1], T.g.bmax[2] - T.g.bmin[2]);
-                alpha = J->alpha_frac * sqrtf(dot(dd, dd));
-            }
-            T.alpha = alpha;
-            T.off = 0.01f * alpha;
-        }
-        __syncwarp();
-        const uint32_t lt = tile - __ldg(tile_off + j);
-        const uint32_t cw = (uint32_t)T.cam.w, chh = (uint32_t)T.cam.h;
-        const uint32_t tx = (cw + tw - 1u) / tw;
-        const uint32_t x = (lt % tx) * tw + lane % tw, y = (lt / tx) * th + lane / tw;
-        const bool valid = x < cw && y < chh;
-        const uint32_t pix = valid ? y * cw + x : 0u;
-        const f3 o = mk(T.cam.pos[0], T.cam.pos[1], T.cam.pos[2]);
-        const f3 d = valid ? primary_dir(T.cam, pix) : mk(1.0f, 0.0f, 0.0f);
-        float* fb = T.fb + 3 * (size_t)pix;
-        Hit h;
-        trace_tl_job<false, STATS>(T.s, T.g, o, d, FLT_MAX, h, valid);
-        add_rays<STATS>(counter, false, valid ? 1u : 0u, h.cells, h.tests);
-        if (T.mode != HR_RENDER_AO) {
-            // primary shading (SimpleIntegrator.h:41-126), as k_render_primary
-            if (valid) {
-                float r = 0.15f, gg = 0.2f, b = 0.3f;
-                if (h.hit) {
-                    const f3 nrm = face_normal(T.s, h.tri, d);
-                    const float cs = fabsf(dot(nrm, d));
-                    r = (1.0f - h.u - h.v) * cs; gg = h.u * cs; b = h.v * cs;
-                }
-                fb[0] = blend(fb[0], r, T.image_id);
-                fb[1] = blend(fb[1], gg, T.image_id);
-                fb[2] = blend(fb[2], b, T.image_id);
-            }
-            __syncwarp();
-            continue;
-        }
-        // ambient occlusion (AOIntegrator.h:234-351) for the hit pixels of the tile
-        const bool hit = valid && h.hit;
-        if (valid && !hit) {
-            const float val = blend(fb[0], 1.0f, T.image_id);
-            fb[0] = val; fb[1] = val; fb[2] = val;
-        }
-        const uint32_t m = __ballot_sync(kFullMask, hit);
-        if (m == 0u) {
-            __syncwarp();
-            continue;
-        }
-        if (hit) {
-            const f3 p = mk(o.x + h.t * d.x, o.y + h.t * d.y, o.z + h.t * d.z);
-            const f3 nrm = face_normal(T.s, h.tri, d);
-            T.px[lane] = p.x; T.py[lane] = p.y; T.pz[lane] = p.z;
-            T.nx[lane] = nrm.x; T.ny[lane] = nrm.y; T.nz[lane] = nrm.z;
-            T.pix[lane] = pix;
-        }
-        __syncwarp();
-        const uint32_t spp = T.spp;
-        const uint32_t rank = __popc(m & ((1u << lane) - 1u));
-        const uint32_t total = (uint32_t)__popc(m) * spp;
-        uint32_t unocc = 0;
-        for (uint32_t base = 0; base < total; base += 32u) {
-            const uint32_t item = base + lane;
-            const bool v2 = item < total;
-            f3 ao = mk(0.0f, 0.0f, 0.0f), w = mk(1.0f, 0.0f, 0.0f);
-            if (v2) {
-                const uint32_t q = item / spp, k = item - q * spp;
-                const uint32_t src = nth_set_bit(m, q);
-                Pcg32 rng;
-                pcg_seed(rng, ((uint64_t)(uint32_t)T.image_id << 32) | T.pix[src], T.seed);
-                for (uint32_t i = 0; i < 2u * k; ++i) pcg_next(rng);
-                const float u1 = pcg_float(rng), u2 = pcg_float(rng);
-                w = cosine_dir(mk(T.nx[src], T.ny[src], T.nz[src]), u1, u2);
-                const float off = T.off;
-                ao = mk(T.px[src] + off * w.x, T.py[src] + off * w.y, T.pz[src] + off * w.z);
-            }
-            Hit hs;
-            trace_tl_job<true, STATS>(T.s, T.g, ao, w, T.alpha, hs, v2);
-            const uint32_t fm = __ballot_sync(kFullMask, v2 && !hs.hit);
-            if (hit) {
-                // this lane's samples are items [rank * spp, rank * spp + spp)
-                const int32_t lo = max((int32_t)(rank * spp) - (int32_t)base, 0);
-                const int32_t hi = min((int32_t)(rank * spp + spp) - (int32_t)base, 32);
-                if (hi > lo) {
-                    const uint32_t span = (uint32_t)(hi - lo);
-                    const uint32_t rm = (span == 32u ? 0xffffffffu : ((1u << span) - 1u)) << lo;
-                    unocc += __popc(fm & rm);
-                }
-            }
-            add_rays<STATS>(counter, true, v2 ? 1u : 0u, hs.cells, hs.tests);
-        }
-        if (hit) {
-            const float vis = (float)unocc / (float)spp;
-            const float val = blend(fb[0], vis, T.image_id);
-            fb[0] = val; fb[1] = val; fb[2] = val;
-        }
-        __syncwarp();   // the tile context is rewritten for the next tile
-    }
-}
-
 template <class T>
 T* dev(const DevBuf& b) { return b.as<T>(); }
 
@@ -664,13 +451,13 @@ int upload_jobs(hr_batch* b, int32_t image_id) {
         J.fb = dev<float>(b->d_fb) + 3 * b->px_off[i];
         const Camera& k = b->cams[i];
         for (int q = 0; q < 3; ++q) {
-            J.cam.pos[q] = k.pos[q]; J.cam.tl[q] = k.top_left[q]; J.cam.sx[q] = k.step_x[q]; J.cam.sy[q] = k.step_y[q];
+            J.cam_pos[q] = k.pos[q]; J.cam_tl[q] = k.top_left[q]; J.cam_sx[q] = k.step_x[q]; J.cam_sy[q] = k.step_y[q];
         }
-        J.cam.w = k.w;
-        J.cam.h = k.h;
+        J.w = k.w;
+        J.h = k.h;
         J.ntri = b->sc[i].ntri;
         J.kind = kTwoLevel;
-        J.mode = b->spp[i] > 0 ? HR_RENDER_AO : HR_RENDER_PRIMARY;
+        J.mode = b->spp[i] > 0 ? kJobAO : kJobPrimary;
         J.spp = b->spp[i];
         J.image_id = image_id;
         J.alpha_frac = b->alpha_frac;
@@ -688,10 +475,12 @@ int upload_jobs(hr_batch* b, int32_t image_id) {
 int upload_tiles(hr_batch* b) {
     hr_ctx* c = b->c;
     std::vector<uint32_t> off(b->nsc + 1, 0u);
-    const uint32_t tw = (uint32_t)b->tile_w, th = 32u / tw;
     for (uint32_t i = 0; i < b->nsc; ++i) {
-        const uint32_t w = (uint32_t)b->cams[i].w, h = (uint32_t)b->cams[i].h;
-        off[i + 1] = off[i] + ((w + tw - 1) / tw) * ((h + th - 1) / th);
+        Job j{};
+        j.mode = kJobAO;
+        j.w = b->cams[i].w;
+        j.h = b->cams[i].h;
+        off[i + 1] = off[i] + job_tiles(j, b->tile_w);
     }
     b->ntiles = off[b->nsc];
     int rc;
@@ -699,12 +488,7 @@ int upload_tiles(hr_batch* b) {
     if ((rc = cuda_check(c, cudaMemcpyAsync(b->d_tile_off.p, off.data(), sizeof(uint32_t) * (b->nsc + 1),
                                             cudaMemcpyHostToDevice, c->stream), "batch tiles")))
         return rc;
-    int nb = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_trace_jobs<false>, b->block_threads, 0) != cudaSuccess) {
-        cudaGetLastError();
-        nb = 1024 / b->block_threads;
-    }
-    b->persist_blocks = std::max(1, nb) * c->num_sms;
+    b->persist_blocks = job_blocks_per_sm(b->block_threads, false) * c->num_sms;
     return cuda_check(c, cudaStreamSynchronize(c->stream), "batch tiles");
 }
 
@@ -713,11 +497,8 @@ int enqueue_render(hr_batch* b) {
     cudaStream_t s = c->stream;
     int rc;
     if ((rc = cuda_check(c, cudaMemsetAsync(b->d_work.p, 0, sizeof(uint32_t), s), "batch work reset"))) return rc;
-    c->launches += 1;
-    k_trace_jobs<false><<<b->persist_blocks, b->block_threads, 0, s>>>(
-        dev<Job>(b->d_jobs), dev<uint32_t>(b->d_tile_off), b->nsc, dev<uint32_t>(b->d_work), b->tile_w,
-        c->counters.as<unsigned long long>());
-    return cuda_check(c, cudaGetLastError(), "batch render launch");
+    return launch_jobs(c, dev<Job>(b->d_jobs), dev<uint32_t>(b->d_tile_off), b->nsc, dev<uint32_t>(b->d_work),
+                       b->tile_w, b->block_threads, b->persist_blocks, false, s);
 }
 
 // one step's work on the stream: build, render, totals to pinned host memory
@@ -1025,7 +806,7 @@ hr_status hr_batch_set_densities(hr_batch* b, uint32_t scene, float top, float l
 
 hr_status hr_batch_set_launch(hr_batch* b, int32_t block_threads, int32_t tile_w) {
     if (!valid_batch(b)) return HR_ERR_INVALID_ARG;
-    if (block_threads < 32 || block_threads > kJobTT || block_threads % 32 != 0 || tile_w < 1 || tile_w > 32 ||
+    if (block_threads < 32 || block_threads > 256 || block_threads % 32 != 0 || tile_w < 1 || tile_w > 32 ||
         (tile_w & (tile_w - 1)) != 0)
         return (hr_status)set_error(b->c, HR_ERR_INVALID_ARG, "batch: launch shape %d threads, tile width %d",
                                     block_threads, tile_w);

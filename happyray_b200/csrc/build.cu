@@ -249,8 +249,10 @@ int radix_passes(int key_bits) { return (key_bits + 7) / 8; }
 
 }  // namespace
 
-// Host orchestration of one build.  Returns HR status code (0 = ok).
-static int build_once(hr_ctx* c, int32_t kind, int32_t exact, uint32_t* ovf_out) {
+// Host orchestration of one build.  With wait, syncs and reports the overflow bits in
+// *ovf_out; without, only enqueues (the descriptor lands in c->desc_pinned when the stream
+// has passed the build).  Returns HR status code (0 = ok).
+static int build_once(hr_ctx* c, int32_t kind, int32_t exact, uint32_t* ovf_out, bool wait) {
     cudaStream_t s = c->stream;
     GridBuffers& B = c->g;
     const uint32_t ntri = c->ntri;
@@ -378,6 +380,14 @@ static int build_once(hr_ctx* c, int32_t kind, int32_t exact, uint32_t* ovf_out)
     }
     c->nstages = ev;
     if ((rc = cuda_check(c, cudaGetLastError(), "build launch"))) return rc;
+    if (!wait) {
+        if (!c->desc_pinned && cudaMallocHost((void**)&c->desc_pinned, sizeof(GridDesc)) != cudaSuccess) {
+            cudaGetLastError();
+            return set_error(c, 2, "pinned descriptor allocation failed");
+        }
+        return cuda_check(c, cudaMemcpyAsync(c->desc_pinned, d, sizeof(GridDesc), cudaMemcpyDeviceToHost, s),
+                          "descriptor download");
+    }
     if ((rc = cuda_check(c, cudaMemcpyAsync(&c->host_desc, d, sizeof(GridDesc), cudaMemcpyDeviceToHost, s),
                          "descriptor download")))
         return rc;
@@ -389,29 +399,60 @@ static int build_once(hr_ctx* c, int32_t kind, int32_t exact, uint32_t* ovf_out)
     return 0;
 }
 
+// grow what overflowed from the exact sizes the device computed
+static void grow_caps(hr_ctx* c, const GridDesc& hd, uint32_t ovf) {
+    GridBuffers& B = c->g;
+    if (ovf & kOvfCells) B.cap_cells = (size_t)hd.req_cells + 64u;
+    if (ovf & (kOvfPairs | kOvfTopPairs)) B.cap_pairs = (size_t)(hd.req_pairs * 1.25) + 4096u;
+    if (ovf & kOvfLeaves) B.cap_leaves = (size_t)(hd.nleaves * 1.25) + 4096u;
+    if (ovf & kOvfLeafPairs) B.cap_leaf_pairs = (size_t)(hd.req_leaf_pairs * 1.25) + 4096u;
+}
+
 int build_grid(hr_ctx* c, int32_t kind, int32_t exact) {
     GridBuffers& B = c->g;
     if (c->built_kind != kind) {
         B.cap_pairs = 0; B.cap_leaf_pairs = 0; B.cap_leaves = 0;
     }
+    c->async_pending = false;
     for (int attempt = 0; attempt < 6; ++attempt) {
         uint32_t ovf = 0;
-        int rc = build_once(c, kind, exact, &ovf);
+        int rc = build_once(c, kind, exact, &ovf, true);
         if (rc) return rc;
-        const GridDesc& hd = c->host_desc;
         if (ovf == 0) {
             c->built_kind = kind;
             c->built = true;
             c->lerp_pending = false;
             return 0;
         }
-        // grow what overflowed from the exact sizes the device computed, and rebuild
-        if (ovf & kOvfCells) B.cap_cells = (size_t)hd.req_cells + 64u;
-        if (ovf & (kOvfPairs | kOvfTopPairs)) B.cap_pairs = (size_t)(hd.req_pairs * 1.25) + 4096u;
-        if (ovf & kOvfLeaves) B.cap_leaves = (size_t)(hd.nleaves * 1.25) + 4096u;
-        if (ovf & kOvfLeafPairs) B.cap_leaf_pairs = (size_t)(hd.req_leaf_pairs * 1.25) + 4096u;
+        grow_caps(c, c->host_desc, ovf);
     }
     return set_error(c, 3, "grid build: capacity did not converge");
+}
+
+int build_grid_async(hr_ctx* c, int32_t kind, int32_t exact) {
+    if (c->built_kind != kind) return build_grid(c, kind, exact);   // a new kind is sized synchronously
+    uint32_t ovf = 0;
+    int rc = build_once(c, kind, exact, &ovf, false);
+    if (rc) return rc;
+    c->built = true;
+    c->lerp_pending = false;
+    c->async_pending = true;
+    return 0;
+}
+
+int build_async_result(hr_ctx* c, bool* fit) {
+    *fit = true;
+    if (!c->async_pending) return 0;
+    c->async_pending = false;
+    c->host_desc = *c->desc_pinned;
+    if (c->host_desc.error) return set_error(c, 1, "triangle index out of range of the uploaded vertices");
+    const uint32_t ovf = c->host_desc.overflow;
+    if (ovf) {
+        *fit = false;
+        c->built = false;
+        grow_caps(c, c->host_desc, ovf);
+    }
+    return 0;
 }
 
 }  // namespace hr

@@ -213,6 +213,7 @@ void hr_destroy(hr_ctx* c) {
     for (auto& e : c->ev) if (e) cudaEventDestroy(e);
     for (auto& e : c->rev) if (e) cudaEventDestroy(e);
     if (c->pinned) cudaFreeHost(c->pinned);
+    if (c->desc_pinned) cudaFreeHost(c->desc_pinned);
     if (c->own_stream) cudaStreamDestroy(c->stream);
     delete c;
 }

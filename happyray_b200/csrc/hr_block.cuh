@@ -49,3 +49,16 @@ __device__ __forceinline__ T block_excl_scan(T x, T* total) {
 
 
 }  // namespace hr
+
+namespace hr {
+// largest s in [0, n) with off[s] <= x, for ascending off with off[0] = 0
+__device__ __forceinline__ uint32_t find_segment(const uint32_t* __restrict__ off, uint32_t n, uint32_t x) {
+    uint32_t lo = 0, hi = n;
+    while (hi - lo > 1u) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (__ldg(off + mid) <= x) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+}  // namespace hr

@@ -88,6 +88,8 @@ struct hr_ctx {
     bool built = false;
     hr::GridBuffers g;
     hr::GridDesc host_desc{};    // last downloaded descriptor
+    hr::GridDesc* desc_pinned = nullptr;   // descriptor of an asynchronous build (pinned)
+    bool async_pending = false;  // an asynchronous build awaits build_async_result
     hr::DevBuf counters;         // uint64 ray counters
     uint64_t launches = 0;       // kernels enqueued by this context (host-side count)
     bool collect_stats = false;  // render kernels accumulate cells visited / triangle tests
@@ -130,6 +132,11 @@ struct DeviceGuard {
 
 // build.cu
 int build_grid(hr_ctx* c, int32_t kind, int32_t exact);
+// Enqueue one build with the current capacities and no host sync (a grid kind not built
+// before is built synchronously).  Once the stream has passed it, build_async_result
+// reports whether it fit; if not, the capacities are grown and the grid must be rebuilt.
+int build_grid_async(hr_ctx* c, int32_t kind, int32_t exact);
+int build_async_result(hr_ctx* c, bool* fit);
 
 // sort.cu
 int radix_sort_pairs(hr_ctx* c, const uint32_t* keys_in, const uint32_t* vals_in,
@@ -146,6 +153,47 @@ size_t scan_partials_words(size_t cap_count);
 // exceeds cap, ovf_bit is set in *ovf, the total to *d_req and *d_total becomes 0.
 int scan_block_sums(hr_ctx* c, uint32_t* sums, uint32_t n, uint32_t* d_total, uint32_t* ovf,
                     uint32_t cap, uint32_t ovf_bit, uint32_t* d_req, cudaStream_t s);
+
+// jobs.cu: persistent rendering of many jobs (batched and served forms).  One job is a
+// grid, a camera or a ray list, an integrator and an output; the kernel's warps take
+// 32-pixel (32-ray) tiles of any job from one work counter.
+enum : int32_t { kJobPrimary = 0, kJobPath = 1, kJobAO = 3, kJobRays = 16 };
+struct Job {
+    const float4* tris;              // per-triangle vertices of the grid's mesh
+    const uint2* cells;
+    const uint2* leaves;
+    const uint32_t* prims;
+    const GridDesc* desc;
+    const uint32_t* cells_offset;    // nullable: added to cells (grids of one batch share arrays)
+    float* fb;                       // render jobs: float RGB per pixel
+    const float* org;                // ray jobs: 3 floats per ray
+    const float* dir;
+    int32_t* out_id;                 // ray jobs: closest hit (triangle id or -1), t, u, v
+    float* out_t;
+    float* out_u;
+    float* out_v;
+    float cam_pos[3], cam_tl[3], cam_sx[3], cam_sy[3];
+    int32_t w, h;                    // render jobs: image size; ray jobs: w = ray count
+    float light_c[3], light_e1[3], light_e2[3];
+    float light_emission;
+    uint32_t ntri;
+    int32_t kind;                    // kTwoLevel
+    int32_t mode;                    // kJob*
+    int32_t spp;                     // AO samples per hit pixel, or paths per pixel
+    int32_t image_id;                // first image id (progressive blend weight 1 / (id + 1))
+    int32_t bounces;
+    float albedo, alpha_frac, alpha_abs, eps_frac;
+    uint64_t seed;
+};
+// tiles of one job for tile width tw (32 / tw rows)
+uint32_t job_tiles(const Job& j, int32_t tw);
+// resident blocks per SM of the job kernel for a block size (pt: the path-tracing variant)
+int job_blocks_per_sm(int32_t block_threads, bool pt);
+// launch the persistent job kernel over njobs jobs whose tile prefix sums are d_tile_off
+// (njobs + 1 entries); *d_work must be zero.  pt selects the variant for kJobPath jobs,
+// which runs only those; the other variant runs every other mode.
+int launch_jobs(hr_ctx* c, const Job* d_jobs, const uint32_t* d_tile_off, uint32_t njobs, uint32_t* d_work,
+                int32_t tile_w, int32_t block_threads, int32_t nblocks, bool pt, cudaStream_t s);
 
 // trace.cu
 int launch_trace_rays(hr_ctx* c, const float* org, const float* dir, uint32_t n, int32_t* id,

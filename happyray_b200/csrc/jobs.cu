@@ -1,0 +1,297 @@
+// jobs.cu -- persistent rendering of many jobs in one launch (batched and served forms).
+//
+// A job is one grid (two-level), a camera or a list of rays, an integrator and an output:
+//   kJobPrimary  camera rays, barycentric shading (SimpleIntegrator.h:41-126)
+//   kJobAO       camera rays + spp AO samples per hit (AOIntegrator.h:234-351)
+//   kJobPath     spp paths per pixel (PathTracer.h:41-372 structure), progressive blend
+//   kJobRays     closest hit of a ray list (SimpleRayTraverser.h:168-261 query form)
+// The reference runs one integrator over one scene per launch sequence; here the warps of
+// one persistent launch take 32-pixel (32-ray) tiles of any job from a global work
+// counter.  Every job's output is bit-identical to the per-scene kernels of trace.cu for
+// the same grid, camera, samples, seed and image ids: the per-pixel random streams, ray
+// construction and traversal are the same functions.
+#include "traverse.cuh"
+#include "../../include/happyray.h"
+
+namespace hr {
+namespace {
+
+constexpr int kJobTT = 256;   // largest block of the persistent kernel
+#ifndef HR_JOB_MIN_BLOCKS
+#define HR_JOB_MIN_BLOCKS 3    // blocks of kJobTT per SM the register budget must allow (3: 80 registers)
+#endif
+
+// closest / any hit on a two-level grid (every job grid is two-level)
+template <bool ANY>
+__device__ __forceinline__ void trace_tl_job(const Scene& s, const G& g, f3 o, f3 d, float tmax, Hit& h, bool active) {
+    h.t = tmax; h.u = 0.0f; h.v = 0.0f; h.tri = 0; h.hit = false; h.cells = 0; h.tests = 0;
+    trace_tl<ANY, false>(s, g, o, d, h, active);
+}
+
+// position of the q-th (0-based) set bit of m; m has more than q set bits
+__device__ __forceinline__ uint32_t nth_set_bit(uint32_t m, uint32_t q) {
+    uint32_t pos = 0;
+#pragma unroll
+    for (uint32_t step = 16; step > 0; step >>= 1) {
+        const uint32_t c = __popc(m & ((1u << step) - 1u));
+        if (q >= c) { q -= c; m >>= step; pos += step; }
+    }
+    return pos;
+}
+
+// Per-warp state of the tile being rendered, in shared memory: the job's scene, grid and
+// integrator parameters (which the per-scene kernels get from their launch parameters)
+// and the hit points of the tile's camera rays, which the AO rounds read by lane.
+struct TileCtx {
+    Scene s;
+    G g;
+    Cam cam;
+    PtConsts pk;
+    float* fb;
+    const float* org;
+    const float* dir;
+    int32_t* out_id;
+    float *out_t, *out_u, *out_v;
+    uint64_t seed;
+    float alpha, off;
+    uint32_t spp;
+    int32_t image_id, mode;
+    float px[32], py[32], pz[32], nx[32], ny[32], nz[32];
+    uint32_t pix[32];
+};
+
+__device__ __forceinline__ void load_tile_ctx(TileCtx& T, const Job* __restrict__ J) {
+    T.s.tris = J->tris;
+    T.s.cells = J->cells + (J->cells_offset ? __ldg(J->cells_offset) : 0u);
+    T.s.leaves = J->leaves;
+    T.s.prims = J->prims;
+    T.s.desc = J->desc;
+    T.s.ntri = J->ntri;
+    T.s.kind = J->kind;
+    T.g = load_g(J->desc);
+    for (int q = 0; q < 3; ++q) {
+        T.cam.pos[q] = J->cam_pos[q]; T.cam.tl[q] = J->cam_tl[q];
+        T.cam.sx[q] = J->cam_sx[q]; T.cam.sy[q] = J->cam_sy[q];
+    }
+    T.cam.w = J->w;
+    T.cam.h = J->h;
+    T.fb = J->fb;
+    T.org = J->org; T.dir = J->dir;
+    T.out_id = J->out_id; T.out_t = J->out_t; T.out_u = J->out_u; T.out_v = J->out_v;
+    T.seed = J->seed;
+    T.spp = (uint32_t)J->spp;
+    T.image_id = J->image_id;
+    T.mode = J->mode;
+    float alpha = J->alpha_abs;
+    if (!(alpha > 0.0f)) {
+        const f3 dd = mk(T.g.bmax[0] - T.g.bmin[0], T.g.bmax[1] - T.g.bmin[1], T.g.bmax[2] - T.g.bmin[2]);
+        alpha = J->alpha_frac * sqrtf(dot(dd, dd));
+    }
+    T.alpha = alpha;
+    T.off = 0.01f * alpha;
+    if (J->mode == kJobPath) {
+        LightP l;
+        for (int q = 0; q < 3; ++q) { l.c[q] = J->light_c[q]; l.e1[q] = J->light_e1[q]; l.e2[q] = J->light_e2[q]; }
+        l.emission = J->light_emission;
+        T.pk = pt_consts(T.g, l, J->bounces, J->albedo, J->eps_frac);
+    }
+}
+
+// Persistent traversal over the tiles of all jobs.  A warp takes a tile from the work
+// counter and, by the job's mode:
+//   rays     traces 32 rays of the list (closest hit) and writes id, t, u, v;
+//   primary  traces the tile's camera rays and shades them as k_render_primary;
+//   AO       traces the camera rays, then the AO samples of the tile's hit pixels in
+//            rounds of 32: item i of a round is sample (i mod spp) of the (i / spp)-th
+//            hit pixel, with the PCG32 stream, direction, origin and radius of
+//            k_ao_samples; each pixel's unoccluded count is summed from the round ballots
+//            in its own lane's register;
+//   path     runs spp paths per pixel with pt_path, image ids image_id .. image_id +
+//            spp - 1, blended in that order as k_render_pt frames.
+// The PT variant runs path jobs only and the other variant every other mode: the host
+// launches them over disjoint ranges of the job table.
+template <bool PT>
+__global__ __launch_bounds__(kJobTT, HR_JOB_MIN_BLOCKS) void k_trace_jobs(const Job* __restrict__ jobs,
+                                                                        const uint32_t* __restrict__ tile_off,
+                                                                        uint32_t njobs, uint32_t* work,
+                                                                        int32_t tile_w,
+                                                                        unsigned long long* counter) {
+    __shared__ TileCtx s_tile[kJobTT / 32];
+    TileCtx& T = s_tile[threadIdx.x >> 5];
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t ntiles = __ldg(tile_off + njobs);
+    const uint32_t tw = (uint32_t)tile_w, th = 32u / tw;
+    while (true) {
+        uint32_t tile = 0;
+        if (lane == 0) tile = atomicAdd(work, 1u);
+        tile = __shfl_sync(kFullMask, tile, 0);
+        if (tile >= ntiles) break;
+        const uint32_t j = find_segment(tile_off, njobs, tile);
+        if (lane == 0) load_tile_ctx(T, jobs + j);
+        __syncwarp();
+        const uint32_t lt = tile - __ldg(tile_off + j);
+        if (PT) {
+            // path jobs only: spp paths per pixel, blended in image-id order
+            const uint32_t cw = (uint32_t)T.cam.w, chh = (uint32_t)T.cam.h;
+            const uint32_t tx = (cw + tw - 1u) / tw;
+            const uint32_t x = (lt % tx) * tw + lane % tw, y = (lt / tx) * th + lane / tw;
+            const bool valid = x < cw && y < chh;
+            const uint32_t pix = valid ? y * cw + x : 0u;
+            float* fb = T.fb + 3 * (size_t)pix;
+            float val = valid ? fb[0] : 0.0f;
+            PtCounts n;
+            for (uint32_t k = 0; k < T.spp; ++k) {
+                const int32_t im = T.image_id + (int32_t)k;
+                const float L = pt_path<false, true>(T.s, T.g, T.cam, T.pk, pix, valid, im, T.seed, n);
+                val = blend(val, L, im);
+            }
+            if (valid) { fb[0] = val; fb[1] = val; fb[2] = val; }
+            add_rays<false>(counter, false, n.rays);
+            add_rays<false>(counter, true, n.srays);
+            __syncwarp();
+            continue;
+        }
+        // one closest-hit call for ray-list and camera rays
+        const bool rays = T.mode == kJobRays;
+        bool valid;
+        uint32_t pix;
+        f3 o, d;
+        if (rays) {
+            pix = lt * 32u + lane;
+            valid = pix < (uint32_t)T.cam.w;
+            o = mk(0.0f, 0.0f, 0.0f);
+            d = mk(1.0f, 0.0f, 0.0f);
+            if (valid) {
+                o = mk(__ldg(T.org + 3 * (size_t)pix), __ldg(T.org + 3 * (size_t)pix + 1), __ldg(T.org + 3 * (size_t)pix + 2));
+                d = mk(__ldg(T.dir + 3 * (size_t)pix), __ldg(T.dir + 3 * (size_t)pix + 1), __ldg(T.dir + 3 * (size_t)pix + 2));
+            }
+        } else {
+            const uint32_t cw = (uint32_t)T.cam.w, chh = (uint32_t)T.cam.h;
+            const uint32_t tx = (cw + tw - 1u) / tw;
+            const uint32_t x = (lt % tx) * tw + lane % tw, y = (lt / tx) * th + lane / tw;
+            valid = x < cw && y < chh;
+            pix = valid ? y * cw + x : 0u;
+            o = mk(T.cam.pos[0], T.cam.pos[1], T.cam.pos[2]);
+            d = valid ? primary_dir(T.cam, pix) : mk(1.0f, 0.0f, 0.0f);
+        }
+        Hit h;
+        trace_tl_job<false>(T.s, T.g, o, d, FLT_MAX, h, valid);
+        add_rays<false>(counter, false, valid ? 1u : 0u);
+        if (rays) {
+            if (valid) {
+                T.out_id[pix] = h.hit ? (int32_t)h.tri : -1;
+                T.out_t[pix] = h.hit ? h.t : FLT_MAX;
+                T.out_u[pix] = h.u;
+                T.out_v[pix] = h.v;
+            }
+            __syncwarp();
+            continue;
+        }
+        float* fb = T.fb + 3 * (size_t)pix;
+        if (T.mode != kJobAO) {
+            if (valid) {
+                float r = 0.15f, gg = 0.2f, b = 0.3f;
+                if (h.hit) {
+                    const f3 nrm = face_normal(T.s, h.tri, d);
+                    const float cs = fabsf(dot(nrm, d));
+                    r = (1.0f - h.u - h.v) * cs; gg = h.u * cs; b = h.v * cs;
+                }
+                fb[0] = blend(fb[0], r, T.image_id);
+                fb[1] = blend(fb[1], gg, T.image_id);
+                fb[2] = blend(fb[2], b, T.image_id);
+            }
+            __syncwarp();
+            continue;
+        }
+        const bool hit = valid && h.hit;
+        if (valid && !hit) {
+            const float val = blend(fb[0], 1.0f, T.image_id);
+            fb[0] = val; fb[1] = val; fb[2] = val;
+        }
+        const uint32_t m = __ballot_sync(kFullMask, hit);
+        if (m == 0u) {
+            __syncwarp();
+            continue;
+        }
+        if (hit) {
+            const f3 p = mk(o.x + h.t * d.x, o.y + h.t * d.y, o.z + h.t * d.z);
+            const f3 nrm = face_normal(T.s, h.tri, d);
+            T.px[lane] = p.x; T.py[lane] = p.y; T.pz[lane] = p.z;
+            T.nx[lane] = nrm.x; T.ny[lane] = nrm.y; T.nz[lane] = nrm.z;
+            T.pix[lane] = pix;
+        }
+        __syncwarp();
+        const uint32_t spp = T.spp;
+        const uint32_t rank = __popc(m & ((1u << lane) - 1u));
+        const uint32_t total = (uint32_t)__popc(m) * spp;
+        uint32_t unocc = 0;
+        for (uint32_t base = 0; base < total; base += 32u) {
+            const uint32_t item = base + lane;
+            const bool v2 = item < total;
+            f3 ao = mk(0.0f, 0.0f, 0.0f), w = mk(1.0f, 0.0f, 0.0f);
+            if (v2) {
+                const uint32_t q = item / spp, k = item - q * spp;
+                const uint32_t src = nth_set_bit(m, q);
+                Pcg32 rng;
+                pcg_seed(rng, ((uint64_t)(uint32_t)T.image_id << 32) | T.pix[src], T.seed);
+                for (uint32_t i = 0; i < 2u * k; ++i) pcg_next(rng);
+                const float u1 = pcg_float(rng), u2 = pcg_float(rng);
+                w = cosine_dir(mk(T.nx[src], T.ny[src], T.nz[src]), u1, u2);
+                const float off = T.off;
+                ao = mk(T.px[src] + off * w.x, T.py[src] + off * w.y, T.pz[src] + off * w.z);
+            }
+            Hit hs;
+            trace_tl_job<true>(T.s, T.g, ao, w, T.alpha, hs, v2);
+            const uint32_t fm = __ballot_sync(kFullMask, v2 && !hs.hit);
+            if (hit) {
+                // this lane's samples are items [rank * spp, rank * spp + spp)
+                const int32_t lo = max((int32_t)(rank * spp) - (int32_t)base, 0);
+                const int32_t hi = min((int32_t)(rank * spp + spp) - (int32_t)base, 32);
+                if (hi > lo) {
+                    const uint32_t span = (uint32_t)(hi - lo);
+                    const uint32_t rm = (span == 32u ? 0xffffffffu : ((1u << span) - 1u)) << lo;
+                    unocc += __popc(fm & rm);
+                }
+            }
+            add_rays<false>(counter, true, v2 ? 1u : 0u);
+        }
+        if (hit) {
+            const float vis = (float)unocc / (float)spp;
+            const float val = blend(fb[0], vis, T.image_id);
+            fb[0] = val; fb[1] = val; fb[2] = val;
+        }
+        __syncwarp();   // the tile context is rewritten for the next tile
+    }
+}
+
+}  // namespace
+
+uint32_t job_tiles(const Job& j, int32_t tw) {
+    if (j.mode == kJobRays) return ((uint32_t)j.w + 31u) / 32u;
+    const uint32_t th = 32u / (uint32_t)tw;
+    return (((uint32_t)j.w + (uint32_t)tw - 1u) / (uint32_t)tw) * (((uint32_t)j.h + th - 1u) / th);
+}
+
+int job_blocks_per_sm(int32_t block_threads, bool pt) {
+    int nb = 0;
+    cudaError_t e = pt ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_trace_jobs<true>, block_threads, 0)
+                       : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_trace_jobs<false>, block_threads, 0);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        nb = 0;
+    }
+    return nb > 0 ? nb : 1;
+}
+
+int launch_jobs(hr_ctx* c, const Job* d_jobs, const uint32_t* d_tile_off, uint32_t njobs, uint32_t* d_work,
+                int32_t tile_w, int32_t block_threads, int32_t nblocks, bool pt, cudaStream_t s) {
+    if (block_threads < 32 || block_threads > kJobTT || block_threads % 32 != 0)
+        return set_error(c, HR_ERR_INVALID_ARG, "jobs: block of %d threads", block_threads);
+    c->launches += 1;
+    unsigned long long* ctr = c->counters.as<unsigned long long>();
+    if (pt) k_trace_jobs<true><<<nblocks, block_threads, 0, s>>>(d_jobs, d_tile_off, njobs, d_work, tile_w, ctr);
+    else k_trace_jobs<false><<<nblocks, block_threads, 0, s>>>(d_jobs, d_tile_off, njobs, d_work, tile_w, ctr);
+    return cuda_check(c, cudaGetLastError(), "jobs launch");
+}
+
+}  // namespace hr

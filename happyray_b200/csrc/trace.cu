@@ -222,89 +222,28 @@ __global__ void k_ao_finish(const uint32_t* __restrict__ queue, const uint32_t* 
     }
 }
 
-// mode 1/2: path tracing with next-event estimation (PathTracer.h:41-372 structure).  The
-// bounce loop runs the same number of iterations on every lane (finished paths pass
-// active = false), so the warp-synchronous traversal can be called inside it.
+// mode 1/2: path tracing with next-event estimation (PathTracer.h:41-372 structure), one
+// path per pixel (pt_path in traverse.cuh).
 template <bool STATS>
 __global__ __launch_bounds__(kTT, 8) void k_render_pt(Scene s, Cam cam, LightP l, int32_t bounces, float albedo,
                                                    float eps_frac, uint64_t seed, int32_t image_id,
                                                    float* __restrict__ fb, unsigned long long* counter) {
     const G g = load_g(s.desc);
-    const f3 dd = mk(g.bmax[0] - g.bmin[0], g.bmax[1] - g.bmin[1], g.bmax[2] - g.bmin[2]);
-    const float ray_eps = eps_frac * sqrtf(dot(dd, dd));
-    const f3 lc = mk(l.c[0], l.c[1], l.c[2]), le1 = mk(l.e1[0], l.e1[1], l.e1[2]), le2 = mk(l.e2[0], l.e2[1], l.e2[2]);
-    const f3 lcr = cross(le1, le2);
-    const float larea = sqrtf(dot(lcr, lcr));
-    const float a_pi = albedo * 0.318309886f;
+    const PtConsts k = pt_consts(g, l, bounces, albedo, eps_frac);
     const uint32_t slots = tile_slots(cam);
     for (uint32_t slot = blockIdx.x * kTT + threadIdx.x; slot < slots; slot += gridDim.x * kTT) {
-        uint32_t pix, rays = 0, ncell = 0, ntest = 0, srays = 0, scell = 0, stest = 0;
+        uint32_t pix;
         const bool valid = tile_pixel(cam, slot, &pix);
-        bool alive = valid;
-        Pcg32 rng;
-        pcg_seed(rng, ((uint64_t)(uint32_t)image_id << 32) | (valid ? pix : 0u), seed);
-        f3 o = mk(cam.pos[0], cam.pos[1], cam.pos[2]);
-        f3 d = valid ? primary_dir(cam, pix) : mk(1.0f, 0.0f, 0.0f);
-        float L = 0.0f, beta = 1.0f;
-        for (int32_t bounce = 0; bounce < bounces; ++bounce) {
-            Hit h;
-            trace_one<false, STATS>(s, g, o, d, FLT_MAX, h, alive);
-            bool shadow = false;
-            f3 p = mk(0.0f, 0.0f, 0.0f), nrm = mk(0.0f, 0.0f, 1.0f), wi = mk(0.0f, 0.0f, 1.0f), so = p;
-            float dist = 0.0f, dist2 = 1.0f, cos_s = 0.0f, cos_l = 0.0f;
-            if (alive) {
-                rays += 1;
-                ncell += h.cells;
-                ntest += h.tests;
-                if (bounce == 0 && d.z > 0.0f) {
-                    const float tl = (lc.z - o.z) / d.z;
-                    const float px = o.x + tl * d.x, py = o.y + tl * d.y;
-                    const float fx = (px - lc.x) / le1.x, fy = (py - lc.y) / le2.y;
-                    if (tl > kIsectEps && tl < h.t && fx >= 0.0f && fx <= 1.0f && fy >= 0.0f && fy <= 1.0f) {
-                        L = L + l.emission;
-                        alive = false;
-                    }
-                }
-                if (alive && !h.hit) alive = false;
-                if (alive) {
-                    p = mk(o.x + h.t * d.x, o.y + h.t * d.y, o.z + h.t * d.z);
-                    nrm = face_normal(s, h.tri, d);
-                    const float u1 = pcg_float(rng), u2 = pcg_float(rng);
-                    const f3 lp = mk(lc.x + u1 * le1.x + u2 * le2.x, lc.y + u1 * le1.y + u2 * le2.y,
-                                     lc.z + u1 * le1.z + u2 * le2.z);
-                    wi = sub(lp, p);
-                    dist2 = dot(wi, wi);
-                    dist = sqrtf(dist2);
-                    wi = mulf(wi, 1.0f / dist);
-                    cos_s = dot(nrm, wi);
-                    cos_l = wi.z;
-                    shadow = cos_s > 0.0f && cos_l > 0.0f;
-                    so = mk(p.x + ray_eps * wi.x, p.y + ray_eps * wi.y, p.z + ray_eps * wi.z);
-                }
-            }
-            Hit hs;
-            trace_one<true, STATS>(s, g, so, wi, dist - ray_eps, hs, shadow);
-            if (alive) {
-                if (shadow) {
-                    srays += 1;
-                    scell += hs.cells;
-                    stest += hs.tests;
-                    if (!hs.hit) L = L + beta * a_pi * l.emission * cos_s * cos_l * larea / dist2;
-                }
-                beta = beta * albedo;
-                const float u3 = pcg_float(rng), u4 = pcg_float(rng);
-                d = cosine_dir(nrm, u3, u4);
-                o = mk(p.x + ray_eps * d.x, p.y + ray_eps * d.y, p.z + ray_eps * d.z);
-            }
-        }
+        PtCounts n;
+        const float L = pt_path<STATS>(s, g, cam, k, pix, valid, image_id, seed, n);
         if (valid) {
             const float val = blend(fb[3 * (size_t)pix], L, image_id);
             fb[3 * (size_t)pix] = val;
             fb[3 * (size_t)pix + 1] = val;
             fb[3 * (size_t)pix + 2] = val;
         }
-        add_rays<STATS>(counter, false, rays, ncell, ntest);
-        add_rays<STATS>(counter, true, srays, scell, stest);
+        add_rays<STATS>(counter, false, n.rays, n.cells, n.tests);
+        add_rays<STATS>(counter, true, n.srays, n.scells, n.stests);
     }
 }
 

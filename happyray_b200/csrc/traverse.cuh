@@ -423,5 +423,114 @@ __device__ __forceinline__ void add_rays(unsigned long long* counter, bool secon
 // warp-uniform bound of a 1-D grid-stride loop over n items
 __device__ __forceinline__ uint32_t round32(uint32_t n) { return (n + 31u) & ~31u; }
 
+// trace_one, or the two-level traversal alone when the grid is known to be two-level
+template <bool TL_ONLY, bool ANY, bool STATS>
+__device__ __forceinline__ void trace_kind(const Scene& s, const G& g, f3 o, f3 d, float tmax, Hit& h, bool active) {
+    if (TL_ONLY) {
+        h.t = tmax; h.u = 0.0f; h.v = 0.0f; h.tri = 0; h.hit = false; h.cells = 0; h.tests = 0;
+        trace_tl<ANY, STATS>(s, g, o, d, h, active);
+    } else {
+        trace_one<ANY, STATS>(s, g, o, d, tmax, h, active);
+    }
+}
+
+// constants of the path tracer for one grid and light
+struct PtConsts {
+    f3 lc, le1, le2;
+    float emission, larea, a_pi, albedo, ray_eps;
+    int32_t bounces;
+};
+__device__ __forceinline__ PtConsts pt_consts(const G& g, const LightP& l, int32_t bounces, float albedo,
+                                              float eps_frac) {
+    PtConsts k;
+    const f3 dd = mk(g.bmax[0] - g.bmin[0], g.bmax[1] - g.bmin[1], g.bmax[2] - g.bmin[2]);
+    k.ray_eps = eps_frac * sqrtf(dot(dd, dd));
+    k.lc = mk(l.c[0], l.c[1], l.c[2]);
+    k.le1 = mk(l.e1[0], l.e1[1], l.e1[2]);
+    k.le2 = mk(l.e2[0], l.e2[1], l.e2[2]);
+    const f3 lcr = cross(k.le1, k.le2);
+    k.larea = sqrtf(dot(lcr, lcr));
+    k.a_pi = albedo * 0.318309886f;
+    k.albedo = albedo;
+    k.emission = l.emission;
+    k.bounces = bounces;
+    return k;
+}
+
+struct PtCounts {
+    uint32_t rays = 0, cells = 0, tests = 0, srays = 0, scells = 0, stests = 0;
+};
+
+// One path of the path tracer (PathTracer.h:41-372 structure) from the centre of pixel
+// pix: camera ray against the quad light at bounce 0, then per bounce the closest hit,
+// one next-event sample of the light (u1, u2) with an any-hit shadow ray to
+// dist - ray_eps, and a cosine-weighted bounce (u3, u4) with throughput x albedo.  The
+// PCG32 stream is keyed by (image_id, pix) and seed.  Returns the radiance.  The bounce
+// loop runs the same number of iterations on every lane (finished paths pass
+// active = false), so the warp-synchronous traversal can be called inside it: all lanes
+// of the warp must call pt_path together.
+template <bool STATS, bool TL_ONLY = false>
+__device__ __forceinline__ float pt_path(const Scene& s, const G& g, const Cam& cam, const PtConsts& k, uint32_t pix,
+                                         bool valid, int32_t image_id, uint64_t seed, PtCounts& n) {
+    bool alive = valid;
+    Pcg32 rng;
+    pcg_seed(rng, ((uint64_t)(uint32_t)image_id << 32) | (valid ? pix : 0u), seed);
+    f3 o = mk(cam.pos[0], cam.pos[1], cam.pos[2]);
+    f3 d = valid ? primary_dir(cam, pix) : mk(1.0f, 0.0f, 0.0f);
+    float L = 0.0f, beta = 1.0f;
+    for (int32_t bounce = 0; bounce < k.bounces; ++bounce) {
+        Hit h;
+        trace_kind<TL_ONLY, false, STATS>(s, g, o, d, FLT_MAX, h, alive);
+        bool shadow = false;
+        f3 p = mk(0.0f, 0.0f, 0.0f), nrm = mk(0.0f, 0.0f, 1.0f), wi = mk(0.0f, 0.0f, 1.0f), so = p;
+        float dist = 0.0f, dist2 = 1.0f, cos_s = 0.0f, cos_l = 0.0f;
+        if (alive) {
+            n.rays += 1;
+            n.cells += h.cells;
+            n.tests += h.tests;
+            if (bounce == 0 && d.z > 0.0f) {
+                const float tl = (k.lc.z - o.z) / d.z;
+                const float px = o.x + tl * d.x, py = o.y + tl * d.y;
+                const float fx = (px - k.lc.x) / k.le1.x, fy = (py - k.lc.y) / k.le2.y;
+                if (tl > kIsectEps && tl < h.t && fx >= 0.0f && fx <= 1.0f && fy >= 0.0f && fy <= 1.0f) {
+                    L = L + k.emission;
+                    alive = false;
+                }
+            }
+            if (alive && !h.hit) alive = false;
+            if (alive) {
+                p = mk(o.x + h.t * d.x, o.y + h.t * d.y, o.z + h.t * d.z);
+                nrm = face_normal(s, h.tri, d);
+                const float u1 = pcg_float(rng), u2 = pcg_float(rng);
+                const f3 lp = mk(k.lc.x + u1 * k.le1.x + u2 * k.le2.x, k.lc.y + u1 * k.le1.y + u2 * k.le2.y,
+                                 k.lc.z + u1 * k.le1.z + u2 * k.le2.z);
+                wi = sub(lp, p);
+                dist2 = dot(wi, wi);
+                dist = sqrtf(dist2);
+                wi = mulf(wi, 1.0f / dist);
+                cos_s = dot(nrm, wi);
+                cos_l = wi.z;
+                shadow = cos_s > 0.0f && cos_l > 0.0f;
+                so = mk(p.x + k.ray_eps * wi.x, p.y + k.ray_eps * wi.y, p.z + k.ray_eps * wi.z);
+            }
+        }
+        Hit hs;
+        trace_kind<TL_ONLY, true, STATS>(s, g, so, wi, dist - k.ray_eps, hs, shadow);
+        if (alive) {
+            if (shadow) {
+                n.srays += 1;
+                n.scells += hs.cells;
+                n.stests += hs.tests;
+                if (!hs.hit) L = L + beta * k.a_pi * k.emission * cos_s * cos_l * k.larea / dist2;
+            }
+            beta = beta * k.albedo;
+            const float u3 = pcg_float(rng), u4 = pcg_float(rng);
+            d = cosine_dir(nrm, u3, u4);
+            o = mk(p.x + k.ray_eps * d.x, p.y + k.ray_eps * d.y, p.z + k.ray_eps * d.z);
+        }
+    }
+    return L;
+}
+
 }  // namespace
 }  // namespace hr

@@ -188,3 +188,61 @@ def batch_scenes(n_scenes: int = 256, seed: int = 0, tri_range=(1_000, 500_000),
             kind = "clusters"
         out.append(dict(v=v, f=f, cam=camera_at_bounds(v, (side, side)), kind=kind))
     return out
+
+
+def curl_keyframes_torch(verts: np.ndarray, n_keyframes: int = 16, amp: float = 0.02, octaves: int = 4,
+                         seed: int = 0, base_freq: float = 2.0, device: str = "cuda"):
+    """curl_keyframes evaluated with torch (float64) on `device`: the same waves and
+    formula, for large meshes (the bench's data generation, not the engine)."""
+    import torch
+    rng = np.random.default_rng(seed)
+    P = torch.from_numpy(verts.astype(np.float64)).to(device)
+    waves = []
+    for o in range(octaves):
+        f = base_freq * (2.0 ** o) * 2.0 * math.pi
+        for comp in range(3):
+            for _ in range(2):
+                kdir = rng.normal(size=3)
+                kdir /= np.linalg.norm(kdir)
+                waves.append((comp, f * kdir, rng.uniform(0, 2 * math.pi), int(rng.integers(1, 3)), 0.5 ** o))
+    frames = np.empty((n_keyframes,) + verts.shape, np.float32)
+    scale = None
+    for k in range(n_keyframes):
+        tau = k / n_keyframes
+        curl = torch.zeros_like(P)
+        for comp, kv, ph, om, a in waves:
+            kt = torch.tensor(kv, dtype=torch.float64, device=device)
+            arg = P @ kt + ph + 2.0 * math.pi * om * tau
+            g = a * torch.cos(arg)[:, None] * kt[None, :]
+            if comp == 0:
+                curl[:, 1] += g[:, 2]
+                curl[:, 2] -= g[:, 1]
+            elif comp == 1:
+                curl[:, 0] -= g[:, 2]
+                curl[:, 2] += g[:, 0]
+            else:
+                curl[:, 0] += g[:, 1]
+                curl[:, 1] -= g[:, 0]
+        if scale is None:
+            scale = amp / max(1e-12, float(torch.sqrt((curl ** 2).sum(1)).max()))
+        frames[k] = (P + scale * curl).float().cpu().numpy()
+    return frames
+
+
+def served_scenes(n_scenes: int = 64, seed: int = 0, tri_range=(10_000, 4_000_000), n_keyframes: int = 16,
+                  device: str | None = None):
+    """Served-workload pool: cluster scenes as the key-frame configuration, triangle counts
+    log-uniform in tri_range, n_keyframes curl-noise key frames each.  Returns
+    (keyframes [K, V, 3] float32, faces [N, 3] uint32) pairs."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n_scenes):
+        nt = int(round(math.exp(rng.uniform(math.log(tri_range[0]), math.log(tri_range[1])))))
+        sseed = int(rng.integers(0, 2**31 - 1))
+        v, f = clusters(nt, sseed)
+        if device:
+            kf = curl_keyframes_torch(v, n_keyframes, amp=0.02, octaves=4, seed=sseed, device=device)
+        else:
+            kf = curl_keyframes(v, n_keyframes, amp=0.02, octaves=4, seed=sseed)
+        out.append((kf, f))
+    return out

@@ -244,6 +244,81 @@ hr_status hr_batch_grid_download(hr_batch *batch, uint32_t scene, uint32_t *cell
  * `reps` graph replays of the current batch; applies and returns the fastest. */
 hr_status hr_batch_autotune(hr_batch *batch, int32_t reps, hr_batch_tuning *best);
 
+/* ---------------------------------------------------------------------------------
+ * Served rendering.  No counterpart in the reference (its CUDAApplication renders one
+ * scene per process, CUDAApplication.cu:116-160).  A server keeps animated scenes
+ * resident (key frames + the grid of one frame time each, hr_set_keyframes /
+ * hr_set_frame_time semantics) and answers render and ray-query requests from any host
+ * thread.  In HR_SERVER_BATCHED mode a worker thread admits queued requests (FIFO) while
+ * their buffers fit the HBM budget, groups them into waves (one frame time per scene per
+ * wave), rebuilds the grids of scenes whose frame time changed -- asynchronously, on the
+ * scene's own stream, after the last wave reading the old grid -- and traces every request
+ * of the wave in one persistent launch (rays batched across requests), with up to two
+ * waves in flight so that the next wave's admission, rebuilds and copies overlap the
+ * current one.  HR_SERVER_SERIAL runs the same requests one at a time through the
+ * per-scene path (hr_build + hr_render / hr_trace_rays), as a caller of the plain API
+ * would.  A request's result depends only on the request: it is bit-identical in both
+ * modes, alone or among others.
+ */
+typedef struct hr_server hr_server;
+#define HR_SERVER_BATCHED 0
+#define HR_SERVER_SERIAL 1
+#define HR_REQUEST_RENDER 0
+#define HR_REQUEST_RAYS 1
+
+typedef struct hr_request {
+    uint32_t scene;
+    float frame_time;             /* key-frame units, as hr_set_frame_time (step 0) */
+    int32_t kind;                 /* HR_REQUEST_RENDER or HR_REQUEST_RAYS */
+    /* render requests */
+    int32_t mode;                 /* HR_RENDER_PRIMARY, HR_RENDER_AO or HR_RENDER_PATH */
+    int32_t spp;                  /* AO samples per hit, or paths per pixel (image ids 0..spp-1) */
+    float cam_position[3], cam_orientation[3], cam_up[3];
+    float cam_fov_deg;
+    int32_t width, height;
+    uint64_t seed;
+    float *out_rgb;               /* host, 3 floats per pixel; pinned memory lets the copy overlap */
+    /* ray-query requests: closest hit of each ray (hr_trace_rays) */
+    const float *ray_org, *ray_dir;   /* host, 3 floats per ray */
+    uint32_t num_rays;
+    int32_t *out_id;
+    float *out_t, *out_u, *out_v;
+} hr_request;
+
+typedef struct hr_request_info {
+    int32_t status;               /* 0 queued, 1 in flight, 2 done, < 0 failed (-hr_status) */
+    uint32_t wave;                /* wave that traced it (batched mode) */
+    uint64_t submit_ns, admit_ns, done_ns;   /* steady-clock times */
+} hr_request_info;
+
+typedef struct hr_server_stats {
+    uint64_t completed, failed, waves, rebuilds, rays;
+    uint64_t resident_bytes;      /* scenes: key frames, grids, vertex arrays */
+    uint64_t peak_inflight_bytes; /* request buffers */
+    uint64_t launches;
+} hr_server_stats;
+
+hr_status hr_server_create(hr_server **out, int32_t device, uint64_t hbm_budget_bytes, int32_t mode);
+/* Finishes every queued request, then stops the worker and frees the scenes. */
+void hr_server_destroy(hr_server *server);
+const char *hr_server_last_error(const hr_server *server);
+/* Makes a scene resident: key frames (host, num_keyframes x num_vertices xyz) and
+ * triangles, two-level grid densities.  The grid capacities are sized by building every
+ * key frame once.  Fails with HR_ERR_OUT_OF_MEMORY above the budget.  Call before the
+ * first request of that scene. */
+hr_status hr_server_add_scene(hr_server *server, const float *keyframes_xyz, uint32_t num_keyframes,
+                              uint32_t num_vertices, const uint32_t *indices, uint32_t num_triangles,
+                              float top_density, float leaf_density, uint32_t *scene_id);
+/* Queues a request; the caller's buffers must stay valid until it is done. */
+hr_status hr_server_submit(hr_server *server, const hr_request *request, uint64_t *request_id);
+/* Waits until the request is done (HR_OK), failed (its error) or timeout_ms passed
+ * (HR_ERR_TIMEOUT; timeout_ms < 0 waits without limit). */
+hr_status hr_server_wait(hr_server *server, uint64_t request_id, int32_t timeout_ms);
+/* Waits until no request is queued or in flight. */
+hr_status hr_server_drain(hr_server *server, int32_t timeout_ms);
+hr_status hr_server_request_info(hr_server *server, uint64_t request_id, hr_request_info *info);
+hr_status hr_server_get_stats(hr_server *server, hr_server_stats *stats);
+
 #ifdef __cplusplus
 }
 #endif
