@@ -489,15 +489,17 @@ def serve_run(pool, reqs, mode, budget, seed=DEFAULT_SEED):
             "waves": int(s1["waves"] - s0["waves"]), "rebuilds": int(s1["rebuilds"] - s0["rebuilds"]),
             "failed": int(s1["failed"] - s0["failed"]), "peak_inflight_bytes": int(s1["peak_inflight_bytes"]),
             "resident_bytes": int(s1["resident_bytes"]), "launches": int(s1["launches"] - s0["launches"]),
+            "trace_ms": float(s1["trace_ms"] - s0["trace_ms"]),
             "scene_load_s": load_s}
 
 
 def run_served(args, rank, ws, local):
     """c5: served rendering (continuous batching over resident animated scenes) against
-    the serial per-scene path, on one replayed Poisson arrival schedule."""
+    the plain per-frame path and the serial per-scene path on resident scenes, on one
+    replayed Poisson arrival schedule."""
     import torch
     from happyray_b200 import scenes as S
-    from happyray_b200.server import BATCHED, SERIAL
+    from happyray_b200.server import BATCHED, PLAIN, SERIAL
     n_req = args.requests
     name = f"c5_served_64_scenes_{n_req}_requests_2000rps"
     if args.impl == "reference":
@@ -515,6 +517,7 @@ def run_served(args, rank, ws, local):
     with ClockSampler(local) as clk:
         served = serve_run(pool, reqs, BATCHED, budget)
         serial = serve_run(pool, reqs, SERIAL, budget)
+        plain = serve_run(pool, reqs, PLAIN, budget)
     if rank != 0:
         return
     line = {
@@ -526,7 +529,13 @@ def run_served(args, rank, ws, local):
                    "frame_times": "U[0,1) snapped to 120 per cycle", "resolution": "log-uniform 128^2..1024^2",
                    "spp": [1, 4, 16], "integrators": ["AO", "PT 4 bounces"], "hbm_budget_gb": 120,
                    "parallelism": f"replicas x{ws}"},
-        "served": served, "serial_path": serial, "speedup_vs_serial": served["mrays_s"] / serial["mrays_s"],
+        "served": served,
+        "plain_path": dict(plain, note="the drop-in per-frame path: one context; per request upload the two key "
+                                      "frames around the frame time, build, render, read back"),
+        "serial_resident_path": dict(serial, note="per-scene path one request at a time on the resident scenes "
+                                                  "(no batching, no overlap)"),
+        "speedup_vs_plain": served["mrays_s"] / plain["mrays_s"],
+        "speedup_vs_serial_resident": served["mrays_s"] / serial["mrays_s"],
         "p50_ms": served["p50_ms"], "p99_ms": served["p99_ms"],
         "timing": "wall clock from each request's submission to its completion (results in pinned host memory); "
                   "throughput = rays / (last completion - first submission)",

@@ -134,7 +134,7 @@ class ServerStats(C.Structure):
     """hr_server_stats"""
     _fields_ = [("completed", C.c_uint64), ("failed", C.c_uint64), ("waves", C.c_uint64), ("rebuilds", C.c_uint64),
                 ("rays", C.c_uint64), ("resident_bytes", C.c_uint64), ("peak_inflight_bytes", C.c_uint64),
-                ("launches", C.c_uint64)]
+                ("launches", C.c_uint64), ("trace_ms", C.c_double)]
 
 
 _lock = threading.Lock()

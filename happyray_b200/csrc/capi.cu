@@ -416,8 +416,10 @@ hr_status hr_render(hr_ctx* c, int32_t mode, int32_t image_id, float* fb) {
     DeviceGuard dg(c->device);
     const size_t bytes = (size_t)c->cam.w * c->cam.h * 3 * sizeof(float);
     if ((rc = ensure(c, c->fb, bytes))) return (hr_status)rc;
-    if (image_id > 0 && (rc = cuda_check(c, cudaMemcpyAsync(c->fb.p, fb, bytes, cudaMemcpyHostToDevice, c->stream), "fb upload")))
-        return (hr_status)rc;
+    // image 0 weighs the old content by 0: start from zeros (the reused buffer may hold anything)
+    if (image_id > 0) rc = cuda_check(c, cudaMemcpyAsync(c->fb.p, fb, bytes, cudaMemcpyHostToDevice, c->stream), "fb upload");
+    else rc = cuda_check(c, cudaMemsetAsync(c->fb.p, 0, bytes, c->stream), "fb clear");
+    if (rc) return (hr_status)rc;
     if ((rc = launch_render(c, mode, image_id, c->fb.as<float>()))) return (hr_status)rc;
     if ((rc = cuda_check(c, cudaMemcpyAsync(fb, c->fb.p, bytes, cudaMemcpyDeviceToHost, c->stream), "fb download")))
         return (hr_status)rc;

@@ -106,8 +106,9 @@ __device__ __forceinline__ void load_tile_ctx(TileCtx& T, const Job* __restrict_
 //            hit pixel, with the PCG32 stream, direction, origin and radius of
 //            k_ao_samples; each pixel's unoccluded count is summed from the round ballots
 //            in its own lane's register;
-//   path     runs spp paths per pixel with pt_path, image ids image_id .. image_id +
-//            spp - 1, blended in that order as k_render_pt frames.
+//   path     runs spp paths per pixel, image ids image_id .. image_id + spp - 1, blended in
+//            that order as k_render_pt frames; lanes regenerate paths (path_refill /
+//            path_step / path_retire) so a warp stays full across bounces and samples.
 // The PT variant runs path jobs only and the other variant every other mode: the host
 // launches them over disjoint ranges of the job table.
 template <bool PT>
@@ -121,6 +122,48 @@ __global__ __launch_bounds__(kJobTT, HR_JOB_MIN_BLOCKS) void k_trace_jobs(const 
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t ntiles = __ldg(tile_off + njobs);
     const uint32_t tw = (uint32_t)tile_w, th = 32u / tw;
+    if (PT) {
+        // path jobs: lanes regenerate paths (next sample of the pixel, or the next pixel of
+        // the warp's tiles); a tile of another job is taken once the warp's paths are done
+        constexpr uint32_t kNone = 0xffffffffu;
+        uint32_t cur_j = kNone, tile_local = 0, next = 32u, pend = kNone;
+        bool more = true;
+        PathLane ln;
+        PtCounts n;
+        while (true) {
+            while (more) {
+                if (next >= 32u) {
+                    if (pend == kNone) {
+                        uint32_t t = 0;
+                        if (lane == 0) t = atomicAdd(work, 1u);
+                        t = __shfl_sync(kFullMask, t, 0);
+                        if (t >= ntiles) {
+                            more = false;
+                            break;
+                        }
+                        pend = t;
+                    }
+                    const uint32_t j = find_segment(tile_off, njobs, pend);
+                    if (j != cur_j) {
+                        if (__any_sync(kFullMask, ln.has)) break;   // finish this job's paths first
+                        if (lane == 0) load_tile_ctx(T, jobs + j);
+                        __syncwarp();
+                        cur_j = j;
+                    }
+                    tile_local = pend - __ldg(tile_off + j);
+                    pend = kNone;
+                    next = 0;
+                }
+                if (path_refill(ln, T.cam, tile_local, &next, T.image_id, T.seed, T.fb) == 0u) break;
+            }
+            if (!__any_sync(kFullMask, ln.has)) break;   // the pool is dry and every path is done
+            const bool cont = path_step<false, true>(T.s, T.g, T.pk, ln.p, ln.has, n);
+            path_retire(ln, cont, T.cam, T.image_id, (int32_t)T.spp, T.seed, T.fb);
+        }
+        add_rays<false>(counter, false, n.rays);
+        add_rays<false>(counter, true, n.srays);
+        return;
+    }
     while (true) {
         uint32_t tile = 0;
         if (lane == 0) tile = atomicAdd(work, 1u);
@@ -130,27 +173,6 @@ __global__ __launch_bounds__(kJobTT, HR_JOB_MIN_BLOCKS) void k_trace_jobs(const 
         if (lane == 0) load_tile_ctx(T, jobs + j);
         __syncwarp();
         const uint32_t lt = tile - __ldg(tile_off + j);
-        if (PT) {
-            // path jobs only: spp paths per pixel, blended in image-id order
-            const uint32_t cw = (uint32_t)T.cam.w, chh = (uint32_t)T.cam.h;
-            const uint32_t tx = (cw + tw - 1u) / tw;
-            const uint32_t x = (lt % tx) * tw + lane % tw, y = (lt / tx) * th + lane / tw;
-            const bool valid = x < cw && y < chh;
-            const uint32_t pix = valid ? y * cw + x : 0u;
-            float* fb = T.fb + 3 * (size_t)pix;
-            float val = valid ? fb[0] : 0.0f;
-            PtCounts n;
-            for (uint32_t k = 0; k < T.spp; ++k) {
-                const int32_t im = T.image_id + (int32_t)k;
-                const float L = pt_path<false, true>(T.s, T.g, T.cam, T.pk, pix, valid, im, T.seed, n);
-                val = blend(val, L, im);
-            }
-            if (valid) { fb[0] = val; fb[1] = val; fb[2] = val; }
-            add_rays<false>(counter, false, n.rays);
-            add_rays<false>(counter, true, n.srays);
-            __syncwarp();
-            continue;
-        }
         // one closest-hit call for ray-list and camera rays
         const bool rays = T.mode == kJobRays;
         bool valid;

@@ -62,7 +62,10 @@ size_t ctx_bytes(const hr_ctx* c) {
 }
 
 struct SrvScene {
-    hr_ctx* ctx = nullptr;
+    hr_ctx* ctx = nullptr;           // resident scene (batched and serial modes)
+    std::vector<float> host_kf;      // plain mode: host key frames (xyz) and triangles
+    std::vector<uint32_t> host_idx;
+    float top = 0.0625f, leaf = 2.0f;   // grid densities
     uint32_t nverts = 0, ntri = 0, nkf = 0;
     float cur_time = -1.0f;          // frame time of the resident grid (< 0: none)
     uint64_t gen = 0;                // build generation of the resident grid
@@ -109,7 +112,8 @@ bool is_pinned(const void* p) {
 }  // namespace
 
 struct hr_server {
-    hr_ctx* c = nullptr;             // server stream, job-kernel ray counters, error text
+    hr_ctx* c = nullptr;             // server stream, job-kernel ray counters, error text;
+                                     // plain mode: the one context every request re-uploads into
     int32_t mode = HR_SERVER_BATCHED;
     uint64_t budget = 0;
     std::vector<std::unique_ptr<SrvScene>> scenes;
@@ -128,6 +132,9 @@ struct hr_server {
     uint32_t* h_tiles[kSlots] = {};
     bool slot_busy[kSlots] = {};
     cudaEvent_t wave_ev[kSlots] = {};
+    cudaEvent_t wave_start[kSlots] = {};   // before a wave's traversal launches
+    cudaEvent_t wave_trace_end[kSlots] = {};
+    double trace_ms = 0.0;
     int32_t max_jobs = 512;
     int32_t tile_w = 8, block_threads = 256;
     int blocks_main = 0, blocks_pt = 0;
@@ -266,11 +273,13 @@ int launch_wave(hr_server* S, Wave& w, std::map<uint32_t, float>& times) {
                          "tiles")) ||
         (rc = cuda_check(c, cudaMemsetAsync(dw, 0, 2 * sizeof(uint32_t), s), "work")))
         return rc;
+    cudaEventRecord(S->wave_start[w.slot], s);
     if (n_main && (rc = launch_jobs(c, dj, dt, n_main, dw, S->tile_w, S->block_threads, S->blocks_main, false, s)))
         return rc;
     if (n_pt && (rc = launch_jobs(c, dj + n_main, dt + tiles_pt0, n_pt, dw + 1, S->tile_w, S->block_threads,
                                   S->blocks_pt, true, s)))
         return rc;
+    cudaEventRecord(S->wave_trace_end[w.slot], s);
     for (auto& kv : times) {
         SrvScene& X = *S->scenes[kv.first];
         cudaEventRecord(X.last_read, s);
@@ -301,6 +310,9 @@ int launch_wave(hr_server* S, Wave& w, std::map<uint32_t, float>& times) {
 std::vector<uint64_t> retire_wave(hr_server* S, Wave& w) {
     hr_ctx* c = S->c;
     std::vector<uint64_t> redo;
+    float ms = 0.0f;
+    if (cudaEventElapsedTime(&ms, S->wave_start[w.slot], S->wave_trace_end[w.slot]) == cudaSuccess) S->trace_ms += ms;
+    cudaGetLastError();
     for (uint32_t sc : w.rebuilt) {
         SrvScene& X = *S->scenes[sc];
         bool fit = true;
@@ -332,17 +344,39 @@ std::vector<uint64_t> retire_wave(hr_server* S, Wave& w) {
     return redo;
 }
 
-// one request through the per-scene path (serial mode)
+int serve_on(hr_server* S, hr_ctx* c, SrvReq& R);
+
+// one request through the per-scene path: serial mode on the scene's resident context,
+// plain mode on the one context after uploading the request's frame (RTEngine::upload)
 int serve_serial(hr_server* S, SrvReq& R) {
     SrvScene& X = *S->scenes[R.r.scene];
-    hr_ctx* c = X.ctx;
     int rc;
+    if (S->mode == HR_SERVER_PLAIN) {
+        hr_ctx* c = S->c;
+        const uint32_t k = (uint32_t)R.r.frame_time;
+        const uint32_t k2 = (k + 1u) % X.nkf;
+        const float coeff = R.r.frame_time - (float)k;
+        const float* a = X.host_kf.data() + (size_t)k * X.nverts * 3;
+        const float* b = X.host_kf.data() + (size_t)k2 * X.nverts * 3;
+        if (hr_upload(c, a, b, X.nverts, X.host_idx.data(), X.ntri, coeff) != HR_OK) return HR_ERR_DEVICE;
+        hr_set_grid_densities(c, X.top, X.leaf);
+        if ((rc = build_grid(c, HR_GRID_TWO_LEVEL, 1))) return rc;
+        S->rebuilds += 1;
+        return serve_on(S, c, R);
+    }
+    hr_ctx* c = X.ctx;
     if (X.cur_time != R.r.frame_time) {
         if (hr_set_frame_time(c, R.r.frame_time, 0.0f) != HR_OK) return HR_ERR_INVALID_ARG;
         if ((rc = build_grid(c, HR_GRID_TWO_LEVEL, 1))) return rc;
         X.cur_time = R.r.frame_time;
         S->rebuilds += 1;
     }
+    return serve_on(S, c, R);
+}
+
+// render or ray query of one request on a context whose grid is built
+int serve_on(hr_server* S, hr_ctx* c, SrvReq& R) {
+    int rc;
     c->ip.seed = R.r.seed;
     if (R.r.kind == HR_REQUEST_RAYS) {
         const size_t n = R.r.num_rays;
@@ -387,7 +421,7 @@ void worker_main(hr_server* S) {
     std::unique_lock<std::mutex> lk(S->m);
     uint32_t next_slot = 0;
     while (true) {
-        if (S->mode == HR_SERVER_SERIAL) {
+        if (S->mode != HR_SERVER_BATCHED) {
             if (S->queue.empty()) {
                 if (S->stop) break;
                 S->cv_work.wait(lk, [&] { return S->stop || !S->queue.empty(); });
@@ -521,7 +555,8 @@ bool valid_server(const hr_server* s) { return s && s->c; }
 extern "C" {
 
 hr_status hr_server_create(hr_server** out, int32_t device, uint64_t budget, int32_t mode) {
-    if (!out || (mode != HR_SERVER_BATCHED && mode != HR_SERVER_SERIAL) || budget == 0) return HR_ERR_INVALID_ARG;
+    if (!out || (mode != HR_SERVER_BATCHED && mode != HR_SERVER_SERIAL && mode != HR_SERVER_PLAIN) || budget == 0)
+        return HR_ERR_INVALID_ARG;
     *out = nullptr;
     hr_server* S = new (std::nothrow) hr_server();
     if (!S) return HR_ERR_OUT_OF_MEMORY;
@@ -546,7 +581,8 @@ hr_status hr_server_create(hr_server** out, int32_t device, uint64_t budget, int
             break;
         if (cudaMallocHost((void**)&S->h_jobs[k], sizeof(Job) * S->max_jobs) != cudaSuccess ||
             cudaMallocHost((void**)&S->h_tiles[k], sizeof(uint32_t) * ntiles) != cudaSuccess ||
-            cudaEventCreateWithFlags(&S->wave_ev[k], cudaEventDisableTiming) != cudaSuccess) {
+            cudaEventCreateWithFlags(&S->wave_ev[k], cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreate(&S->wave_start[k]) != cudaSuccess || cudaEventCreate(&S->wave_trace_end[k]) != cudaSuccess) {
             cudaGetLastError();
             rc = HR_ERR_OUT_OF_MEMORY;
         }
@@ -575,12 +611,14 @@ void hr_server_destroy(hr_server* S) {
         for (auto& X : S->scenes) {
             if (X->last_read) cudaEventDestroy(X->last_read);
             if (X->built) cudaEventDestroy(X->built);
-            hr_destroy(X->ctx);
+            if (X->ctx) hr_destroy(X->ctx);
         }
         for (int k = 0; k < kSlots; ++k) {
             if (S->h_jobs[k]) cudaFreeHost(S->h_jobs[k]);
             if (S->h_tiles[k]) cudaFreeHost(S->h_tiles[k]);
             if (S->wave_ev[k]) cudaEventDestroy(S->wave_ev[k]);
+            if (S->wave_start[k]) cudaEventDestroy(S->wave_start[k]);
+            if (S->wave_trace_end[k]) cudaEventDestroy(S->wave_trace_end[k]);
             if (S->d_jobs[k].p) cudaFreeAsync(S->d_jobs[k].p, S->c->stream);
             if (S->d_tiles[k].p) cudaFreeAsync(S->d_tiles[k].p, S->c->stream);
             if (S->d_work[k].p) cudaFreeAsync(S->d_work[k].p, S->c->stream);
@@ -602,6 +640,21 @@ hr_status hr_server_add_scene(hr_server* S, const float* kf, uint32_t nkf, uint3
         return HR_ERR_INVALID_ARG;
     DeviceGuard dg(S->c->device);
     std::unique_ptr<SrvScene> X(new SrvScene());
+    if (S->mode == HR_SERVER_PLAIN) {
+        // nothing resident: every request uploads its frame, as the per-frame path does
+        X->host_kf.assign(kf, kf + (size_t)nkf * nv * 3);
+        X->host_idx.assign(idx, idx + (size_t)ntri * 3);
+        X->nverts = nv;
+        X->ntri = ntri;
+        X->nkf = nkf;
+        X->top = top;
+        X->leaf = leaf;
+        std::lock_guard<std::mutex> g(S->m);
+        if (S->scenes.size() >= kMaxScenes) return HR_ERR_OUT_OF_MEMORY;
+        *scene_id = (uint32_t)S->scenes.size();
+        S->scenes.push_back(std::move(X));
+        return HR_OK;
+    }
     hr_status st = hr_create(&X->ctx, S->c->device, nullptr);
     if (st != HR_OK) return st;
     hr_ctx* c = X->ctx;
@@ -725,7 +778,8 @@ hr_status hr_server_get_stats(hr_server* S, hr_server_stats* st) {
     uint64_t rays = S->host_rays;
     uint64_t launches = S->c->launches;
     std::vector<hr_ctx*> ctxs{S->c};
-    for (auto& X : S->scenes) ctxs.push_back(X->ctx);
+    for (auto& X : S->scenes)
+        if (X->ctx) ctxs.push_back(X->ctx);
     for (hr_ctx* c : ctxs) {
         uint64_t w[8];
         if (cudaMemcpy(w, c->counters.p, sizeof(w), cudaMemcpyDeviceToHost) == cudaSuccess) rays += w[0] + w[4];
@@ -740,6 +794,7 @@ hr_status hr_server_get_stats(hr_server* S, hr_server_stats* st) {
     st->resident_bytes = S->resident;
     st->peak_inflight_bytes = S->peak_inflight;
     st->launches = launches;
+    st->trace_ms = S->trace_ms;
     return HR_OK;
 }
 

@@ -222,29 +222,48 @@ __global__ void k_ao_finish(const uint32_t* __restrict__ queue, const uint32_t* 
     }
 }
 
+#ifndef HR_PT_MIN_BLOCKS
+#define HR_PT_MIN_BLOCKS 6   // blocks of kTT per SM the path tracer's register budget must allow (6: 80 registers)
+#endif
+
 // mode 1/2: path tracing with next-event estimation (PathTracer.h:41-372 structure), one
-// path per pixel (pt_path in traverse.cuh).
+// path per pixel.  Persistent: each warp takes 32-pixel tiles from *work, and a lane whose
+// path ends takes the next pixel at once (path_refill / path_step / path_retire), so lanes
+// do not idle through the bounces of their warp's longest path.
 template <bool STATS>
-__global__ __launch_bounds__(kTT, 8) void k_render_pt(Scene s, Cam cam, LightP l, int32_t bounces, float albedo,
-                                                   float eps_frac, uint64_t seed, int32_t image_id,
-                                                   float* __restrict__ fb, unsigned long long* counter) {
+__global__ __launch_bounds__(kTT, HR_PT_MIN_BLOCKS) void k_render_pt(Scene s, Cam cam, LightP l, int32_t bounces,
+                                                                  float albedo, float eps_frac, uint64_t seed,
+                                                                  int32_t image_id, float* __restrict__ fb,
+                                                                  unsigned long long* counter, uint32_t* work) {
     const G g = load_g(s.desc);
     const PtConsts k = pt_consts(g, l, bounces, albedo, eps_frac);
-    const uint32_t slots = tile_slots(cam);
-    for (uint32_t slot = blockIdx.x * kTT + threadIdx.x; slot < slots; slot += gridDim.x * kTT) {
-        uint32_t pix;
-        const bool valid = tile_pixel(cam, slot, &pix);
-        PtCounts n;
-        const float L = pt_path<STATS>(s, g, cam, k, pix, valid, image_id, seed, n);
-        if (valid) {
-            const float val = blend(fb[3 * (size_t)pix], L, image_id);
-            fb[3 * (size_t)pix] = val;
-            fb[3 * (size_t)pix + 1] = val;
-            fb[3 * (size_t)pix + 2] = val;
+    const uint32_t ntiles = tile_slots(cam) >> 5;
+    const uint32_t lane = threadIdx.x & 31u;
+    PathLane ln;
+    PtCounts n;
+    uint32_t tile = 0, next = 32u;
+    bool more = true;
+    while (true) {
+        while (more) {
+            if (next >= 32u) {
+                uint32_t t = 0;
+                if (lane == 0) t = atomicAdd(work, 1u);
+                t = __shfl_sync(kFullMask, t, 0);
+                if (t >= ntiles) {
+                    more = false;
+                    break;
+                }
+                tile = t;
+                next = 0;
+            }
+            if (path_refill(ln, cam, tile, &next, image_id, seed, fb) == 0u) break;
         }
-        add_rays<STATS>(counter, false, n.rays, n.cells, n.tests);
-        add_rays<STATS>(counter, true, n.srays, n.scells, n.stests);
+        if (!__any_sync(kFullMask, ln.has)) break;
+        const bool cont = path_step<STATS, false>(s, g, k, ln.p, ln.has, n);
+        path_retire(ln, cont, cam, image_id, 1, seed, fb);
     }
+    add_rays<STATS>(counter, false, n.rays, n.cells, n.tests);
+    add_rays<STATS>(counter, true, n.srays, n.scells, n.stests);
 }
 
 Scene make_scene(hr_ctx* c) {
@@ -335,14 +354,23 @@ int launch_render(hr_ctx* c, int32_t mode, int32_t image_id, float* d_fb) {
         LightP l;
         for (int i = 0; i < 3; ++i) { l.c[i] = c->light.corner[i]; l.e1[i] = c->light.e1[i]; l.e2[i] = c->light.e2[i]; }
         l.emission = c->light.emission;
+        uint32_t* work = reinterpret_cast<uint32_t*>(ctr + 7);
+        int rc;
+        if ((rc = cuda_check(c, cudaMemsetAsync(work, 0, sizeof(uint32_t), strm), "tile counter reset"))) return rc;
+        int nb = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_render_pt<false>, kTT, 0) != cudaSuccess || nb < 1) {
+            cudaGetLastError();
+            nb = 1;
+        }
+        const int gp = std::min(gb, nb * c->num_sms);
         c->launches += 1;
         mark(0);
         if (st)
-            k_render_pt<true><<<gb, kTT, 0, strm>>>(s, k, l, c->ip.pt_bounces, c->ip.albedo, c->ip.ray_eps_frac,
-                                                    c->ip.seed, image_id, d_fb, ctr);
+            k_render_pt<true><<<gp, kTT, 0, strm>>>(s, k, l, c->ip.pt_bounces, c->ip.albedo, c->ip.ray_eps_frac,
+                                                    c->ip.seed, image_id, d_fb, ctr, work);
         else
-            k_render_pt<false><<<gb, kTT, 0, strm>>>(s, k, l, c->ip.pt_bounces, c->ip.albedo, c->ip.ray_eps_frac,
-                                                     c->ip.seed, image_id, d_fb, ctr);
+            k_render_pt<false><<<gp, kTT, 0, strm>>>(s, k, l, c->ip.pt_bounces, c->ip.albedo, c->ip.ray_eps_frac,
+                                                     c->ip.seed, image_id, d_fb, ctr, work);
         mark(1);
         c->nrender_ev = 2;
         break;

@@ -461,75 +461,141 @@ struct PtCounts {
     uint32_t rays = 0, cells = 0, tests = 0, srays = 0, scells = 0, stests = 0;
 };
 
-// One path of the path tracer (PathTracer.h:41-372 structure) from the centre of pixel
-// pix: camera ray against the quad light at bounce 0, then per bounce the closest hit,
-// one next-event sample of the light (u1, u2) with an any-hit shadow ray to
-// dist - ray_eps, and a cosine-weighted bounce (u3, u4) with throughput x albedo.  The
-// PCG32 stream is keyed by (image_id, pix) and seed.  Returns the radiance.  The bounce
-// loop runs the same number of iterations on every lane (finished paths pass
-// active = false), so the warp-synchronous traversal can be called inside it: all lanes
-// of the warp must call pt_path together.
-template <bool STATS, bool TL_ONLY = false>
-__device__ __forceinline__ float pt_path(const Scene& s, const G& g, const Cam& cam, const PtConsts& k, uint32_t pix,
-                                         bool valid, int32_t image_id, uint64_t seed, PtCounts& n) {
-    bool alive = valid;
+// State of one path of the path tracer (PathTracer.h:41-372 structure).
+struct PathState {
+    f3 o, d;
+    float L, beta;
     Pcg32 rng;
-    pcg_seed(rng, ((uint64_t)(uint32_t)image_id << 32) | (valid ? pix : 0u), seed);
-    f3 o = mk(cam.pos[0], cam.pos[1], cam.pos[2]);
-    f3 d = valid ? primary_dir(cam, pix) : mk(1.0f, 0.0f, 0.0f);
-    float L = 0.0f, beta = 1.0f;
-    for (int32_t bounce = 0; bounce < k.bounces; ++bounce) {
-        Hit h;
-        trace_kind<TL_ONLY, false, STATS>(s, g, o, d, FLT_MAX, h, alive);
-        bool shadow = false;
-        f3 p = mk(0.0f, 0.0f, 0.0f), nrm = mk(0.0f, 0.0f, 1.0f), wi = mk(0.0f, 0.0f, 1.0f), so = p;
-        float dist = 0.0f, dist2 = 1.0f, cos_s = 0.0f, cos_l = 0.0f;
-        if (alive) {
-            n.rays += 1;
-            n.cells += h.cells;
-            n.tests += h.tests;
-            if (bounce == 0 && d.z > 0.0f) {
-                const float tl = (k.lc.z - o.z) / d.z;
-                const float px = o.x + tl * d.x, py = o.y + tl * d.y;
-                const float fx = (px - k.lc.x) / k.le1.x, fy = (py - k.lc.y) / k.le2.y;
-                if (tl > kIsectEps && tl < h.t && fx >= 0.0f && fx <= 1.0f && fy >= 0.0f && fy <= 1.0f) {
-                    L = L + k.emission;
-                    alive = false;
-                }
-            }
-            if (alive && !h.hit) alive = false;
-            if (alive) {
-                p = mk(o.x + h.t * d.x, o.y + h.t * d.y, o.z + h.t * d.z);
-                nrm = face_normal(s, h.tri, d);
-                const float u1 = pcg_float(rng), u2 = pcg_float(rng);
-                const f3 lp = mk(k.lc.x + u1 * k.le1.x + u2 * k.le2.x, k.lc.y + u1 * k.le1.y + u2 * k.le2.y,
-                                 k.lc.z + u1 * k.le1.z + u2 * k.le2.z);
-                wi = sub(lp, p);
-                dist2 = dot(wi, wi);
-                dist = sqrtf(dist2);
-                wi = mulf(wi, 1.0f / dist);
-                cos_s = dot(nrm, wi);
-                cos_l = wi.z;
-                shadow = cos_s > 0.0f && cos_l > 0.0f;
-                so = mk(p.x + k.ray_eps * wi.x, p.y + k.ray_eps * wi.y, p.z + k.ray_eps * wi.z);
+    int32_t bounce;
+};
+
+// A path from the centre of pixel pix; its PCG32 stream is keyed by (image_id, pix) and seed.
+__device__ __forceinline__ void path_begin(PathState& p, const Cam& cam, uint32_t pix, int32_t image_id,
+                                           uint64_t seed) {
+    pcg_seed(p.rng, ((uint64_t)(uint32_t)image_id << 32) | pix, seed);
+    p.o = mk(cam.pos[0], cam.pos[1], cam.pos[2]);
+    p.d = primary_dir(cam, pix);
+    p.L = 0.0f;
+    p.beta = 1.0f;
+    p.bounce = 0;
+}
+
+// One bounce: the closest hit (at bounce 0 first the camera ray against the quad light),
+// one next-event sample of the light (u1, u2) with an any-hit shadow ray to
+// dist - ray_eps, and a cosine-weighted continuation (u3, u4) with throughput x albedo.
+// Returns true while the path goes on (it ends on a miss, on hitting the light, or after
+// k.bounces bounces); p.L is then its radiance.  Warp-synchronous: all lanes call it,
+// lanes without a path pass alive = false.
+template <bool STATS, bool TL_ONLY>
+__device__ __forceinline__ bool path_step(const Scene& s, const G& g, const PtConsts& k, PathState& p, bool alive,
+                                          PtCounts& n) {
+    if (k.bounces <= 0) return false;   // no bounce: radiance 0 (uniform over the warp)
+    Hit h;
+    trace_kind<TL_ONLY, false, STATS>(s, g, p.o, p.d, FLT_MAX, h, alive);
+    bool shadow = false;
+    f3 q = mk(0.0f, 0.0f, 0.0f), nrm = mk(0.0f, 0.0f, 1.0f), wi = mk(0.0f, 0.0f, 1.0f), so = q;
+    float dist = 0.0f, dist2 = 1.0f, cos_s = 0.0f, cos_l = 0.0f;
+    if (alive) {
+        n.rays += 1;
+        n.cells += h.cells;
+        n.tests += h.tests;
+        if (p.bounce == 0 && p.d.z > 0.0f) {
+            const float tl = (k.lc.z - p.o.z) / p.d.z;
+            const float px = p.o.x + tl * p.d.x, py = p.o.y + tl * p.d.y;
+            const float fx = (px - k.lc.x) / k.le1.x, fy = (py - k.lc.y) / k.le2.y;
+            if (tl > kIsectEps && tl < h.t && fx >= 0.0f && fx <= 1.0f && fy >= 0.0f && fy <= 1.0f) {
+                p.L = p.L + k.emission;
+                alive = false;
             }
         }
-        Hit hs;
-        trace_kind<TL_ONLY, true, STATS>(s, g, so, wi, dist - k.ray_eps, hs, shadow);
+        if (alive && !h.hit) alive = false;
         if (alive) {
-            if (shadow) {
-                n.srays += 1;
-                n.scells += hs.cells;
-                n.stests += hs.tests;
-                if (!hs.hit) L = L + beta * k.a_pi * k.emission * cos_s * cos_l * k.larea / dist2;
-            }
-            beta = beta * k.albedo;
-            const float u3 = pcg_float(rng), u4 = pcg_float(rng);
-            d = cosine_dir(nrm, u3, u4);
-            o = mk(p.x + k.ray_eps * d.x, p.y + k.ray_eps * d.y, p.z + k.ray_eps * d.z);
+            q = mk(p.o.x + h.t * p.d.x, p.o.y + h.t * p.d.y, p.o.z + h.t * p.d.z);
+            nrm = face_normal(s, h.tri, p.d);
+            const float u1 = pcg_float(p.rng), u2 = pcg_float(p.rng);
+            const f3 lp = mk(k.lc.x + u1 * k.le1.x + u2 * k.le2.x, k.lc.y + u1 * k.le1.y + u2 * k.le2.y,
+                             k.lc.z + u1 * k.le1.z + u2 * k.le2.z);
+            wi = sub(lp, q);
+            dist2 = dot(wi, wi);
+            dist = sqrtf(dist2);
+            wi = mulf(wi, 1.0f / dist);
+            cos_s = dot(nrm, wi);
+            cos_l = wi.z;
+            shadow = cos_s > 0.0f && cos_l > 0.0f;
+            so = mk(q.x + k.ray_eps * wi.x, q.y + k.ray_eps * wi.y, q.z + k.ray_eps * wi.z);
         }
     }
-    return L;
+    Hit hs;
+    trace_kind<TL_ONLY, true, STATS>(s, g, so, wi, dist - k.ray_eps, hs, shadow);
+    if (alive) {
+        if (shadow) {
+            n.srays += 1;
+            n.scells += hs.cells;
+            n.stests += hs.tests;
+            if (!hs.hit) p.L = p.L + p.beta * k.a_pi * k.emission * cos_s * cos_l * k.larea / dist2;
+        }
+        p.beta = p.beta * k.albedo;
+        const float u3 = pcg_float(p.rng), u4 = pcg_float(p.rng);
+        p.d = cosine_dir(nrm, u3, u4);
+        p.o = mk(q.x + k.ray_eps * p.d.x, q.y + k.ray_eps * p.d.y, q.z + k.ray_eps * p.d.z);
+    }
+    p.bounce += 1;
+    return alive && p.bounce < k.bounces;
+}
+
+// Lanes of a warp take pixels from a pool of 32-pixel tiles and run `spp` paths per pixel,
+// one bounce per step for all lanes together; a lane whose path ends starts the pixel's
+// next path (image id + 1) or takes the next pixel, so the warp stays full until the pool
+// runs dry.  The per-pixel result is the progressive blend of its paths in image-id order,
+// the same values as spp one-path frames.
+struct PathLane {
+    PathState p;
+    uint32_t pix = 0;
+    int32_t sample = 0;
+    float val = 0.0f;
+    bool has = false;
+};
+
+// Fill the lanes without a path from tile `tile` starting at slot *next (tile pixels as
+// tile_pixel); advances *next.  Returns the lanes still without a path.
+__device__ __forceinline__ uint32_t path_refill(PathLane& ln, const Cam& cam, uint32_t tile, uint32_t* next,
+                                               int32_t image_id, uint64_t seed, const float* __restrict__ fb) {
+    const uint32_t lane = threadIdx.x & 31u;
+    uint32_t need = __ballot_sync(kFullMask, !ln.has);
+    while (need && *next < 32u) {
+        const uint32_t rank = __popc(need & ((1u << lane) - 1u));
+        const uint32_t take = min((uint32_t)__popc(need), 32u - *next);
+        if (!ln.has && rank < take) {
+            uint32_t q;
+            if (tile_pixel(cam, tile * 32u + *next + rank, &q)) {
+                ln.pix = q;
+                ln.has = true;
+                ln.sample = 0;
+                ln.val = fb[3 * (size_t)q];
+                path_begin(ln.p, cam, q, image_id, seed);
+            }
+        }
+        *next += take;
+        need = __ballot_sync(kFullMask, !ln.has);
+    }
+    return need;
+}
+
+// After a step: a lane whose path ended blends it in and starts the pixel's next path, or
+// writes the pixel and frees itself.
+__device__ __forceinline__ void path_retire(PathLane& ln, bool cont, const Cam& cam, int32_t image_id, int32_t spp,
+                                            uint64_t seed, float* __restrict__ fb) {
+    if (!ln.has || cont) return;
+    const int32_t im = image_id + ln.sample;
+    ln.val = blend(ln.val, ln.p.L, im);
+    ln.sample += 1;
+    if (ln.sample < spp) {
+        path_begin(ln.p, cam, ln.pix, im + 1, seed);
+        return;
+    }
+    float* o = fb + 3 * (size_t)ln.pix;
+    o[0] = ln.val; o[1] = ln.val; o[2] = ln.val;
+    ln.has = false;
 }
 
 }  // namespace

@@ -4,9 +4,11 @@ A Server keeps animated scenes resident and answers render and ray-query request
 batched mode its worker thread admits queued requests under the HBM budget, rebuilds a
 scene's grid only when a request asks for another frame time, and traces every admitted
 request of a wave in one persistent launch, with two waves in flight.  Serial mode runs
-the same requests one at a time through the per-scene path.  Results do not depend on the
-mode or on the other requests.  The reference has no server: its application renders one
-scene per process (src/Application/CUDAApplication.cu:116-160).
+the same requests one at a time through the per-scene path on the resident scenes; plain
+mode is the drop-in per-frame path (one context; per request upload the frame, build,
+render, read back).  Results do not depend on the mode or on the other requests.  The
+reference has no server: its application renders one scene per process
+(src/Application/CUDAApplication.cu:116-160).
 """
 from __future__ import annotations
 
@@ -18,7 +20,7 @@ import numpy as np
 from . import _lib
 from ._lib import HRError, Request, RequestInfo, ServerStats
 
-BATCHED, SERIAL = 0, 1
+BATCHED, SERIAL, PLAIN = 0, 1, 2
 RENDER, RAYS = 0, 1
 
 

@@ -113,7 +113,9 @@ hr_status hr_set_light(hr_ctx *ctx, const float corner[3], const float edge1[3],
 hr_status hr_set_integrator(hr_ctx *ctx, int32_t ao_samples, float ao_radius,
                             int32_t pt_bounces, float albedo, uint64_t seed);
 /* RTEngine::renderFrame (RTEngine.h:59, RTEngine.cu:398-444): progressive blend into a
- * float3-per-pixel frame buffer.  Host buffer: copied in and out. */
+ * float3-per-pixel frame buffer, new = old * (1 - 1/(image_id+1)) + value / (image_id+1).
+ * Host buffer: copied in and out (image 0 starts from zeros).  Device buffer: blended in
+ * place, so it must hold finite values (e.g. zeros) before image 0. */
 hr_status hr_render(hr_ctx *ctx, int32_t mode, int32_t image_id, float *framebuffer_rgb);
 hr_status hr_render_device(hr_ctx *ctx, int32_t mode, int32_t image_id, float *d_framebuffer_rgb);
 /* Ray query (SimpleRayTraverser.h:168-181 + RayTracingKernels.h:47-152): closest hit per
@@ -256,13 +258,17 @@ hr_status hr_batch_autotune(hr_batch *batch, int32_t reps, hr_batch_tuning *best
  * of the wave in one persistent launch (rays batched across requests), with up to two
  * waves in flight so that the next wave's admission, rebuilds and copies overlap the
  * current one.  HR_SERVER_SERIAL runs the same requests one at a time through the
- * per-scene path (hr_build + hr_render / hr_trace_rays), as a caller of the plain API
- * would.  A request's result depends only on the request: it is bit-identical in both
- * modes, alone or among others.
+ * per-scene path (hr_build + hr_render / hr_trace_rays) over the same resident scenes.
+ * HR_SERVER_PLAIN is the drop-in per-frame path as the reference's application drives it
+ * (one context holding one scene, CUDAApplication.cu:116-160): per request hr_upload of the
+ * two key frames around the frame time and the triangles (host copies kept by the server),
+ * hr_build, hr_render, read back.  A request's result depends only on the request: it is
+ * bit-identical in every mode, alone or among others.
  */
 typedef struct hr_server hr_server;
 #define HR_SERVER_BATCHED 0
 #define HR_SERVER_SERIAL 1
+#define HR_SERVER_PLAIN 2
 #define HR_REQUEST_RENDER 0
 #define HR_REQUEST_RAYS 1
 
@@ -296,6 +302,7 @@ typedef struct hr_server_stats {
     uint64_t resident_bytes;      /* scenes: key frames, grids, vertex arrays */
     uint64_t peak_inflight_bytes; /* request buffers */
     uint64_t launches;
+    double trace_ms;              /* device time of the waves' traversal launches (batched) */
 } hr_server_stats;
 
 hr_status hr_server_create(hr_server **out, int32_t device, uint64_t hbm_budget_bytes, int32_t mode);

@@ -8,7 +8,7 @@ import pytest
 
 from happyray_b200 import GRID_TWO_LEVEL, RENDER_AO, RENDER_PATH, RENDER_PRIMARY, Engine, HRError
 from happyray_b200 import scenes as S
-from happyray_b200.server import BATCHED, SERIAL, Server
+from happyray_b200.server import BATCHED, PLAIN, SERIAL, Server
 
 pytestmark = pytest.mark.gpu
 
@@ -72,7 +72,7 @@ def make_server(pool, mode, budget=8 << 30):
 
 @pytest.fixture(scope="module")
 def served(hrlib, pool):
-    """Results of the mix in batched mode, all submitted at once, and in serial mode."""
+    """Results of the mix in batched mode (all submitted at once), serial and plain modes."""
     qs = requests(pool)
     with make_server(pool, BATCHED) as srv:
         pend = [submit(srv, q) for q in qs]
@@ -81,13 +81,16 @@ def served(hrlib, pool):
         st = srv.stats()
     with make_server(pool, SERIAL) as srv:
         ser = [submit(srv, q).wait(60_000) for q in qs]
-    return qs, mix, ser, infos, st
+    with make_server(pool, PLAIN) as srv:
+        pla = [submit(srv, q).wait(60_000) for q in qs]
+    return qs, mix, ser, infos, st, pla
 
 
-def test_served_mix_equals_serial(served):
-    qs, mix, ser, infos, st = served
-    for i, (a, b) in enumerate(zip(mix, ser)):
-        assert same(a, b), f"request {i} ({qs[i]['kind']})"
+def test_served_mix_equals_serial_and_plain(served):
+    qs, mix, ser, infos, st, pla = served
+    for i, (a, b, c) in enumerate(zip(mix, ser, pla)):
+        assert same(a, b), f"request {i} ({qs[i]['kind']}) serial"
+        assert same(a, c), f"request {i} ({qs[i]['kind']}) plain"
     assert st["completed"] == len(qs) and st["failed"] == 0
     assert all(i["status"] == 2 and i["done_ns"] >= i["submit_ns"] for i in infos)
     # the mix was batched: fewer waves than requests
@@ -95,14 +98,14 @@ def test_served_mix_equals_serial(served):
 
 
 def test_served_alone_equals_mix(served, pool):
-    qs, mix, _, _, _ = served
+    qs, mix, _, _, _, _ = served
     with make_server(pool, BATCHED) as srv:
         for i in range(0, len(qs), 5):
             assert same(submit(srv, qs[i]).wait(60_000), mix[i]), f"request {i}"
 
 
 def test_served_equals_plain_engine(served, pool):
-    qs, mix, _, _, _ = served
+    qs, mix, _, _, _, _ = served
     for i in range(8):
         q = qs[i]
         kf, f = pool[q["scene"]]
