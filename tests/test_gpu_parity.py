@@ -3,6 +3,8 @@ inputs.  Integer results (cells, leaves, primitive lists, hit ids) and the float
 (t, u, v, AO / PT pixels) are compared bit-exact: both sides evaluate the same binary32
 expressions in the same order without FMA contraction.  t/u/v are additionally held to
 1e-5 relative against the FP64 brute-force oracle (see test_oracle.compare_fp64)."""
+from pathlib import Path
+
 import numpy as np
 import pytest
 
@@ -286,3 +288,34 @@ def test_empty_mesh(engine):
     assert np.all(hid == -1)
     with pytest.raises(HRError):
         engine.build(7)
+
+
+# The product path against the reference's own kernels (tests/golden/ref_*.npz, made by
+# tests/golden/make_ref_golden.py from the reference's build kernels and traversers).
+GOLDEN = sorted((Path(__file__).resolve().parent / "golden").glob("ref_*.npz"))
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=lambda p: p.stem)
+def test_gpu_matches_reference_golden(engine, path):
+    from tests.test_oracle import cell_lists
+    z = np.load(path)
+    kind = int(z["kind"])
+    dens, leaf = float(z["density"]), float(z["leaf_density"])
+    gi, cells, leaves, prims = gpu_build(engine, z["vertices"], z["faces"], kind, bool(z["exact"]), ug=dens,
+                                         top=dens, leaf=leaf if leaf > 0 else 2.0)
+    assert gi["res"] == tuple(z["strict_res"])
+    assert np.array_equal(gi["bounds_min"], z["strict_bmin"]) and np.array_equal(gi["cell_size_rcp"], z["strict_rcp"])
+    if kind == GRID_UNIFORM:
+        rc, rl = cell_lists(z["strict_cells"], z["strict_prims"])
+        gc, gl = cell_lists(cells, prims)
+    else:
+        assert np.array_equal(cells, z["strict_cells"])
+        rc, rl = cell_lists(z["strict_leaves"], z["strict_prims"])
+        gc, gl = cell_lists(leaves, prims)
+    assert np.array_equal(rc, gc) and np.array_equal(rl, gl)
+    hid, t, _, _ = engine.trace_rays(z["ray_org"], z["ray_dir"])
+    rid = z["strict_hit_id"].astype(np.int64)
+    rid[rid == 0xFFFFFFFF] = -1
+    assert np.array_equal(rid, hid)
+    hit = hid >= 0
+    assert np.all(np.abs(z["strict_hit_t"][hit] - t[hit]) <= 1e-5 * np.abs(t[hit]))

@@ -2,6 +2,7 @@
 reference keeps as commented-out debug checks (UGridSortBuilder.h:253-399,
 TLGridSortBuilder.h:411-428)."""
 import math
+from pathlib import Path
 
 import numpy as np
 import pytest
@@ -300,3 +301,65 @@ def test_edge_cases(oracle):
     hid, *_ = oracle.trace(b, np.array([[0.2, 0.2, 3.0], [1.0, 1.0, 3.0]], np.float32),
                            np.array([[0, 0, -1.0], [0, 0, -1.0]], np.float32))
     assert hid[0] == 1 and hid[1] == -1
+
+
+# ---------------------------------------------------------------------------------
+# Pin against the reference itself: tests/golden/ref_*.npz hold what the reference's own
+# build kernels and traversers computed on a B200 (tests/golden/make_ref_golden.py runs
+# them through oracle/ref_pin), for an IEEE build of the reference (strict) and for its
+# shipped -use_fast_math build (fast).
+
+GOLDEN = sorted((Path(__file__).resolve().parent / "golden").glob("ref_*.npz"))
+
+
+def cell_lists(cells, prims):
+    """(per-cell counts, the concatenated per-cell lists each sorted by triangle id): the
+    reference's order inside a cell depends on atomics, the oracle's is ascending."""
+    cells = np.asarray(cells, np.int64).reshape(-1, 2)
+    cnt = np.where(cells[:, 1] > cells[:, 0], cells[:, 1] - cells[:, 0], 0)
+    parts = [np.sort(prims[cells[c, 0]:cells[c, 1]]) for c in np.nonzero(cnt)[0]]
+    return cnt, (np.concatenate(parts) if parts else np.zeros(0, np.uint32))
+
+
+def oracle_for_golden(O, z):
+    v, f = z["vertices"], z["faces"]
+    v4, bmin, bmax = O.lerp_bounds(v, v, 1.0)
+    if int(z["kind"]) == 0:
+        return O.build_ug(v4, f, bmin, bmax, float(z["density"]), bool(z["exact"]))
+    return O.build_tl(v4, f, bmin, bmax, float(z["density"]), float(z["leaf_density"]))
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=lambda p: p.stem)
+@pytest.mark.parametrize("variant", ["strict", "fast"])
+def test_oracle_matches_reference_golden(oracle, path, variant):
+    z = np.load(path)
+    b = oracle_for_golden(oracle, z)
+    g = b.grid
+
+    def r(k):
+        return z[f"{variant}_{k}"]
+
+    # grid parameters: bit-exact
+    assert tuple(r("res")) == tuple(g.res)
+    for k in ("bmin", "bmax", "cs", "rcp"):
+        assert np.array_equal(r(k), np.array(getattr(g, k), np.float32)), k
+    # per-cell (uniform) or packed top cells + per-leaf (two-level) lists: exact
+    if int(z["kind"]) == 0:
+        rc, rl = cell_lists(r("cells"), r("prims"))
+        oc, ol = cell_lists(b.cells, np.asarray(b.prims))
+    else:
+        assert np.array_equal(r("cells"), np.asarray(b.cells, np.uint32).reshape(-1, 2))
+        rc, rl = cell_lists(r("leaves"), r("prims"))
+        oc, ol = cell_lists(b.leaves, np.asarray(b.prims))
+    assert np.array_equal(rc, oc)
+    assert np.array_equal(rl, ol)
+    # closest hits of the camera rays: ids equal, t within 1e-5 relative (the reference
+    # re-derives the direction from its reciprocal with an approximate division)
+    hid, t, _, _ = oracle.trace(b, z["ray_org"], z["ray_dir"])
+    rid = r("hit_id").astype(np.int64)
+    rid[rid == 0xFFFFFFFF] = -1
+    assert np.array_equal(rid, hid)
+    hit = hid >= 0
+    assert hit.sum() > 500
+    rel = np.abs(r("hit_t")[hit] - t[hit]) / np.abs(t[hit])
+    assert rel.max() <= 1e-5
