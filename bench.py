@@ -141,6 +141,25 @@ def dist_setup():
     return rank, ws, local
 
 
+def max_over_ranks(x: float, ws: int) -> float:
+    """Largest value over the ranks -- the slowest replica's device time -- or x itself at
+    N = 1.  Works on a NCCL (GPU tensor) or gloo (CPU tensor) process group."""
+    if ws <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    dev = torch.device("cuda", torch.cuda.current_device()) if dist.get_backend() == "nccl" else torch.device("cpu")
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(units_per_rank_step: float, steps: int, total_ms: float, ws: int) -> float:
+    """Whole-job throughput in millions of units per second: the units every replica
+    processed over the slowest replica's time (weak scaling: fixed work per GPU)."""
+    return ws * units_per_rank_step * steps / (total_ms * 1e-3) / 1e6
+
+
 def cpu_baseline(W, kind_budget_s=25.0):
     """The oracle (CPU restatement of the reference's build and traversal) on a bounded
     sample of the workload, all host threads: full build + a strided pixel sample, scaled."""
@@ -296,13 +315,8 @@ def run_batched(args, rank, ws, local):
             step_ms.append(tt)
         torch.cuda.synchronize()
     launches = b.counters()[1] - l0
-    total_ms = sum(step_ms)
-    if ws > 1:
-        import torch.distributed as dist
-        tt = torch.tensor([total_ms], dtype=torch.float64, device=f"cuda:{dev}")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        total_ms = float(tt.item())
-    value = ws * rays_per_step * args.steps / (total_ms * 1e-3) / 1e6
+    total_ms = max_over_ranks(sum(step_ms), ws)
+    value = replica_value(rays_per_step, args.steps, total_ms, ws)
 
     # end to end through the public API: new vertex positions of every scene from pinned
     # host memory, build + render, every image back to pinned host memory
@@ -325,8 +339,8 @@ def run_batched(args, rank, ws, local):
             z.synchronize()
             if i >= args.warmup:
                 e_ms.append(a.elapsed_time(z))
-        et = sum(e_ms)
-        e2e = {"value": ws * rays_per_step * args.steps / (et * 1e-3) / 1e6, "unit": "Mrays/s",
+        et = max_over_ranks(sum(e_ms), ws)
+        e2e = {"value": replica_value(rays_per_step, args.steps, et, ws), "unit": "Mrays/s",
                "h2d_bytes_per_step": int(hv.nbytes), "d2h_bytes_per_step": int(himg.nbytes),
                "ms_per_step": et / args.steps}
 
@@ -554,7 +568,7 @@ def run_served(args, rank, ws, local):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3", "c4", "c5"])
@@ -656,13 +670,8 @@ def main():
     build_ms = [e[0].elapsed_time(e[1]) for e in evs]
     trace_ms = [e[1].elapsed_time(e[2]) for e in evs]
     step_ms = [b + t for b, t in zip(build_ms, trace_ms)]
-    total_ms = sum(step_ms)
-    if ws > 1:
-        import torch.distributed as dist
-        tt = torch.tensor([total_ms], dtype=torch.float64, device=f"cuda:{dev}")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        total_ms = float(tt.item())
-    value = ws * rays_per_step * args.steps / (total_ms * 1e-3) / 1e6
+    total_ms = max_over_ranks(sum(step_ms), ws)
+    value = replica_value(rays_per_step, args.steps, total_ms, ws)
 
     # end to end through the public API: pinned host inputs, upload + build + render + readback
     e2e = None
@@ -683,13 +692,8 @@ def main():
             b.synchronize()
             if i >= args.warmup:
                 e_ms.append(a.elapsed_time(b))
-        et = sum(e_ms)
-        if ws > 1:
-            import torch.distributed as dist
-            tt = torch.tensor([et], dtype=torch.float64, device=f"cuda:{dev}")
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            et = float(tt.item())
-        e2e = {"value": ws * rays_per_step * args.steps / (et * 1e-3) / 1e6, "unit": "Mrays/s",
+        et = max_over_ranks(sum(e_ms), ws)
+        e2e = {"value": replica_value(rays_per_step, args.steps, et, ws), "unit": "Mrays/s",
                "h2d_bytes_per_step": int(2 * hv.nbytes + hf.nbytes), "d2h_bytes_per_step": int(hfb.nbytes),
                "ms_per_step": et / args.steps}
 
