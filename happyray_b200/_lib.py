@@ -98,6 +98,21 @@ SIGNATURES = {
     "hr_server_drain": (C.c_int, [P, C.c_int32]),
     "hr_server_request_info": (C.c_int, [P, C.c_uint64, P]),
     "hr_server_get_stats": (C.c_int, [P, P]),
+    # scene input, ray files, images
+    "hr_scene_load": (C.c_int, [C.c_char_p, C.c_int32, C.POINTER(P)]),
+    "hr_scene_load_obj": (C.c_int, [C.c_char_p, C.c_int32, C.POINTER(P)]),
+    "hr_scene_free": (None, [P]),
+    "hr_io_last_error": (C.c_char_p, []),
+    "hr_scene_get_info": (C.c_int, [P, P]),
+    "hr_scene_keyframes": (P, [P]),
+    "hr_scene_indices": (P, [P]),
+    "hr_scene_get_light": (C.c_int, [P, C.c_uint32, P, P, P, P, P]),
+    "hr_scene_upload": (C.c_int, [P, P]),
+    "hr_rays_file_count": (C.c_int, [C.c_char_p, C.POINTER(C.c_uint32)]),
+    "hr_rays_file_read": (C.c_int, [C.c_char_p, P, C.c_uint32]),
+    "hr_rays_file_write": (C.c_int, [C.c_char_p, P, P, C.c_uint32]),
+    "hr_hits_file_write": (C.c_int, [C.c_char_p, P, P, P, P, C.c_uint32]),
+    "hr_image_write": (C.c_int, [C.c_char_p, P, C.c_int32, C.c_int32, C.c_int32]),
 }
 
 
@@ -113,6 +128,14 @@ class BatchTuning(C.Structure):
     """hr_batch_tuning"""
     _fields_ = [("top_density", C.c_float), ("leaf_density", C.c_float), ("block_threads", C.c_int32),
                 ("tile_width", C.c_int32), ("ms_per_step", C.c_float), ("trials", C.c_int32)]
+
+
+class SceneInfo(C.Structure):
+    """hr_scene_info"""
+    _fields_ = [("num_vertices", C.c_uint32), ("num_triangles", C.c_uint32), ("num_keyframes", C.c_uint32),
+                ("frame_step", C.c_float), ("has_camera", C.c_int32), ("cam_position", C.c_float * 3),
+                ("cam_orientation", C.c_float * 3), ("cam_up", C.c_float * 3), ("cam_fov_deg", C.c_float),
+                ("width", C.c_int32), ("height", C.c_int32), ("num_lights", C.c_uint32)]
 
 
 class Request(C.Structure):

@@ -1,0 +1,619 @@
+// io.cpp -- scene input, ray files and image output (host side, no GPU).
+//
+// Reference formats (javorkk/happyray):
+//   scene.cfg      src/Application/SceneConfigurationReader.cpp:29-190
+//   frame names    src/Application/AnimationLoader.cpp:50-101
+//   OBJ            src/Application/WFObjectReader.cpp:320-560
+//   camera.cfg     src/Application/CameraManager.cpp:33-168
+//   light.cfg      src/Application/LightSourceLoader.cpp:29-110
+//   .rays          src/RT/Integrator/SimpleRayTraverser.h:200-261
+//   PNG            src/Utils/ImagePNG.cpp:160-215
+// The OBJ reader parses line chunks of the file in parallel (the reference parses one
+// line at a time): each chunk collects its vertices and raw face indices, the chunks'
+// vertex counts give every chunk's first global vertex, and relative (negative) indices
+// are resolved against them.  The PNG writer emits stored (uncompressed) deflate blocks
+// with its own CRC-32 and Adler-32, so it needs no compression library.
+#include "../../include/happyray.h"
+
+#include <cstdint>
+#include <functional>
+
+#include <algorithm>
+#include <cerrno>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <new>
+#include <sstream>
+#include <string>
+#include <thread>
+#include <vector>
+
+struct hr_scene {
+    std::vector<float> kf;          // K x V x 3
+    std::vector<uint32_t> idx;      // N x 3
+    uint32_t nv = 0, nt = 0, nkf = 0;
+    float frame_step = 0.0f;
+    bool has_camera = false;
+    float pos[3] = {0, 0, 0}, orient[3] = {0, 0, -1}, up[3] = {0, 1, 0};
+    float fov = 60.0f;
+    int32_t w = 0, h = 0;
+    struct QuadLight { float position[3], normal[3], intensity[3], edge1[3], edge2[3]; };
+    std::vector<QuadLight> lights;
+};
+
+namespace {
+
+thread_local std::string g_err;
+
+hr_status io_error(hr_status code, const char* fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+bool read_file(const std::string& path, std::string& out) {
+    std::ifstream f(path, std::ios::binary);
+    if (!f) return false;
+    f.seekg(0, std::ios::end);
+    const std::streamoff n = f.tellg();
+    if (n < 0) return false;
+    out.resize((size_t)n);
+    f.seekg(0, std::ios::beg);
+    if (n > 0) f.read(&out[0], n);
+    return (bool)f;
+}
+
+// ---------------------------------------------------------------------------------
+// OBJ
+
+struct ObjChunk {
+    std::vector<float> v;
+    std::vector<int64_t> face;       // triangle corners: > 0 global 1-based, < 0 relative
+    std::vector<uint32_t> face_vcount;   // local vertex count when the corner was read
+    size_t first_line = 0;
+    std::string err;
+};
+
+inline const char* skip_ws(const char* s, const char* e) {
+    while (s < e && (*s == ' ' || *s == '\t' || *s == '\r')) ++s;
+    return s;
+}
+
+// one line of an OBJ file; returns false with c.err set on a malformed line
+bool obj_line(const char* s, const char* e, ObjChunk& c, size_t line) {
+    s = skip_ws(s, e);
+    // comments end the line
+    const char* hash = (const char*)std::memchr(s, '#', (size_t)(e - s));
+    if (hash) e = hash;
+    while (e > s && (e[-1] == ' ' || e[-1] == '\t' || e[-1] == '\r')) --e;
+    if (s >= e) return true;
+    const char k = (char)std::tolower((unsigned char)s[0]);
+    if (k == 'v') {
+        if (s + 1 < e && (s[1] == ' ' || s[1] == '\t')) {
+            // position: exactly three numbers (WFObjectReader.cpp:354-386)
+            const char* p = s + 1;
+            float xyz[3];
+            int n = 0;
+            std::string tmp(p, e);
+            const char* q = tmp.c_str();
+            for (;;) {
+                while (*q == ' ' || *q == '\t') ++q;
+                if (!*q) break;
+                char* end;
+                const double d = std::strtod(q, &end);
+                if (end == q || n >= 3) {
+                    c.err = "line " + std::to_string(line) + ": a vertex needs three numbers";
+                    return false;
+                }
+                xyz[n++] = (float)d;
+                q = end;
+            }
+            if (n != 3) {
+                c.err = "line " + std::to_string(line) + ": a vertex needs three numbers";
+                return false;
+            }
+            c.v.insert(c.v.end(), xyz, xyz + 3);
+        }
+        return true;   // vn, vt: not needed by the hot path
+    }
+    // 'f' (or "fo") and, as in the reference, 'l': three or more corners make triangles
+    if ((k == 'f' || k == 'l') && s + 1 < e && (s[1] == ' ' || s[1] == '\t' || s[1] == 'o' || s[1] == 'O')) {
+        std::string tmp(s + (s[1] == 'o' || s[1] == 'O' ? 2 : 1), e);
+        const char* q = tmp.c_str();
+        std::vector<int64_t> poly;
+        for (;;) {
+            while (*q == ' ' || *q == '\t') ++q;
+            if (!*q) break;
+            char* end;
+            const long long vi = std::strtoll(q, &end, 10);
+            if (end == q || vi == 0) {
+                c.err = "line " + std::to_string(line) + ": bad face index";
+                return false;
+            }
+            q = end;
+            // skip the texture / normal indices of this corner
+            while (*q == '/' || (*q >= '0' && *q <= '9') || *q == '-') ++q;
+            poly.push_back(vi);
+        }
+        if (poly.size() < 3) return true;   // points and lines are not triangles
+        const uint32_t vc = (uint32_t)(c.v.size() / 3);
+        for (size_t i = 1; i + 1 < poly.size(); ++i) {   // fan from the first corner
+            const int64_t tri[3] = {poly[0], poly[i], poly[i + 1]};
+            for (int t = 0; t < 3; ++t) {
+                c.face.push_back(tri[t]);
+                c.face_vcount.push_back(vc);
+            }
+        }
+        return true;
+    }
+    return true;   // o, g, s, p, usemtl, mtllib and anything else: skipped
+}
+
+void obj_parse_chunk(const char* b, const char* e, ObjChunk& c) {
+    size_t line = c.first_line;
+    while (b < e) {
+        const char* nl = (const char*)std::memchr(b, '\n', (size_t)(e - b));
+        const char* le = nl ? nl : e;
+        ++line;
+        if (!obj_line(b, le, c, line)) return;
+        b = nl ? nl + 1 : e;
+    }
+}
+
+hr_status read_obj(const std::string& path, int threads, std::vector<float>& v, std::vector<uint32_t>& idx) {
+    std::string text;
+    if (!read_file(path, text)) return io_error(HR_ERR_INVALID_ARG, "cannot read %s", path.c_str());
+    if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
+    const size_t n = text.size();
+    const int nc = (int)std::max<size_t>(1, std::min<size_t>((size_t)threads, n / (1u << 20) + 1));
+    std::vector<size_t> cut(nc + 1, 0);
+    cut[nc] = n;
+    for (int i = 1; i < nc; ++i) {   // chunk boundaries just after a newline
+        size_t p = std::max(cut[i - 1], n * (size_t)i / (size_t)nc);
+        while (p < n && text[p - 1] != '\n') ++p;
+        cut[i] = p;
+    }
+    std::vector<ObjChunk> ch(nc);
+    for (int i = 0; i < nc; ++i)   // line numbers for messages
+        ch[i].first_line = i == 0 ? 0 : ch[i - 1].first_line +
+                                            (size_t)std::count(text.begin() + cut[i - 1], text.begin() + cut[i], '\n');
+    std::vector<std::thread> th;
+    for (int i = 1; i < nc; ++i)
+        th.emplace_back(obj_parse_chunk, text.data() + cut[i], text.data() + cut[i + 1], std::ref(ch[i]));
+    obj_parse_chunk(text.data() + cut[0], text.data() + cut[1], ch[0]);
+    for (auto& t : th) t.join();
+    size_t nv = 0, nf = 0;
+    for (auto& c : ch) {
+        if (!c.err.empty()) return io_error(HR_ERR_INVALID_ARG, "%s: %s", path.c_str(), c.err.c_str());
+        nv += c.v.size() / 3;
+        nf += c.face.size();
+    }
+    if (nv > 0xffffffffull || nf / 3 > 0xffffffffull) return io_error(HR_ERR_INVALID_ARG, "%s: too large", path.c_str());
+    v.clear();
+    v.reserve(nv * 3);
+    idx.clear();
+    idx.reserve(nf);
+    uint64_t voff = 0;
+    for (auto& c : ch) {
+        v.insert(v.end(), c.v.begin(), c.v.end());
+        for (size_t i = 0; i < c.face.size(); ++i) {
+            const int64_t f = c.face[i];
+            // 1-based global, or relative to the vertices read before this line
+            const int64_t g = f > 0 ? f - 1 : (int64_t)(voff + c.face_vcount[i]) + f;
+            if (g < 0 || (uint64_t)g >= nv)
+                return io_error(HR_ERR_INVALID_ARG, "%s: face index %lld out of range of %zu vertices", path.c_str(),
+                                (long long)f, nv);
+            idx.push_back((uint32_t)g);
+        }
+        voff += c.v.size() / 3;
+    }
+    return HR_OK;
+}
+
+// ---------------------------------------------------------------------------------
+// configuration files
+
+std::string trim(const std::string& s) {
+    const size_t b = s.find_first_not_of(" \t\r");
+    if (b == std::string::npos) return "";
+    const size_t e = s.find_last_not_of(" \t\r");
+    return s.substr(b, e - b + 1);
+}
+
+std::string dir_of(const std::string& p) {
+    const size_t s = p.find_last_of('/');
+    return s == std::string::npos ? std::string() : p.substr(0, s + 1);
+}
+
+std::string resolve(const std::string& p, const std::string& base_dir) {
+    std::ifstream f(p);
+    if (f || p.empty() || p[0] == '/' || base_dir.empty()) return p;
+    return base_dir + p;
+}
+
+bool file_exists(const std::string& p) { return (bool)std::ifstream(p); }
+
+// CameraManager::rotate (CameraManager.cpp:33-66): Euler angles in degrees applied to
+// the orientation and up vectors
+void camera_rotate(float* o, float* u, const float* r) {
+    const float ax = r[0] * 3.14159265358979323846f / 180.0f;
+    const float ay = r[1] * 3.14159265358979323846f / 180.0f;
+    const float az = r[2] * 3.14159265358979323846f / 180.0f;
+    const float sx = std::sin(ax), cx = std::cos(ax), sy = std::sin(ay), cy = std::cos(ay), sz = std::sin(az),
+                cz = std::cos(az);
+    const float c1[3] = {cy * cz, sx * sy * cz - cx * sz, cx * sy * cz + sx * sz};
+    const float c2[3] = {cy * sz, sx * sy * sz + cx * cz, sx * sy * sz - sx * cz};
+    const float c3[3] = {-sy, sx * cy, cx * cy};
+    float no[3], nu[3];
+    for (int k = 0; k < 3; ++k) {
+        no[k] = c1[k] * o[0] + c2[k] * o[1] + c3[k] * o[2];
+        nu[k] = c1[k] * u[0] + c2[k] * u[1] + c3[k] * u[2];
+    }
+    std::memcpy(o, no, sizeof(no));
+    std::memcpy(u, nu, sizeof(nu));
+}
+
+hr_status read_camera(const std::string& path, hr_scene& sc) {
+    std::ifstream in(path);
+    if (!in) return io_error(HR_ERR_INVALID_ARG, "cannot read camera file %s", path.c_str());
+    float rot[3] = {0, 0, 0};
+    std::string line;
+    while (std::getline(in, line)) {
+        const size_t hash = line.find('#');
+        if (hash != std::string::npos) line = line.substr(0, hash);
+        std::stringstream ss(line);
+        std::string key;
+        if (!(ss >> key)) continue;
+        if (key == "position") ss >> sc.pos[0] >> sc.pos[1] >> sc.pos[2];
+        else if (key == "orientation") ss >> sc.orient[0] >> sc.orient[1] >> sc.orient[2];
+        else if (key == "up") ss >> sc.up[0] >> sc.up[1] >> sc.up[2];
+        else if (key == "rotation") ss >> rot[0] >> rot[1] >> rot[2];
+        else if (key == "resX") ss >> sc.w;
+        else if (key == "resY") ss >> sc.h;
+        else if (key == "FOV") ss >> sc.fov;
+    }
+    camera_rotate(sc.orient, sc.up, rot);
+    sc.has_camera = true;
+    return HR_OK;
+}
+
+hr_status read_lights(const std::string& path, hr_scene& sc) {
+    std::ifstream in(path);
+    if (!in) return io_error(HR_ERR_INVALID_ARG, "cannot read light file %s", path.c_str());
+    hr_scene::QuadLight cur;
+    std::memset(&cur, 0, sizeof(cur));
+    bool hp = false, hn = false, hi = false, h1 = false, h2 = false;
+    std::string line;
+    while (std::getline(in, line)) {
+        const size_t hash = line.find('#');
+        if (hash != std::string::npos) line = line.substr(0, hash);
+        std::stringstream ss(line);
+        std::string key;
+        if (!(ss >> key)) continue;
+        if (key == "position") { ss >> cur.position[0] >> cur.position[1] >> cur.position[2]; hp = true; }
+        else if (key == "normal") { ss >> cur.normal[0] >> cur.normal[1] >> cur.normal[2]; hn = true; }
+        else if (key == "intensity") { ss >> cur.intensity[0] >> cur.intensity[1] >> cur.intensity[2]; hi = true; }
+        else if (key == "edge1") { ss >> cur.edge1[0] >> cur.edge1[1] >> cur.edge1[2]; h1 = true; }
+        else if (key == "edge2") { ss >> cur.edge2[0] >> cur.edge2[1] >> cur.edge2[2]; h2 = true; }
+        if (hp && hi && h1 && h2) {   // a complete light (LightSourceLoader.cpp:84-104)
+            if (!hn) {
+                const float* a = cur.edge1;
+                const float* b = cur.edge2;
+                float n[3] = {a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]};
+                const float len = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+                for (int k = 0; k < 3; ++k) cur.normal[k] = len > 0.0f ? n[k] / len : 0.0f;
+            }
+            sc.lights.push_back(cur);
+            std::memset(&cur, 0, sizeof(cur));
+            hp = hn = hi = h1 = h2 = false;
+        }
+    }
+    return HR_OK;
+}
+
+// frame name of AnimationManager::read: the index zero-padded to the digit count of
+// (frames - 1)
+std::string frame_name(const std::string& prefix, const std::string& suffix, uint32_t frame, uint32_t frames) {
+    int digits = 0;
+    for (int n = (int)frames - 1; n > 0; n /= 10) ++digits;
+    std::string id = std::to_string(frame);
+    while ((int)id.size() < digits) id = "0" + id;
+    return prefix + id + suffix;
+}
+
+hr_status finish_scene(hr_scene& sc, std::vector<std::vector<float>>& frames, std::vector<uint32_t>& idx) {
+    if (frames.empty()) return io_error(HR_ERR_INVALID_ARG, "the scene has no geometry");
+    const size_t nv3 = frames[0].size();
+    for (const auto& f : frames)
+        if (f.size() != nv3)
+            return io_error(HR_ERR_INVALID_ARG, "key frames differ in vertex count (%zu vs %zu)", f.size() / 3, nv3 / 3);
+    sc.nv = (uint32_t)(nv3 / 3);
+    sc.nt = (uint32_t)(idx.size() / 3);
+    sc.nkf = (uint32_t)frames.size();
+    sc.kf.reserve(nv3 * frames.size());
+    for (const auto& f : frames) sc.kf.insert(sc.kf.end(), f.begin(), f.end());
+    sc.idx.swap(idx);
+    return HR_OK;
+}
+
+// ---------------------------------------------------------------------------------
+// PNG (RFC 2083) with stored deflate blocks (RFC 1950 / 1951)
+
+uint32_t crc32_update(uint32_t crc, const uint8_t* p, size_t n) {
+    static uint32_t table[256];
+    static bool init = false;
+    if (!init) {
+        for (uint32_t i = 0; i < 256; ++i) {
+            uint32_t c = i;
+            for (int k = 0; k < 8; ++k) c = (c & 1u) ? 0xEDB88320u ^ (c >> 1) : (c >> 1);
+            table[i] = c;
+        }
+        init = true;
+    }
+    for (size_t i = 0; i < n; ++i) crc = table[(crc ^ p[i]) & 0xFFu] ^ (crc >> 8);
+    return crc;
+}
+
+void put_be32(std::vector<uint8_t>& o, uint32_t x) {
+    o.push_back((uint8_t)(x >> 24)); o.push_back((uint8_t)(x >> 16)); o.push_back((uint8_t)(x >> 8)); o.push_back((uint8_t)x);
+}
+
+void png_chunk(std::vector<uint8_t>& o, const char* type, const std::vector<uint8_t>& data) {
+    put_be32(o, (uint32_t)data.size());
+    const size_t at = o.size();
+    o.insert(o.end(), type, type + 4);
+    o.insert(o.end(), data.begin(), data.end());
+    put_be32(o, crc32_update(0xFFFFFFFFu, o.data() + at, data.size() + 4) ^ 0xFFFFFFFFu);
+}
+
+hr_status write_png(const std::string& path, const float* rgb, int32_t w, int32_t h) {
+    std::vector<uint8_t> raw;   // filter byte 0 + RGB per row
+    raw.reserve((size_t)h * ((size_t)w * 3 + 1));
+    for (int32_t y = 0; y < h; ++y) {
+        raw.push_back(0);
+        for (int32_t x = 0; x < w; ++x)
+            for (int k = 0; k < 3; ++k) {
+                float c = rgb[((size_t)y * w + x) * 3 + k];
+                c = std::max(std::min(c, 1.0f), 0.0f);   // NaN -> 0
+                raw.push_back((uint8_t)(c * 255.0f));
+            }
+    }
+    std::vector<uint8_t> z = {0x78, 0x01};   // zlib header, no compression
+    uint32_t a = 1, b = 0;                   // Adler-32
+    for (size_t off = 0; off < raw.size() || off == 0;) {
+        const size_t len = std::min<size_t>(65535, raw.size() - off);
+        const bool last = off + len >= raw.size();
+        z.push_back(last ? 1 : 0);
+        z.push_back((uint8_t)len); z.push_back((uint8_t)(len >> 8));
+        z.push_back((uint8_t)~len); z.push_back((uint8_t)(~len >> 8));
+        z.insert(z.end(), raw.begin() + off, raw.begin() + off + len);
+        for (size_t i = off; i < off + len; ++i) { a = (a + raw[i]) % 65521u; b = (b + a) % 65521u; }
+        off += len;
+        if (last) break;
+    }
+    put_be32(z, (b << 16) | a);
+    std::vector<uint8_t> o = {0x89, 'P', 'N', 'G', '\r', '\n', 0x1A, '\n'};
+    std::vector<uint8_t> ihdr;
+    put_be32(ihdr, (uint32_t)w);
+    put_be32(ihdr, (uint32_t)h);
+    ihdr.insert(ihdr.end(), {8, 2, 0, 0, 0});   // 8-bit RGB, deflate, no filter method, no interlace
+    png_chunk(o, "IHDR", ihdr);
+    png_chunk(o, "IDAT", z);
+    png_chunk(o, "IEND", {});
+    std::ofstream f(path, std::ios::binary);
+    if (!f) return io_error(HR_ERR_INVALID_ARG, "cannot write %s", path.c_str());
+    f.write((const char*)o.data(), (std::streamsize)o.size());
+    return f ? HR_OK : io_error(HR_ERR_INVALID_ARG, "cannot write %s", path.c_str());
+}
+
+hr_status write_pfm(const std::string& path, const float* rgb, int32_t w, int32_t h) {
+    std::ofstream f(path, std::ios::binary);
+    if (!f) return io_error(HR_ERR_INVALID_ARG, "cannot write %s", path.c_str());
+    f << "PF\n" << w << " " << h << "\n-1.0\n";   // little-endian floats, rows bottom to top
+    for (int32_t y = h - 1; y >= 0; --y) f.write((const char*)(rgb + (size_t)y * w * 3), (std::streamsize)w * 12);
+    return f ? HR_OK : io_error(HR_ERR_INVALID_ARG, "cannot write %s", path.c_str());
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* hr_io_last_error(void) { return g_err.c_str(); }
+
+hr_status hr_scene_load_obj(const char* path, int32_t threads, hr_scene** out) {
+    if (!path || !out) return io_error(HR_ERR_INVALID_ARG, "null argument");
+    *out = nullptr;
+    hr_scene* sc = new (std::nothrow) hr_scene();
+    if (!sc) return HR_ERR_OUT_OF_MEMORY;
+    std::vector<std::vector<float>> frames(1);
+    std::vector<uint32_t> idx;
+    hr_status st = read_obj(path, threads, frames[0], idx);
+    if (st == HR_OK) st = finish_scene(*sc, frames, idx);
+    if (st != HR_OK) { delete sc; return st; }
+    *out = sc;
+    return HR_OK;
+}
+
+hr_status hr_scene_load(const char* cfg, int32_t threads, hr_scene** out) {
+    if (!cfg || !out) return io_error(HR_ERR_INVALID_ARG, "null argument");
+    *out = nullptr;
+    std::ifstream in(cfg);
+    if (!in) return io_error(HR_ERR_INVALID_ARG, "cannot read %s", cfg);
+    const std::string base = dir_of(cfg);
+    std::vector<std::string> objs;
+    std::string prefix, suffix, camera, light;
+    uint32_t nframes = 0;
+    float step = 0.0f;
+    std::string line;
+    while (std::getline(in, line)) {
+        const size_t hash = line.find('#');
+        if (hash != std::string::npos) line = line.substr(0, hash);
+        const size_t eq = line.find('=');
+        if (eq == std::string::npos) continue;
+        const std::string key = trim(line.substr(0, eq));
+        const std::string val = trim(line.substr(eq + 1));
+        if (key == "obj" || key == "scene") objs.push_back(val);
+        else if (key == "camera" || key == "view" || key == "cam") camera = val;
+        else if (key == "frame prefix" || key == "frameprefix" || key == "framename") prefix = val;
+        else if (key == "frame suffix" || key == "framesuffix") suffix = val;
+        else if (key == "frame number" || key == "number" || key == "framenumber" || key == "number of frames")
+            nframes = (uint32_t)std::strtoul(val.c_str(), nullptr, 10);
+        else if (key == "frame step" || key == "framestep" || key == "step size")
+            step = std::strtof(val.c_str(), nullptr);
+        else if (key == "light sources" || key == "light source" || key == "light" || key == "lights")
+            light = val;
+        // camera path, instances and unknown keys: not used by the hot path
+    }
+    hr_scene* sc = new (std::nothrow) hr_scene();
+    if (!sc) return HR_ERR_OUT_OF_MEMORY;
+    std::vector<std::vector<float>> frames;
+    std::vector<uint32_t> idx;
+    hr_status st = HR_OK;
+    if (nframes > 0 && (!prefix.empty() || !suffix.empty())) {
+        // key frames (AnimationManager::read): the last frame's triangles are kept
+        for (uint32_t k = 0; k < nframes && st == HR_OK; ++k) {
+            std::vector<float> v;
+            st = read_obj(resolve(frame_name(prefix, suffix, k, nframes), base), threads, v, idx);
+            frames.push_back(std::move(v));
+        }
+    } else {
+        // one static frame: the listed OBJ files concatenated
+        frames.emplace_back();
+        for (size_t i = 0; i < objs.size() && st == HR_OK; ++i) {
+            std::vector<float> v;
+            std::vector<uint32_t> fi;
+            st = read_obj(resolve(objs[i], base), threads, v, fi);
+            const uint32_t off = (uint32_t)(frames[0].size() / 3);
+            for (uint32_t& x : fi) x += off;
+            frames[0].insert(frames[0].end(), v.begin(), v.end());
+            idx.insert(idx.end(), fi.begin(), fi.end());
+        }
+    }
+    sc->frame_step = step;
+    if (st == HR_OK) st = finish_scene(*sc, frames, idx);
+    if (st == HR_OK && !camera.empty()) st = read_camera(resolve(camera, base), *sc);
+    if (st == HR_OK && !light.empty() && file_exists(resolve(light, base))) st = read_lights(resolve(light, base), *sc);
+    if (st != HR_OK) { delete sc; return st; }
+    *out = sc;
+    return HR_OK;
+}
+
+void hr_scene_free(hr_scene* sc) { delete sc; }
+
+hr_status hr_scene_get_info(const hr_scene* sc, hr_scene_info* info) {
+    if (!sc || !info) return io_error(HR_ERR_INVALID_ARG, "null argument");
+    info->num_vertices = sc->nv;
+    info->num_triangles = sc->nt;
+    info->num_keyframes = sc->nkf;
+    info->frame_step = sc->frame_step;
+    info->has_camera = sc->has_camera ? 1 : 0;
+    for (int k = 0; k < 3; ++k) {
+        info->cam_position[k] = sc->pos[k]; info->cam_orientation[k] = sc->orient[k]; info->cam_up[k] = sc->up[k];
+    }
+    info->cam_fov_deg = sc->fov;
+    info->width = sc->w;
+    info->height = sc->h;
+    info->num_lights = (uint32_t)sc->lights.size();
+    return HR_OK;
+}
+
+const float* hr_scene_keyframes(const hr_scene* sc) { return sc ? sc->kf.data() : nullptr; }
+const uint32_t* hr_scene_indices(const hr_scene* sc) { return sc ? sc->idx.data() : nullptr; }
+
+hr_status hr_scene_get_light(const hr_scene* sc, uint32_t i, float pos[3], float e1[3], float e2[3], float n[3],
+                             float inten[3]) {
+    if (!sc || i >= sc->lights.size()) return io_error(HR_ERR_INVALID_ARG, "no light %u", i);
+    const hr_scene::QuadLight& L = sc->lights[i];
+    for (int k = 0; k < 3; ++k) {
+        if (pos) pos[k] = L.position[k];
+        if (e1) e1[k] = L.edge1[k];
+        if (e2) e2[k] = L.edge2[k];
+        if (n) n[k] = L.normal[k];
+        if (inten) inten[k] = L.intensity[k];
+    }
+    return HR_OK;
+}
+
+hr_status hr_scene_upload(hr_ctx* ctx, const hr_scene* sc) {
+    if (!ctx || !sc) return io_error(HR_ERR_INVALID_ARG, "null argument");
+    hr_status st = hr_set_keyframes(ctx, sc->kf.data(), sc->nkf, sc->nv, sc->idx.data(), sc->nt);
+    if (st != HR_OK) return st;
+    if (sc->has_camera && sc->w > 0 && sc->h > 0 &&
+        (st = hr_set_camera(ctx, sc->pos, sc->orient, sc->up, sc->fov, sc->w, sc->h)) != HR_OK)
+        return st;
+    if (!sc->lights.empty()) {
+        const hr_scene::QuadLight& L = sc->lights[0];
+        const float em = (L.intensity[0] + L.intensity[1] + L.intensity[2]) / 3.0f;
+        if ((st = hr_set_light(ctx, L.position, L.edge1, L.edge2, em)) != HR_OK) return st;
+    }
+    return hr_set_frame_time(ctx, 0.0f, 0.0f);
+}
+
+hr_status hr_rays_file_count(const char* path, uint32_t* n) {
+    if (!path || !n) return io_error(HR_ERR_INVALID_ARG, "null argument");
+    std::ifstream f(path, std::ios::binary | std::ios::ate);
+    if (!f) return io_error(HR_ERR_INVALID_ARG, "cannot read %s", path);
+    const std::streamoff sz = f.tellg();
+    if (sz < 0 || sz % 24 != 0) return io_error(HR_ERR_INVALID_ARG, "%s: size is not a multiple of 24 bytes", path);
+    if (sz / 24 > 0xffffffffll) return io_error(HR_ERR_INVALID_ARG, "%s: too many rays", path);
+    *n = (uint32_t)(sz / 24);
+    return HR_OK;
+}
+
+hr_status hr_rays_file_read(const char* path, float* org_dir, uint32_t n) {
+    uint32_t have = 0;
+    hr_status st = hr_rays_file_count(path, &have);
+    if (st != HR_OK) return st;
+    if (!org_dir || n != have) return io_error(HR_ERR_INVALID_ARG, "%s holds %u rays, %u asked", path, have, n);
+    std::ifstream f(path, std::ios::binary);
+    f.read((char*)org_dir, (std::streamsize)n * 24);
+    return f ? HR_OK : io_error(HR_ERR_INVALID_ARG, "cannot read %s", path);
+}
+
+hr_status hr_rays_file_write(const char* path, const float* org, const float* dir, uint32_t n) {
+    if (!path || (n && (!org || !dir))) return io_error(HR_ERR_INVALID_ARG, "null argument");
+    std::ofstream f(path, std::ios::binary);
+    if (!f) return io_error(HR_ERR_INVALID_ARG, "cannot write %s", path);
+    std::vector<float> buf((size_t)std::min<uint32_t>(n, 1u << 20) * 6);
+    for (uint32_t b = 0; b < n; b += 1u << 20) {
+        const uint32_t m = std::min<uint32_t>(n - b, 1u << 20);
+        for (uint32_t i = 0; i < m; ++i)
+            for (int k = 0; k < 3; ++k) {
+                buf[6 * (size_t)i + k] = org[3 * ((size_t)b + i) + k];
+                buf[6 * (size_t)i + 3 + k] = dir[3 * ((size_t)b + i) + k];
+            }
+        f.write((const char*)buf.data(), (std::streamsize)m * 24);
+    }
+    return f ? HR_OK : io_error(HR_ERR_INVALID_ARG, "cannot write %s", path);
+}
+
+hr_status hr_hits_file_write(const char* path, const int32_t* id, const float* t, const float* u, const float* v,
+                             uint32_t n) {
+    if (!path || (n && (!id || !t || !u || !v))) return io_error(HR_ERR_INVALID_ARG, "null argument");
+    std::ofstream f(path, std::ios::binary);
+    if (!f) return io_error(HR_ERR_INVALID_ARG, "cannot write %s", path);
+    for (uint32_t i = 0; i < n; ++i) {
+        f.write((const char*)(id + i), 4);
+        f.write((const char*)(t + i), 4);
+        f.write((const char*)(u + i), 4);
+        f.write((const char*)(v + i), 4);
+    }
+    return f ? HR_OK : io_error(HR_ERR_INVALID_ARG, "cannot write %s", path);
+}
+
+hr_status hr_image_write(const char* path, const float* rgb, int32_t w, int32_t h, int32_t format) {
+    if (!path || !rgb || w <= 0 || h <= 0) return io_error(HR_ERR_INVALID_ARG, "bad image arguments");
+    if (format == HR_IMAGE_PNG) return write_png(path, rgb, w, h);
+    if (format == HR_IMAGE_PFM) return write_pfm(path, rgb, w, h);
+    return io_error(HR_ERR_INVALID_ARG, "unknown image format %d", format);
+}
+
+}  // extern "C"

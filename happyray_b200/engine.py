@@ -94,6 +94,27 @@ class Engine:
         self._chk(self.L.hr_set_frame_time(self.ctx, t, step), "hr_set_frame_time")
 
     # -- RTEngine::setGridDensities / buildAccStruct -----------------------------
+    def upload_scene(self, path: str, threads: int = 0):
+        """Load a scene.cfg (or one .obj) and make it current: key frames, camera and first
+        light (hr_scene_load / hr_scene_upload; CUDAApplication.cu:63-71 reads the same
+        files at start-up).  Returns the camera resolution, or None without a camera."""
+        h = C.c_void_p()
+        fn = self.L.hr_scene_load_obj if str(path).lower().endswith(".obj") else self.L.hr_scene_load
+        st = fn(str(path).encode(), threads, C.byref(h))
+        if st != 0:
+            m = self.L.hr_io_last_error()
+            raise HRError(st, f"load {path}: {m.decode() if m else ''}")
+        try:
+            self._chk(self.L.hr_scene_upload(self.ctx, h), "hr_scene_upload")
+            info = _lib.SceneInfo()
+            self.L.hr_scene_get_info(h, C.byref(info))
+            if info.has_camera and info.width > 0 and info.height > 0:
+                self.res = (info.width, info.height)
+                return self.res
+            return None
+        finally:
+            self.L.hr_scene_free(h)
+
     def setGridDensities(self, top: float, leaf: float):
         self._chk(self.L.hr_set_grid_densities(self.ctx, top, leaf), "hr_set_grid_densities")
 
@@ -171,6 +192,15 @@ class Engine:
         self._chk(self.L.hr_trace_rays(self.ctx, _ptr(org), _ptr(dirs), n, _ptr(hid), _ptr(t), _ptr(u), _ptr(v)),
                   "hr_trace_rays")
         return hid, t, u, v
+
+    def trace_rays_file(self, rays_path: str, hits_path: str) -> int:
+        """Ray query from a .rays file (6 float32 per ray, SimpleRayTraverser.h:200-261) to a
+        hits file (int32 id, float32 t, u, v per ray).  Returns the number of rays."""
+        from . import sceneio
+        org, d = sceneio.read_rays(rays_path)
+        hid, t, u, v = self.trace_rays(org, d)
+        sceneio.write_hits(hits_path, hid, t, u, v)
+        return org.shape[0]
 
     def trace_rays_device(self, d_org, d_dir, n, d_id, d_t, d_u, d_v):
         self._chk(self.L.hr_trace_rays_device(self.ctx, _ptr(d_org), _ptr(d_dir), n, _ptr(d_id), _ptr(d_t),

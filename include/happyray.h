@@ -326,6 +326,66 @@ hr_status hr_server_drain(hr_server *server, int32_t timeout_ms);
 hr_status hr_server_request_info(hr_server *server, uint64_t request_id, hr_request_info *info);
 hr_status hr_server_get_stats(hr_server *server, hr_server_stats *stats);
 
+/* ---------------------------------------------------------------------------------
+ * Scene input, ray files and images (host side; no GPU needed).
+ *   scene.cfg            SceneConfigurationReader.cpp:29-190 ("obj", "frame prefix",
+ *                        "frame suffix", "number of frames", "frame step", "camera",
+ *                        "light", with their aliases; '#' comments)
+ *   key-frame sequences  AnimationManager::read (AnimationLoader.cpp:50-101): frame i is
+ *                        prefix + i zero-padded to the digits of (frames - 1) + suffix
+ *   OBJ                  WFObject::read (WFObjectReader.cpp:320-560): v / f (v, v/t, v//n,
+ *                        v/t/n; polygons fanned from their first vertex); vn, vt, o, g, s,
+ *                        usemtl, mtllib are skipped; parsed in parallel over line chunks
+ *   camera.cfg           CameraManager::read (CameraManager.cpp:33-168): position,
+ *                        orientation, up, rotation (degrees), resX, resY, FOV
+ *   light.cfg            LightSourceLoader::loadFromFile (LightSourceLoader.cpp:29-110)
+ *   .rays                SimpleRayTraverser::loadRaysFromFile (SimpleRayTraverser.h:200-261):
+ *                        headerless float32, 6 per ray (origin xyz, direction xyz)
+ *   images               Image::writePNG (ImagePNG.cpp:160-215): each channel clamped to
+ *                        [0, 1] and truncated to 8 bits; or PFM (float)
+ */
+typedef struct hr_scene hr_scene;
+
+typedef struct hr_scene_info {
+    uint32_t num_vertices, num_triangles, num_keyframes;
+    float frame_step;
+    int32_t has_camera;
+    float cam_position[3], cam_orientation[3], cam_up[3];
+    float cam_fov_deg;
+    int32_t width, height;
+    uint32_t num_lights;
+} hr_scene_info;
+
+#define HR_IMAGE_PNG 0
+#define HR_IMAGE_PFM 1
+
+/* A scene.cfg (animated or static, with its camera and lights), or one OBJ file as a
+ * one-key-frame scene.  Paths inside scene.cfg are taken relative to the working
+ * directory, else to the scene.cfg's directory.  threads <= 0: all hardware threads. */
+hr_status hr_scene_load(const char *scene_cfg_path, int32_t threads, hr_scene **out);
+hr_status hr_scene_load_obj(const char *obj_path, int32_t threads, hr_scene **out);
+void hr_scene_free(hr_scene *scene);
+/* Message of the last failing hr_scene_* / file call of the calling thread. */
+const char *hr_io_last_error(void);
+hr_status hr_scene_get_info(const hr_scene *scene, hr_scene_info *info);
+/* num_keyframes x num_vertices x 3 floats, and num_triangles x 3 indices; owned by the scene. */
+const float *hr_scene_keyframes(const hr_scene *scene);
+const uint32_t *hr_scene_indices(const hr_scene *scene);
+hr_status hr_scene_get_light(const hr_scene *scene, uint32_t light, float position[3], float edge1[3],
+                             float edge2[3], float normal[3], float intensity[3]);
+/* hr_set_keyframes with the scene's frames; its camera (hr_set_camera) if it has one; its
+ * first light (hr_set_light: corner = position, emission = mean intensity) if any. */
+hr_status hr_scene_upload(hr_ctx *ctx, const hr_scene *scene);
+
+hr_status hr_rays_file_count(const char *path, uint32_t *num_rays);
+hr_status hr_rays_file_read(const char *path, float *org_dir, uint32_t num_rays);
+hr_status hr_rays_file_write(const char *path, const float *org, const float *dir, uint32_t num_rays);
+/* Closest hits of a ray query: per ray int32 id, then float32 t, u, v (16 bytes). */
+hr_status hr_hits_file_write(const char *path, const int32_t *id, const float *t, const float *u,
+                             const float *v, uint32_t num_rays);
+/* A float RGB framebuffer (row 0 first) as PNG (8-bit RGB) or PFM (float RGB). */
+hr_status hr_image_write(const char *path, const float *rgb, int32_t width, int32_t height, int32_t format);
+
 #ifdef __cplusplus
 }
 #endif

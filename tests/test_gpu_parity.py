@@ -319,3 +319,48 @@ def test_gpu_matches_reference_golden(engine, path):
     assert np.array_equal(rid, hid)
     hit = hid >= 0
     assert np.all(np.abs(z["strict_hit_t"][hit] - t[hit]) <= 1e-5 * np.abs(t[hit]))
+
+
+def test_scene_file_upload_renders_like_arrays(engine, tmp_path):
+    """A scene.cfg key-frame sequence with camera and light, uploaded from files, renders
+    the same AO and PT images as the same arrays given directly."""
+    from tests.test_io import write_obj
+    v, f = S.clusters(6_000, seed=4)
+    frames = S.curl_keyframes(v, 3, amp=0.02, octaves=2, seed=4)
+    for k in range(3):
+        write_obj(tmp_path / ("fr%d.obj" % k), frames[k], f)
+    cam = S.camera_at_bounds(v, (64, 48))
+    (tmp_path / "camera.cfg").write_text(
+        "position %r %r %r\norientation %r %r %r\nup 0 0 1\nresX 64\nresY 48\nFOV 60\n"
+        % tuple(float(x) for x in list(cam["position"]) + list(cam["orientation"])))
+    (tmp_path / "light.cfg").write_text("position 0.4 0.4 1\nintensity 20 20 20\nedge1 0.2 0 0\nedge2 0 0.2 0\n")
+    (tmp_path / "scene.cfg").write_text("frame prefix = fr\nframe suffix = .obj\nnumber of frames = 3\n"
+                                        "camera = camera.cfg\nlight = light.cfg\n")
+    assert engine.upload_scene(str(tmp_path / "scene.cfg")) == (64, 48)
+    outs = []
+    for use_files in (True, False):
+        if not use_files:
+            engine.set_keyframes(frames, f)
+            engine.setCamera(cam["position"], cam["orientation"], (0, 0, 1), 60.0, 64, 48)
+            engine.setLights((0.4, 0.4, 1.0), (0.2, 0, 0), (0, 0.2, 0), 20.0)
+        engine.set_frame_time(1.25, 0.0)
+        engine.setGridDensities(0.0625, 2.0)
+        engine.build(GRID_TWO_LEVEL)
+        engine.set_integrator(ao_samples=4, ao_radius=-0.1, seed=3)
+        outs.append((engine.renderFrame(None, 0, RENDER_AO), engine.renderFrame(None, 0, RENDER_PATH)))
+    assert np.array_equal(outs[0][0], outs[1][0]) and np.array_equal(outs[0][1], outs[1][1])
+
+
+def test_ray_query_files(engine, oracle, small_clusters, tmp_path):
+    """.rays in, hits out: the ids and t of the oracle's closest hits."""
+    from happyray_b200 import sceneio
+    v, f = small_clusters
+    gpu_build(engine, v, f, GRID_TWO_LEVEL)
+    b = oracle_build(oracle, v, f, GRID_TWO_LEVEL)
+    cam = S.camera_at_bounds(v, (40, 30))
+    org, d = oracle.primary_rays(ocam(oracle, cam))
+    sceneio.write_rays(str(tmp_path / "q.rays"), org, d)
+    assert engine.trace_rays_file(str(tmp_path / "q.rays"), str(tmp_path / "q.hits")) == org.shape[0]
+    rec = np.fromfile(tmp_path / "q.hits", dtype=[("id", "<i4"), ("t", "<f4"), ("u", "<f4"), ("v", "<f4")])
+    hid, t, u, vv = oracle.trace(b, org, d)
+    assert np.array_equal(rec["id"], hid) and np.array_equal(rec["t"], t) and np.array_equal(rec["u"], u)
