@@ -549,6 +549,15 @@ int plan(hr_batch* b) {
         if (hd.error & 2u) return berr(b, HR_ERR_INVALID_ARG, "batch: a scene's top-level grid exceeds 4M cells");
         const uint32_t ovf = hd.overflow;
         if (ovf == 0) {
+            // capacities (which size the per-reference passes, radix tiles and scans) follow
+            // the planned sizes plus 15% instead of the first estimates
+            auto fit = [](size_t& cap, size_t need) {
+                const size_t want = need + need / 7 + 4096;
+                if (cap > want + want / 2) cap = want;
+            };
+            fit(B.cap_pairs, hd.ntop_pairs);
+            fit(B.cap_leaf_pairs, hd.npairs);
+            fit(B.cap_leaves, hd.nleaves);
             b->planned = true;
             break;
         }

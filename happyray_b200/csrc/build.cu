@@ -24,6 +24,7 @@
 //     later passes and the traversal read with one contiguous load per triangle.
 #include "build_dev.cuh"
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 
@@ -408,10 +409,31 @@ static void grow_caps(hr_ctx* c, const GridDesc& hd, uint32_t ovf) {
     if (ovf & kOvfLeafPairs) B.cap_leaf_pairs = (size_t)(hd.req_leaf_pairs * 1.25) + 4096u;
 }
 
+// After a build that fit: capacities follow the largest sizes seen so far plus 15%
+// (an overflow later grows them again and rebuilds).  Smaller capacities mean fewer
+// blocks in the per-reference passes, fewer radix tiles and shorter histogram scans.
+static void fit_caps(hr_ctx* c, const GridDesc& hd, int32_t kind) {
+    GridBuffers& B = c->g;
+    const size_t top = kind == kUniform ? hd.npairs : hd.ntop_pairs;
+    B.seen_pairs = std::max(B.seen_pairs, top);
+    auto fit = [](size_t& cap, size_t seen) {
+        const size_t want = seen + seen / 7 + 4096;
+        if (cap > want + want / 2) cap = want;   // only when the estimate is far above
+    };
+    fit(B.cap_pairs, B.seen_pairs);
+    if (kind == kTwoLevel) {
+        B.seen_leaves = std::max(B.seen_leaves, (size_t)hd.nleaves);
+        B.seen_leaf_pairs = std::max(B.seen_leaf_pairs, (size_t)hd.npairs);
+        fit(B.cap_leaves, B.seen_leaves);
+        fit(B.cap_leaf_pairs, B.seen_leaf_pairs);
+    }
+}
+
 int build_grid(hr_ctx* c, int32_t kind, int32_t exact) {
     GridBuffers& B = c->g;
     if (c->built_kind != kind) {
         B.cap_pairs = 0; B.cap_leaf_pairs = 0; B.cap_leaves = 0;
+        B.seen_pairs = B.seen_leaves = B.seen_leaf_pairs = 0;
     }
     c->async_pending = false;
     for (int attempt = 0; attempt < 6; ++attempt) {
@@ -422,6 +444,7 @@ int build_grid(hr_ctx* c, int32_t kind, int32_t exact) {
             c->built_kind = kind;
             c->built = true;
             c->lerp_pending = false;
+            fit_caps(c, c->host_desc, kind);
             return 0;
         }
         grow_caps(c, c->host_desc, ovf);

@@ -55,6 +55,9 @@ struct GridBuffers {
     DevBuf lkeys_a, lvals_a, lkeys_b, lvals_b;   // two-level: leaf pair ping-pong
     DevBuf scan_partials; // generic scan partial sums
     size_t cap_cells = 0, cap_pairs = 0, cap_top_pairs = 0, cap_leaves = 0, cap_leaf_pairs = 0;
+    // largest sizes seen by a completed build: the capacities (which size the count, scan
+    // and sort launches) follow them with headroom instead of the first estimates
+    size_t seen_pairs = 0, seen_leaves = 0, seen_leaf_pairs = 0;
 };
 
 struct Stats {

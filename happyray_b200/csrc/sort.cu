@@ -127,6 +127,10 @@ __global__ __launch_bounds__(kThreads) void k_radix_upsweep(const uint32_t* __re
     const uint32_t n = *d_count;
     const size_t base = (size_t)blockIdx.x * kTile;
     const int lane = threadIdx.x & 31;
+    if (base >= n) {   // a tile past the count: an empty histogram column
+        for (uint32_t d = threadIdx.x; d <= mask; d += kThreads) tile_hist[(size_t)d * ntiles_cap + blockIdx.x] = 0u;
+        return;
+    }
 #pragma unroll
     for (int k = 0; k < kItems; ++k) {
         size_t i = base + threadIdx.x + (size_t)k * kThreads;
@@ -272,22 +276,33 @@ int exclusive_scan_u32x2(hr_ctx* c, uint2* data, const uint32_t* d_count, size_t
 __global__ __launch_bounds__(1024) void k_scan_block_sums(uint32_t* sums, uint32_t n, uint32_t* d_total,
                                                           uint32_t* ovf, uint32_t cap, uint32_t ovf_bit,
                                                           uint32_t* d_req) {
-    uint32_t carry = 0;
-    for (uint32_t b = 0; b < n; b += 1024) {
-        uint32_t i = b + threadIdx.x;
-        uint32_t x = i < n ? sums[i] : 0u;
+    // 8 consecutive counts per thread, 8192 per round
+    constexpr uint32_t kIpt = 8, kChunk = 1024 * kIpt;
+    uint64_t carry = 0;
+    for (uint32_t b = 0; b < n; b += kChunk) {
+        const uint32_t i0 = b + threadIdx.x * kIpt;
+        uint32_t x[kIpt], s = 0;
+#pragma unroll
+        for (uint32_t k = 0; k < kIpt; ++k) {
+            x[k] = i0 + k < n ? sums[i0 + k] : 0u;
+            s += x[k];
+        }
         uint32_t tot;
-        uint32_t ex = block_excl_scan<uint32_t, 1024>(x, &tot);
-        if (i < n) sums[i] = carry + ex;
+        uint32_t run = (uint32_t)carry + block_excl_scan<uint32_t, 1024>(s, &tot);
+#pragma unroll
+        for (uint32_t k = 0; k < kIpt; ++k) {
+            if (i0 + k < n) sums[i0 + k] = run;
+            run += x[k];
+        }
         carry += tot;
     }
     if (threadIdx.x == 0) {
         if (carry > cap) {
             atomicOr(ovf, ovf_bit);
-            *d_req = carry;
+            *d_req = carry > 0xffffffffull ? 0xffffffffu : (uint32_t)carry;
             *d_total = 0u;
         } else {
-            *d_total = carry;
+            *d_total = (uint32_t)carry;
         }
     }
 }
