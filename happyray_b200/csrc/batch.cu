@@ -387,7 +387,7 @@ int enqueue_build(hr_batch* b) {
     uint32_t* sorted_keys = (passes % 2 == 1) ? B.keys_b.as<uint32_t>() : B.keys_a.as<uint32_t>();
     if ((rc = radix_sort_pairs(c, B.keys_a.as<uint32_t>(), B.vals_a.as<uint32_t>(), B.keys_b.as<uint32_t>(),
                                B.vals_b.as<uint32_t>(), sorted_keys, B.top_refs.as<uint32_t>(), &bd->ntop_pairs,
-                               cap_pairs, key_bits, B.tile_hist.as<uint32_t>(), B.row_total.as<uint32_t>(), s)))
+                               cap_pairs, key_bits, B.tile_hist.as<uint32_t>(), B.tile_hist.bytes, B.row_total.as<uint32_t>(), s)))
         return rc;
     uint2* ranges = B.top_ranges.as<uint2>();
     const int gcells = std::max(1, std::min((int)((B.cap_cells + 255) / 256), c->num_sms * 16));
@@ -414,7 +414,7 @@ int enqueue_build(hr_batch* b) {
     uint32_t* leaf_keys = (lpasses % 2 == 1) ? B.lkeys_b.as<uint32_t>() : B.lkeys_a.as<uint32_t>();
     if ((rc = radix_sort_pairs(c, B.lkeys_a.as<uint32_t>(), B.lvals_a.as<uint32_t>(), B.lkeys_b.as<uint32_t>(),
                                B.lvals_b.as<uint32_t>(), leaf_keys, B.prims.as<uint32_t>(), &bd->npairs,
-                               B.cap_leaf_pairs, leaf_bits, B.tile_hist.as<uint32_t>(), B.row_total.as<uint32_t>(),
+                               B.cap_leaf_pairs, leaf_bits, B.tile_hist.as<uint32_t>(), B.tile_hist.bytes, B.row_total.as<uint32_t>(),
                                s)))
         return rc;
     const int gleaves = std::max(1, std::min((int)((B.cap_leaves + 255) / 256), c->num_sms * 16));
@@ -448,6 +448,7 @@ int upload_jobs(hr_batch* b, int32_t image_id) {
         J.prims = c->g.prims.as<uint32_t>();
         J.desc = dev<GridDesc>(b->d_descs) + i;
         J.cells_offset = dev<uint32_t>(b->d_cell_off) + i;
+        J.status = dev<GridDesc>(b->d_bdesc);   // overflow and error bits of the whole batch build
         J.fb = dev<float>(b->d_fb) + 3 * b->px_off[i];
         const Camera& k = b->cams[i];
         for (int q = 0; q < 3; ++q) {
@@ -567,6 +568,10 @@ int plan(hr_batch* b) {
         if (ovf & kOvfLeafPairs) B.cap_leaf_pairs = (size_t)(hd.req_leaf_pairs * 1.125) + 4096u;
     }
     if (!b->planned) return berr(b, HR_ERR_CAPACITY_RETRY, "batch: grid capacities did not converge");
+    // the fitted capacities can need a LARGER radix histogram than the ones allocated
+    // above: fewer key bits may mean fewer passes of wider digits (17 bits: 3 passes of
+    // 6-bit digits; 16 bits: 2 passes of 8-bit digits, 4x the words per tile)
+    if ((rc = batch_alloc(b))) return rc;
     b->jobs_valid = false;   // grid buffers may have moved
     if (!b->use_graph) return 0;
     const uint64_t l0 = c->launches;

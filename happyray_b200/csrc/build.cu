@@ -336,7 +336,7 @@ static int build_once(hr_ctx* c, int32_t kind, int32_t exact, uint32_t* ovf_out,
     uint32_t* sorted_vals = kind == kUniform ? B.prims.as<uint32_t>() : B.top_refs.as<uint32_t>();
     if ((rc = radix_sort_pairs(c, B.keys_a.as<uint32_t>(), B.vals_a.as<uint32_t>(), B.keys_b.as<uint32_t>(),
                                B.vals_b.as<uint32_t>(), sorted_keys, sorted_vals, d_np, cap_pairs, key_bits,
-                               B.tile_hist.as<uint32_t>(), B.row_total.as<uint32_t>(), s)))
+                               B.tile_hist.as<uint32_t>(), B.tile_hist.bytes, B.row_total.as<uint32_t>(), s)))
         return rc;
     mark();
     uint2* ranges = kind == kUniform ? B.cells.as<uint2>() : B.top_ranges.as<uint2>();
@@ -369,7 +369,7 @@ static int build_once(hr_ctx* c, int32_t kind, int32_t exact, uint32_t* ovf_out,
         uint32_t* leaf_keys = (leaf_passes % 2 == 1) ? B.lkeys_b.as<uint32_t>() : B.lkeys_a.as<uint32_t>();
         if ((rc = radix_sort_pairs(c, B.lkeys_a.as<uint32_t>(), B.lvals_a.as<uint32_t>(), B.lkeys_b.as<uint32_t>(),
                                    B.lvals_b.as<uint32_t>(), leaf_keys, B.prims.as<uint32_t>(), &d->npairs,
-                                   B.cap_leaf_pairs, leaf_bits, B.tile_hist.as<uint32_t>(),
+                                   B.cap_leaf_pairs, leaf_bits, B.tile_hist.as<uint32_t>(), B.tile_hist.bytes,
                                    B.row_total.as<uint32_t>(), s)))
             return rc;
         mark();

@@ -583,11 +583,11 @@ hr_status hr_radix_sort_pairs_device(hr_ctx* c, uint32_t* keys, uint32_t* vals, 
         // passes: b -> keys(tmp) ... ends in `keys`
         if ((rc = ensure(c, B.keys_a, (size_t)n * 4)) || (rc = ensure(c, B.vals_a, (size_t)n * 4))) return (hr_status)rc;
         rc = radix_sort_pairs(c, B.keys_b.as<uint32_t>(), B.vals_b.as<uint32_t>(), B.keys_a.as<uint32_t>(),
-                              B.vals_a.as<uint32_t>(), keys, vals, cnt, n, key_bits, B.tile_hist.as<uint32_t>(),
+                              B.vals_a.as<uint32_t>(), keys, vals, cnt, n, key_bits, B.tile_hist.as<uint32_t>(), B.tile_hist.bytes,
                               B.row_total.as<uint32_t>(), c->stream);
     } else {
         rc = radix_sort_pairs(c, keys, vals, B.keys_b.as<uint32_t>(), B.vals_b.as<uint32_t>(), keys, vals, cnt, n,
-                              key_bits, B.tile_hist.as<uint32_t>(), B.row_total.as<uint32_t>(), c->stream);
+                              key_bits, B.tile_hist.as<uint32_t>(), B.tile_hist.bytes, B.row_total.as<uint32_t>(), c->stream);
     }
     if (rc) return (hr_status)rc;
     return (hr_status)cuda_check(c, cudaStreamSynchronize(c->stream), "radix_sort");

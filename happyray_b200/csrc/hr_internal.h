@@ -145,7 +145,7 @@ int build_async_result(hr_ctx* c, bool* fit);
 int radix_sort_pairs(hr_ctx* c, const uint32_t* keys_in, const uint32_t* vals_in,
                      uint32_t* keys_tmp, uint32_t* vals_tmp, uint32_t* keys_out, uint32_t* vals_out,
                      const uint32_t* d_count, size_t cap_count, int key_bits,
-                     uint32_t* tile_hist, uint32_t* row_total, cudaStream_t s);
+                     uint32_t* tile_hist, size_t tile_hist_bytes, uint32_t* row_total, cudaStream_t s);
 size_t radix_tile_hist_words(size_t cap_count, int key_bits);
 int exclusive_scan_u32(hr_ctx* c, uint32_t* data, const uint32_t* d_count, size_t cap_count,
                        uint32_t* d_total, uint32_t* partials, cudaStream_t s);
@@ -168,6 +168,7 @@ struct Job {
     const uint32_t* prims;
     const GridDesc* desc;
     const uint32_t* cells_offset;    // nullable: added to cells (grids of one batch share arrays)
+    const GridDesc* status;          // nullable (then desc): a grid whose build overflowed or failed is not traced
     float* fb;                       // render jobs: float RGB per pixel
     const float* org;                // ray jobs: 3 floats per ray
     const float* dir;

@@ -21,13 +21,6 @@ constexpr int kJobTT = 256;   // largest block of the persistent kernel
 #define HR_JOB_MIN_BLOCKS 3    // blocks of kJobTT per SM the register budget must allow (3: 80 registers)
 #endif
 
-// closest / any hit on a two-level grid (every job grid is two-level)
-template <bool ANY>
-__device__ __forceinline__ void trace_tl_job(const Scene& s, const G& g, f3 o, f3 d, float tmax, Hit& h, bool active) {
-    h.t = tmax; h.u = 0.0f; h.v = 0.0f; h.tri = 0; h.hit = false; h.cells = 0; h.tests = 0;
-    trace_tl<ANY, false>(s, g, o, d, h, active);
-}
-
 // position of the q-th (0-based) set bit of m; m has more than q set bits
 __device__ __forceinline__ uint32_t nth_set_bit(uint32_t m, uint32_t q) {
     uint32_t pos = 0;
@@ -66,7 +59,10 @@ __device__ __forceinline__ void load_tile_ctx(TileCtx& T, const Job* __restrict_
     T.s.leaves = J->leaves;
     T.s.prims = J->prims;
     T.s.desc = J->desc;
-    T.s.ntri = J->ntri;
+    // a step whose build overflowed (or failed) renders on stale or partial arrays and is
+    // redone by the host: its grid is not traversed
+    const GridDesc* st = J->status ? J->status : J->desc;
+    T.s.ntri = (__ldg(&st->overflow) | __ldg(&st->error)) ? 0u : J->ntri;
     T.s.kind = J->kind;
     T.g = load_g(J->desc);
     for (int q = 0; q < 3; ++q) {
@@ -157,7 +153,7 @@ __global__ __launch_bounds__(kJobTT, HR_JOB_MIN_BLOCKS) void k_trace_jobs(const 
                 if (path_refill(ln, T.cam, tile_local, &next, T.image_id, T.seed, T.fb) == 0u) break;
             }
             if (!__any_sync(kFullMask, ln.has)) break;   // the pool is dry and every path is done
-            const bool cont = path_step<false, true>(T.s, T.g, T.pk, ln.p, ln.has, n);
+            const bool cont = path_step<kTwoLevel, false>(T.s, T.g, T.pk, ln.p, ln.has, n);
             path_retire(ln, cont, T.cam, T.image_id, (int32_t)T.spp, T.seed, T.fb);
         }
         add_rays<false>(counter, false, n.rays);
@@ -197,7 +193,7 @@ __global__ __launch_bounds__(kJobTT, HR_JOB_MIN_BLOCKS) void k_trace_jobs(const 
             d = valid ? primary_dir(T.cam, pix) : mk(1.0f, 0.0f, 0.0f);
         }
         Hit h;
-        trace_tl_job<false>(T.s, T.g, o, d, FLT_MAX, h, valid);
+        trace_one<kTwoLevel, false, false>(T.s, T.g, o, d, FLT_MAX, h, valid);
         add_rays<false>(counter, false, valid ? 1u : 0u);
         if (rays) {
             if (valid) {
@@ -263,7 +259,7 @@ __global__ __launch_bounds__(kJobTT, HR_JOB_MIN_BLOCKS) void k_trace_jobs(const 
                 ao = mk(T.px[src] + off * w.x, T.py[src] + off * w.y, T.pz[src] + off * w.z);
             }
             Hit hs;
-            trace_tl_job<true>(T.s, T.g, ao, w, T.alpha, hs, v2);
+            trace_one<kTwoLevel, true, false>(T.s, T.g, ao, w, T.alpha, hs, v2);
             const uint32_t fm = __ballot_sync(kFullMask, v2 && !hs.hit);
             if (hit) {
                 // this lane's samples are items [rank * spp, rank * spp + spp)

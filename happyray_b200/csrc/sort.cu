@@ -331,7 +331,11 @@ size_t radix_tile_hist_words(size_t cap_count, int key_bits) {
 int radix_sort_pairs(hr_ctx* c, const uint32_t* keys_in, const uint32_t* vals_in,
                      uint32_t* keys_tmp, uint32_t* vals_tmp, uint32_t* keys_out, uint32_t* vals_out,
                      const uint32_t* d_count, size_t cap_count, int key_bits,
-                     uint32_t* tile_hist, uint32_t* row_total, cudaStream_t s) {
+                     uint32_t* tile_hist, size_t tile_hist_bytes, uint32_t* row_total, cudaStream_t s) {
+    // the histogram holds 2^digit words per tile: fewer key bits can need more of them
+    if (radix_tile_hist_words(cap_count, key_bits) * sizeof(uint32_t) > tile_hist_bytes)
+        return set_error(c, 4, "radix sort: histogram of %zu bytes is too small for %zu keys of %d bits",
+                         tile_hist_bytes, cap_count, key_bits);
     int passes, db;
     radix_plan(key_bits, &passes, &db);
     const uint32_t mask = (1u << db) - 1u;

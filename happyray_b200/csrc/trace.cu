@@ -20,16 +20,19 @@
 // The traversal itself (warp-synchronous DDA + intersection) lives in traverse.cuh.
 #include "traverse.cuh"
 
+#include <type_traits>
+
 namespace hr {
 
 namespace {
 
-template <bool STATS>
+template <int KIND, bool STATS>
 __global__ __launch_bounds__(kTT, 8) void k_trace_rays(Scene s, const float* __restrict__ org, const float* __restrict__ dir,
                                                     uint32_t n, int32_t* __restrict__ oid, float* __restrict__ ot,
                                                     float* __restrict__ ou, float* __restrict__ ov,
                                                     uint32_t* __restrict__ stats) {
     const G g = load_g(s.desc);
+    gate_scene(s);
     const uint32_t nl = round32(n);
     for (uint32_t i = blockIdx.x * kTT + threadIdx.x; i < nl; i += gridDim.x * kTT) {
         const bool valid = i < n;
@@ -39,7 +42,7 @@ __global__ __launch_bounds__(kTT, 8) void k_trace_rays(Scene s, const float* __r
             d = mk(__ldg(dir + 3 * (size_t)i), __ldg(dir + 3 * (size_t)i + 1), __ldg(dir + 3 * (size_t)i + 2));
         }
         Hit h;
-        trace_one<false, STATS>(s, g, o, d, FLT_MAX, h, valid);
+        trace_one<KIND, false, STATS>(s, g, o, d, FLT_MAX, h, valid);
         if (valid) {
             oid[i] = h.hit ? (int32_t)h.tri : -1;
             ot[i] = h.hit ? h.t : FLT_MAX;
@@ -50,18 +53,19 @@ __global__ __launch_bounds__(kTT, 8) void k_trace_rays(Scene s, const float* __r
     }
 }
 
-template <bool STATS>
+template <int KIND, bool STATS>
 __global__ __launch_bounds__(kTT, 8) void k_trace_primary(Scene s, Cam cam, int32_t* __restrict__ oid,
                                                        float* __restrict__ ot, float* __restrict__ ou,
                                                        float* __restrict__ ov, uint32_t* __restrict__ stats) {
     const G g = load_g(s.desc);
+    gate_scene(s);
     const uint32_t slots = tile_slots(cam);
     const f3 o = mk(cam.pos[0], cam.pos[1], cam.pos[2]);
     for (uint32_t slot = blockIdx.x * kTT + threadIdx.x; slot < slots; slot += gridDim.x * kTT) {
         uint32_t i;
         const bool valid = tile_pixel(cam, slot, &i);
         Hit h;
-        trace_one<false, STATS>(s, g, o, valid ? primary_dir(cam, i) : mk(1.0f, 0.0f, 0.0f), FLT_MAX, h, valid);
+        trace_one<KIND, false, STATS>(s, g, o, valid ? primary_dir(cam, i) : mk(1.0f, 0.0f, 0.0f), FLT_MAX, h, valid);
         if (valid) {
             oid[i] = h.hit ? (int32_t)h.tri : -1;
             ot[i] = h.hit ? h.t : FLT_MAX;
@@ -72,9 +76,11 @@ __global__ __launch_bounds__(kTT, 8) void k_trace_primary(Scene s, Cam cam, int3
     }
 }
 
+template <int KIND>
 __global__ __launch_bounds__(kTT, 8) void k_occluded(Scene s, const float* __restrict__ org, const float* __restrict__ dir,
                                                   const float* __restrict__ tmax, uint32_t n, uint8_t* __restrict__ occ) {
     const G g = load_g(s.desc);
+    gate_scene(s);
     const uint32_t nl = round32(n);
     for (uint32_t i = blockIdx.x * kTT + threadIdx.x; i < nl; i += gridDim.x * kTT) {
         const bool valid = i < n;
@@ -86,16 +92,17 @@ __global__ __launch_bounds__(kTT, 8) void k_occluded(Scene s, const float* __res
             tm = tmax[i];
         }
         Hit h;
-        trace_one<true, false>(s, g, o, d, tm, h, valid);
+        trace_one<KIND, true, false>(s, g, o, d, tm, h, valid);
         if (valid) occ[i] = h.hit ? 1 : 0;
     }
 }
 
 // mode 0: primary rays with barycentric false colour (SimpleIntegrator.h:41-126)
-template <bool STATS>
+template <int KIND, bool STATS>
 __global__ __launch_bounds__(kTT, 8) void k_render_primary(Scene s, Cam cam, int32_t image_id, float* __restrict__ fb,
                                                         unsigned long long* counter) {
     const G g = load_g(s.desc);
+    gate_scene(s);
     const uint32_t slots = tile_slots(cam);
     const f3 o = mk(cam.pos[0], cam.pos[1], cam.pos[2]);
     for (uint32_t slot = blockIdx.x * kTT + threadIdx.x; slot < slots; slot += gridDim.x * kTT) {
@@ -103,7 +110,7 @@ __global__ __launch_bounds__(kTT, 8) void k_render_primary(Scene s, Cam cam, int
         const bool valid = tile_pixel(cam, slot, &i);
         const f3 d = valid ? primary_dir(cam, i) : mk(1.0f, 0.0f, 0.0f);
         Hit h;
-        trace_one<false, STATS>(s, g, o, d, FLT_MAX, h, valid);
+        trace_one<KIND, false, STATS>(s, g, o, d, FLT_MAX, h, valid);
         if (valid) {
             float r = 0.15f, gg = 0.2f, b = 0.3f;
             if (h.hit) {
@@ -128,12 +135,13 @@ __global__ __launch_bounds__(kTT, 8) void k_render_primary(Scene s, Cam cam, int
 //                 the pixel (sample k uses draws 2k and 2k+1), any-hit traversal, and the
 //                 unoccluded count of the pixel (match_any-aggregated atomics);
 //   k_ao_finish   visibility = unoccluded / samples, progressive blend (AOIntegrator.h:168-175).
-template <bool STATS>
+template <int KIND, bool STATS>
 __global__ __launch_bounds__(kTT, 8) void k_ao_primary(Scene s, Cam cam, int32_t image_id, float* __restrict__ fb,
                                                     float* __restrict__ hit_t, uint32_t* __restrict__ hit_tri,
                                                     uint32_t* __restrict__ unocc, uint32_t* __restrict__ queue,
                                                     uint32_t* qcount, unsigned long long* counter) {
     const G g = load_g(s.desc);
+    gate_scene(s);
     const uint32_t slots = tile_slots(cam);
     const f3 o = mk(cam.pos[0], cam.pos[1], cam.pos[2]);
     const uint32_t lane = threadIdx.x & 31u, lt = (1u << lane) - 1u;
@@ -141,7 +149,7 @@ __global__ __launch_bounds__(kTT, 8) void k_ao_primary(Scene s, Cam cam, int32_t
         uint32_t pix;
         const bool valid = tile_pixel(cam, slot, &pix);
         Hit h;
-        trace_one<false, STATS>(s, g, o, valid ? primary_dir(cam, pix) : mk(1.0f, 0.0f, 0.0f), FLT_MAX, h, valid);
+        trace_one<KIND, false, STATS>(s, g, o, valid ? primary_dir(cam, pix) : mk(1.0f, 0.0f, 0.0f), FLT_MAX, h, valid);
         const bool hit = valid && h.hit;
         if (hit) {
             hit_t[pix] = h.t;
@@ -165,13 +173,14 @@ __global__ __launch_bounds__(kTT, 8) void k_ao_primary(Scene s, Cam cam, int32_t
     }
 }
 
-template <bool STATS>
+template <int KIND, bool STATS>
 __global__ __launch_bounds__(kTT, 8) void k_ao_samples(Scene s, Cam cam, int32_t spp, float alpha_frac, float alpha_abs,
                                                     uint64_t seed, int32_t image_id, const float* __restrict__ hit_t,
                                                     const uint32_t* __restrict__ hit_tri,
                                                     const uint32_t* __restrict__ queue, const uint32_t* qcount,
                                                     uint32_t* __restrict__ unocc, unsigned long long* counter) {
     const G g = load_g(s.desc);
+    gate_scene(s);
     float alpha = alpha_abs;
     if (!(alpha > 0.0f)) {
         const f3 dd = mk(g.bmax[0] - g.bmin[0], g.bmax[1] - g.bmin[1], g.bmax[2] - g.bmin[2]);
@@ -200,7 +209,7 @@ __global__ __launch_bounds__(kTT, 8) void k_ao_samples(Scene s, Cam cam, int32_t
             ao = mk(p.x + off * w.x, p.y + off * w.y, p.z + off * w.z);
         }
         Hit hs;
-        trace_one<true, STATS>(s, g, ao, w, alpha, hs, valid);
+        trace_one<KIND, true, STATS>(s, g, ao, w, alpha, hs, valid);
         const bool free = valid && !hs.hit;
         const uint32_t peers = __match_any_sync(kFullMask, pix);
         const uint32_t nfree = __popc(__ballot_sync(kFullMask, free) & peers);
@@ -230,12 +239,13 @@ __global__ void k_ao_finish(const uint32_t* __restrict__ queue, const uint32_t* 
 // path per pixel.  Persistent: each warp takes 32-pixel tiles from *work, and a lane whose
 // path ends takes the next pixel at once (path_refill / path_step / path_retire), so lanes
 // do not idle through the bounces of their warp's longest path.
-template <bool STATS>
+template <int KIND, bool STATS>
 __global__ __launch_bounds__(kTT, HR_PT_MIN_BLOCKS) void k_render_pt(Scene s, Cam cam, LightP l, int32_t bounces,
                                                                   float albedo, float eps_frac, uint64_t seed,
                                                                   int32_t image_id, float* __restrict__ fb,
                                                                   unsigned long long* counter, uint32_t* work) {
     const G g = load_g(s.desc);
+    gate_scene(s);
     const PtConsts k = pt_consts(g, l, bounces, albedo, eps_frac);
     const uint32_t ntiles = tile_slots(cam) >> 5;
     const uint32_t lane = threadIdx.x & 31u;
@@ -259,7 +269,7 @@ __global__ __launch_bounds__(kTT, HR_PT_MIN_BLOCKS) void k_render_pt(Scene s, Ca
             if (path_refill(ln, cam, tile, &next, image_id, seed, fb) == 0u) break;
         }
         if (!__any_sync(kFullMask, ln.has)) break;
-        const bool cont = path_step<STATS, false>(s, g, k, ln.p, ln.has, n);
+        const bool cont = path_step<KIND, STATS>(s, g, k, ln.p, ln.has, n);
         path_retire(ln, cont, cam, image_id, 1, seed, fb);
     }
     add_rays<STATS>(counter, false, n.rays, n.cells, n.tests);
@@ -298,6 +308,21 @@ uint32_t slots_for(const hr_ctx* c) {
     return (((uint32_t)c->cam.w + 7u) / 8u) * (((uint32_t)c->cam.h + 3u) / 4u) * 32u;
 }
 
+template <int V> using IntC = std::integral_constant<int, V>;
+template <bool V> using BoolC = std::integral_constant<bool, V>;
+
+// f(IntC<kind>, BoolC<stats>): picks the kernel instance of the built grid's kind
+template <class F>
+void by_kind(int32_t kind, bool stats, F&& f) {
+    if (kind == kUniform) {
+        if (stats) f(IntC<kUniform>{}, BoolC<true>{});
+        else f(IntC<kUniform>{}, BoolC<false>{});
+    } else {
+        if (stats) f(IntC<kTwoLevel>{}, BoolC<true>{});
+        else f(IntC<kTwoLevel>{}, BoolC<false>{});
+    }
+}
+
 }  // namespace
 
 int launch_trace_rays(hr_ctx* c, const float* org, const float* dir, uint32_t n, int32_t* id, float* t, float* u,
@@ -305,8 +330,9 @@ int launch_trace_rays(hr_ctx* c, const float* org, const float* dir, uint32_t n,
     if (n == 0) return 0;
     Scene s = make_scene(c);
     c->launches += 1;
-    if (stats) k_trace_rays<true><<<grid_for(c, n), kTT, 0, c->stream>>>(s, org, dir, n, id, t, u, v, stats);
-    else k_trace_rays<false><<<grid_for(c, n), kTT, 0, c->stream>>>(s, org, dir, n, id, t, u, v, nullptr);
+    by_kind(s.kind, stats != nullptr, [&](auto K, auto S) {
+        k_trace_rays<K(), S()><<<grid_for(c, n), kTT, 0, c->stream>>>(s, org, dir, n, id, t, u, v, stats);
+    });
     return cuda_check(c, cudaGetLastError(), "trace_rays launch");
 }
 
@@ -317,15 +343,17 @@ int launch_trace_primary(hr_ctx* c, int32_t* id, float* t, float* u, float* v, u
     if (n == 0) return 0;
     c->launches += 1;
     const int gb = grid_for(c, slots_for(c));
-    if (stats) k_trace_primary<true><<<gb, kTT, 0, c->stream>>>(s, k, id, t, u, v, stats);
-    else k_trace_primary<false><<<gb, kTT, 0, c->stream>>>(s, k, id, t, u, v, nullptr);
+    by_kind(s.kind, stats != nullptr, [&](auto K, auto S) {
+        k_trace_primary<K(), S()><<<gb, kTT, 0, c->stream>>>(s, k, id, t, u, v, stats);
+    });
     return cuda_check(c, cudaGetLastError(), "trace_primary launch");
 }
 
 int launch_occluded(hr_ctx* c, const float* org, const float* dir, const float* tmax, uint32_t n, uint8_t* occ) {
     if (n == 0) return 0;
     c->launches += 1;
-    k_occluded<<<grid_for(c, n), kTT, 0, c->stream>>>(make_scene(c), org, dir, tmax, n, occ);
+    const Scene s = make_scene(c);
+    by_kind(s.kind, false, [&](auto K, auto) { k_occluded<K()><<<grid_for(c, n), kTT, 0, c->stream>>>(s, org, dir, tmax, n, occ); });
     return cuda_check(c, cudaGetLastError(), "occluded launch");
 }
 
@@ -344,8 +372,7 @@ int launch_render(hr_ctx* c, int32_t mode, int32_t image_id, float* d_fb) {
     case 0:
         c->launches += 1;
         mark(0);
-        if (st) k_render_primary<true><<<gb, kTT, 0, strm>>>(s, k, image_id, d_fb, ctr);
-        else k_render_primary<false><<<gb, kTT, 0, strm>>>(s, k, image_id, d_fb, ctr);
+        by_kind(s.kind, st, [&](auto K, auto S) { k_render_primary<K(), S()><<<gb, kTT, 0, strm>>>(s, k, image_id, d_fb, ctr); });
         mark(1);
         c->nrender_ev = 2;
         break;
@@ -357,20 +384,18 @@ int launch_render(hr_ctx* c, int32_t mode, int32_t image_id, float* d_fb) {
         uint32_t* work = reinterpret_cast<uint32_t*>(ctr + 7);
         int rc;
         if ((rc = cuda_check(c, cudaMemsetAsync(work, 0, sizeof(uint32_t), strm), "tile counter reset"))) return rc;
-        int nb = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_render_pt<false>, kTT, 0) != cudaSuccess || nb < 1) {
-            cudaGetLastError();
-            nb = 1;
-        }
-        const int gp = std::min(gb, nb * c->num_sms);
         c->launches += 1;
         mark(0);
-        if (st)
-            k_render_pt<true><<<gp, kTT, 0, strm>>>(s, k, l, c->ip.pt_bounces, c->ip.albedo, c->ip.ray_eps_frac,
-                                                    c->ip.seed, image_id, d_fb, ctr, work);
-        else
-            k_render_pt<false><<<gp, kTT, 0, strm>>>(s, k, l, c->ip.pt_bounces, c->ip.albedo, c->ip.ray_eps_frac,
-                                                     c->ip.seed, image_id, d_fb, ctr, work);
+        by_kind(s.kind, st, [&](auto K, auto S) {
+            int nb = 0;
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_render_pt<K(), S()>, kTT, 0) != cudaSuccess || nb < 1) {
+                cudaGetLastError();
+                nb = 1;
+            }
+            const int gp = std::min(gb, nb * c->num_sms);
+            k_render_pt<K(), S()><<<gp, kTT, 0, strm>>>(s, k, l, c->ip.pt_bounces, c->ip.albedo, c->ip.ray_eps_frac,
+                                                        c->ip.seed, image_id, d_fb, ctr, work);
+        });
         mark(1);
         c->nrender_ev = 2;
         break;
@@ -385,22 +410,19 @@ int launch_render(hr_ctx* c, int32_t mode, int32_t image_id, float* d_fb) {
         const int spp = c->ip.ao_samples;
         c->launches += 3;
         mark(0);
-        if (st)
-            k_ao_primary<true><<<gb, kTT, 0, strm>>>(s, k, image_id, d_fb, c->hit_t.as<float>(), c->hit_tri.as<uint32_t>(),
-                                                     c->unocc.as<uint32_t>(), c->queue.as<uint32_t>(), qcount, ctr);
-        else
-            k_ao_primary<false><<<gb, kTT, 0, strm>>>(s, k, image_id, d_fb, c->hit_t.as<float>(), c->hit_tri.as<uint32_t>(),
-                                                      c->unocc.as<uint32_t>(), c->queue.as<uint32_t>(), qcount, ctr);
+        by_kind(s.kind, st, [&](auto K, auto S) {
+            k_ao_primary<K(), S()><<<gb, kTT, 0, strm>>>(s, k, image_id, d_fb, c->hit_t.as<float>(),
+                                                         c->hit_tri.as<uint32_t>(), c->unocc.as<uint32_t>(),
+                                                         c->queue.as<uint32_t>(), qcount, ctr);
+        });
         mark(1);
         const int gs = c->num_sms * 16;
-        if (st)
-            k_ao_samples<true><<<gs, kTT, 0, strm>>>(s, k, spp, c->ip.ao_radius_frac, c->ip.ao_radius_abs, c->ip.seed,
-                                                     image_id, c->hit_t.as<float>(), c->hit_tri.as<uint32_t>(),
-                                                     c->queue.as<uint32_t>(), qcount, c->unocc.as<uint32_t>(), ctr);
-        else
-            k_ao_samples<false><<<gs, kTT, 0, strm>>>(s, k, spp, c->ip.ao_radius_frac, c->ip.ao_radius_abs, c->ip.seed,
-                                                      image_id, c->hit_t.as<float>(), c->hit_tri.as<uint32_t>(),
-                                                      c->queue.as<uint32_t>(), qcount, c->unocc.as<uint32_t>(), ctr);
+        by_kind(s.kind, st, [&](auto K, auto S) {
+            k_ao_samples<K(), S()><<<gs, kTT, 0, strm>>>(s, k, spp, c->ip.ao_radius_frac, c->ip.ao_radius_abs,
+                                                         c->ip.seed, image_id, c->hit_t.as<float>(),
+                                                         c->hit_tri.as<uint32_t>(), c->queue.as<uint32_t>(), qcount,
+                                                         c->unocc.as<uint32_t>(), ctr);
+        });
         mark(2);
         k_ao_finish<<<c->num_sms * 4, 256, 0, strm>>>(c->queue.as<uint32_t>(), qcount, c->unocc.as<uint32_t>(), spp,
                                                       image_id, d_fb);

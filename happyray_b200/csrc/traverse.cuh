@@ -8,12 +8,12 @@
 //   camera                 src/RT/Primitive/Camera.h:35-72
 //
 // Execution model: the traversal is warp-synchronous.  Every lane advances its own DDA
-// to its next non-empty cell or leaf, then the warp tests the triangle lists together:
-// a lane with a short list tests it alone; a long list (more than kCoopMin triangles,
-// e.g. a whole small sphere inside one leaf) is tested by all 32 lanes, strided, and
-// reduced by (smallest t, then smallest list position), which is exactly the
-// first-tested-wins rule of the sequential intersector.  Traversal functions must
-// therefore be called by all lanes of a warp; lanes without a ray pass active = false.
+// to its next cell or leaf, then the warp tests the triangle lists of all its lanes
+// together, packed 32 (lane, triangle) pairs per round (test_lists), so that no lane idles
+// while another walks a longer list.  Hits are applied in list order with the strict
+// t < best rule, which is exactly the first-tested-wins result of the sequential
+// intersector.  Traversal functions must therefore be called by all lanes of a warp;
+// lanes without a ray pass active = false.
 #pragma once
 
 #include "hr_internal.h"
@@ -21,8 +21,6 @@
 
 namespace hr {
 namespace {
-
-constexpr uint32_t kCoopMin = 8;   // longer triangle lists are intersected by the whole warp
 
 struct Scene {
     const float4* __restrict__ tris;   // 3 float4 per triangle (current frame)
@@ -38,6 +36,12 @@ struct G {
     float bmin[3], bmax[3], cs[3], rcp[3];
     int32_t res[3];
 };
+// A grid whose build overflowed or failed holds stale or partial arrays (the host redoes
+// the frame): kernels trace no triangle of it.
+__device__ __forceinline__ void gate_scene(Scene& s) {
+    if (__ldg(&s.desc->overflow) | __ldg(&s.desc->error)) s.ntri = 0u;
+}
+
 __device__ __forceinline__ G load_g(const GridDesc* d) {
     G g;
 #pragma unroll
@@ -74,73 +78,78 @@ __device__ __forceinline__ bool mt_test(const Scene& s, uint32_t tri, f3 o, f3 d
     return u >= 0.0f && v >= 0.0f && u + v <= 1.0f && t > kIsectEps && t < tbest;
 }
 
-// prims[b, e) tested in order by one lane; first-tested wins ties (strict <)
-template <bool ANY, bool STATS>
-__device__ __forceinline__ bool isect_range(const Scene& s, f3 o, f3 d, uint32_t b, uint32_t e, Hit& h) {
-    for (uint32_t it = b; it < e; ++it) {
-        const uint32_t tri = __ldg(s.prims + it);
-        float t, u, v;
-        if (STATS) h.tests++;
-        if (mt_test(s, tri, o, d, h.t, &t, &u, &v)) {
-            h.t = t; h.u = u; h.v = v; h.tri = tri; h.hit = true;
-            if (ANY) return true;
-        }
-    }
-    return false;
-}
-
 __device__ __forceinline__ float shfl(float x, int src) { return __shfl_sync(kFullMask, x, src); }
 __device__ __forceinline__ uint32_t shfl(uint32_t x, int src) { return __shfl_sync(kFullMask, x, src); }
 
-// Warp-wide test of every lane's list prims[b, e).  Must be called by all 32 lanes.
-// Returns true on the lanes whose any-hit query is answered (ANY) by this test.
+// Warp-wide test of every lane's list prims[b, e); must be called by all 32 lanes, and
+// returns true on the lanes whose any-hit query it answers.  The (lane, triangle) pairs of
+// all lanes are numbered in lane order and tested 32 per round, one pair per lane, so no
+// lane idles while another walks a longer list.  Pair j belongs to the lane whose
+// [exclusive, inclusive) prefix of list lengths holds j and is tested with that lane's
+// ray and current bound.  Closest hit: the hits of a round are applied one by one in pair
+// order, each only if its t is strictly below the lane's best so far -- the
+// first-tested-wins rule of a one-lane loop over the list.  Any hit: a lane is answered
+// when one of its pairs hits; its later pairs are skipped.  STATS counts the pairs
+// tested: all of a list for closest hit (as the sequential loop), whole rounds for any hit.
 template <bool ANY, bool STATS>
 __device__ __forceinline__ bool test_lists(const Scene& s, f3 o, f3 d, uint32_t b, uint32_t e, Hit& h) {
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t n = e - b;
-    const bool coop = n > kCoopMin;
-    bool done = false;
-    if (!coop && n) done = isect_range<ANY, STATS>(s, o, d, b, e, h);
-    uint32_t m = __ballot_sync(kFullMask, coop);
-    while (m) {
-        const int src = __ffs(m) - 1;
-        m &= m - 1;
-        const f3 so = mk(shfl(o.x, src), shfl(o.y, src), shfl(o.z, src));
-        const f3 sd = mk(shfl(d.x, src), shfl(d.y, src), shfl(d.z, src));
-        const uint32_t sb = shfl(b, src), se = shfl(e, src);
-        float bt = shfl(h.t, src), bu = 0.0f, bv = 0.0f;
-        uint32_t bit = 0xffffffffu;
-        uint32_t tested = 0;
-        for (uint32_t base = sb; base < se; base += 32u) {
-            const uint32_t it = base + lane;
-            if (it < se) {
-                float t, u, v;
-                if (mt_test(s, __ldg(s.prims + it), so, sd, bt, &t, &u, &v)) { bt = t; bu = u; bv = v; bit = it; }
-            }
-            tested += min(32u, se - base);
-            if (ANY && __any_sync(kFullMask, bit != 0xffffffffu)) break;
-        }
-        // (smallest t, smallest position) over the warp = the sequential first-tested-wins hit
-        float rt = bt;
-        uint32_t rit = bit;
+    if (__ballot_sync(kFullMask, n != 0u) == 0u) return false;   // most leaves a ray crosses are empty
+    uint32_t incl = n;
 #pragma unroll
-        for (int off = 16; off > 0; off >>= 1) {
-            const float ot = __shfl_xor_sync(kFullMask, rt, off);
-            const uint32_t oit = __shfl_xor_sync(kFullMask, rit, off);
-            if (ot < rt || (ot == rt && oit < rit)) { rt = ot; rit = oit; }
+    for (int off = 1; off < 32; off <<= 1) {
+        const uint32_t x = __shfl_up_sync(kFullMask, incl, off);
+        if (lane >= (uint32_t)off) incl += x;
+    }
+    const uint32_t total = __shfl_sync(kFullMask, incl, 31);
+    // prims index of pair j of this lane: rel + j, summed in 32 bits (rel wraps when b is
+    // below the lane's exclusive prefix; the sum does not)
+    const uint32_t rel = b - (incl - n);
+    uint32_t best = 0xffffffffu;           // pair number of this lane's best hit of this call
+    uint32_t answered = 0u;                // ANY: lanes with a hit
+    for (uint32_t base = 0; base < total; base += 32u) {
+        const uint32_t j = base + lane;
+        uint32_t own = 0;                  // number of lanes whose inclusive prefix is <= j
+#pragma unroll
+        for (uint32_t step = 16; step > 0; step >>= 1) {
+            if (__shfl_sync(kFullMask, incl, own + step - 1u) <= j) own += step;
         }
-        const uint32_t own = __ballot_sync(kFullMask, bit == rit && rit != 0xffffffffu);
-        if (rit != 0xffffffffu) {
-            const int w = __ffs(own) - 1;
-            const float wu = shfl(bu, w), wv = shfl(bv, w);
-            if ((int)lane == src) {
-                h.t = rt; h.u = wu; h.v = wv; h.tri = __ldg(s.prims + rit); h.hit = true;
-                if (ANY) done = true;
+        const f3 so = mk(shfl(o.x, own), shfl(o.y, own), shfl(o.z, own));
+        const f3 sd = mk(shfl(d.x, own), shfl(d.y, own), shfl(d.z, own));
+        const float bt = shfl(h.t, own);
+        const uint32_t srel = shfl(rel, own);
+        const bool live = j < total && !(ANY && ((answered >> own) & 1u));
+        float t = 0.0f, u = 0.0f, v = 0.0f;
+        bool hit = false;
+        if (live) hit = mt_test(s, __ldg(s.prims + (srel + j)), so, sd, bt, &t, &u, &v);
+        if (STATS && !(ANY && ((answered >> lane) & 1u))) {   // this lane's pairs tested in the round
+            const uint32_t lo = max(incl - n, base), hi = min(incl, base + 32u);
+            if (hi > lo) h.tests += hi - lo;
+        }
+        if (ANY) {
+            answered |= __reduce_or_sync(kFullMask, hit ? 1u << own : 0u);
+        } else {
+            uint32_t hm = __ballot_sync(kFullMask, hit);
+            while (hm) {
+                const int src = __ffs(hm) - 1;
+                hm &= hm - 1u;
+                const uint32_t ow = shfl(own, src), hj = shfl(j, src);
+                const float ht = shfl(t, src), hu = shfl(u, src), hv = shfl(v, src);
+                if (lane == ow && ht < h.t) {
+                    h.t = ht; h.u = hu; h.v = hv; h.hit = true;
+                    best = hj;
+                }
             }
         }
-        if (STATS && (int)lane == src) h.tests += tested;
     }
-    return done;
+    if (ANY) {
+        const bool done = (answered >> lane) & 1u;
+        if (done) h.hit = true;
+        return done;
+    }
+    if (best != 0xffffffffu) h.tri = __ldg(s.prims + (rel + best));
+    return false;
 }
 
 __device__ __forceinline__ int min_dim(float a, float b, float c) { return a < b ? (a < c ? 0 : 2) : (b < c ? 1 : 2); }
@@ -251,10 +260,11 @@ __device__ __forceinline__ void tl_enter(TL& q, const G& g, f3 o, f3 d, uint2 tc
         const float srcp = g.rcp[k] * cres;
         const float mb = (float)q.cell[k] * g.cs[k] + g.bmin[k];
         float cf = floorf((comp(e2, k) - mb) * srcp);
-        q.scs[k] = 1.0f / srcp;
+        const float scs = 1.0f / srcp;
+        q.scs[k] = scs;
         cf = hmin(cres - 1.0f, hmax(cf, 0.0f));
         const float stp = q.rcp[k] > 0.0f ? 1.0f : 0.0f;
-        q.tm2[k] = ((cf + stp) * q.scs[k] + mb - comp(o, k)) * q.rcp[k];
+        q.tm2[k] = ((cf + stp) * scs + mb - comp(o, k)) * q.rcp[k];
         q.c2[k] = f2i(cf);
     }
 }
@@ -281,6 +291,18 @@ __device__ __forceinline__ bool tl_seek(TL& q, const Scene& s, const G& g, f3 o,
         }
         if (!tl_outer_step(q, g, h)) return false;
     }
+}
+
+// Inner step (TLGridTraverser.h:225-290): stop when the hit lies before the leaf's exit,
+// else step; leaving the sub-grid continues in the top grid.  False when the ray is done.
+template <bool STATS>
+__device__ __forceinline__ bool tl_advance(TL& q, const Scene& s, const G& g, f3 o, f3 d, Hit& h) {
+    const int32_t lres[3] = {(int32_t)q.lres[0], (int32_t)q.lres[1], (int32_t)q.lres[2]};
+    float tk;
+    const bool inside = dda_step(q.tm2, q.c2, q.rcp, q.scs, lres, &tk);
+    if (h.t < tk) return false;
+    if (inside) return true;
+    return tl_outer_step(q, g, h) && tl_seek<STATS>(q, s, g, o, d, h);
 }
 
 // a15: two-level DDA, warp-synchronous
@@ -316,32 +338,18 @@ __device__ void trace_tl(const Scene& s, const G& g, f3 o, f3 d, Hit& h, bool ac
             if (STATS) h.cells++;
         }
         const bool done = test_lists<ANY, STATS>(s, o, d, b, e, h);
-        if (active) {
-            if (done) {
-                active = false;
-            } else {
-                // inner step (TLGridTraverser.h:225-290): stop when the hit lies before the
-                // leaf's exit, else step; leaving the sub-grid continues in the top grid
-                const int32_t lres[3] = {(int32_t)q.lres[0], (int32_t)q.lres[1], (int32_t)q.lres[2]};
-                float tk;
-                const bool inside = dda_step(q.tm2, q.c2, q.rcp, q.scs, lres, &tk);
-                if (h.t < tk) {
-                    active = false;
-                } else if (!inside) {
-                    active = tl_outer_step(q, g, h);
-                    if (active) active = tl_seek<STATS>(q, s, g, o, d, h);
-                }
-            }
-        }
+        if (active) active = !done && tl_advance<STATS>(q, s, g, o, d, h);
     }
 }
 
-// Closest hit (ANY = false) or any hit within (1e-4, tmax).  Warp-synchronous.
-template <bool ANY, bool STATS>
+// Closest hit (ANY = false) or any hit within (1e-4, tmax) on a grid of kind KIND
+// (kUniform or kTwoLevel).  The kind is a template argument so that a kernel holds the
+// registers of one traversal only.  Warp-synchronous.
+template <int KIND, bool ANY, bool STATS>
 __device__ __forceinline__ void trace_one(const Scene& s, const G& g, f3 o, f3 d, float tmax, Hit& h, bool active) {
     h.t = tmax; h.u = 0.0f; h.v = 0.0f; h.tri = 0; h.hit = false; h.cells = 0; h.tests = 0;
     if (s.ntri == 0) return;
-    if (s.kind == kUniform) trace_ug<ANY, STATS>(s, g, o, d, h, active);
+    if (KIND == kUniform) trace_ug<ANY, STATS>(s, g, o, d, h, active);
     else trace_tl<ANY, STATS>(s, g, o, d, h, active);
 }
 
@@ -423,17 +431,6 @@ __device__ __forceinline__ void add_rays(unsigned long long* counter, bool secon
 // warp-uniform bound of a 1-D grid-stride loop over n items
 __device__ __forceinline__ uint32_t round32(uint32_t n) { return (n + 31u) & ~31u; }
 
-// trace_one, or the two-level traversal alone when the grid is known to be two-level
-template <bool TL_ONLY, bool ANY, bool STATS>
-__device__ __forceinline__ void trace_kind(const Scene& s, const G& g, f3 o, f3 d, float tmax, Hit& h, bool active) {
-    if (TL_ONLY) {
-        h.t = tmax; h.u = 0.0f; h.v = 0.0f; h.tri = 0; h.hit = false; h.cells = 0; h.tests = 0;
-        trace_tl<ANY, STATS>(s, g, o, d, h, active);
-    } else {
-        trace_one<ANY, STATS>(s, g, o, d, tmax, h, active);
-    }
-}
-
 // constants of the path tracer for one grid and light
 struct PtConsts {
     f3 lc, le1, le2;
@@ -486,12 +483,12 @@ __device__ __forceinline__ void path_begin(PathState& p, const Cam& cam, uint32_
 // Returns true while the path goes on (it ends on a miss, on hitting the light, or after
 // k.bounces bounces); p.L is then its radiance.  Warp-synchronous: all lanes call it,
 // lanes without a path pass alive = false.
-template <bool STATS, bool TL_ONLY>
+template <int KIND, bool STATS>
 __device__ __forceinline__ bool path_step(const Scene& s, const G& g, const PtConsts& k, PathState& p, bool alive,
                                           PtCounts& n) {
     if (k.bounces <= 0) return false;   // no bounce: radiance 0 (uniform over the warp)
     Hit h;
-    trace_kind<TL_ONLY, false, STATS>(s, g, p.o, p.d, FLT_MAX, h, alive);
+    trace_one<KIND, false, STATS>(s, g, p.o, p.d, FLT_MAX, h, alive);
     bool shadow = false;
     f3 q = mk(0.0f, 0.0f, 0.0f), nrm = mk(0.0f, 0.0f, 1.0f), wi = mk(0.0f, 0.0f, 1.0f), so = q;
     float dist = 0.0f, dist2 = 1.0f, cos_s = 0.0f, cos_l = 0.0f;
@@ -526,7 +523,7 @@ __device__ __forceinline__ bool path_step(const Scene& s, const G& g, const PtCo
         }
     }
     Hit hs;
-    trace_kind<TL_ONLY, true, STATS>(s, g, so, wi, dist - k.ray_eps, hs, shadow);
+    trace_one<KIND, true, STATS>(s, g, so, wi, dist - k.ray_eps, hs, shadow);
     if (alive) {
         if (shadow) {
             n.srays += 1;
