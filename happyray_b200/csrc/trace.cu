@@ -22,12 +22,16 @@
 
 #include <type_traits>
 
+#ifndef HR_TRACE_MIN_BLOCKS
+#define HR_TRACE_MIN_BLOCKS 8   // blocks of kTT per SM the ray kernels' register budget must allow (8: 64 registers)
+#endif
+
 namespace hr {
 
 namespace {
 
 template <int KIND, bool STATS>
-__global__ __launch_bounds__(kTT, 8) void k_trace_rays(Scene s, const float* __restrict__ org, const float* __restrict__ dir,
+__global__ __launch_bounds__(kTT, HR_TRACE_MIN_BLOCKS) void k_trace_rays(Scene s, const float* __restrict__ org, const float* __restrict__ dir,
                                                     uint32_t n, int32_t* __restrict__ oid, float* __restrict__ ot,
                                                     float* __restrict__ ou, float* __restrict__ ov,
                                                     uint32_t* __restrict__ stats) {
@@ -54,7 +58,7 @@ __global__ __launch_bounds__(kTT, 8) void k_trace_rays(Scene s, const float* __r
 }
 
 template <int KIND, bool STATS>
-__global__ __launch_bounds__(kTT, 8) void k_trace_primary(Scene s, Cam cam, int32_t* __restrict__ oid,
+__global__ __launch_bounds__(kTT, HR_TRACE_MIN_BLOCKS) void k_trace_primary(Scene s, Cam cam, int32_t* __restrict__ oid,
                                                        float* __restrict__ ot, float* __restrict__ ou,
                                                        float* __restrict__ ov, uint32_t* __restrict__ stats) {
     const G g = load_g(s.desc);
@@ -77,7 +81,7 @@ __global__ __launch_bounds__(kTT, 8) void k_trace_primary(Scene s, Cam cam, int3
 }
 
 template <int KIND>
-__global__ __launch_bounds__(kTT, 8) void k_occluded(Scene s, const float* __restrict__ org, const float* __restrict__ dir,
+__global__ __launch_bounds__(kTT, HR_TRACE_MIN_BLOCKS) void k_occluded(Scene s, const float* __restrict__ org, const float* __restrict__ dir,
                                                   const float* __restrict__ tmax, uint32_t n, uint8_t* __restrict__ occ) {
     const G g = load_g(s.desc);
     gate_scene(s);
@@ -99,7 +103,7 @@ __global__ __launch_bounds__(kTT, 8) void k_occluded(Scene s, const float* __res
 
 // mode 0: primary rays with barycentric false colour (SimpleIntegrator.h:41-126)
 template <int KIND, bool STATS>
-__global__ __launch_bounds__(kTT, 8) void k_render_primary(Scene s, Cam cam, int32_t image_id, float* __restrict__ fb,
+__global__ __launch_bounds__(kTT, HR_TRACE_MIN_BLOCKS) void k_render_primary(Scene s, Cam cam, int32_t image_id, float* __restrict__ fb,
                                                         unsigned long long* counter) {
     const G g = load_g(s.desc);
     gate_scene(s);
@@ -136,7 +140,7 @@ __global__ __launch_bounds__(kTT, 8) void k_render_primary(Scene s, Cam cam, int
 //                 unoccluded count of the pixel (match_any-aggregated atomics);
 //   k_ao_finish   visibility = unoccluded / samples, progressive blend (AOIntegrator.h:168-175).
 template <int KIND, bool STATS>
-__global__ __launch_bounds__(kTT, 8) void k_ao_primary(Scene s, Cam cam, int32_t image_id, float* __restrict__ fb,
+__global__ __launch_bounds__(kTT, HR_TRACE_MIN_BLOCKS) void k_ao_primary(Scene s, Cam cam, int32_t image_id, float* __restrict__ fb,
                                                     float* __restrict__ hit_t, uint32_t* __restrict__ hit_tri,
                                                     uint32_t* __restrict__ unocc, uint32_t* __restrict__ queue,
                                                     uint32_t* qcount, unsigned long long* counter) {
@@ -174,7 +178,7 @@ __global__ __launch_bounds__(kTT, 8) void k_ao_primary(Scene s, Cam cam, int32_t
 }
 
 template <int KIND, bool STATS>
-__global__ __launch_bounds__(kTT, 8) void k_ao_samples(Scene s, Cam cam, int32_t spp, float alpha_frac, float alpha_abs,
+__global__ __launch_bounds__(kTT, HR_TRACE_MIN_BLOCKS) void k_ao_samples(Scene s, Cam cam, int32_t spp, float alpha_frac, float alpha_abs,
                                                     uint64_t seed, int32_t image_id, const float* __restrict__ hit_t,
                                                     const uint32_t* __restrict__ hit_tri,
                                                     const uint32_t* __restrict__ queue, const uint32_t* qcount,

@@ -293,6 +293,11 @@ __device__ __forceinline__ bool tl_seek(TL& q, const Scene& s, const G& g, f3 o,
     }
 }
 
+// index of the current leaf: first leaf of the top cell + x + rx * (y + ry * z)
+__device__ __forceinline__ uint32_t tl_leaf(const TL& q) {
+    return q.lbase + (uint32_t)q.c2[0] + q.lres[0] * (uint32_t)q.c2[1] + q.lres[0] * q.lres[1] * (uint32_t)q.c2[2];
+}
+
 // Inner step (TLGridTraverser.h:225-290): stop when the hit lies before the leaf's exit,
 // else step; leaving the sub-grid continues in the top grid.  False when the ray is done.
 template <bool STATS>
@@ -332,8 +337,7 @@ __device__ void trace_tl(const Scene& s, const G& g, f3 o, f3 d, Hit& h, bool ac
     while (__any_sync(kFullMask, active)) {
         uint32_t b = 0, e = 0;
         if (active) {
-            const uint2 lr = __ldg(s.leaves + (q.lbase + (uint32_t)q.c2[0] + q.lres[0] * (uint32_t)q.c2[1] +
-                                               q.lres[0] * q.lres[1] * (uint32_t)q.c2[2]));
+            const uint2 lr = __ldg(s.leaves + tl_leaf(q));
             b = lr.x; e = lr.y;
             if (STATS) h.cells++;
         }
