@@ -78,6 +78,9 @@ __device__ __forceinline__ bool mt_test(const Scene& s, uint32_t tri, f3 o, f3 d
     return u >= 0.0f && v >= 0.0f && u + v <= 1.0f && t > kIsectEps && t < tbest;
 }
 
+// hit modes of a traversal: closest hit, any hit, or per lane (the lane's `any` argument)
+constexpr int kHitClosest = 0, kHitAny = 1, kHitMixed = 2;
+
 __device__ __forceinline__ float shfl(float x, int src) { return __shfl_sync(kFullMask, x, src); }
 __device__ __forceinline__ uint32_t shfl(uint32_t x, int src) { return __shfl_sync(kFullMask, x, src); }
 
@@ -91,11 +94,13 @@ __device__ __forceinline__ uint32_t shfl(uint32_t x, int src) { return __shfl_sy
 // first-tested-wins rule of a one-lane loop over the list.  Any hit: a lane is answered
 // when one of its pairs hits; its later pairs are skipped.  STATS counts the pairs
 // tested: all of a list for closest hit (as the sequential loop), whole rounds for any hit.
-template <bool ANY, bool STATS>
-__device__ __forceinline__ bool test_lists(const Scene& s, f3 o, f3 d, uint32_t b, uint32_t e, Hit& h) {
+template <int HM, bool STATS>
+__device__ __forceinline__ bool test_lists(const Scene& s, f3 o, f3 d, uint32_t b, uint32_t e, bool any, Hit& h) {
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t n = e - b;
     if (__ballot_sync(kFullMask, n != 0u) == 0u) return false;   // most leaves a ray crosses are empty
+    // lanes whose query is an any-hit query
+    const uint32_t anym = HM == kHitAny ? kFullMask : (HM == kHitClosest ? 0u : __ballot_sync(kFullMask, any));
     uint32_t incl = n;
 #pragma unroll
     for (int off = 1; off < 32; off <<= 1) {
@@ -107,7 +112,7 @@ __device__ __forceinline__ bool test_lists(const Scene& s, f3 o, f3 d, uint32_t 
     // below the lane's exclusive prefix; the sum does not)
     const uint32_t rel = b - (incl - n);
     uint32_t best = 0xffffffffu;           // pair number of this lane's best hit of this call
-    uint32_t answered = 0u;                // ANY: lanes with a hit
+    uint32_t answered = 0u;                // any-hit lanes with a hit
     for (uint32_t base = 0; base < total; base += 32u) {
         const uint32_t j = base + lane;
         uint32_t own = 0;                  // number of lanes whose inclusive prefix is <= j
@@ -119,18 +124,18 @@ __device__ __forceinline__ bool test_lists(const Scene& s, f3 o, f3 d, uint32_t 
         const f3 sd = mk(shfl(d.x, own), shfl(d.y, own), shfl(d.z, own));
         const float bt = shfl(h.t, own);
         const uint32_t srel = shfl(rel, own);
-        const bool live = j < total && !(ANY && ((answered >> own) & 1u));
+        const bool own_any = (anym >> own) & 1u;
+        const bool live = j < total && !(own_any && ((answered >> own) & 1u));
         float t = 0.0f, u = 0.0f, v = 0.0f;
         bool hit = false;
         if (live) hit = mt_test(s, __ldg(s.prims + (srel + j)), so, sd, bt, &t, &u, &v);
-        if (STATS && !(ANY && ((answered >> lane) & 1u))) {   // this lane's pairs tested in the round
+        if (STATS && !((anym & answered) >> lane & 1u)) {   // this lane's pairs tested in the round
             const uint32_t lo = max(incl - n, base), hi = min(incl, base + 32u);
             if (hi > lo) h.tests += hi - lo;
         }
-        if (ANY) {
-            answered |= __reduce_or_sync(kFullMask, hit ? 1u << own : 0u);
-        } else {
-            uint32_t hm = __ballot_sync(kFullMask, hit);
+        if (HM != kHitClosest) answered |= __reduce_or_sync(kFullMask, (hit && own_any) ? 1u << own : 0u);
+        if (HM != kHitAny) {
+            uint32_t hm = __ballot_sync(kFullMask, hit && !own_any);
             while (hm) {
                 const int src = __ffs(hm) - 1;
                 hm &= hm - 1u;
@@ -143,13 +148,13 @@ __device__ __forceinline__ bool test_lists(const Scene& s, f3 o, f3 d, uint32_t 
             }
         }
     }
-    if (ANY) {
-        const bool done = (answered >> lane) & 1u;
+    bool done = false;
+    if (HM != kHitClosest) {
+        done = (answered >> lane) & 1u;
         if (done) h.hit = true;
-        return done;
     }
-    if (best != 0xffffffffu) h.tri = __ldg(s.prims + (rel + best));
-    return false;
+    if (HM != kHitAny && best != 0xffffffffu) h.tri = __ldg(s.prims + (rel + best));
+    return done;
 }
 
 __device__ __forceinline__ int min_dim(float a, float b, float c) { return a < b ? (a < c ? 0 : 2) : (b < c ? 1 : 2); }
@@ -193,8 +198,8 @@ __device__ __forceinline__ bool clip(const G& g, f3 o, const float* rcp, float* 
 }
 
 // a14: uniform grid DDA (UGridTraverser.h:76-172), warp-synchronous
-template <bool ANY, bool STATS>
-__device__ void trace_ug(const Scene& s, const G& g, f3 o, f3 d, Hit& h, bool active) {
+template <int HM, bool STATS>
+__device__ void trace_ug(const Scene& s, const G& g, f3 o, f3 d, bool any, Hit& h, bool active) {
     float rcp[3] = {0.0f, 0.0f, 0.0f}, tmax[3] = {0.0f, 0.0f, 0.0f};
     int32_t cell[3] = {0, 0, 0};
     if (active) {
@@ -227,7 +232,7 @@ __device__ void trace_ug(const Scene& s, const G& g, f3 o, f3 d, Hit& h, bool ac
             b = cr.x; e = cr.y;
             if (STATS) h.cells++;
         }
-        const bool done = test_lists<ANY, STATS>(s, o, d, b, e, h);
+        const bool done = test_lists<HM, STATS>(s, o, d, b, e, any, h);
         if (active) {
             if (done) {
                 active = false;
@@ -311,8 +316,8 @@ __device__ __forceinline__ bool tl_advance(TL& q, const Scene& s, const G& g, f3
 }
 
 // a15: two-level DDA, warp-synchronous
-template <bool ANY, bool STATS>
-__device__ void trace_tl(const Scene& s, const G& g, f3 o, f3 d, Hit& h, bool active) {
+template <int HM, bool STATS>
+__device__ void trace_tl(const Scene& s, const G& g, f3 o, f3 d, bool any, Hit& h, bool active) {
     TL q;
     if (active) {
         q.rcp[0] = 1.0f / d.x; q.rcp[1] = 1.0f / d.y; q.rcp[2] = 1.0f / d.z;
@@ -341,7 +346,7 @@ __device__ void trace_tl(const Scene& s, const G& g, f3 o, f3 d, Hit& h, bool ac
             b = lr.x; e = lr.y;
             if (STATS) h.cells++;
         }
-        const bool done = test_lists<ANY, STATS>(s, o, d, b, e, h);
+        const bool done = test_lists<HM, STATS>(s, o, d, b, e, any, h);
         if (active) active = !done && tl_advance<STATS>(q, s, g, o, d, h);
     }
 }
@@ -353,8 +358,20 @@ template <int KIND, bool ANY, bool STATS>
 __device__ __forceinline__ void trace_one(const Scene& s, const G& g, f3 o, f3 d, float tmax, Hit& h, bool active) {
     h.t = tmax; h.u = 0.0f; h.v = 0.0f; h.tri = 0; h.hit = false; h.cells = 0; h.tests = 0;
     if (s.ntri == 0) return;
-    if (KIND == kUniform) trace_ug<ANY, STATS>(s, g, o, d, h, active);
-    else trace_tl<ANY, STATS>(s, g, o, d, h, active);
+    constexpr int HM = ANY ? kHitAny : kHitClosest;
+    if (KIND == kUniform) trace_ug<HM, STATS>(s, g, o, d, false, h, active);
+    else trace_tl<HM, STATS>(s, g, o, d, false, h, active);
+}
+
+// As trace_one, with the hit mode chosen per lane: any hit where `any` is set, closest
+// hit elsewhere (one traversal for the path and the shadow rays of a warp's lanes).
+template <int KIND, bool STATS>
+__device__ __forceinline__ void trace_mixed(const Scene& s, const G& g, f3 o, f3 d, float tmax, bool any, Hit& h,
+                                            bool active) {
+    h.t = tmax; h.u = 0.0f; h.v = 0.0f; h.tri = 0; h.hit = false; h.cells = 0; h.tests = 0;
+    if (s.ntri == 0) return;
+    if (KIND == kUniform) trace_ug<kHitMixed, STATS>(s, g, o, d, any, h, active);
+    else trace_tl<kHitMixed, STATS>(s, g, o, d, any, h, active);
 }
 
 struct Cam {
@@ -462,12 +479,18 @@ struct PtCounts {
     uint32_t rays = 0, cells = 0, tests = 0, srays = 0, scells = 0, stests = 0;
 };
 
-// State of one path of the path tracer (PathTracer.h:41-372 structure).
+// State of one path of the path tracer (PathTracer.h:41-372 structure).  A bounce takes
+// two traversals, the path ray (closest hit) and then, if the light sample faces both
+// surfaces, its shadow ray (any hit); `shadow` says which one the lane traces next.
 struct PathState {
-    f3 o, d;
+    f3 o, d;          // the ray traced next: the path ray, or the shadow ray while `shadow`
+    f3 no, nd;        // while `shadow`: the path's continuation ray
     float L, beta;
+    float c;          // while `shadow`: the light sample's radiance if the shadow ray is free
+    float tmax;       // FLT_MAX for the path ray, the distance to the light sample for the shadow ray
     Pcg32 rng;
     int32_t bounce;
+    bool shadow, last;   // last: the path ends after the shadow ray
 };
 
 // A path from the centre of pixel pix; its PCG32 stream is keyed by (image_id, pix) and seed.
@@ -478,74 +501,90 @@ __device__ __forceinline__ void path_begin(PathState& p, const Cam& cam, uint32_
     p.d = primary_dir(cam, pix);
     p.L = 0.0f;
     p.beta = 1.0f;
+    p.tmax = FLT_MAX;
     p.bounce = 0;
+    p.shadow = false;
 }
 
-// One bounce: the closest hit (at bounce 0 first the camera ray against the quad light),
-// one next-event sample of the light (u1, u2) with an any-hit shadow ray to
-// dist - ray_eps, and a cosine-weighted continuation (u3, u4) with throughput x albedo.
-// Returns true while the path goes on (it ends on a miss, on hitting the light, or after
-// k.bounces bounces); p.L is then its radiance.  Warp-synchronous: all lanes call it,
-// lanes without a path pass alive = false.
+// One traversal of each lane's next ray: a warp traces path rays and shadow rays together
+// (trace_mixed), so lanes whose light sample needs no shadow ray do not idle while the
+// others trace theirs.  Per path the operations are those of the sequential bounce loop:
+// the closest hit (at bounce 0 first the camera ray against the quad light), one
+// next-event sample of the light (u1, u2) whose shadow ray runs to dist - ray_eps, and a
+// cosine-weighted continuation (u3, u4) with throughput x albedo; the light sample's
+// radiance, formed with the throughput before the albedo factor, is added when its shadow
+// ray comes back free.  Returns true while the path goes on (it ends on a miss, on hitting
+// the light, or after k.bounces bounces); p.L is then its radiance.  Warp-synchronous: all
+// lanes call it, lanes without a path pass alive = false.
 template <int KIND, bool STATS>
 __device__ __forceinline__ bool path_step(const Scene& s, const G& g, const PtConsts& k, PathState& p, bool alive,
                                           PtCounts& n) {
     if (k.bounces <= 0) return false;   // no bounce: radiance 0 (uniform over the warp)
     Hit h;
-    trace_one<KIND, false, STATS>(s, g, p.o, p.d, FLT_MAX, h, alive);
-    bool shadow = false;
-    f3 q = mk(0.0f, 0.0f, 0.0f), nrm = mk(0.0f, 0.0f, 1.0f), wi = mk(0.0f, 0.0f, 1.0f), so = q;
-    float dist = 0.0f, dist2 = 1.0f, cos_s = 0.0f, cos_l = 0.0f;
-    if (alive) {
-        n.rays += 1;
-        n.cells += h.cells;
-        n.tests += h.tests;
-        if (p.bounce == 0 && p.d.z > 0.0f) {
-            const float tl = (k.lc.z - p.o.z) / p.d.z;
-            const float px = p.o.x + tl * p.d.x, py = p.o.y + tl * p.d.y;
-            const float fx = (px - k.lc.x) / k.le1.x, fy = (py - k.lc.y) / k.le2.y;
-            if (tl > kIsectEps && tl < h.t && fx >= 0.0f && fx <= 1.0f && fy >= 0.0f && fy <= 1.0f) {
-                p.L = p.L + k.emission;
-                alive = false;
-            }
-        }
-        if (alive && !h.hit) alive = false;
-        if (alive) {
-            q = mk(p.o.x + h.t * p.d.x, p.o.y + h.t * p.d.y, p.o.z + h.t * p.d.z);
-            nrm = face_normal(s, h.tri, p.d);
-            const float u1 = pcg_float(p.rng), u2 = pcg_float(p.rng);
-            const f3 lp = mk(k.lc.x + u1 * k.le1.x + u2 * k.le2.x, k.lc.y + u1 * k.le1.y + u2 * k.le2.y,
-                             k.lc.z + u1 * k.le1.z + u2 * k.le2.z);
-            wi = sub(lp, q);
-            dist2 = dot(wi, wi);
-            dist = sqrtf(dist2);
-            wi = mulf(wi, 1.0f / dist);
-            cos_s = dot(nrm, wi);
-            cos_l = wi.z;
-            shadow = cos_s > 0.0f && cos_l > 0.0f;
-            so = mk(q.x + k.ray_eps * wi.x, q.y + k.ray_eps * wi.y, q.z + k.ray_eps * wi.z);
+    trace_mixed<KIND, STATS>(s, g, p.o, p.d, p.tmax, p.shadow, h, alive);
+    if (!alive) return false;
+    if (p.shadow) {
+        n.srays += 1;
+        n.scells += h.cells;
+        n.stests += h.tests;
+        if (!h.hit) p.L = p.L + p.c;
+        p.shadow = false;
+        if (p.last) return false;
+        p.o = p.no;
+        p.d = p.nd;
+        p.tmax = FLT_MAX;
+        return true;
+    }
+    n.rays += 1;
+    n.cells += h.cells;
+    n.tests += h.tests;
+    if (p.bounce == 0 && p.d.z > 0.0f) {
+        const float tl = (k.lc.z - p.o.z) / p.d.z;
+        const float px = p.o.x + tl * p.d.x, py = p.o.y + tl * p.d.y;
+        const float fx = (px - k.lc.x) / k.le1.x, fy = (py - k.lc.y) / k.le2.y;
+        if (tl > kIsectEps && tl < h.t && fx >= 0.0f && fx <= 1.0f && fy >= 0.0f && fy <= 1.0f) {
+            p.L = p.L + k.emission;
+            return false;
         }
     }
-    Hit hs;
-    trace_one<KIND, true, STATS>(s, g, so, wi, dist - k.ray_eps, hs, shadow);
-    if (alive) {
-        if (shadow) {
-            n.srays += 1;
-            n.scells += hs.cells;
-            n.stests += hs.tests;
-            if (!hs.hit) p.L = p.L + p.beta * k.a_pi * k.emission * cos_s * cos_l * k.larea / dist2;
-        }
-        p.beta = p.beta * k.albedo;
-        const float u3 = pcg_float(p.rng), u4 = pcg_float(p.rng);
-        p.d = cosine_dir(nrm, u3, u4);
-        p.o = mk(q.x + k.ray_eps * p.d.x, q.y + k.ray_eps * p.d.y, q.z + k.ray_eps * p.d.z);
-    }
+    if (!h.hit) return false;
+    const f3 q = mk(p.o.x + h.t * p.d.x, p.o.y + h.t * p.d.y, p.o.z + h.t * p.d.z);
+    const f3 nrm = face_normal(s, h.tri, p.d);
+    const float u1 = pcg_float(p.rng), u2 = pcg_float(p.rng);
+    const f3 lp = mk(k.lc.x + u1 * k.le1.x + u2 * k.le2.x, k.lc.y + u1 * k.le1.y + u2 * k.le2.y,
+                     k.lc.z + u1 * k.le1.z + u2 * k.le2.z);
+    f3 wi = sub(lp, q);
+    const float dist2 = dot(wi, wi);
+    const float dist = sqrtf(dist2);
+    wi = mulf(wi, 1.0f / dist);
+    const float cos_s = dot(nrm, wi);
+    const float cos_l = wi.z;
+    const bool shadow = cos_s > 0.0f && cos_l > 0.0f;
+    if (shadow) p.c = p.beta * k.a_pi * k.emission * cos_s * cos_l * k.larea / dist2;
+    p.beta = p.beta * k.albedo;
+    const float u3 = pcg_float(p.rng), u4 = pcg_float(p.rng);
+    const f3 nd = cosine_dir(nrm, u3, u4);
+    const f3 no = mk(q.x + k.ray_eps * nd.x, q.y + k.ray_eps * nd.y, q.z + k.ray_eps * nd.z);
     p.bounce += 1;
-    return alive && p.bounce < k.bounces;
+    const bool more = p.bounce < k.bounces;
+    if (shadow) {
+        p.no = no;
+        p.nd = nd;
+        p.last = !more;
+        p.o = mk(q.x + k.ray_eps * wi.x, q.y + k.ray_eps * wi.y, q.z + k.ray_eps * wi.z);
+        p.d = wi;
+        p.tmax = dist - k.ray_eps;
+        p.shadow = true;
+        return true;
+    }
+    if (!more) return false;
+    p.o = no;
+    p.d = nd;
+    return true;
 }
 
 // Lanes of a warp take pixels from a pool of 32-pixel tiles and run `spp` paths per pixel,
-// one bounce per step for all lanes together; a lane whose path ends starts the pixel's
+// one ray per lane per step (path_step); a lane whose path ends starts the pixel's
 // next path (image id + 1) or takes the next pixel, so the warp stays full until the pool
 // runs dry.  The per-pixel result is the progressive blend of its paths in image-id order,
 // the same values as spp one-path frames.
