@@ -20,6 +20,9 @@ constexpr int kJobTT = 256;   // largest block of the persistent kernel
 #ifndef HR_JOB_MIN_BLOCKS
 #define HR_JOB_MIN_BLOCKS 3    // blocks of kJobTT per SM the register budget must allow (3: 80 registers)
 #endif
+#ifndef HR_JOB_PT_MIN_BLOCKS
+#define HR_JOB_PT_MIN_BLOCKS HR_JOB_MIN_BLOCKS   // the same for the path-tracing instance
+#endif
 
 // position of the q-th (0-based) set bit of m; m has more than q set bits
 __device__ __forceinline__ uint32_t nth_set_bit(uint32_t m, uint32_t q) {
@@ -108,7 +111,7 @@ __device__ __forceinline__ void load_tile_ctx(TileCtx& T, const Job* __restrict_
 // The PT variant runs path jobs only and the other variant every other mode: the host
 // launches them over disjoint ranges of the job table.
 template <bool PT>
-__global__ __launch_bounds__(kJobTT, HR_JOB_MIN_BLOCKS) void k_trace_jobs(const Job* __restrict__ jobs,
+__global__ __launch_bounds__(kJobTT, PT ? HR_JOB_PT_MIN_BLOCKS : HR_JOB_MIN_BLOCKS) void k_trace_jobs(const Job* __restrict__ jobs,
                                                                         const uint32_t* __restrict__ tile_off,
                                                                         uint32_t njobs, uint32_t* work,
                                                                         int32_t tile_w,
