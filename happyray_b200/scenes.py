@@ -246,3 +246,66 @@ def served_scenes(n_scenes: int = 64, seed: int = 0, tri_range=(10_000, 4_000_00
             kf = curl_keyframes(v, n_keyframes, amp=0.02, octaves=4, seed=sseed)
         out.append((kf, f))
     return out
+
+
+INSTANCE_DTYPE = np.dtype([("obj", "<u4"), ("m", "<f4", 12), ("bmin", "<f4", 3), ("bmax", "<f4", 3)])
+
+
+def instance_record(obj: int, to_world: np.ndarray, obj_lo, obj_hi):
+    """An instance of an object: the world -> object rows of the reference's instances
+    file (x' = m0 x + m1 y + m2 z + m3, ...) and the world box of the object's box corners.
+    to_world: 3x4 object -> world map (float64)."""
+    W = np.asarray(to_world, np.float64)
+    A, T = W[:, :3], W[:, 3]
+    Ai = np.linalg.inv(A)
+    M = np.concatenate([Ai, (-Ai @ T)[:, None]], axis=1)
+    lo, hi = np.asarray(obj_lo, np.float64), np.asarray(obj_hi, np.float64)
+    corners = np.array([[x, y, z] for x in (lo[0], hi[0]) for y in (lo[1], hi[1]) for z in (lo[2], hi[2])])
+    wc = corners @ A.T + T
+    span = np.abs(wc).max() + 1.0
+    rec = np.zeros((), INSTANCE_DTYPE)
+    rec["obj"] = obj
+    rec["m"] = M.reshape(-1).astype(np.float32)
+    rec["bmin"] = (wc.min(0) - 1e-5 * span).astype(np.float32)   # outward: the box holds the object
+    rec["bmax"] = (wc.max(0) + 1e-5 * span).astype(np.float32)
+    return rec
+
+
+def instanced_scene(n_objects: int = 16, n_instances: int = 1024, seed: int = 0, tri_range=(320, 20_480),
+                    world: float = 1.0, scale_range=(0.02, 0.08)):
+    """Seeded instanced scene: objects (icospheres of levels 2-5 and heightfield tiles, each
+    centred at its origin with extent about 1) and instances with random rotations,
+    uniform scales and positions in [0, world]^3 (ground objects lie flat).  Returns
+    (vertices, faces, object triangle counts, instance records)."""
+    rng = np.random.default_rng(seed)
+    verts, faces, counts, boxes = [], [], [], []
+    nv = 0
+    for k in range(n_objects):
+        target = int(math.exp(rng.uniform(math.log(tri_range[0]), math.log(tri_range[1]))))
+        if k % 2 == 0:
+            level = max(2, min(5, int(round(math.log(max(target, 80) / 20.0, 4)))))
+            v, f = icosphere(level)
+            v = np.asarray(v, np.float64) * 0.5
+        else:
+            n = max(3, int(math.sqrt(target / 2.0)) + 1)
+            v, f = heightfield(n, int(rng.integers(1 << 30)), amp=0.05)
+            v = np.asarray(v, np.float64) - np.array([0.5, 0.5, 0.0])
+        v = v.astype(np.float32)
+        verts.append(v)
+        faces.append(np.asarray(f, np.uint32) + nv)
+        counts.append(len(f))
+        boxes.append((v.min(0), v.max(0)))
+        nv += v.shape[0]
+    inst = np.zeros(n_instances, INSTANCE_DTYPE)
+    for i in range(n_instances):
+        obj = int(rng.integers(0, n_objects))
+        q = rng.normal(size=4)
+        q /= np.linalg.norm(q)
+        a, b, c, d = q
+        R = np.array([[a * a + b * b - c * c - d * d, 2 * (b * c - a * d), 2 * (b * d + a * c)],
+                      [2 * (b * c + a * d), a * a - b * b + c * c - d * d, 2 * (c * d - a * b)],
+                      [2 * (b * d - a * c), 2 * (c * d + a * b), a * a - b * b - c * c + d * d]])
+        s = math.exp(rng.uniform(math.log(scale_range[0]), math.log(scale_range[1])))
+        T = rng.uniform(0.0, world, 3)
+        inst[i] = instance_record(obj, np.concatenate([R * s, T[:, None]], axis=1), *boxes[obj])
+    return np.concatenate(verts), np.concatenate(faces), np.asarray(counts, np.uint32), inst

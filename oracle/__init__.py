@@ -33,6 +33,21 @@ class Scene(C.Structure):
                 ("g", Grid), ("cells", C.c_void_p), ("leaves", C.c_void_p), ("prims", C.c_void_p)]
 
 
+class Obj(C.Structure):
+    _fields_ = [("bmin", C.c_float * 3), ("bmax", C.c_float * 3), ("cs", C.c_float * 3), ("rcp", C.c_float * 3),
+                ("res", C.c_int32 * 3), ("cell_off", C.c_uint32), ("tri_begin", C.c_uint32), ("tri_count", C.c_uint32)]
+
+
+class Inst(C.Structure):
+    _fields_ = [("obj", C.c_uint32), ("m", C.c_float * 12), ("bmin", C.c_float * 3), ("bmax", C.c_float * 3)]
+
+
+class Hier(C.Structure):
+    _fields_ = [("v4", C.c_void_p), ("idx", C.c_void_p), ("ntri", C.c_uint32), ("nobj", C.c_uint32),
+                ("ninst", C.c_uint32), ("objs", C.c_void_p), ("inst", C.c_void_p), ("top", Grid),
+                ("top_cells", C.c_void_p), ("inst_ids", C.c_void_p), ("obj_cells", C.c_void_p), ("prims", C.c_void_p)]
+
+
 class Camera(C.Structure):
     _fields_ = [("pos", C.c_float * 3), ("top_left", C.c_float * 3), ("step_x", C.c_float * 3),
                 ("step_y", C.c_float * 3), ("w", C.c_int32), ("h", C.c_int32)]
@@ -82,6 +97,10 @@ def lib():
                 "orc_sincos2pi": (None, [F, C.POINTER(F), C.POINTER(F)]),
                 "orc_pcg32_first_floats": (F, [U64, U64, I32, P]),
                 "orc_num_threads": (C.c_int, []),
+                "orc_hier_build": (C.c_int, [P, P, U32, P, U32, P, U32, F, F, P, C.POINTER(Grid), C.POINTER(P),
+                                             C.POINTER(U32), C.POINTER(P), C.POINTER(U32), C.POINTER(P), C.POINTER(P),
+                                             C.POINTER(U32)]),
+                "orc_hier_trace": (None, [C.POINTER(Hier), P, P, P, U32, C.c_int, P, P, P, P, P]),
             }
             for name, (res, args) in sig.items():
                 fn = getattr(L, name)
@@ -312,3 +331,63 @@ def pcg32_floats(initstate: int, initseq: int, k: int):
     out = np.empty(k, np.float32)
     lib().orc_pcg32_first_floats(initstate, initseq, k, _p(out))
     return out
+
+
+# ---- instanced two-level grid hierarchy -------------------------------------------
+
+INST_DTYPE = np.dtype([("obj", "<u4"), ("m", "<f4", 12), ("bmin", "<f4", 3), ("bmax", "<f4", 3)])
+
+
+class BuiltHier:
+    """Result of an oracle hierarchy build (TLGridHierarchySortBuilder.cu:373-682); keeps
+    the arrays alive for traversal calls."""
+
+    def __init__(self, v4, idx, objs, inst, top, obj_cells, prims, top_cells, inst_ids):
+        self.v4, self.idx, self.objs, self.inst, self.top = v4, idx, objs, inst, top
+        self.obj_cells, self.prims, self.top_cells, self.inst_ids = obj_cells, prims, top_cells, inst_ids
+
+    def struct(self) -> Hier:
+        h = Hier()
+        h.v4, h.idx = _p(self.v4), _p(self.idx)
+        h.ntri, h.nobj, h.ninst = self.idx.shape[0], len(self.objs), self.inst.shape[0]
+        h.objs = C.cast(self.objs, C.c_void_p)
+        h.inst = _p(self.inst)
+        h.top = self.top
+        h.top_cells, h.inst_ids = _p(self.top_cells), _p(self.inst_ids)
+        h.obj_cells, h.prims = _p(self.obj_cells), _p(self.prims)
+        return h
+
+
+def hier_build(v, idx, obj_tri_counts, inst, top=1.2, leaf=1.2) -> BuiltHier:
+    """Object grids (one uniform grid per object: a consecutive triangle range) and the
+    instance grid.  v: (nv, 3) object-space vertices; inst: INST_DTYPE records."""
+    v = np.asarray(v, np.float32)
+    v4 = np.zeros((v.shape[0], 4), np.float32)
+    v4[:, :3] = v
+    idx = np.ascontiguousarray(idx, np.uint32)
+    counts = np.ascontiguousarray(obj_tri_counts, np.uint32)
+    inst = np.ascontiguousarray(inst, INST_DTYPE)
+    objs = (Obj * len(counts))()
+    g = Grid()
+    oc, pr, tc, ii = C.c_void_p(), C.c_void_p(), C.c_void_p(), C.c_void_p()
+    noc, np_, ntp = C.c_uint32(), C.c_uint32(), C.c_uint32()
+    rc = lib().orc_hier_build(_p(v4), _p(idx), idx.shape[0], _p(counts), len(counts), _p(inst), inst.shape[0],
+                              top, leaf, C.cast(objs, C.c_void_p), C.byref(g), C.byref(oc), C.byref(noc),
+                              C.byref(pr), C.byref(np_), C.byref(tc), C.byref(ii), C.byref(ntp))
+    if rc != 0:
+        raise ValueError("oracle hier_build failed (object triangle counts must sum to the triangle count)")
+    return BuiltHier(v4, idx, objs, inst, g, _take(oc, 2 * noc.value).reshape(-1, 2), _take(pr, np_.value),
+                     _take(tc, 2 * g.ncells).reshape(-1, 2), _take(ii, ntp.value))
+
+
+def hier_trace(h: BuiltHier, org, dirs, tmax=None, anyhit=False):
+    """Closest hit (instance id, triangle id, t, u, v), or any hit below tmax."""
+    org = np.ascontiguousarray(org, np.float32)
+    dirs = np.ascontiguousarray(dirs, np.float32)
+    n = org.shape[0]
+    tm = None if tmax is None else np.ascontiguousarray(np.broadcast_to(np.asarray(tmax, np.float32), (n,)))
+    out = [np.empty(n, np.int32), np.empty(n, np.int32), np.empty(n, np.float32), np.empty(n, np.float32),
+           np.empty(n, np.float32)]
+    s = h.struct()
+    lib().orc_hier_trace(C.byref(s), _p(org), _p(dirs), _p(tm), n, 1 if anyhit else 0, *[_p(a) for a in out])
+    return tuple(out)

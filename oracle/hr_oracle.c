@@ -936,3 +936,308 @@ void orc_brute_f64(const float *v4, const uint32_t *idx, uint32_t ntri,
         id[i] = best; t[i] = best >= 0 ? bt : INFINITY; u[i] = bu; v[i] = bv; flags[i] = f;
     }
 }
+
+/* ------------------------------------------------------------------------- */
+/* Instanced two-level grid hierarchy.                                        */
+
+/* object grid cell range of a triangle box: countPairsMultiUniformGrid,
+ * TLGridHierarchySortBuilder.cu:122-145 (both ends clamped into [0, res)) */
+static inline uint32_t obj_cell_range(f3 lo, f3 hi, const orc_obj *g, crange *r) {
+    float af[3] = {(lo.x - g->bmin[0]) * g->rcp[0], (lo.y - g->bmin[1]) * g->rcp[1], (lo.z - g->bmin[2]) * g->rcp[2]};
+    float bf[3] = {(hi.x - g->bmin[0]) * g->rcp[0] + 1.0f, (hi.y - g->bmin[1]) * g->rcp[1] + 1.0f,
+                   (hi.z - g->bmin[2]) * g->rcp[2] + 1.0f};
+    uint32_t n = 1;
+    for (int k = 0; k < 3; ++k) {
+        r->lo[k] = imin(g->res[k] - 1, imax(0, f2i(af[k])));
+        r->hi[k] = imax(1, imin(g->res[k], f2i(bf[k])));
+        int32_t e = r->hi[k] - r->lo[k];
+        n *= (uint32_t)(e > 0 ? e : 0);
+    }
+    return n;
+}
+
+/* object grid geometry: bounds padded by 10 EPS (RTEngine.cu:268-300) and the
+ * resolution of countGridCellsMultiUniformGrid (TLGridHierarchySortBuilder.cu:31-57) */
+static void obj_setup(orc_obj *g, f3 lo, f3 hi, float density) {
+    const float pad = 10.0f * ORC_EPS;
+    g->bmin[0] = lo.x - pad; g->bmin[1] = lo.y - pad; g->bmin[2] = lo.z - pad;
+    g->bmax[0] = hi.x + pad; g->bmax[1] = hi.y + pad; g->bmax[2] = hi.z + pad;
+    f3 d = mk(g->bmax[0] - g->bmin[0], g->bmax[1] - g->bmin[1], g->bmax[2] - g->bmin[2]);
+    float vol = d.x * d.y * d.z;
+    float m = orc_pow_third(density * (float)g->tri_count / vol);
+    f3 r = mulf(d, m);
+    int32_t ri[3] = {f2i(r.x), f2i(r.y), f2i(r.z)};
+    for (int k = 0; k < 3; ++k) {
+        g->res[k] = ri[k] > 0 ? ri[k] : 1;
+        float dk = comp(d, k), rk = (float)g->res[k];
+        g->cs[k] = dk / rk;
+        g->rcp[k] = rk / dk;
+    }
+}
+
+/* instance grid: union of the instance boxes padded as the scene bounds
+ * (WFObjectUploader.h:112-114), resolution of TLGridHierarchySortBuilder.cu:275-286,
+ * cell size diagonal / res (TLGridHierarchyMemoryManager.h:111-119) */
+static void top_setup(orc_grid *g, const orc_inst *inst, uint32_t ninst, float density) {
+    f3 lo = mk(FLT_MAX, FLT_MAX, FLT_MAX), hi = mk(-FLT_MAX, -FLT_MAX, -FLT_MAX);
+    for (uint32_t i = 0; i < ninst; ++i) {
+        lo = vmin(lo, ld3(inst[i].bmin));
+        hi = vmax(hi, ld3(inst[i].bmax));
+    }
+    f3 dd = sub(hi, lo);
+    float pad = 0.001f * sqrtf(dot(dd, dd));
+    g->bmin[0] = lo.x - pad; g->bmin[1] = lo.y - pad; g->bmin[2] = lo.z - pad;
+    g->bmax[0] = hi.x + pad; g->bmax[1] = hi.y + pad; g->bmax[2] = hi.z + pad;
+    f3 d = mk(g->bmax[0] - g->bmin[0], g->bmax[1] - g->bmin[1], g->bmax[2] - g->bmin[2]);
+    float vol = d.x * d.y * d.z;
+    float m = orc_pow_third(density * (float)ninst / vol);
+    f3 r = mulf(d, m);
+    g->res[0] = imax(1, f2i(r.x)); g->res[1] = imax(1, f2i(r.y)); g->res[2] = imax(1, f2i(r.z));
+    for (int k = 0; k < 3; ++k) {
+        float dk = comp(d, k), rk = (float)g->res[k];
+        g->cs[k] = dk / rk;
+        g->rcp[k] = rk / dk;
+    }
+    g->ncells = (uint32_t)g->res[0] * (uint32_t)g->res[1] * (uint32_t)g->res[2];
+}
+
+int orc_hier_build(const float *v4, const uint32_t *idx, uint32_t ntri, const uint32_t *obj_tri_counts,
+                   uint32_t nobj, const orc_inst *inst, uint32_t ninst, float top_density, float leaf_density,
+                   orc_obj *objs, orc_grid *top, uint32_t **obj_cells, uint32_t *nobj_cells, uint32_t **prims,
+                   uint32_t *npairs, uint32_t **top_cells, uint32_t **inst_ids, uint32_t *ntop_pairs) {
+    /* level two: one uniform grid per object, cells of all objects in one array */
+    uint32_t begin = 0, cells = 0;
+    for (uint32_t k = 0; k < nobj; ++k) {
+        orc_obj *g = &objs[k];
+        g->tri_begin = begin;
+        g->tri_count = obj_tri_counts[k];
+        f3 lo = mk(FLT_MAX, FLT_MAX, FLT_MAX), hi = mk(-FLT_MAX, -FLT_MAX, -FLT_MAX);
+        for (uint32_t t = begin; t < begin + g->tri_count; ++t)
+            for (int c = 0; c < 3; ++c) {
+                f3 p = vtx(v4, idx[3 * (size_t)t + c]);
+                lo = vmin(lo, p);
+                hi = vmax(hi, p);
+            }
+        obj_setup(g, lo, hi, leaf_density);
+        g->cell_off = cells;
+        cells += (uint32_t)g->res[0] * (uint32_t)g->res[1] * (uint32_t)g->res[2];
+        begin += g->tri_count;
+    }
+    if (begin != ntri) return -1;
+    /* pairs in triangle order (writeKeysAndValuesMultiUniformGrid, .cu:151-225), keys
+     * offset by the object's first cell, then a stable sort by key */
+    size_t *off = (size_t *)malloc(sizeof(size_t) * ((size_t)ntri + 1));
+    uint32_t *tobj = (uint32_t *)malloc(sizeof(uint32_t) * ((size_t)ntri + 1));
+    if (!off || !tobj) { free(off); free(tobj); return -1; }
+    for (uint32_t k = 0; k < nobj; ++k)
+        for (uint32_t t = objs[k].tri_begin; t < objs[k].tri_begin + objs[k].tri_count; ++t) tobj[t] = k;
+    off[0] = 0;
+    for (uint32_t t = 0; t < ntri; ++t) {
+        f3 lo, hi, p[3];
+        crange r;
+        tri_bbox(v4, idx, t, &lo, &hi, p);
+        off[t + 1] = off[t] + obj_cell_range(lo, hi, &objs[tobj[t]], &r);
+    }
+    size_t np = off[ntri];
+    uint32_t *keys = (uint32_t *)malloc(sizeof(uint32_t) * (np + 1));
+    uint32_t *vals = (uint32_t *)malloc(sizeof(uint32_t) * (np + 1));
+    uint32_t *sk = (uint32_t *)malloc(sizeof(uint32_t) * (np + 1));
+    uint32_t *sv = (uint32_t *)malloc(sizeof(uint32_t) * (np + 1));
+    uint32_t *oc = (uint32_t *)malloc(sizeof(uint32_t) * 2 * ((size_t)cells + 1));
+    if (!keys || !vals || !sk || !sv || !oc) {
+        free(off); free(tobj); free(keys); free(vals); free(sk); free(sv); free(oc);
+        return -1;
+    }
+    for (uint32_t t = 0; t < ntri; ++t) {
+        const orc_obj *g = &objs[tobj[t]];
+        f3 lo, hi, p[3];
+        crange r;
+        tri_bbox(v4, idx, t, &lo, &hi, p);
+        obj_cell_range(lo, hi, g, &r);
+        size_t w = off[t];
+        const uint32_t rx = (uint32_t)g->res[0], rxy = (uint32_t)g->res[0] * (uint32_t)g->res[1];
+        for (int32_t z = r.lo[2]; z < r.hi[2]; ++z)
+            for (int32_t y = r.lo[1]; y < r.hi[1]; ++y)
+                for (int32_t x = r.lo[0]; x < r.hi[0]; ++x) {
+                    keys[w] = (uint32_t)x + (uint32_t)y * rx + (uint32_t)z * rxy + g->cell_off;
+                    vals[w] = t;
+                    ++w;
+                }
+    }
+    stable_sort_pairs(keys, vals, np, cells + 1, sk, sv);
+    cell_ranges(sk, np, cells, oc);
+    free(off); free(tobj); free(keys); free(vals); free(sk);
+    *obj_cells = oc; *nobj_cells = cells; *prims = sv; *npairs = (uint32_t)np;
+
+    /* level one: instance boxes into a uniform grid (countPairs / writeKeysAndValues
+     * over GeometryInstance boxes, UniformGridBuildKernels.h:40-105, 180-252) */
+    top_setup(top, inst, ninst, top_density);
+    size_t *ioff = (size_t *)malloc(sizeof(size_t) * ((size_t)ninst + 1));
+    if (!ioff) return -1;
+    ioff[0] = 0;
+    for (uint32_t i = 0; i < ninst; ++i) {
+        crange r;
+        ioff[i + 1] = ioff[i] + cell_range(ld3(inst[i].bmin), ld3(inst[i].bmax), ld3(top->bmin), top->rcp, top->res, &r);
+    }
+    size_t ntp = ioff[ninst];
+    uint32_t *ik = (uint32_t *)malloc(sizeof(uint32_t) * (ntp + 1));
+    uint32_t *iv = (uint32_t *)malloc(sizeof(uint32_t) * (ntp + 1));
+    uint32_t *isk = (uint32_t *)malloc(sizeof(uint32_t) * (ntp + 1));
+    uint32_t *isv = (uint32_t *)malloc(sizeof(uint32_t) * (ntp + 1));
+    uint32_t *tc = (uint32_t *)malloc(sizeof(uint32_t) * 2 * ((size_t)top->ncells + 1));
+    if (!ik || !iv || !isk || !isv || !tc) {
+        free(ioff); free(ik); free(iv); free(isk); free(isv); free(tc);
+        return -1;
+    }
+    const uint32_t rx = (uint32_t)top->res[0], rxy = (uint32_t)top->res[0] * (uint32_t)top->res[1];
+    for (uint32_t i = 0; i < ninst; ++i) {
+        crange r;
+        cell_range(ld3(inst[i].bmin), ld3(inst[i].bmax), ld3(top->bmin), top->rcp, top->res, &r);
+        size_t w = ioff[i];
+        for (int32_t z = r.lo[2]; z < r.hi[2]; ++z)
+            for (int32_t y = r.lo[1]; y < r.hi[1]; ++y)
+                for (int32_t x = r.lo[0]; x < r.hi[0]; ++x) {
+                    ik[w] = (uint32_t)x + (uint32_t)y * rx + (uint32_t)z * rxy;
+                    iv[w] = i;
+                    ++w;
+                }
+    }
+    stable_sort_pairs(ik, iv, ntp, top->ncells + 1, isk, isv);
+    cell_ranges(isk, ntp, top->ncells, tc);
+    free(ioff); free(ik); free(iv); free(isk);
+    *top_cells = tc; *inst_ids = isv; *ntop_pairs = (uint32_t)ntp;
+    return 0;
+}
+
+/* slab test against a box (BBox.hpp:64-79 fastClip) */
+static inline void box_clip(const float *bmin, const float *bmax, f3 o, const float rcp[3], float *t0, float *t1) {
+    float tn[3], tf[3];
+    for (int k = 0; k < 3; ++k) {
+        float a = (bmin[k] - comp(o, k)) * rcp[k];
+        float b = (bmax[k] - comp(o, k)) * rcp[k];
+        tn[k] = hmin(a, b); tf[k] = hmax(a, b);
+    }
+    *t0 = hmax(hmax(tn[0], tn[1]), tn[2]);
+    *t1 = hmin(hmin(tf[0], tf[1]), tf[2]);
+}
+
+typedef struct { float t, u, v; int32_t inst, tri; } hhit;
+
+/* one instance: world box test, ray into object space, object grid DDA
+ * (GeometryInstanceTraverser, TLGridHierarchyTraverser.h:45-205).  Returns 1 when the
+ * instance's hit is accepted. */
+static int hier_instance(const orc_hier *H, uint32_t ii, f3 o, f3 d, const float rcp[3], hhit *h) {
+    const orc_inst *I = &H->inst[ii];
+    float te1, tx1;
+    box_clip(I->bmin, I->bmax, o, rcp, &te1, &tx1);
+    if (!(tx1 > te1 && tx1 >= 0.0f && te1 < h->t)) return 0;
+    const float *m = I->m;
+    /* transformRay (TwoLevelGridHierarchy.h:636-646): rows of the world -> object map;
+     * the direction is carried, not re-derived from its reciprocal */
+    f3 ot = mk(m[0] * o.x + m[1] * o.y + m[2] * o.z + m[3], m[4] * o.x + m[5] * o.y + m[6] * o.z + m[7],
+               m[8] * o.x + m[9] * o.y + m[10] * o.z + m[11]);
+    f3 dt = mk(m[0] * d.x + m[1] * d.y + m[2] * d.z, m[4] * d.x + m[5] * d.y + m[6] * d.z,
+               m[8] * d.x + m[9] * d.y + m[10] * d.z);
+    float rt[3] = {1.0f / dt.x, 1.0f / dt.y, 1.0f / dt.z};
+    const orc_obj *g = &H->objs[I->obj];
+    float rayT = h->t, bu = 0.0f, bv = 0.0f;
+    int32_t best = -1;
+    float te, tx;
+    box_clip(g->bmin, g->bmax, ot, rt, &te, &tx);
+    int flag = tx > te && tx >= 0.0f && te < rayT;
+    f3 ep = ot;
+    if (te >= 0.0f) { float s = te + ORC_EPS; ep = mk(ot.x + s * dt.x, ot.y + s * dt.y, ot.z + s * dt.z); }
+    float tmax[3];
+    int32_t cell[3];
+    for (int k = 0; k < 3; ++k) {
+        float cf = floorf((comp(ep, k) - g->bmin[k]) * g->rcp[k]);
+        cf = rt[k] > 0.0f ? hmin((float)g->res[k] - 1.0f, cf) : hmax(cf, 0.0f);
+        float stp = rt[k] > 0.0f ? 1.0f : 0.0f;
+        tmax[k] = ((cf + stp) * g->cs[k] + g->bmin[k] - comp(ot, k)) * rt[k];
+        cell[k] = f2i(cf);
+        flag = flag && (rt[k] > 0.0f ? cell[k] < g->res[k] : cell[k] > -1);
+    }
+    const uint32_t rx = (uint32_t)g->res[0], rxy = (uint32_t)g->res[0] * (uint32_t)g->res[1];
+    while (flag) {
+        if (cell[0] < g->res[0] && cell[0] > -1 && cell[1] < g->res[1] && cell[1] > -1 && cell[2] < g->res[2] &&
+            cell[2] > -1) {
+            size_t c = g->cell_off + (uint32_t)cell[0] + (uint32_t)cell[1] * rx + (uint32_t)cell[2] * rxy;
+            for (uint32_t it = H->obj_cells[2 * c]; it < H->obj_cells[2 * c + 1]; ++it) {
+                uint32_t tri = H->prims[it];
+                f3 v0 = vtx(H->v4, H->idx[3 * (size_t)tri]);
+                f3 v1 = vtx(H->v4, H->idx[3 * (size_t)tri + 1]);
+                f3 v2 = vtx(H->v4, H->idx[3 * (size_t)tri + 2]);
+                f3 e1 = sub(v1, v0), e2 = sub(v2, v0);
+                f3 p = cross(dt, e2);
+                float det = dot(e1, p);
+                float inv = 1.0f / det;
+                f3 sv = sub(ot, v0);
+                float u = dot(sv, p) * inv;
+                f3 q = cross(sv, e1);
+                float v = dot(q, dt) * inv;
+                float t = dot(e2, q) * inv;
+                if (u >= 0.0f && v >= 0.0f && u + v <= 1.0f && t > ORC_ISECT_EPS && t < rayT) {
+                    rayT = t; bu = u; bv = v; best = (int32_t)tri;
+                }
+            }
+        }
+        int k = MIN_DIM(tmax[0], tmax[1], tmax[2]);
+        flag = flag && rayT > tmax[k];
+        cell[k] += rt[k] > 0.0f ? 1 : -1;
+        tmax[k] += g->cs[k] * fabsf(rt[k]);
+        flag = flag && (rt[k] > 0.0f ? cell[k] < g->res[k] : cell[k] > -1);
+    }
+    if (best >= 0 && rayT < h->t && rayT >= te1 && rayT < tx1) {
+        h->t = rayT; h->u = bu; h->v = bv; h->inst = (int32_t)ii; h->tri = best;
+        return 1;
+    }
+    return 0;
+}
+
+/* instance-grid DDA, TLGridHierarchyTraverser.h:220-405 */
+static void trace_hier(const orc_hier *H, f3 o, f3 d, int anyhit, hhit *h) {
+    const orc_grid *g = &H->top;
+    float rcp[3] = {1.0f / d.x, 1.0f / d.y, 1.0f / d.z};
+    float t0, t1;
+    box_clip(g->bmin, g->bmax, o, rcp, &t0, &t1);
+    if (!(t1 > t0 && t1 >= 0.0f)) return;
+    f3 ep = o;
+    if (t0 >= 0.0f) { float s = t0 + ORC_EPS; ep = mk(o.x + s * d.x, o.y + s * d.y, o.z + s * d.z); }
+    float tmax[3];
+    int32_t cell[3];
+    int active = 1;
+    for (int k = 0; k < 3; ++k) {
+        float cf = floorf((comp(ep, k) - g->bmin[k]) * g->rcp[k]);
+        float stp = rcp[k] > 0.0f ? 1.0f : 0.0f;
+        tmax[k] = ((cf + stp) * g->cs[k] + g->bmin[k] - comp(o, k)) * rcp[k];
+        cell[k] = f2i(cf);
+        active = active && (rcp[k] > 0.0f ? cell[k] < g->res[k] : cell[k] > -1);
+    }
+    const uint32_t rx = (uint32_t)g->res[0], rxy = (uint32_t)g->res[0] * (uint32_t)g->res[1];
+    while (active) {
+        if (cell[0] < g->res[0] && cell[0] > -1 && cell[1] < g->res[1] && cell[1] > -1 && cell[2] < g->res[2] &&
+            cell[2] > -1) {
+            size_t c = (uint32_t)cell[0] + (uint32_t)cell[1] * rx + (uint32_t)cell[2] * rxy;
+            for (uint32_t it = H->top_cells[2 * c]; it < H->top_cells[2 * c + 1]; ++it)
+                if (hier_instance(H, H->inst_ids[it], o, d, rcp, h) && anyhit) return;
+        }
+        int k = MIN_DIM(tmax[0], tmax[1], tmax[2]);
+        active = h->t > tmax[k];
+        cell[k] += rcp[k] > 0.0f ? 1 : -1;
+        tmax[k] += g->cs[k] * fabsf(rcp[k]);
+        active = active && (rcp[k] > 0.0f ? cell[k] < g->res[k] : cell[k] > -1);
+    }
+}
+
+void orc_hier_trace(const orc_hier *H, const float *org, const float *dir, const float *tmax, uint32_t n,
+                    int anyhit, int32_t *inst_id, int32_t *tri_id, float *t, float *u, float *v) {
+#pragma omp parallel for schedule(dynamic, 64)
+    for (long long ii = 0; ii < (long long)n; ++ii) {
+        size_t i = (size_t)ii;
+        hhit h;
+        h.t = tmax ? tmax[i] : FLT_MAX; h.u = 0.0f; h.v = 0.0f; h.inst = -1; h.tri = -1;
+        trace_hier(H, ld3(org + 3 * i), ld3(dir + 3 * i), anyhit, &h);
+        inst_id[i] = h.inst; tri_id[i] = h.tri;
+        t[i] = h.inst >= 0 ? h.t : FLT_MAX; u[i] = h.u; v[i] = h.v;
+    }
+}

@@ -125,6 +125,47 @@ void  orc_sincos2pi(float u, float *s, float *c);
 float orc_pcg32_first_floats(uint64_t initstate, uint64_t initseq, int32_t k, float *out);
 int   orc_num_threads(void);
 
+/* ---- instanced two-level grid hierarchy ----
+ * Objects are consecutive triangle ranges of one mesh (object-space vertices), each
+ * with its own uniform grid (TLGridHierarchySortBuilder.cu:522-682 buildLevelTwo); the
+ * instances (object, world -> object transform, world AABB) are binned into a uniform
+ * grid over the instance boxes (TLGridHierarchySortBuilder.cu:373-520).  Traversal as
+ * TLGridHierarchyTraverser.h:45-405. */
+typedef struct {
+    float    bmin[3], bmax[3], cs[3], rcp[3];
+    int32_t  res[3];
+    uint32_t cell_off, tri_begin, tri_count;
+} orc_obj;
+
+typedef struct {
+    uint32_t obj;
+    float    m[12];          /* world -> object rows: x' = m0 x + m1 y + m2 z + m3, y' = m4.., z' = m8.. */
+    float    bmin[3], bmax[3];   /* world-space box of the instance */
+} orc_inst;
+
+typedef struct {
+    const float    *v4;      /* object-space vertices (float4) */
+    const uint32_t *idx;
+    uint32_t        ntri, nobj, ninst;
+    const orc_obj  *objs;
+    const orc_inst *inst;
+    orc_grid        top;     /* instance grid */
+    const uint32_t *top_cells;   /* uint2 ranges into inst_ids */
+    const uint32_t *inst_ids;
+    const uint32_t *obj_cells;   /* uint2 ranges into prims; object k's cells start at cell_off */
+    const uint32_t *prims;
+} orc_hier;
+
+/* objs (nobj) and top are filled; the arrays are malloc'd (orc_free). */
+int orc_hier_build(const float *v4, const uint32_t *idx, uint32_t ntri, const uint32_t *obj_tri_counts,
+                   uint32_t nobj, const orc_inst *inst, uint32_t ninst, float top_density, float leaf_density,
+                   orc_obj *objs, orc_grid *top, uint32_t **obj_cells, uint32_t *nobj_cells, uint32_t **prims,
+                   uint32_t *npairs, uint32_t **top_cells, uint32_t **inst_ids, uint32_t *ntop_pairs);
+/* closest hit (tmax NULL: unbounded), or any hit below tmax[i] (anyhit = 1: inst_id >= 0
+ * marks an occluded ray); inst_id / tri_id -1 on a miss */
+void orc_hier_trace(const orc_hier *H, const float *org, const float *dir, const float *tmax, uint32_t n,
+                    int anyhit, int32_t *inst_id, int32_t *tri_id, float *t, float *u, float *v);
+
 #ifdef __cplusplus
 }
 #endif
