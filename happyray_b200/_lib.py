@@ -113,7 +113,42 @@ SIGNATURES = {
     "hr_rays_file_write": (C.c_int, [C.c_char_p, P, P, C.c_uint32]),
     "hr_hits_file_write": (C.c_int, [C.c_char_p, P, P, P, P, C.c_uint32]),
     "hr_image_write": (C.c_int, [C.c_char_p, P, C.c_int32, C.c_int32, C.c_int32]),
+    # instanced two-level grid hierarchy
+    "hr_hier_create": (C.c_int, [C.POINTER(P), C.c_int32, P]),
+    "hr_hier_destroy": (None, [P]),
+    "hr_hier_last_error": (C.c_char_p, [P]),
+    "hr_hier_set_objects": (C.c_int, [P, P, C.c_uint32, P, C.c_uint32, P, C.c_uint32]),
+    "hr_hier_set_instances": (C.c_int, [P, P, C.c_uint32]),
+    "hr_hier_set_densities": (C.c_int, [P, C.c_float, C.c_float]),
+    "hr_hier_build": (C.c_int, [P]),
+    "hr_hier_get_info": (C.c_int, [P, P]),
+    "hr_hier_download": (C.c_int, [P, P, P, P, P, P]),
+    "hr_hier_trace_rays": (C.c_int, [P, P, P, C.c_uint32, P, P, P, P, P]),
+    "hr_hier_trace_rays_device": (C.c_int, [P, P, P, C.c_uint32, P, P, P, P, P]),
+    "hr_hier_occluded": (C.c_int, [P, P, P, P, C.c_uint32, P]),
+    "hr_instances_file_read": (C.c_int, [C.c_char_p, P, C.c_uint32, C.POINTER(C.c_uint32)]),
+    "hr_instances_file_write": (C.c_int, [C.c_char_p, P, C.c_uint32]),
 }
+
+
+class Instance(C.Structure):
+    """hr_instance"""
+    _fields_ = [("object", C.c_uint32), ("m", C.c_float * 12), ("bmin", C.c_float * 3), ("bmax", C.c_float * 3)]
+
+
+class HierInfo(C.Structure):
+    """hr_hier_info"""
+    _fields_ = [("num_objects", C.c_uint32), ("num_instances", C.c_uint32), ("num_triangles", C.c_uint32),
+                ("num_object_cells", C.c_uint32), ("num_pairs", C.c_uint32), ("top_res", C.c_int32 * 3),
+                ("num_top_cells", C.c_uint32), ("num_top_pairs", C.c_uint32), ("top_bmin", C.c_float * 3),
+                ("top_bmax", C.c_float * 3)]
+
+
+class HierObject(C.Structure):
+    """hr_hier_object"""
+    _fields_ = [("bmin", C.c_float * 3), ("bmax", C.c_float * 3), ("cell_size", C.c_float * 3),
+                ("cell_size_rcp", C.c_float * 3), ("res", C.c_int32 * 3), ("first_cell", C.c_uint32),
+                ("first_triangle", C.c_uint32), ("num_triangles", C.c_uint32)]
 
 
 class BatchScene(C.Structure):

@@ -20,6 +20,7 @@
 
 #include <algorithm>
 #include <cerrno>
+#include <cfloat>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -607,6 +608,78 @@ hr_status hr_hits_file_write(const char* path, const int32_t* id, const float* t
         f.write((const char*)(v + i), 4);
     }
     return f ? HR_OK : io_error(HR_ERR_INVALID_ARG, "cannot write %s", path);
+}
+
+// The reference's instances file (WFObject::loadInstances, WFObjectReader.cpp:762-825):
+// "obj_id" starts an instance (identity map, empty box), "m_row_0..2" give the rows of
+// the world -> object map (rotation column entries, then translation), "AABB_min" /
+// "AABB_max" the world box; '#' starts a comment.
+hr_status hr_instances_file_read(const char* path, hr_instance* inst, uint32_t cap, uint32_t* n_out) {
+    if (!path || !n_out) return io_error(HR_ERR_INVALID_ARG, "null argument");
+    std::ifstream in(path);
+    if (!in) return io_error(HR_ERR_INVALID_ARG, "cannot read instances file %s", path);
+    std::string line;
+    size_t lineno = 0;
+    uint32_t n = 0;
+    hr_instance cur{};
+    auto flush = [&]() {
+        if (n > 0 && inst && n - 1 < cap) inst[n - 1] = cur;
+    };
+    while (std::getline(in, line)) {
+        ++lineno;
+        const size_t hash = line.find('#');
+        if (hash != std::string::npos) line = line.substr(0, hash);
+        std::stringstream ss(line);
+        std::string key;
+        if (!(ss >> key)) continue;
+        if (key == "obj_id") {
+            flush();
+            cur = hr_instance{};
+            cur.m[0] = cur.m[5] = cur.m[10] = 1.0f;
+            for (int k = 0; k < 3; ++k) { cur.bmin[k] = FLT_MAX; cur.bmax[k] = -FLT_MAX; }
+            long long id = -1;
+            if (!(ss >> id) || id < 0 || id > 0xffffffffLL)
+                return io_error(HR_ERR_INVALID_ARG, "%s line %zu: bad obj_id", path, lineno);
+            cur.object = (uint32_t)id;
+            ++n;
+            continue;
+        }
+        float* dst = nullptr;
+        int cnt = 0;
+        if (key == "m_row_0") { dst = cur.m; cnt = 4; }
+        else if (key == "m_row_1") { dst = cur.m + 4; cnt = 4; }
+        else if (key == "m_row_2") { dst = cur.m + 8; cnt = 4; }
+        else if (key == "AABB_min") { dst = cur.bmin; cnt = 3; }
+        else if (key == "AABB_max") { dst = cur.bmax; cnt = 3; }
+        else continue;   // other keys are ignored, as the reference does
+        if (n == 0) return io_error(HR_ERR_INVALID_ARG, "%s line %zu: %s before obj_id", path, lineno, key.c_str());
+        for (int k = 0; k < cnt; ++k)
+            if (!(ss >> dst[k])) return io_error(HR_ERR_INVALID_ARG, "%s line %zu: %s needs %d numbers", path, lineno,
+                                                 key.c_str(), cnt);
+    }
+    flush();
+    *n_out = n;
+    return HR_OK;
+}
+
+// ObjWriter::writeInstance (WFObjWriter.cpp:94-111) layout; numbers with 9 significant
+// digits so that a file read back gives the same floats
+hr_status hr_instances_file_write(const char* path, const hr_instance* inst, uint32_t n) {
+    if (!path || (n && !inst)) return io_error(HR_ERR_INVALID_ARG, "null argument");
+    FILE* f = std::fopen(path, "w");
+    if (!f) return io_error(HR_ERR_INVALID_ARG, "cannot write %s", path);
+    for (uint32_t i = 0; i < n; ++i) {
+        const hr_instance& r = inst[i];
+        std::fprintf(f, "#new instance#\nobj_id %u\n", r.object);
+        for (int row = 0; row < 3; ++row)
+            std::fprintf(f, "m_row_%d %.9g %.9g %.9g %.9g\n", row, r.m[4 * row], r.m[4 * row + 1], r.m[4 * row + 2],
+                         r.m[4 * row + 3]);
+        std::fprintf(f, "AABB_min %.9g %.9g %.9g\nAABB_max %.9g %.9g %.9g\n", r.bmin[0], r.bmin[1], r.bmin[2], r.bmax[0],
+                     r.bmax[1], r.bmax[2]);
+    }
+    const bool ok = std::ferror(f) == 0;
+    std::fclose(f);
+    return ok ? HR_OK : io_error(HR_ERR_INVALID_ARG, "cannot write %s", path);
 }
 
 hr_status hr_image_write(const char* path, const float* rgb, int32_t w, int32_t h, int32_t format) {

@@ -386,6 +386,77 @@ hr_status hr_hits_file_write(const char *path, const int32_t *id, const float *t
 /* A float RGB framebuffer (row 0 first) as PNG (8-bit RGB) or PFM (float RGB). */
 hr_status hr_image_write(const char *path, const float *rgb, int32_t width, int32_t height, int32_t format);
 
+/* ---------------------------------------------------------------------------------------
+ * Instanced two-level grid hierarchy (reference: TwoLevelGridHierarchy.h,
+ * TLGridHierarchySortBuilder.cu, TLGridHierarchyTraverser.h; RTEngine.cu:68-73 selects it
+ * with densities 1.2 / 1.2).  Objects are consecutive triangle ranges of one mesh in their
+ * own coordinates, each with its own uniform grid; instances place objects in the world
+ * and are binned into a uniform grid over their world boxes.  A rigid-body frame only
+ * changes the instances: hr_hier_build then rebuilds the instance grid alone.
+ * ------------------------------------------------------------------------------------- */
+typedef struct hr_hier hr_hier;
+
+/* One instance: object index, the world -> object map as the three rows of the
+ * reference's instances file (m_row_0..2: x' = m[0] x + m[1] y + m[2] z + m[3], y' from
+ * m[4..7], z' from m[8..11]) and the instance's world-space box (AABB_min / AABB_max),
+ * which must hold the transformed object. */
+typedef struct hr_instance {
+    uint32_t object;
+    float m[12];
+    float bmin[3], bmax[3];
+} hr_instance;
+
+typedef struct hr_hier_info {
+    uint32_t num_objects, num_instances, num_triangles;
+    uint32_t num_object_cells;   /* cells of all object grids */
+    uint32_t num_pairs;          /* (cell, triangle) references of the object grids */
+    int32_t top_res[3];          /* instance grid */
+    uint32_t num_top_cells, num_top_pairs;
+    float top_bmin[3], top_bmax[3];
+} hr_hier_info;
+
+/* Per-object grid as built (72 bytes, the layout hr_hier_download returns). */
+typedef struct hr_hier_object {
+    float bmin[3], bmax[3], cell_size[3], cell_size_rcp[3];
+    int32_t res[3];
+    uint32_t first_cell, first_triangle, num_triangles;
+} hr_hier_object;
+
+hr_status hr_hier_create(hr_hier **out, int32_t device, void *stream);
+void hr_hier_destroy(hr_hier *h);
+const char *hr_hier_last_error(const hr_hier *h);
+/* Object-space mesh: nv xyz vertices, ntri index triples, object k = the next
+ * object_tri_counts[k] triangles (every count > 0, the counts sum to ntri). */
+hr_status hr_hier_set_objects(hr_hier *h, const float *verts_xyz, uint32_t nv, const uint32_t *idx, uint32_t ntri,
+                              const uint32_t *object_tri_counts, uint32_t num_objects);
+hr_status hr_hier_set_instances(hr_hier *h, const hr_instance *inst, uint32_t n);
+/* instance-grid and object-grid densities (defaults 1.2, 1.2) */
+hr_status hr_hier_set_densities(hr_hier *h, float top_density, float object_density);
+/* Builds what changed: the object grids after hr_hier_set_objects / set_densities, the
+ * instance grid always.  Synchronous. */
+hr_status hr_hier_build(hr_hier *h);
+hr_status hr_hier_get_info(hr_hier *h, hr_hier_info *info);
+/* Host copies of the built arrays (any may be NULL): objects (num_objects records),
+ * object cells (2 x num_object_cells), triangle lists (num_pairs), instance-grid cells
+ * (2 x num_top_cells), instance lists (num_top_pairs). */
+hr_status hr_hier_download(hr_hier *h, hr_hier_object *objects, uint32_t *object_cells, uint32_t *triangles,
+                           uint32_t *top_cells, uint32_t *instances);
+/* Closest hit through the hierarchy: instance id and triangle id (-1 on a miss), t, u, v.
+ * Host buffers; the _device form takes device pointers and runs on the hierarchy's
+ * stream without a sync. */
+hr_status hr_hier_trace_rays(hr_hier *h, const float *org, const float *dir, uint32_t n, int32_t *inst_id,
+                             int32_t *tri_id, float *t, float *u, float *v);
+hr_status hr_hier_trace_rays_device(hr_hier *h, const float *org, const float *dir, uint32_t n, int32_t *inst_id,
+                                    int32_t *tri_id, float *t, float *u, float *v);
+/* Any hit below tmax[i]: occluded[i] = 1 / 0 (host buffers). */
+hr_status hr_hier_occluded(hr_hier *h, const float *org, const float *dir, const float *tmax, uint32_t n,
+                           uint8_t *occluded);
+/* The reference's instances file (WFObjectReader.cpp:762-825, WFObjWriter.cpp:94-111):
+ * per instance "obj_id", "m_row_0..2" and "AABB_min / AABB_max" lines.  read: n_out gets
+ * the count; up to cap records are stored (inst may be NULL to count). */
+hr_status hr_instances_file_read(const char *path, hr_instance *inst, uint32_t cap, uint32_t *n_out);
+hr_status hr_instances_file_write(const char *path, const hr_instance *inst, uint32_t n);
+
 #ifdef __cplusplus
 }
 #endif

@@ -131,3 +131,29 @@ def test_oracle_hier_identity_instances_equal_plain_objects(oracle):
     assert clear.sum() > 100
     assert np.array_equal(ht[clear], bt[clear])
     assert np.array_equal(hi[clear], np.where(bt[clear] < len(f), 0, 1))
+
+
+def test_instances_file_round_trip(hrlib, tmp_path):
+    from happyray_b200 import hier as Hh
+    from happyray_b200 import HRError
+    import pytest
+    _, _, _, inst = small_scene()
+    p = tmp_path / "scene.instances"
+    Hh.write_instances(str(p), inst)
+    text = p.read_text()
+    assert text.count("obj_id") == len(inst) and "m_row_2" in text and "AABB_max" in text
+    back = Hh.read_instances(str(p))
+    assert back.dtype == Hh.INSTANCE_DTYPE
+    for k in ("obj", "m", "bmin", "bmax"):
+        assert np.array_equal(back[k], inst[k])
+    # the reference's reader: defaults for missing rows, comments, other keys ignored
+    q = tmp_path / "b.instances"
+    q.write_text("# header\nobj_id 3\nm_row_0 1 0 0 5 # translated\nfoo bar\nAABB_min 0 0 0\nAABB_max 1 1 1\n"
+                 "obj_id 1\n")
+    r = Hh.read_instances(str(q))
+    assert list(r["obj"]) == [3, 1]
+    assert np.array_equal(r["m"][0], [1, 0, 0, 5, 0, 1, 0, 0, 0, 0, 1, 0])
+    assert np.array_equal(r["bmax"][0], [1, 1, 1])
+    (tmp_path / "c.instances").write_text("m_row_0 1 0 0 0\n")
+    with pytest.raises(HRError):
+        Hh.read_instances(str(tmp_path / "c.instances"))
