@@ -565,13 +565,204 @@ def run_served(args, rank, ws, local):
     print(json.dumps(line), flush=True)
 
 
+def hier_workload(seed: int = 0, frames: int = 8):
+    """Instanced hierarchy workload: 64 objects (icospheres and heightfield tiles, 320-20480
+    triangles) x 16,384 rigid instances (scales 0.01-0.05 in [0, 1]^3), 8 rigid-body frames
+    (every instance shifted by a seeded offset per frame), 1920x1080 pinhole rays at the
+    instance bounds, object / instance densities 1.2 / 1.2 (RTEngine.cu:72-73)."""
+    from happyray_b200 import scenes as S
+    v, f, counts, inst = S.instanced_scene(64, 16384, seed=seed, tri_range=(320, 20480), world=1.0,
+                                           scale_range=(0.01, 0.05))
+    rng = np.random.default_rng(seed + 1)
+    seq = []
+    for k in range(frames):
+        m = inst.copy()
+        shift = (rng.normal(0, 0.01, (len(inst), 3)) * k).astype(np.float32)
+        m["bmin"] += shift
+        m["bmax"] += shift
+        mm = m["m"].reshape(-1, 3, 4).astype(np.float64)
+        mm[:, :, 3] -= np.einsum("nij,nj->ni", mm[:, :, :3], shift.astype(np.float64))
+        m["m"] = mm.reshape(-1, 12).astype(np.float32)
+        seq.append(m)
+    W, H = 1920, 1080
+    lo, hi = inst["bmin"].min(0).astype(np.float64), inst["bmax"].max(0).astype(np.float64)
+    c = 0.5 * (lo + hi)
+    pos = np.array([0.5, -0.8, 0.9]) * (hi - lo) + lo
+    fwd = (c - pos) / np.linalg.norm(c - pos)
+    right = np.cross(fwd, [0.0, 0.0, 1.0]); right /= np.linalg.norm(right)
+    up = np.cross(right, fwd)
+    th = math.tan(math.radians(60.0) / 2)
+    xs = ((np.arange(W) + 0.5) / W * 2 - 1) * th * W / H
+    ys = (1 - (np.arange(H) + 0.5) / H * 2) * th
+    d = fwd[None, None, :] + xs[None, :, None] * right[None, None, :] + ys[:, None, None] * up[None, None, :]
+    d = (d / np.linalg.norm(d, axis=2, keepdims=True)).reshape(-1, 3).astype(np.float32)
+    org = np.broadcast_to(pos.astype(np.float32), d.shape).copy()
+    return dict(name="c6_instanced_hierarchy_64_objects_16384_instances_1080p", v=v, f=f, counts=counts,
+                frames=seq, org=org, dir=d, res=(W, H))
+
+
+def hier_bytes(rays, st):
+    """Algorithmic traversal bytes of the hierarchy: per ray 24 B ray + 20 B hit, 8 B per
+    instance-grid cell, 80 B per instance record tested, 72 B per object record of an
+    entered instance, 8 B per object-grid cell, 52 B per triangle test."""
+    s = st.sum(axis=0).astype(np.float64)
+    return 44.0 * rays + 8 * s[0] + 80 * s[1] + 72 * s[2] + 8 * s[3] + 52 * s[4]
+
+
+def cpu_baseline_hier(W, stride=16):
+    import oracle as O
+    t0 = time.perf_counter()
+    ob = O.hier_build(W["v"], W["f"], W["counts"], W["frames"][0], 1.2, 1.2)
+    tb = time.perf_counter() - t0
+    org, d = W["org"][::stride], W["dir"][::stride]
+    t0 = time.perf_counter()
+    O.hier_trace(ob, org, d)
+    tt = time.perf_counter() - t0
+    n = W["org"].shape[0]
+    return {"value": n / (tb + tt * stride) / 1e6, "unit": "Mrays/s", "cores": O.num_threads(), "kind": "port",
+            "sample": f"full build ({tb * 1e3:.0f} ms) + every {stride}th ray ({org.shape[0]} rays, "
+                      f"{tt * 1e3:.0f} ms) scaled to the full frame", "build_ms": tb * 1e3}
+
+
+def run_hier(args, rank, ws, local):
+    """c6: the instanced two-level grid hierarchy, one rigid-body frame per step: the
+    frame's instances to the device, the instance grid rebuilt, 1080p primary rays traced
+    (closest hit) through instance grid and object grids."""
+    W = hier_workload()
+    n = W["org"].shape[0]
+    if args.impl == "reference":
+        if rank == 0:
+            vals = [cpu_baseline_hier(W) for _ in range(max(1, args.steps // 10))]
+            cb = vals[-1]
+            v = statistics.median(x["value"] for x in vals)
+            print(json.dumps({"metric": METRIC, "value": v, "unit": "Mrays/s", "n_gpus": 1, "steps": len(vals),
+                              "warmup": 0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                              "dtype": "f32", "data": "synthetic (seeded)", "config": {"workload": W["name"]},
+                              "impl": "reference", "cpu_baseline": dict(cb, value=v),
+                              "e2e": {"value": v, "unit": "Mrays/s", "h2d_bytes_per_step": 0,
+                                      "d2h_bytes_per_step": 0}}), flush=True)
+        return
+    import torch
+    from happyray_b200.hier import Hierarchy
+    dev = local
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream(device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{dev}")
+    h = Hierarchy(dev, stream.cuda_stream)
+    t0 = time.perf_counter()
+    h.set_objects(W["v"], W["f"], W["counts"])
+    h.set_instances(W["frames"][0])
+    h.build()
+    full_build_s = time.perf_counter() - t0
+    dorg = torch.from_numpy(W["org"]).to(f"cuda:{dev}")
+    ddir = torch.from_numpy(W["dir"]).to(f"cuda:{dev}")
+    outs = [torch.empty(n, dtype=torch.int32, device=f"cuda:{dev}"), torch.empty(n, dtype=torch.int32, device=f"cuda:{dev}")]
+    outs += [torch.empty(n, dtype=torch.float32, device=f"cuda:{dev}") for _ in range(3)]
+    stats = torch.empty((n, 5), dtype=torch.int32, device=f"cuda:{dev}")
+    h.trace_stats_device(dorg, ddir, *outs, stats)
+    torch.cuda.synchronize()
+    st = stats.cpu().numpy().astype(np.int64)
+    b_trace = hier_bytes(n, st)
+    hit_frac = float((outs[0] >= 0).float().mean())
+    K = len(W["frames"])
+
+    def step(i, evs=None):
+        if evs:
+            evs[0].record(stream)
+        h.set_instances(W["frames"][i % K])
+        h.build()
+        if evs:
+            evs[1].record(stream)
+        h.trace_rays_device(dorg, ddir, *outs)
+        if evs:
+            evs[2].record(stream)
+
+    for i in range(args.warmup):
+        step(i)
+    torch.cuda.synchronize()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    l0 = h.info()["launches"]
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    with ClockSampler(dev) as clk:
+        for i in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+            step(i, evs[i])
+        torch.cuda.synchronize()
+    launches = h.info()["launches"] - l0
+    build_ms = [e[0].elapsed_time(e[1]) for e in evs]
+    trace_ms = [e[1].elapsed_time(e[2]) for e in evs]
+    total_ms = max_over_ranks(sum(b + t for b, t in zip(build_ms, trace_ms)), ws)
+    value = replica_value(n, args.steps, total_ms, ws)
+    e2e = None
+    if not args.no_e2e:
+        horg = torch.from_numpy(W["org"]).pin_memory().numpy()
+        hdir = torch.from_numpy(W["dir"]).pin_memory().numpy()
+        e_ms = []
+        for i in range(args.warmup + args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+            a, z = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            h.set_instances(W["frames"][i % K])
+            h.build()
+            res = h.trace_rays(horg, hdir)
+            z.record(stream)
+            z.synchronize()
+            if i >= args.warmup:
+                e_ms.append(a.elapsed_time(z))
+        et = max_over_ranks(sum(e_ms), ws)
+        e2e = {"value": replica_value(n, args.steps, et, ws), "unit": "Mrays/s",
+               "h2d_bytes_per_step": int(horg.nbytes + hdir.nbytes + W["frames"][0].nbytes),
+               "d2h_bytes_per_step": int(sum(a.nbytes for a in res)), "ms_per_step": et / args.steps}
+    if rank != 0:
+        h.close()
+        return
+    peak, peak_kind = peaks()
+    tmed, bmed = statistics.median(trace_ms), statistics.median(build_ms)
+    info = h.info()
+    line = {
+        "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene generators, no dataset)",
+        "config": {"workload": W["name"], "objects": int(len(W["counts"])), "triangles": int(W["f"].shape[0]),
+                   "instances": int(len(W["frames"][0])),
+                   "instanced_triangles": int(W["counts"][W["frames"][0]["obj"]].sum()),
+                   "resolution": list(W["res"]), "densities": [1.2, 1.2], "rigid_frames": K,
+                   "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{ws}"},
+        "rays_per_step": n, "hit_fraction": hit_frac,
+        "instance_rebuild_ms_per_frame": bmed, "trace_ms_per_frame": tmed, "full_build_s_first": full_build_s,
+        "grid": info,
+        "per_ray": {k: float(st[:, j].mean()) for j, k in enumerate(
+            ["instance_grid_cells", "instance_boxes_tested", "instances_entered", "object_grid_cells",
+             "triangle_tests"])},
+        "roofline": {"bound": "hbm", "kernel": "k_hier_trace", "achieved": b_trace / (tmed * 1e-3) / 1e9,
+                     "peak": peak, "unit": "GB/s", "frac": b_trace / (tmed * 1e-3) / 1e9 / peak, "traffic": None,
+                     "peak_source": peak_kind, "algorithmic_bytes_per_launch": b_trace, "kernel_ms": tmed},
+        "gpu_launches": launches,
+        "e2e": e2e,
+    }
+    clk_s = clk.summary()
+    if clk_s:
+        line["clocks"] = clk_s
+    if not args.no_cpu and ws == 1:
+        try:
+            line["cpu_baseline"] = cpu_baseline_hier(W)
+        except Exception as ex:   # the CPU leg is a reported baseline only
+            line["cpu_baseline"] = {"error": str(ex)}
+    print(json.dumps(line), flush=True)
+    h.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3", "c4", "c5"])
+    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3", "c4", "c5", "c6"])
     ap.add_argument("--requests", type=int, default=1000, help="c5: requests replayed per mode")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true")
@@ -583,6 +774,9 @@ def main():
         return
     if args.config == "c5":
         run_served(args, rank, ws, local)
+        return
+    if args.config == "c6":
+        run_hier(args, rank, ws, local)
         return
 
     W = workload(args.config)

@@ -125,6 +125,7 @@ SIGNATURES = {
     "hr_hier_download": (C.c_int, [P, P, P, P, P, P]),
     "hr_hier_trace_rays": (C.c_int, [P, P, P, C.c_uint32, P, P, P, P, P]),
     "hr_hier_trace_rays_device": (C.c_int, [P, P, P, C.c_uint32, P, P, P, P, P]),
+    "hr_hier_trace_stats_device": (C.c_int, [P, P, P, C.c_uint32, P, P, P, P, P, P]),
     "hr_hier_occluded": (C.c_int, [P, P, P, P, C.c_uint32, P]),
     "hr_instances_file_read": (C.c_int, [C.c_char_p, P, C.c_uint32, C.POINTER(C.c_uint32)]),
     "hr_instances_file_write": (C.c_int, [C.c_char_p, P, C.c_uint32]),
@@ -141,7 +142,7 @@ class HierInfo(C.Structure):
     _fields_ = [("num_objects", C.c_uint32), ("num_instances", C.c_uint32), ("num_triangles", C.c_uint32),
                 ("num_object_cells", C.c_uint32), ("num_pairs", C.c_uint32), ("top_res", C.c_int32 * 3),
                 ("num_top_cells", C.c_uint32), ("num_top_pairs", C.c_uint32), ("top_bmin", C.c_float * 3),
-                ("top_bmax", C.c_float * 3)]
+                ("top_bmax", C.c_float * 3), ("launches", C.c_uint64)]
 
 
 class HierObject(C.Structure):

@@ -331,15 +331,24 @@ struct HHit {
     int32_t inst, tri;
 };
 
+// per-ray work counters (STATS instances): instance-grid cells, instance boxes tested,
+// instances entered, object-grid cells, triangle tests
+struct HCount {
+    uint32_t top_cells = 0, inst_tests = 0, inst_entered = 0, obj_cells = 0, tri_tests = 0;
+};
+
 // One instance (GeometryInstanceTraverser, TLGridHierarchyTraverser.h:45-205): the world
 // box interval, the ray in object space, the object grid's DDA from the current best t.
 // Returns true when the instance's hit is accepted (inside the box interval, closer).
-__device__ bool hier_instance(const HierView& H, uint32_t ii, f3 o, f3 d, const float* rcp, HHit& h) {
+template <bool STATS>
+__device__ bool hier_instance(const HierView& H, uint32_t ii, f3 o, f3 d, const float* rcp, HHit& h, HCount& n) {
     const HierInst I = H.inst[ii];
     const float blo[3] = {I.lo.x, I.lo.y, I.lo.z}, bhi[3] = {I.hi.x, I.hi.y, I.hi.z};
     float te1, tx1;
     box_clip(blo, bhi, o, rcp, &te1, &tx1);
+    if (STATS) n.inst_tests++;
     if (!(tx1 > te1 && tx1 >= 0.0f && te1 < h.t)) return false;
+    if (STATS) n.inst_entered++;
     const f3 ot = mk(I.r0.x * o.x + I.r0.y * o.y + I.r0.z * o.z + I.r0.w,
                      I.r1.x * o.x + I.r1.y * o.y + I.r1.z * o.z + I.r1.w,
                      I.r2.x * o.x + I.r2.y * o.y + I.r2.z * o.z + I.r2.w);
@@ -376,6 +385,10 @@ __device__ bool hier_instance(const HierView& H, uint32_t ii, f3 o, f3 d, const 
             cell[2] > -1) {
             const uint2 cr = __ldg(H.obj_cells + (g.cell_off + (uint32_t)cell[0] + (uint32_t)cell[1] * rx +
                                                   (uint32_t)cell[2] * rxy));
+            if (STATS) {
+                n.obj_cells++;
+                n.tri_tests += cr.y - cr.x;
+            }
             for (uint32_t it = cr.x; it < cr.y; ++it) {
                 const uint32_t tri = __ldg(H.prims + it);
                 float t, u, v;
@@ -412,8 +425,8 @@ __device__ bool hier_instance(const HierView& H, uint32_t ii, f3 o, f3 d, const 
 
 // instance-grid DDA (TLGridHierarchyTraverser.h:220-405); ANY stops at the first
 // accepted hit
-template <bool ANY>
-__device__ void hier_trace(const HierView& H, const GridDesc& g, f3 o, f3 d, HHit& h) {
+template <bool ANY, bool STATS>
+__device__ void hier_trace(const HierView& H, const GridDesc& g, f3 o, f3 d, HHit& h, HCount& n) {
     const float rcp[3] = {1.0f / d.x, 1.0f / d.y, 1.0f / d.z};
     float t0, t1;
     box_clip(g.bmin, g.bmax, o, rcp, &t0, &t1);
@@ -439,8 +452,9 @@ __device__ void hier_trace(const HierView& H, const GridDesc& g, f3 o, f3 d, HHi
         if (cell[0] < g.res[0] && cell[0] > -1 && cell[1] < g.res[1] && cell[1] > -1 && cell[2] < g.res[2] &&
             cell[2] > -1) {
             const uint2 cr = __ldg(H.top_cells + ((uint32_t)cell[0] + (uint32_t)cell[1] * rx + (uint32_t)cell[2] * rxy));
+            if (STATS) n.top_cells++;
             for (uint32_t it = cr.x; it < cr.y; ++it)
-                if (hier_instance(H, __ldg(H.inst_ids + it), o, d, rcp, h) && ANY) return;
+                if (hier_instance<STATS>(H, __ldg(H.inst_ids + it), o, d, rcp, h, n) && ANY) return;
         }
         const int k = min_dim(tmax[0], tmax[1], tmax[2]);
         float tk;
@@ -463,13 +477,13 @@ __device__ void hier_trace(const HierView& H, const GridDesc& g, f3 o, f3 d, HHi
     }
 }
 
-template <bool ANY>
+template <bool ANY, bool STATS>
 __global__ __launch_bounds__(kTT, 8) void k_hier_trace(HierView H, const float* __restrict__ org,
                                                        const float* __restrict__ dir, const float* __restrict__ tmax,
                                                        uint32_t n, int32_t* __restrict__ oinst,
                                                        int32_t* __restrict__ otri, float* __restrict__ ot,
                                                        float* __restrict__ ou, float* __restrict__ ov,
-                                                       uint8_t* __restrict__ occ) {
+                                                       uint8_t* __restrict__ occ, uint32_t* __restrict__ stats) {
     const GridDesc g = *H.top;
     for (uint32_t i = blockIdx.x * kTT + threadIdx.x; i < n; i += gridDim.x * kTT) {
         const f3 o = mk(__ldg(org + 3 * (size_t)i), __ldg(org + 3 * (size_t)i + 1), __ldg(org + 3 * (size_t)i + 2));
@@ -477,7 +491,12 @@ __global__ __launch_bounds__(kTT, 8) void k_hier_trace(HierView H, const float* 
         HHit h;
         h.t = ANY ? __ldg(tmax + i) : FLT_MAX;
         h.u = 0.0f; h.v = 0.0f; h.inst = -1; h.tri = -1;
-        if (!g.error) hier_trace<ANY>(H, g, o, d, h);
+        HCount c;
+        if (!g.error) hier_trace<ANY, STATS>(H, g, o, d, h, c);
+        if (STATS) {
+            uint32_t* st = stats + 5 * (size_t)i;
+            st[0] = c.top_cells; st[1] = c.inst_tests; st[2] = c.inst_entered; st[3] = c.obj_cells; st[4] = c.tri_tests;
+        }
         if (ANY) {
             occ[i] = h.inst >= 0 ? 1 : 0;
         } else {
@@ -543,7 +562,7 @@ int build_objects(hr_hier* h) {
         (rc = ensure(c, B.block_sums, sizeof(uint32_t) * (nb + 1))) ||
         (rc = ensure(c, B.scan_partials, sizeof(uint32_t) * (scan_partials_words(h->nobj) + 2))))
         return rc;
-    c->launches += 7;
+    c->launches += 6;   // five kernels and the block-sum scan; the other scan counts its own
     k_hier_obj_init<<<grid_of(c, h->nobj, 256), 256, 0, s>>>(h->enc.as<int32_t>(), h->nobj);
     k_hier_tris<<<grid_of(c, h->ntri, kBT), kBT, 0, s>>>(c->verts.as<float4>(), c->idx.as<uint32_t>(),
                                                          h->tri_begin.as<uint32_t>(), h->nobj, h->ntri,
@@ -578,7 +597,7 @@ int build_objects(hr_hier* h) {
         (rc = ensure(c, B.tile_hist, sizeof(uint32_t) * radix_tile_hist_words(np, kb))) ||
         (rc = ensure(c, B.row_total, sizeof(uint32_t) * 256)))
         return rc;
-    c->launches += 3;
+    c->launches += 1;
     k_hier_write<<<nb, kBT, 0, s>>>(c->tris.as<float4>(), h->objs.as<HierObj>(), h->tri_begin.as<uint32_t>(), h->nobj,
                                     h->ntri, B.block_sums.as<uint32_t>(), B.keys_a.as<uint32_t>(),
                                     B.vals_a.as<uint32_t>());
@@ -593,6 +612,7 @@ int build_objects(hr_hier* h) {
     GridDesc* td = h->top_desc.as<GridDesc>();
     if ((rc = cuda_check(c, cudaMemsetAsync(td, 0, sizeof(GridDesc), s), "hier desc"))) return rc;
     const int gc = grid_of(c, h->num_obj_cells, 256);
+    c->launches += 2;
     k_fill_u2<<<gc, 256, 0, s>>>(h->obj_cells.as<uint2>(), words + 0, td, make_uint2(0u, 0u));
     k_cell_ranges<<<grid_of(c, np, 256), 256, 0, s>>>(sorted, words + 1, words + 0, td, h->obj_cells.as<uint2>());
     return cuda_check(c, cudaGetLastError(), "hier object grids");
@@ -631,7 +651,7 @@ int build_instances(hr_hier* h) {
         (rc = ensure(c, B.tile_hist, sizeof(uint32_t) * radix_tile_hist_words(np, kb))) ||
         (rc = ensure(c, B.row_total, sizeof(uint32_t) * 256)))
         return rc;
-    c->launches += 3;
+    c->launches += 1;
     k_hier_inst_write<<<grid_of(c, h->ninst, 256), 256, 0, s>>>(h->inst.as<HierInst>(), h->ninst, td,
                                                                 h->icnt.as<uint32_t>(), B.keys_a.as<uint32_t>(),
                                                                 B.vals_a.as<uint32_t>());
@@ -641,6 +661,7 @@ int build_instances(hr_hier* h) {
                                B.vals_b.as<uint32_t>(), sorted, h->inst_ids.as<uint32_t>(), words + 2, np, kb,
                                B.tile_hist.as<uint32_t>(), B.tile_hist.bytes, B.row_total.as<uint32_t>(), s)))
         return rc;
+    c->launches += 2;
     k_fill_u2<<<grid_of(c, h->top.ncells, 256), 256, 0, s>>>(h->top_cells.as<uint2>(), &td->ncells, td,
                                                              make_uint2(0u, 0u));
     k_cell_ranges<<<grid_of(c, np, 256), 256, 0, s>>>(sorted, words + 2, &td->ncells, td, h->top_cells.as<uint2>());
@@ -822,6 +843,7 @@ hr_status hr_hier_get_info(hr_hier* h, hr_hier_info* info) {
     }
     info->num_top_cells = h->top.ncells;
     info->num_top_pairs = h->num_top_pairs;
+    info->launches = h->c->launches;
     return HR_OK;
 }
 
@@ -854,8 +876,21 @@ hr_status hr_hier_trace_rays_device(hr_hier* h, const float* org, const float* d
     if (n == 0) return HR_OK;
     DeviceGuard dg(c->device);
     c->launches += 1;
-    k_hier_trace<false><<<grid_of(c, n, kTT), kTT, 0, c->stream>>>(view(h), org, dir, nullptr, n, inst_id, tri_id, t, u,
-                                                                    v, nullptr);
+    k_hier_trace<false, false><<<grid_of(c, n, kTT), kTT, 0, c->stream>>>(view(h), org, dir, nullptr, n, inst_id, tri_id,
+                                                                           t, u, v, nullptr, nullptr);
+    return (hr_status)cuda_check(c, cudaGetLastError(), "hier trace launch");
+}
+
+hr_status hr_hier_trace_stats_device(hr_hier* h, const float* org, const float* dir, uint32_t n, int32_t* inst_id,
+                                     int32_t* tri_id, float* t, float* u, float* v, uint32_t* stats) {
+    if (bad_hier(h) || (n && (!org || !dir || !inst_id || !tri_id || !t || !u || !v || !stats))) return HR_ERR_INVALID_ARG;
+    hr_ctx* c = h->c;
+    if (!h->built) return (hr_status)set_error(c, HR_ERR_NOT_READY, "hier: build first");
+    if (n == 0) return HR_OK;
+    DeviceGuard dg(c->device);
+    c->launches += 1;
+    k_hier_trace<false, true><<<grid_of(c, n, kTT), kTT, 0, c->stream>>>(view(h), org, dir, nullptr, n, inst_id, tri_id,
+                                                                          t, u, v, nullptr, stats);
     return (hr_status)cuda_check(c, cudaGetLastError(), "hier trace launch");
 }
 
@@ -907,8 +942,8 @@ hr_status hr_hier_occluded(hr_hier* h, const float* org, const float* dir, const
         (rc = cuda_check(c, cudaMemcpyAsync(dtm, tmax, 4 * (size_t)n, cudaMemcpyHostToDevice, s), "rays")))
         return (hr_status)rc;
     c->launches += 1;
-    k_hier_trace<true><<<grid_of(c, n, kTT), kTT, 0, s>>>(view(h), dorg, ddir, dtm, n, nullptr, nullptr, nullptr, nullptr,
-                                                          nullptr, docc);
+    k_hier_trace<true, false><<<grid_of(c, n, kTT), kTT, 0, s>>>(view(h), dorg, ddir, dtm, n, nullptr, nullptr, nullptr,
+                                                                 nullptr, nullptr, docc, nullptr);
     if ((rc = cuda_check(c, cudaGetLastError(), "hier occluded launch")) ||
         (rc = cuda_check(c, cudaMemcpyAsync(occluded, docc, n, cudaMemcpyDeviceToHost, s), "occluded")))
         return (hr_status)rc;

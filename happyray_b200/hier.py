@@ -109,6 +109,14 @@ class Hierarchy:
                                                         tri.data_ptr(), t.data_ptr(), u.data_ptr(), v.data_ptr()),
                     "trace_rays_device")
 
+    def trace_stats_device(self, org, dirs, inst, tri, t, u, v, stats):
+        """trace_rays_device plus 5 counters per ray in stats ((n, 5) int32 tensor): instance-grid
+        cells, instance boxes tested, instances entered, object-grid cells, triangle tests."""
+        n = org.shape[0]
+        self._check(self._lib.hr_hier_trace_stats_device(self._h, org.data_ptr(), dirs.data_ptr(), n, inst.data_ptr(),
+                                                         tri.data_ptr(), t.data_ptr(), u.data_ptr(), v.data_ptr(),
+                                                         stats.data_ptr()), "trace_stats_device")
+
     def occluded(self, org, dirs, tmax):
         org = np.ascontiguousarray(org, np.float32)
         dirs = np.ascontiguousarray(dirs, np.float32)

@@ -413,6 +413,7 @@ typedef struct hr_hier_info {
     int32_t top_res[3];          /* instance grid */
     uint32_t num_top_cells, num_top_pairs;
     float top_bmin[3], top_bmax[3];
+    uint64_t launches;           /* kernels enqueued by this hierarchy so far */
 } hr_hier_info;
 
 /* Per-object grid as built (72 bytes, the layout hr_hier_download returns). */
@@ -448,6 +449,11 @@ hr_status hr_hier_trace_rays(hr_hier *h, const float *org, const float *dir, uin
                              int32_t *tri_id, float *t, float *u, float *v);
 hr_status hr_hier_trace_rays_device(hr_hier *h, const float *org, const float *dir, uint32_t n, int32_t *inst_id,
                                     int32_t *tri_id, float *t, float *u, float *v);
+/* hr_hier_trace_rays_device that also writes 5 counters per ray to stats (device):
+ * instance-grid cells visited, instance boxes tested, instances entered, object-grid
+ * cells visited, triangle tests. */
+hr_status hr_hier_trace_stats_device(hr_hier *h, const float *org, const float *dir, uint32_t n, int32_t *inst_id,
+                                     int32_t *tri_id, float *t, float *u, float *v, uint32_t *stats);
 /* Any hit below tmax[i]: occluded[i] = 1 / 0 (host buffers). */
 hr_status hr_hier_occluded(hr_hier *h, const float *org, const float *dir, const float *tmax, uint32_t n,
                            uint8_t *occluded);
