@@ -2,6 +2,7 @@
 and nested traversal (TLGridHierarchySortBuilder.cu, TLGridHierarchyTraverser.h) checked
 against their invariants and against an FP64 brute force over every instance."""
 import numpy as np
+import pytest
 
 from happyray_b200 import scenes as S
 
@@ -157,3 +158,75 @@ def test_instances_file_round_trip(hrlib, tmp_path):
     (tmp_path / "c.instances").write_text("m_row_0 1 0 0 0\n")
     with pytest.raises(HRError):
         Hh.read_instances(str(tmp_path / "c.instances"))
+
+
+HIER_GOLDEN = sorted((__import__("pathlib").Path(__file__).resolve().parent / "golden").glob("ref_hier_*.npz"))
+
+
+@pytest.mark.parametrize("path", HIER_GOLDEN, ids=lambda p: p.stem)
+@pytest.mark.parametrize("variant", ["strict", "fast"])
+def test_oracle_hier_matches_reference_golden(oracle, path, variant):
+    """The oracle against the reference's own hierarchy builder and traverser
+    (oracle/ref_pin/ref_pin_hier.cu, fixtures by tests/golden/make_ref_golden.py --hier).
+    Everything is exact but the object-cell lists: the reference's UniformGrid recomputes
+    each object grid's cell size and reciprocal with an approximate division on the device
+    (fastDivide, UniformGrid.h:58-75), so a triangle lying exactly on a cell boundary can
+    be binned one cell over; the oracle keeps the IEEE quotients RTEngine computes
+    (RTEngine.cu:325-327).  Those triangles must still sit in the same cells up to one
+    boundary layer, and every hit must agree."""
+    from test_oracle import cell_lists
+    z = np.load(path)
+    ob = oracle.hier_build(z["vertices"], z["faces"], z["counts"], z["instances"], float(z["top_density"]),
+                           float(z["object_density"]))
+
+    def r(k):
+        return z[f"{variant}_{k}"]
+
+    for k in range(len(z["counts"])):
+        o = ob.objs[k]
+        assert tuple(r("obj_res")[k]) == tuple(o.res)
+        assert np.array_equal(r("obj_geo")[k], np.array([list(o.bmin), list(o.bmax), list(o.cs), list(o.rcp)], np.float32))
+        assert r("obj_first")[k] == o.cell_off
+    assert tuple(r("top_res")) == tuple(ob.top.res)
+    assert np.array_equal(r("top_geo"), np.array([list(ob.top.bmin), list(ob.top.bmax), list(ob.top.cs),
+                                                  list(ob.top.rcp)], np.float32))
+    rc, rl = cell_lists(r("top_cells"), r("inst_ids"))
+    oc, ol = cell_lists(ob.top_cells, ob.inst_ids)
+    assert np.array_equal(rc, oc) and np.array_equal(rl, ol)
+    # object cells: identical but for boundary-layer moves of a few triangles
+    rcl, rp = r("obj_cells"), r("prims")
+    ocl, op = ob.obj_cells, ob.prims
+    assert rcl.shape == ocl.shape
+    ref_cells, orc_cells = {}, {}
+    for c in range(rcl.shape[0]):
+        for t in rp[rcl[c, 0]:rcl[c, 1]]:
+            ref_cells.setdefault(int(t), set()).add(c)
+        for t in op[ocl[c, 0]:ocl[c, 1]]:
+            orc_cells.setdefault(int(t), set()).add(c)
+    assert set(ref_cells) == set(orc_cells) == set(range(z["faces"].shape[0]))
+    moved = [t for t in ref_cells if ref_cells[t] != orc_cells[t]]
+    assert len(moved) <= 0.05 * len(ref_cells)   # heightfield tiles put many vertices on cell planes
+    firsts = [ob.objs[k].cell_off for k in range(len(z["counts"]))]
+    for t in moved:
+        k = int(np.searchsorted(firsts, min(orc_cells[t]), side="right") - 1)
+        o = ob.objs[k]
+        rx, ry = o.res[0], o.res[1]
+
+        def xyz(c):
+            c -= o.cell_off
+            return np.array([c % rx, (c // rx) % ry, c // (rx * ry)])
+        a = np.array([xyz(c) for c in ref_cells[t]])
+        b = np.array([xyz(c) for c in orc_cells[t]])
+        assert np.all(np.abs(a.min(0) - b.min(0)) <= 1) and np.all(np.abs(a.max(0) - b.max(0)) <= 1)
+    # hits: the same instance and triangle for every ray; t within the precision the
+    # reference's reciprocal-derived directions allow
+    hi, ht, t, _, _ = oracle.hier_trace(ob, z["ray_org"], z["ray_dir"])
+    ri = r("hit_inst").astype(np.int64)
+    ri[ri == 0xFFFFFFFF] = -1
+    rt = r("hit_tri").astype(np.int64)
+    rt[rt == 0xFFFFFFFF] = -1
+    assert np.array_equal(ri, hi) and np.array_equal(rt, ht)
+    hit = hi >= 0
+    assert hit.sum() > 1000
+    rel = np.abs(r("hit_t")[hit] - t[hit]) / np.abs(t[hit])
+    assert rel.max() <= (5e-6 if variant == "strict" else 2e-4)
