@@ -346,7 +346,7 @@ int batch_alloc(hr_batch* b) {
     if ((rc = ensure(c, B.top_refs, sizeof(uint32_t) * cap_pairs))) return rc;
     if ((rc = ensure(c, B.block_sums, sizeof(uint32_t) * (std::max((size_t)b->ntchunk, nref_blocks) + 1)))) return rc;
     if ((rc = ensure(c, B.tile_hist, sizeof(uint32_t) * hist))) return rc;
-    if ((rc = ensure(c, B.row_total, sizeof(uint32_t) * 256))) return rc;
+    if ((rc = ensure(c, B.row_total, sizeof(uint32_t) * kRadixRowWords))) return rc;
     if ((rc = ensure(c, B.leaves, sizeof(uint2) * B.cap_leaves))) return rc;
     if ((rc = ensure(c, B.lkeys_a, sizeof(uint32_t) * B.cap_leaf_pairs))) return rc;
     if ((rc = ensure(c, B.lvals_a, sizeof(uint32_t) * B.cap_leaf_pairs))) return rc;
@@ -383,7 +383,7 @@ int enqueue_build(hr_batch* b) {
         return rc;
     kb_write_pairs<<<b->ntchunk, kBT, 0, s>>>(tris, tch, sc, descs, cell_off, bd, bsum, B.keys_a.as<uint32_t>(),
                                               B.vals_a.as<uint32_t>());
-    const int passes = (key_bits + 7) / 8;
+    const int passes = radix_sort_passes(key_bits);
     uint32_t* sorted_keys = (passes % 2 == 1) ? B.keys_b.as<uint32_t>() : B.keys_a.as<uint32_t>();
     if ((rc = radix_sort_pairs(c, B.keys_a.as<uint32_t>(), B.vals_a.as<uint32_t>(), B.keys_b.as<uint32_t>(),
                                B.vals_b.as<uint32_t>(), sorted_keys, B.top_refs.as<uint32_t>(), &bd->ntop_pairs,
@@ -410,7 +410,7 @@ int enqueue_build(hr_batch* b) {
     kb_leaf_write_pairs<<<nref_blocks, kBT, 0, s>>>(sorted_keys, B.top_refs.as<uint32_t>(), tris, descs, cell_off,
                                                     b->nsc, bd, B.cells.as<uint2>(), bsum, B.lkeys_a.as<uint32_t>(),
                                                     B.lvals_a.as<uint32_t>());
-    const int lpasses = (leaf_bits + 7) / 8;
+    const int lpasses = radix_sort_passes(leaf_bits);
     uint32_t* leaf_keys = (lpasses % 2 == 1) ? B.lkeys_b.as<uint32_t>() : B.lkeys_a.as<uint32_t>();
     if ((rc = radix_sort_pairs(c, B.lkeys_a.as<uint32_t>(), B.lvals_a.as<uint32_t>(), B.lkeys_b.as<uint32_t>(),
                                B.lvals_b.as<uint32_t>(), leaf_keys, B.prims.as<uint32_t>(), &bd->npairs,
@@ -569,8 +569,8 @@ int plan(hr_batch* b) {
     }
     if (!b->planned) return berr(b, HR_ERR_CAPACITY_RETRY, "batch: grid capacities did not converge");
     // the fitted capacities can need a LARGER radix histogram than the ones allocated
-    // above: fewer key bits may mean fewer passes of wider digits (17 bits: 3 passes of
-    // 6-bit digits; 16 bits: 2 passes of 8-bit digits, 4x the words per tile)
+    // above: fewer key bits may mean fewer passes of wider digits (19 bits: 3 passes of
+    // 7-bit digits; 18 bits: 2 passes of 9-bit digits, 4x the words per tile)
     if ((rc = batch_alloc(b))) return rc;
     b->jobs_valid = false;   // grid buffers may have moved
     if (!b->use_graph) return 0;

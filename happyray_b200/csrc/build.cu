@@ -246,7 +246,6 @@ int key_bits_for(size_t max_key) {
     return b;
 }
 
-int radix_passes(int key_bits) { return (key_bits + 7) / 8; }
 
 }  // namespace
 
@@ -269,9 +268,9 @@ static int build_once(hr_ctx* c, int32_t kind, int32_t exact, uint32_t* ovf_out,
     const size_t cap_pairs = B.cap_pairs;   // uniform pairs, or top-level pairs for two-level
     const uint32_t nblocks = (ntri + kBT - 1) / kBT;
     const int key_bits = key_bits_for(B.cap_cells);
-    const int passes = radix_passes(key_bits);
+    const int passes = radix_sort_passes(key_bits);
     const int leaf_bits = key_bits_for(B.cap_leaves);
-    const int leaf_passes = radix_passes(leaf_bits);
+    const int leaf_passes = radix_sort_passes(leaf_bits);
     const uint32_t nref_blocks = (uint32_t)((cap_pairs + kBT - 1) / kBT);   // per top-level reference
     size_t hist_words = radix_tile_hist_words(cap_pairs, key_bits);
     if (kind == kTwoLevel) hist_words = std::max(hist_words, radix_tile_hist_words(B.cap_leaf_pairs, leaf_bits));
@@ -285,7 +284,7 @@ static int build_once(hr_ctx* c, int32_t kind, int32_t exact, uint32_t* ovf_out,
     if ((rc = ensure(c, B.vals_b, sizeof(uint32_t) * cap_pairs))) return rc;
     if ((rc = ensure(c, B.block_sums, sizeof(uint32_t) * (std::max(nblocks, nref_blocks) + 1)))) return rc;
     if ((rc = ensure(c, B.tile_hist, sizeof(uint32_t) * hist_words))) return rc;
-    if ((rc = ensure(c, B.row_total, sizeof(uint32_t) * 256))) return rc;
+    if ((rc = ensure(c, B.row_total, sizeof(uint32_t) * kRadixRowWords))) return rc;
     if (kind == kUniform) {
         if ((rc = ensure(c, B.prims, sizeof(uint32_t) * cap_pairs))) return rc;
     } else {

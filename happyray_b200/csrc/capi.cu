@@ -569,12 +569,12 @@ hr_status hr_radix_sort_pairs_device(hr_ctx* c, uint32_t* keys, uint32_t* vals, 
     int rc;
     GridBuffers& B = c->g;
     if ((rc = ensure(c, B.keys_b, (size_t)n * 4)) || (rc = ensure(c, B.vals_b, (size_t)n * 4)) ||
-        (rc = ensure(c, B.tile_hist, 4 * radix_tile_hist_words(n, key_bits))) || (rc = ensure(c, B.row_total, 4 * 256)) ||
+        (rc = ensure(c, B.tile_hist, 4 * radix_tile_hist_words(n, key_bits))) || (rc = ensure(c, B.row_total, 4 * kRadixRowWords)) ||
         (rc = ensure(c, B.scan_partials, 64)))
         return (hr_status)rc;
     uint32_t* cnt = B.scan_partials.as<uint32_t>();
     if ((rc = cuda_check(c, cudaMemcpyAsync(cnt, &n, 4, cudaMemcpyHostToDevice, c->stream), "sort count"))) return (hr_status)rc;
-    const int passes = (key_bits + 7) / 8;
+    const int passes = radix_sort_passes(key_bits);
     // the final pass lands in (keys, vals): odd pass counts go through the scratch pair first
     if (passes % 2 == 1) {
         if ((rc = cuda_check(c, cudaMemcpyAsync(B.keys_b.p, keys, (size_t)n * 4, cudaMemcpyDeviceToDevice, c->stream), "sort copy")) ||

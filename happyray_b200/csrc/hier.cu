@@ -595,13 +595,13 @@ int build_objects(hr_hier* h) {
         (rc = ensure(c, B.vals_b, 4 * np)) || (rc = ensure(c, h->prims, 4 * np)) ||
         (rc = ensure(c, h->obj_cells, sizeof(uint2) * std::max<uint32_t>(h->num_obj_cells, 1))) ||
         (rc = ensure(c, B.tile_hist, sizeof(uint32_t) * radix_tile_hist_words(np, kb))) ||
-        (rc = ensure(c, B.row_total, sizeof(uint32_t) * 256)))
+        (rc = ensure(c, B.row_total, sizeof(uint32_t) * kRadixRowWords)))
         return rc;
     c->launches += 1;
     k_hier_write<<<nb, kBT, 0, s>>>(c->tris.as<float4>(), h->objs.as<HierObj>(), h->tri_begin.as<uint32_t>(), h->nobj,
                                     h->ntri, B.block_sums.as<uint32_t>(), B.keys_a.as<uint32_t>(),
                                     B.vals_a.as<uint32_t>());
-    const int passes = (kb + 7) / 8;
+    const int passes = radix_sort_passes(kb);
     uint32_t* sorted = (passes % 2 == 1) ? B.keys_b.as<uint32_t>() : B.keys_a.as<uint32_t>();
     if ((rc = radix_sort_pairs(c, B.keys_a.as<uint32_t>(), B.vals_a.as<uint32_t>(), B.keys_b.as<uint32_t>(),
                                B.vals_b.as<uint32_t>(), sorted, h->prims.as<uint32_t>(), words + 1, np, kb,
@@ -649,13 +649,13 @@ int build_instances(hr_hier* h) {
         (rc = ensure(c, B.vals_b, 4 * np)) || (rc = ensure(c, h->inst_ids, 4 * np)) ||
         (rc = ensure(c, h->top_cells, sizeof(uint2) * h->top.ncells)) ||
         (rc = ensure(c, B.tile_hist, sizeof(uint32_t) * radix_tile_hist_words(np, kb))) ||
-        (rc = ensure(c, B.row_total, sizeof(uint32_t) * 256)))
+        (rc = ensure(c, B.row_total, sizeof(uint32_t) * kRadixRowWords)))
         return rc;
     c->launches += 1;
     k_hier_inst_write<<<grid_of(c, h->ninst, 256), 256, 0, s>>>(h->inst.as<HierInst>(), h->ninst, td,
                                                                 h->icnt.as<uint32_t>(), B.keys_a.as<uint32_t>(),
                                                                 B.vals_a.as<uint32_t>());
-    const int passes = (kb + 7) / 8;
+    const int passes = radix_sort_passes(kb);
     uint32_t* sorted = (passes % 2 == 1) ? B.keys_b.as<uint32_t>() : B.keys_a.as<uint32_t>();
     if ((rc = radix_sort_pairs(c, B.keys_a.as<uint32_t>(), B.vals_a.as<uint32_t>(), B.keys_b.as<uint32_t>(),
                                B.vals_b.as<uint32_t>(), sorted, h->inst_ids.as<uint32_t>(), words + 2, np, kb,

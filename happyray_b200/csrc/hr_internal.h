@@ -147,6 +147,10 @@ int radix_sort_pairs(hr_ctx* c, const uint32_t* keys_in, const uint32_t* vals_in
                      const uint32_t* d_count, size_t cap_count, int key_bits,
                      uint32_t* tile_hist, size_t tile_hist_bytes, uint32_t* row_total, cudaStream_t s);
 size_t radix_tile_hist_words(size_t cap_count, int key_bits);
+// passes radix_sort_pairs makes for keys of key_bits bits (the output of an odd count ends in
+// the temporary buffers' pass parity: the caller picks keys_out accordingly)
+int radix_sort_passes(int key_bits);
+constexpr int kRadixRowWords = 512;   // row_total words radix_sort_pairs needs (9-bit digits)
 int exclusive_scan_u32(hr_ctx* c, uint32_t* data, const uint32_t* d_count, size_t cap_count,
                        uint32_t* d_total, uint32_t* partials, cudaStream_t s);
 int exclusive_scan_u32x2(hr_ctx* c, uint2* data, const uint32_t* d_count, size_t cap_count,

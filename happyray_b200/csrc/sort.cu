@@ -19,7 +19,7 @@ namespace {
 constexpr int kThreads = 256;
 constexpr int kItems = 8;
 constexpr int kTile = kThreads * kItems;   // 2048 keys per tile
-constexpr int kRadix = 256;                // max digit width 8 bits
+constexpr int kRadix = 512;                // max digit width 9 bits (two digits per thread below)
 constexpr int kWarps = kThreads / 32;
 // ----------------------------------------------------------------------------------
 // generic exclusive scan: reduce -> scan partials -> apply
@@ -175,13 +175,14 @@ __global__ __launch_bounds__(kThreads) void k_radix_downsweep(
     const uint32_t lt_mask = (1u << lane) - 1u;
 
     for (int i = threadIdx.x; i < kWarps * kRadix; i += kThreads) (&s_whist[0][0])[i] = 0u;
-    // digit start = exclusive scan of the digit totals
+    // digit start = exclusive scan of the digit totals (digits 2t and 2t + 1 on thread t)
     {
-        uint32_t d = threadIdx.x;
-        uint32_t tot = d <= mask ? row_total[d] : 0u;
+        const uint32_t d0 = 2u * threadIdx.x, d1 = d0 + 1u;
+        const uint32_t t0 = d0 <= mask ? row_total[d0] : 0u, t1 = d1 <= mask ? row_total[d1] : 0u;
         uint32_t all;
-        uint32_t ex = block_excl_scan<uint32_t, kThreads>(tot, &all);
-        if (d <= mask) s_goff[d] = ex + tile_hist[(size_t)d * ntiles_cap + blockIdx.x];
+        const uint32_t ex = block_excl_scan<uint32_t, kThreads>(t0 + t1, &all);
+        if (d0 <= mask) s_goff[d0] = ex + tile_hist[(size_t)d0 * ntiles_cap + blockIdx.x];
+        if (d1 <= mask) s_goff[d1] = ex + t0 + tile_hist[(size_t)d1 * ntiles_cap + blockIdx.x];
     }
     __syncthreads();
 
@@ -205,22 +206,27 @@ __global__ __launch_bounds__(kThreads) void k_radix_downsweep(
         __syncwarp();
     }
     __syncthreads();
-    // per digit: exclusive prefix over warps, tile-local digit totals
-    uint32_t tcount = 0;
-    if (threadIdx.x <= mask) {
-        uint32_t run = 0;
+    // per digit: exclusive prefix over warps, tile-local digit totals (digits 2t, 2t + 1)
+    uint32_t tcount[2] = {0u, 0u};
 #pragma unroll
-        for (int ww = 0; ww < kWarps; ++ww) {
-            uint32_t cnt = s_whist[ww][threadIdx.x];
-            s_whist[ww][threadIdx.x] = run;
-            run += cnt;
+    for (int j = 0; j < 2; ++j) {
+        const uint32_t d = 2u * threadIdx.x + (uint32_t)j;
+        if (d <= mask) {
+            uint32_t run = 0;
+#pragma unroll
+            for (int ww = 0; ww < kWarps; ++ww) {
+                uint32_t cnt = s_whist[ww][d];
+                s_whist[ww][d] = run;
+                run += cnt;
+            }
+            tcount[j] = run;
         }
-        tcount = run;
     }
     {
         uint32_t all;
-        uint32_t ex = block_excl_scan<uint32_t, kThreads>(tcount, &all);
-        if (threadIdx.x <= mask) s_loff[threadIdx.x] = ex;
+        const uint32_t ex = block_excl_scan<uint32_t, kThreads>(tcount[0] + tcount[1], &all);
+        if (2u * threadIdx.x <= mask) s_loff[2u * threadIdx.x] = ex;
+        if (2u * threadIdx.x + 1u <= mask) s_loff[2u * threadIdx.x + 1u] = ex + tcount[0];
     }
     __syncthreads();
 #pragma unroll
@@ -313,16 +319,26 @@ int scan_block_sums(hr_ctx* c, uint32_t* sums, uint32_t n, uint32_t* d_total, ui
     return cuda_check(c, cudaGetLastError(), "scan_block_sums");
 }
 
-static void radix_plan(int key_bits, int* passes, int* db) {
+// fewest passes of at most max_db-bit digits, the bits spread evenly over them (the
+// context path takes 9-bit digits: 17-18-bit cell keys sort in two passes, not three)
+static void radix_plan(int key_bits, int max_db, int* passes, int* db) {
     if (key_bits < 1) key_bits = 1;
     if (key_bits > 32) key_bits = 32;
-    *passes = (key_bits + 7) / 8;
+    *passes = (key_bits + max_db - 1) / max_db;
     *db = (key_bits + *passes - 1) / *passes;
+}
+
+constexpr int kMaxDigitBits = 9;   // context sorts; the allocation-free sort keeps 8 (its static scratch)
+
+int radix_sort_passes(int key_bits) {
+    int passes, db;
+    radix_plan(key_bits, kMaxDigitBits, &passes, &db);
+    return passes;
 }
 
 size_t radix_tile_hist_words(size_t cap_count, int key_bits) {
     int passes, db;
-    radix_plan(key_bits, &passes, &db);
+    radix_plan(key_bits, kMaxDigitBits, &passes, &db);
     size_t ntiles = (cap_count + kTile - 1) / kTile;
     if (ntiles == 0) ntiles = 1;
     return ntiles * ((size_t)1 << db);
@@ -337,7 +353,7 @@ int radix_sort_pairs(hr_ctx* c, const uint32_t* keys_in, const uint32_t* vals_in
         return set_error(c, 4, "radix sort: histogram of %zu bytes is too small for %zu keys of %d bits",
                          tile_hist_bytes, cap_count, key_bits);
     int passes, db;
-    radix_plan(key_bits, &passes, &db);
+    radix_plan(key_bits, kMaxDigitBits, &passes, &db);
     const uint32_t mask = (1u << db) - 1u;
     const uint32_t ntiles = (uint32_t)((cap_count + kTile - 1) / kTile);
     if (ntiles == 0) return 0;
@@ -366,7 +382,7 @@ cudaError_t radix_sort_pairs_raw(const uint32_t* keys_in, const uint32_t* vals_i
                                  const uint32_t* d_count, size_t cap_count, int key_bits, uint32_t* tile_hist,
                                  uint32_t* row_total, cudaStream_t s) {
     int passes, db;
-    radix_plan(key_bits, &passes, &db);
+    radix_plan(key_bits, 8, &passes, &db);
     const uint32_t mask = (1u << db) - 1u;
     const uint32_t ntiles = (uint32_t)((cap_count + kTile - 1) / kTile);
     if (ntiles == 0) return cudaSuccess;
