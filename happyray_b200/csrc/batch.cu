@@ -172,17 +172,12 @@ __global__ __launch_bounds__(kBT) void kb_write_pairs(const float4* __restrict__
         tri_bbox(p, &lo, &hi);
         n = cell_range(lo, hi, g.bmin, g.rcp, g.res, &r);
     }
-    uint32_t tot;
-    uint32_t slot = block_excl_scan<uint32_t, kBT>(n, &tot) + block_sums[blockIdx.x];
-    if (n == 0) return;
     const uint32_t base = __ldg(cell_off + ch.x);
     const uint32_t rx = (uint32_t)g.res[0], rxy = (uint32_t)g.res[0] * (uint32_t)g.res[1];
-    for (int32_t z = r.lo[2]; z < r.hi[2]; ++z)
-        for (int32_t y = r.lo[1]; y < r.hi[1]; ++y)
-            for (int32_t x = r.lo[0]; x < r.hi[0]; ++x, ++slot) {
-                keys[slot] = base + (uint32_t)x + (uint32_t)y * rx + (uint32_t)z * rxy;
-                vals[slot] = t;
-            }
+    PairRun run;
+    if (n) run = {base + (uint32_t)r.lo[0] + (uint32_t)r.lo[1] * rx + (uint32_t)r.lo[2] * rxy,
+                  (uint32_t)(r.hi[0] - r.lo[0]), (uint32_t)(r.hi[1] - r.lo[1]), rx, rxy, t};
+    block_write_runs<kBT>(n, run, block_sums[blockIdx.x], keys, vals);
 }
 
 // a8 per global top cell, with the cell's scene found by binary search
@@ -264,16 +259,11 @@ __global__ __launch_bounds__(kBT) void kb_leaf_write_pairs(const uint32_t* __res
     CRange r;
     if (i < bd->ntop_pairs)
         n = bref_leaf_range(descs, cell_off, nsc, top_keys, top_refs, tris, top_cells, i, &cell, &tri, lres, &r);
-    uint32_t tot;
-    uint32_t slot = block_excl_scan<uint32_t, kBT>(n, &tot) + block_sums[blockIdx.x];
-    if (n == 0) return;
-    const uint32_t base = top_cells[cell].x;
-    for (int32_t z = r.lo[2]; z < r.hi[2]; ++z)
-        for (int32_t yy = r.lo[1]; yy < r.hi[1]; ++yy)
-            for (int32_t x = r.lo[0]; x < r.hi[0]; ++x, ++slot) {
-                keys[slot] = base + (uint32_t)x + (uint32_t)yy * lres[0] + (uint32_t)z * lres[0] * lres[1];
-                vals[slot] = tri;
-            }
+    PairRun run;
+    if (n) run = {top_cells[cell].x + (uint32_t)r.lo[0] + (uint32_t)r.lo[1] * lres[0] +
+                      (uint32_t)r.lo[2] * lres[0] * lres[1],
+                  (uint32_t)(r.hi[0] - r.lo[0]), (uint32_t)(r.hi[1] - r.lo[1]), lres[0], lres[0] * lres[1], tri};
+    block_write_runs<kBT>(n, run, block_sums[blockIdx.x], keys, vals);
 }
 
 template <class T>

@@ -77,9 +77,30 @@ __global__ void k_grid_setup(GridDesc* d, float density, uint32_t cap_cells) {
 // a3: pair count, one triangle per thread; block sums for the scan (UniformGridBuildKernels.h:40-105).
 // Also writes the per-triangle vertex array (3 float4) that the later build passes and the
 // traversal read instead of gathering through the index buffer.
+// Cell ranges of up to 16-bit coordinates are kept per triangle (x: lo | hi << 16 per axis
+// in .x .y .z, pair count in .w) so that the scatter pass reads 16 bytes per triangle
+// instead of its 48-byte vertex record; a grid with an axis of more than 65,535 cells
+// keeps recomputing them from the vertices.
+__device__ __forceinline__ bool ranges_fit(const int32_t* res) {
+    return res[0] <= 65535 && res[1] <= 65535 && res[2] <= 65535;
+}
+__device__ __forceinline__ uint4 pack_range(const CRange& r, uint32_t n) {
+    uint32_t w[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+        w[k] = (uint32_t)min(max(r.lo[k], 0), 65535) | ((uint32_t)min(max(r.hi[k], 0), 65535) << 16);
+    return make_uint4(w[0], w[1], w[2], n);
+}
+__device__ __forceinline__ uint32_t unpack_range(uint4 q, CRange* r) {
+    r->lo[0] = (int32_t)(q.x & 0xFFFFu); r->hi[0] = (int32_t)(q.x >> 16);
+    r->lo[1] = (int32_t)(q.y & 0xFFFFu); r->hi[1] = (int32_t)(q.y >> 16);
+    r->lo[2] = (int32_t)(q.z & 0xFFFFu); r->hi[2] = (int32_t)(q.z >> 16);
+    return q.w;
+}
+
 __global__ __launch_bounds__(kBT) void k_count_pairs(const float4* __restrict__ v, const uint32_t* __restrict__ idx,
                                                      uint32_t ntri, const GridDesc* d, uint32_t* block_sums,
-                                                     float4* __restrict__ tris) {
+                                                     float4* __restrict__ tris, uint4* __restrict__ rng) {
     if (d->overflow | d->error) {
         if (threadIdx.x == 0) block_sums[blockIdx.x] = 0u;
         return;
@@ -97,6 +118,7 @@ __global__ __launch_bounds__(kBT) void k_count_pairs(const float4* __restrict__ 
         q[2] = make_float4(p[2].x, p[2].y, p[2].z, 0.0f);
         tri_bbox(p, &lo, &hi);
         n = cell_range(lo, hi, g.bmin, g.rcp, g.res, &r);
+        if (rng && ranges_fit(g.res)) rng[t] = pack_range(r, n);
     }
     uint32_t tot;
     block_excl_scan<uint32_t, kBT>(n, &tot);
@@ -107,8 +129,8 @@ __global__ __launch_bounds__(kBT) void k_count_pairs(const float4* __restrict__ 
 // with EXACT a cell rejected by the SAT test gets key = ncells (sorted last, skipped).
 template <bool EXACT>
 __global__ __launch_bounds__(kBT) void k_write_pairs(const float4* __restrict__ tris, uint32_t ntri, const GridDesc* d,
-                                                     const uint32_t* block_sums, uint32_t* __restrict__ keys,
-                                                     uint32_t* __restrict__ vals) {
+                                                     const uint32_t* block_sums, const uint4* __restrict__ rng,
+                                                     uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
     if (d->overflow | d->error) return;
     const DescRegs g = load_desc(d);
     const uint32_t t = blockIdx.x * kBT + threadIdx.x;
@@ -116,23 +138,25 @@ __global__ __launch_bounds__(kBT) void k_write_pairs(const float4* __restrict__ 
     f3 p[3], lo, hi;
     CRange r;
     if (t < ntri) {
-        tri_fetch(tris, t, p);
-        tri_bbox(p, &lo, &hi);
-        n = cell_range(lo, hi, g.bmin, g.rcp, g.res, &r);
+        if (!EXACT && rng && ranges_fit(g.res)) {
+            n = unpack_range(__ldg(rng + t), &r);   // the range k_count_pairs found
+        } else {
+            tri_fetch(tris, t, p);
+            tri_bbox(p, &lo, &hi);
+            n = cell_range(lo, hi, g.bmin, g.rcp, g.res, &r);
+        }
+    }
+    const uint32_t rx = (uint32_t)g.res[0], rxy = (uint32_t)g.res[0] * (uint32_t)g.res[1];
+    if (!EXACT) {
+        PairRun run;
+        if (n) run = {(uint32_t)r.lo[0] + (uint32_t)r.lo[1] * rx + (uint32_t)r.lo[2] * rxy,
+                      (uint32_t)(r.hi[0] - r.lo[0]), (uint32_t)(r.hi[1] - r.lo[1]), rx, rxy, t};
+        block_write_runs<kBT>(n, run, block_sums[blockIdx.x], keys, vals);
+        return;
     }
     uint32_t tot;
     uint32_t slot = block_excl_scan<uint32_t, kBT>(n, &tot) + block_sums[blockIdx.x];
     if (n == 0) return;
-    const uint32_t rx = (uint32_t)g.res[0], rxy = (uint32_t)g.res[0] * (uint32_t)g.res[1];
-    if (!EXACT) {
-        for (int32_t z = r.lo[2]; z < r.hi[2]; ++z)
-            for (int32_t y = r.lo[1]; y < r.hi[1]; ++y)
-                for (int32_t x = r.lo[0]; x < r.hi[0]; ++x, ++slot) {
-                    keys[slot] = (uint32_t)x + (uint32_t)y * rx + (uint32_t)z * rxy;
-                    vals[slot] = t;
-                }
-        return;
-    }
     const f3 nrm = normalize(cross(sub(p[1], p[0]), sub(p[2], p[0])));
     const f3 h = mulf(g.cs, 0.505f);
     f3 mc = mk((float)r.lo[0], (float)r.lo[1], (float)r.lo[2]);
@@ -192,11 +216,25 @@ __device__ __forceinline__ uint32_t ref_leaf_range(const DescRegs& g, const uint
 
 // a10: leaf pair count per top-level reference, block sums (countLeafLevelPairs,
 // TLGridBuildKernels.h:304-409)
+// Per top-level reference the count pass keeps what the scatter pass needs, 16 bytes:
+// .x = lo.x | lo.y << 8 | lo.z << 16 | lres.x << 24, .y = hi.x | hi.y << 8 | hi.z << 16 |
+// lres.y << 24 (sub-grid coordinates and resolutions are below 256), .z = the top cell's
+// first leaf, .w = the triangle.
+__device__ __forceinline__ uint4 pack_ref(const CRange& r, const uint32_t* lres, uint32_t base, uint32_t tri) {
+    uint32_t a = 0, b = 0;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        a |= (uint32_t)min(max(r.lo[k], 0), 255) << (8 * k);
+        b |= (uint32_t)min(max(r.hi[k], 0), 255) << (8 * k);
+    }
+    return make_uint4(a | (lres[0] << 24), b | (lres[1] << 24), base, tri);
+}
+
 __global__ __launch_bounds__(kBT) void k_leaf_count_pairs(const uint32_t* __restrict__ top_keys,
                                                           const uint32_t* __restrict__ top_refs,
                                                           const float4* __restrict__ tris,
                                                           const GridDesc* d, const uint2* __restrict__ top_cells,
-                                                          uint32_t* block_sums) {
+                                                          uint32_t* block_sums, uint4* __restrict__ refrng) {
     if (d->overflow | d->error) {
         if (threadIdx.x == 0) block_sums[blockIdx.x] = 0u;
         return;
@@ -208,6 +246,7 @@ __global__ __launch_bounds__(kBT) void k_leaf_count_pairs(const uint32_t* __rest
         uint32_t cell, tri, lres[3];
         CRange r;
         n = ref_leaf_range(g, top_keys, top_refs, tris, top_cells, i, &cell, &tri, lres, &r);
+        if (refrng) refrng[i] = pack_ref(r, lres, top_cells[cell].x, tri);
     }
     uint32_t tot;
     block_excl_scan<uint32_t, kBT>(n, &tot);
@@ -216,28 +255,32 @@ __global__ __launch_bounds__(kBT) void k_leaf_count_pairs(const uint32_t* __rest
 
 // a11: leaf pairs in reference order at each reference's scan offset; key = first leaf of
 // the top cell + local sub-cell index (writeLeafLevelKeysAndValues, TLGridBuildKernels.h:536-663)
-__global__ __launch_bounds__(kBT) void k_leaf_write_pairs(const uint32_t* __restrict__ top_keys,
-                                                          const uint32_t* __restrict__ top_refs,
-                                                          const float4* __restrict__ tris,
-                                                          const GridDesc* d, const uint2* __restrict__ top_cells,
+__global__ __launch_bounds__(kBT) void k_leaf_write_pairs(const uint4* __restrict__ refrng, const GridDesc* d,
                                                           const uint32_t* block_sums, uint32_t* __restrict__ keys,
                                                           uint32_t* __restrict__ vals) {
     if (d->overflow | d->error) return;
-    const DescRegs g = load_desc(d);
     const uint32_t i = blockIdx.x * kBT + threadIdx.x;
-    uint32_t n = 0, cell = 0, tri = 0, lres[3] = {1u, 1u, 1u};
+    uint32_t n = 0, tri = 0, base = 0, lres[2] = {1u, 1u};
     CRange r;
-    if (i < d->ntop_pairs) n = ref_leaf_range(g, top_keys, top_refs, tris, top_cells, i, &cell, &tri, lres, &r);
-    uint32_t tot;
-    uint32_t slot = block_excl_scan<uint32_t, kBT>(n, &tot) + block_sums[blockIdx.x];
-    if (n == 0) return;
-    const uint32_t base = top_cells[cell].x;
-    for (int32_t z = r.lo[2]; z < r.hi[2]; ++z)
-        for (int32_t yy = r.lo[1]; yy < r.hi[1]; ++yy)
-            for (int32_t x = r.lo[0]; x < r.hi[0]; ++x, ++slot) {
-                keys[slot] = base + (uint32_t)x + (uint32_t)yy * lres[0] + (uint32_t)z * lres[0] * lres[1];
-                vals[slot] = tri;
-            }
+    if (i < d->ntop_pairs) {   // the sub-cell range k_leaf_count_pairs found
+        const uint4 q = __ldg(refrng + i);
+        n = 1;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            r.lo[k] = (int32_t)((q.x >> (8 * k)) & 0xFFu);
+            r.hi[k] = (int32_t)((q.y >> (8 * k)) & 0xFFu);
+            const int32_t e = r.hi[k] - r.lo[k];
+            n *= (uint32_t)(e > 0 ? e : 0);
+        }
+        lres[0] = q.x >> 24;
+        lres[1] = q.y >> 24;
+        base = q.z;
+        tri = q.w;
+    }
+    PairRun run;
+    if (n) run = {base + (uint32_t)r.lo[0] + (uint32_t)r.lo[1] * lres[0] + (uint32_t)r.lo[2] * lres[0] * lres[1],
+                  (uint32_t)(r.hi[0] - r.lo[0]), (uint32_t)(r.hi[1] - r.lo[1]), lres[0], lres[0] * lres[1], tri};
+    block_write_runs<kBT>(n, run, block_sums[blockIdx.x], keys, vals);
 }
 
 int key_bits_for(size_t max_key) {
@@ -279,6 +322,7 @@ static int build_once(hr_ctx* c, int32_t kind, int32_t exact, uint32_t* ovf_out,
     if ((rc = ensure(c, c->tris, sizeof(float4) * 3 * (size_t)ntri))) return rc;
     if ((rc = ensure(c, B.cells, sizeof(uint2) * B.cap_cells))) return rc;
     if ((rc = ensure(c, B.keys_a, sizeof(uint32_t) * cap_pairs))) return rc;
+    if ((rc = ensure(c, B.tri_ranges, sizeof(uint4) * (size_t)ntri))) return rc;
     if ((rc = ensure(c, B.vals_a, sizeof(uint32_t) * cap_pairs))) return rc;
     if ((rc = ensure(c, B.keys_b, sizeof(uint32_t) * cap_pairs))) return rc;
     if ((rc = ensure(c, B.vals_b, sizeof(uint32_t) * cap_pairs))) return rc;
@@ -290,6 +334,7 @@ static int build_once(hr_ctx* c, int32_t kind, int32_t exact, uint32_t* ovf_out,
     } else {
         if ((rc = ensure(c, B.top_ranges, sizeof(uint2) * B.cap_cells))) return rc;
         if ((rc = ensure(c, B.top_refs, sizeof(uint32_t) * cap_pairs))) return rc;
+        if ((rc = ensure(c, B.ref_ranges, sizeof(uint4) * cap_pairs))) return rc;
         if ((rc = ensure(c, B.leaf_cnt, sizeof(uint32_t) * B.cap_cells))) return rc;
         if ((rc = ensure(c, B.scan_partials, sizeof(uint32_t) * (scan_partials_words(B.cap_cells) + 2)))) return rc;
         if ((rc = ensure(c, B.leaves, sizeof(uint2) * B.cap_leaves))) return rc;
@@ -321,14 +366,16 @@ static int build_once(hr_ctx* c, int32_t kind, int32_t exact, uint32_t* ovf_out,
     uint32_t* bsum = B.block_sums.as<uint32_t>();
     uint32_t* d_np = kind == kUniform ? &d->npairs : &d->ntop_pairs;
     if (nblocks > 0) {
-        k_count_pairs<<<nblocks, kBT, 0, s>>>(v, ix, ntri, d, bsum, c->tris.as<float4>());
+        k_count_pairs<<<nblocks, kBT, 0, s>>>(v, ix, ntri, d, bsum, c->tris.as<float4>(), B.tri_ranges.as<uint4>());
         if ((rc = scan_block_sums(c, bsum, nblocks, d_np, &d->overflow, (uint32_t)std::min(cap_pairs, (size_t)0xffffffffu),
                                   kind == kUniform ? kOvfPairs : kOvfTopPairs, &d->req_pairs, s)))
             return rc;
         if (kind == kUniform && exact)
-            k_write_pairs<true><<<nblocks, kBT, 0, s>>>(c->tris.as<float4>(), ntri, d, bsum, B.keys_a.as<uint32_t>(), B.vals_a.as<uint32_t>());
+            k_write_pairs<true><<<nblocks, kBT, 0, s>>>(c->tris.as<float4>(), ntri, d, bsum, nullptr,
+                                                        B.keys_a.as<uint32_t>(), B.vals_a.as<uint32_t>());
         else
-            k_write_pairs<false><<<nblocks, kBT, 0, s>>>(c->tris.as<float4>(), ntri, d, bsum, B.keys_a.as<uint32_t>(), B.vals_a.as<uint32_t>());
+            k_write_pairs<false><<<nblocks, kBT, 0, s>>>(c->tris.as<float4>(), ntri, d, bsum, B.tri_ranges.as<uint4>(),
+                                                         B.keys_a.as<uint32_t>(), B.vals_a.as<uint32_t>());
     }
     mark();
     uint32_t* sorted_keys = (passes % 2 == 1) ? B.keys_b.as<uint32_t>() : B.keys_a.as<uint32_t>();
@@ -356,13 +403,12 @@ static int build_once(hr_ctx* c, int32_t kind, int32_t exact, uint32_t* ovf_out,
         mark();
         uint32_t* lsum = B.block_sums.as<uint32_t>();
         k_leaf_count_pairs<<<nref_blocks, kBT, 0, s>>>(sorted_keys, B.top_refs.as<uint32_t>(), c->tris.as<float4>(), d,
-                                                       B.cells.as<uint2>(), lsum);
+                                                       B.cells.as<uint2>(), lsum, B.ref_ranges.as<uint4>());
         if ((rc = scan_block_sums(c, lsum, nref_blocks, &d->npairs, &d->overflow,
                                   (uint32_t)std::min(B.cap_leaf_pairs, (size_t)0xffffffffu), kOvfLeafPairs,
                                   &d->req_leaf_pairs, s)))
             return rc;
-        k_leaf_write_pairs<<<nref_blocks, kBT, 0, s>>>(sorted_keys, B.top_refs.as<uint32_t>(), c->tris.as<float4>(), d,
-                                                       B.cells.as<uint2>(), lsum, B.lkeys_a.as<uint32_t>(),
+        k_leaf_write_pairs<<<nref_blocks, kBT, 0, s>>>(B.ref_ranges.as<uint4>(), d, lsum, B.lkeys_a.as<uint32_t>(),
                                                        B.lvals_a.as<uint32_t>());
         mark();
         uint32_t* leaf_keys = (leaf_passes % 2 == 1) ? B.lkeys_b.as<uint32_t>() : B.lkeys_a.as<uint32_t>();

@@ -47,6 +47,49 @@ __device__ __forceinline__ T block_excl_scan(T x, T* total) {
     return before + (inc - x);
 }
 
+// Largest k in [0, NT) with off[k] <= j, for a non-decreasing off[] (off[0] = 0 <= j): the
+// item whose output run [off[k], off[k + 1]) holds output j of a block.
+template <int NT>
+__device__ __forceinline__ int block_owner(const uint32_t* off, uint32_t j) {
+    int k = 0;
+#pragma unroll
+    for (int step = NT / 2; step > 0; step >>= 1)
+        if (off[k + step] <= j) k += step;
+    return k;
+}
+
+// One item's run of (cell key, value) pairs: the cells of an ex x ey x ez box, x fastest,
+// then y, then z, keyed key0 + dx + dy * sx + dz * sxy, all with value val.
+struct PairRun { uint32_t key0, ex, ey, sx, sxy, val; };
+
+// Writes a block's pairs with all its threads: the runs follow one another in thread order
+// from out0, and pair j of the block is stored by thread j mod NT, so a run of thousands of
+// cells costs its block a few strides instead of one thread a serial loop, and consecutive
+// threads store consecutive slots.  n is this thread's run length, run is read when n > 0.
+// Every thread of the block calls it.
+template <int NT>
+__device__ __forceinline__ void block_write_runs(uint32_t n, const PairRun& run, uint32_t out0,
+                                                 uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+    __shared__ uint32_t s_off[NT];
+    __shared__ PairRun s_run[NT];
+    uint32_t tot;
+    s_off[threadIdx.x] = block_excl_scan<uint32_t, NT>(n, &tot);
+    if (n) s_run[threadIdx.x] = run;
+    __syncthreads();
+    for (uint32_t j = threadIdx.x; j < tot; j += NT) {
+        const int k = block_owner<NT>(s_off, j);
+        const PairRun q = s_run[k];
+        const uint32_t l = j - s_off[k];
+        uint32_t key = q.key0;
+        if (l) {
+            const uint32_t a = l / q.ex, z = a / q.ey;
+            key += (l - a * q.ex) + (a - z * q.ey) * q.sx + z * q.sxy;
+        }
+        keys[out0 + j] = key;
+        vals[out0 + j] = q.val;
+    }
+}
+
 
 }  // namespace hr
 

@@ -54,6 +54,8 @@ struct GridBuffers {
     DevBuf leaf_cnt;      // two-level: leaf cells per top cell, scanned in place to the first leaf
     DevBuf lkeys_a, lvals_a, lkeys_b, lvals_b;   // two-level: leaf pair ping-pong
     DevBuf scan_partials; // generic scan partial sums
+    DevBuf tri_ranges;    // uint4 per triangle: its cell range (16-bit coordinates) and pair count
+    DevBuf ref_ranges;    // two-level: uint4 per top-level reference: sub-cell range, first leaf, triangle
     size_t cap_cells = 0, cap_pairs = 0, cap_top_pairs = 0, cap_leaves = 0, cap_leaf_pairs = 0;
     // largest sizes seen by a completed build: the capacities (which size the count, scan
     // and sort launches) follow them with headroom instead of the first estimates
