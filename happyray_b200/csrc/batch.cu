@@ -126,7 +126,8 @@ __global__ __launch_bounds__(1024) void kb_setup(const BScene* __restrict__ sc, 
 __global__ __launch_bounds__(kBT) void kb_count_pairs(const float4* __restrict__ v, const uint32_t* __restrict__ idx,
                                                       const uint2* __restrict__ tchunk, const BScene* __restrict__ sc,
                                                       const GridDesc* __restrict__ descs, const GridDesc* bd,
-                                                      uint32_t* block_sums, float4* __restrict__ tris) {
+                                                      uint32_t* block_sums, float4* __restrict__ tris,
+                                                      uint4* __restrict__ rng) {
     if (bd->overflow | bd->error) {
         if (threadIdx.x == 0) block_sums[blockIdx.x] = 0u;
         return;
@@ -146,6 +147,7 @@ __global__ __launch_bounds__(kBT) void kb_count_pairs(const float4* __restrict__
         q[2] = make_float4(p[2].x, p[2].y, p[2].z, 0.0f);
         tri_bbox(p, &lo, &hi);
         n = cell_range(lo, hi, g.bmin, g.rcp, g.res, &r);
+        if (ranges_fit(g.res)) rng[t] = pack_range(r, n);
     }
     uint32_t tot;
     block_excl_scan<uint32_t, kBT>(n, &tot);
@@ -157,8 +159,8 @@ __global__ __launch_bounds__(kBT) void kb_count_pairs(const float4* __restrict__
 __global__ __launch_bounds__(kBT) void kb_write_pairs(const float4* __restrict__ tris, const uint2* __restrict__ tchunk,
                                                       const BScene* __restrict__ sc, const GridDesc* __restrict__ descs,
                                                       const uint32_t* __restrict__ cell_off, const GridDesc* bd,
-                                                      const uint32_t* block_sums, uint32_t* __restrict__ keys,
-                                                      uint32_t* __restrict__ vals) {
+                                                      const uint32_t* block_sums, const uint4* __restrict__ rng,
+                                                      uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
     if (bd->overflow | bd->error) return;
     const uint2 ch = tchunk[blockIdx.x];
     const uint32_t end = sc[ch.x].tri_off + sc[ch.x].ntri;
@@ -167,10 +169,14 @@ __global__ __launch_bounds__(kBT) void kb_write_pairs(const float4* __restrict__
     uint32_t n = 0;
     CRange r;
     if (t < end) {
-        f3 p[3], lo, hi;
-        tri_fetch(tris, t, p);
-        tri_bbox(p, &lo, &hi);
-        n = cell_range(lo, hi, g.bmin, g.rcp, g.res, &r);
+        if (ranges_fit(g.res)) {
+            n = unpack_range(__ldg(rng + t), &r);   // the range kb_count_pairs found
+        } else {
+            f3 p[3], lo, hi;
+            tri_fetch(tris, t, p);
+            tri_bbox(p, &lo, &hi);
+            n = cell_range(lo, hi, g.bmin, g.rcp, g.res, &r);
+        }
     }
     const uint32_t base = __ldg(cell_off + ch.x);
     const uint32_t rx = (uint32_t)g.res[0], rxy = (uint32_t)g.res[0] * (uint32_t)g.res[1];
@@ -227,7 +233,7 @@ __global__ __launch_bounds__(kBT) void kb_leaf_count_pairs(const uint32_t* __res
                                                            const GridDesc* __restrict__ descs,
                                                            const uint32_t* __restrict__ cell_off, uint32_t nsc,
                                                            const GridDesc* bd, const uint2* __restrict__ top_cells,
-                                                           uint32_t* block_sums) {
+                                                           uint32_t* block_sums, uint4* __restrict__ refrng) {
     if (bd->overflow | bd->error) {
         if (threadIdx.x == 0) block_sums[blockIdx.x] = 0u;
         return;
@@ -238,31 +244,36 @@ __global__ __launch_bounds__(kBT) void kb_leaf_count_pairs(const uint32_t* __res
         uint32_t cell, tri, lres[3];
         CRange r;
         n = bref_leaf_range(descs, cell_off, nsc, top_keys, top_refs, tris, top_cells, i, &cell, &tri, lres, &r);
+        refrng[i] = pack_ref(r, lres, top_cells[cell].x, tri);
     }
     uint32_t tot;
     block_excl_scan<uint32_t, kBT>(n, &tot);
     if (threadIdx.x == 0) block_sums[blockIdx.x] = tot;
 }
 
-// a11: key = first (global) leaf of the top cell + local sub-cell index
-__global__ __launch_bounds__(kBT) void kb_leaf_write_pairs(const uint32_t* __restrict__ top_keys,
-                                                           const uint32_t* __restrict__ top_refs,
-                                                           const float4* __restrict__ tris,
-                                                           const GridDesc* __restrict__ descs,
-                                                           const uint32_t* __restrict__ cell_off, uint32_t nsc,
-                                                           const GridDesc* bd, const uint2* __restrict__ top_cells,
+// a11: key = first (global) leaf of the top cell + local sub-cell index, from the packed
+// sub-cell range kb_leaf_count_pairs kept for every reference
+__global__ __launch_bounds__(kBT) void kb_leaf_write_pairs(const uint4* __restrict__ refrng, const GridDesc* bd,
                                                            const uint32_t* block_sums, uint32_t* __restrict__ keys,
                                                            uint32_t* __restrict__ vals) {
     if (bd->overflow | bd->error) return;
     const uint32_t i = blockIdx.x * kBT + threadIdx.x;
-    uint32_t n = 0, cell = 0, tri = 0, lres[3] = {1u, 1u, 1u};
-    CRange r;
-    if (i < bd->ntop_pairs)
-        n = bref_leaf_range(descs, cell_off, nsc, top_keys, top_refs, tris, top_cells, i, &cell, &tri, lres, &r);
+    uint32_t n = 0;
     PairRun run;
-    if (n) run = {top_cells[cell].x + (uint32_t)r.lo[0] + (uint32_t)r.lo[1] * lres[0] +
-                      (uint32_t)r.lo[2] * lres[0] * lres[1],
-                  (uint32_t)(r.hi[0] - r.lo[0]), (uint32_t)(r.hi[1] - r.lo[1]), lres[0], lres[0] * lres[1], tri};
+    if (i < bd->ntop_pairs) {
+        const uint4 q = __ldg(refrng + i);
+        int32_t lo[3], e[3];
+        n = 1;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            lo[k] = (int32_t)((q.x >> (8 * k)) & 0xFFu);
+            e[k] = (int32_t)((q.y >> (8 * k)) & 0xFFu) - lo[k];
+            n *= (uint32_t)(e[k] > 0 ? e[k] : 0);
+        }
+        const uint32_t l0 = q.x >> 24, l1 = q.y >> 24;
+        if (n) run = {q.z + (uint32_t)lo[0] + (uint32_t)lo[1] * l0 + (uint32_t)lo[2] * l0 * l1, (uint32_t)e[0],
+                      (uint32_t)e[1], l0, l0 * l1, q.w};
+    }
     block_write_runs<kBT>(n, run, block_sums[blockIdx.x], keys, vals);
 }
 
@@ -334,6 +345,8 @@ int batch_alloc(hr_batch* b) {
     if ((rc = ensure(c, B.keys_b, sizeof(uint32_t) * cap_pairs))) return rc;
     if ((rc = ensure(c, B.vals_b, sizeof(uint32_t) * cap_pairs))) return rc;
     if ((rc = ensure(c, B.top_refs, sizeof(uint32_t) * cap_pairs))) return rc;
+    if ((rc = ensure(c, B.ref_ranges, sizeof(uint4) * cap_pairs))) return rc;
+    if ((rc = ensure(c, B.tri_ranges, sizeof(uint4) * std::max<size_t>(b->ntri, 1)))) return rc;
     if ((rc = ensure(c, B.block_sums, sizeof(uint32_t) * (std::max((size_t)b->ntchunk, nref_blocks) + 1)))) return rc;
     if ((rc = ensure(c, B.tile_hist, sizeof(uint32_t) * hist))) return rc;
     if ((rc = ensure(c, B.row_total, sizeof(uint32_t) * kRadixRowWords))) return rc;
@@ -367,12 +380,13 @@ int enqueue_build(hr_batch* b) {
     kb_init<<<(b->nsc + 255) / 256, 256, 0, s>>>(sc, b->nsc, descs, bd, b->ntri, dev<uint32_t>(b->d_bad));
     kb_bounds<<<b->nvchunk, kBT, 0, s>>>(c->verts.as<float4>(), dev<uint2>(b->d_vchunk), sc, descs);
     kb_setup<<<1, 1024, 0, s>>>(sc, b->nsc, descs, cell_off, bd, (uint32_t)std::min(B.cap_cells, (size_t)0xffffffffu));
-    kb_count_pairs<<<b->ntchunk, kBT, 0, s>>>(c->verts.as<float4>(), c->idx.as<uint32_t>(), tch, sc, descs, bd, bsum, tris);
+    kb_count_pairs<<<b->ntchunk, kBT, 0, s>>>(c->verts.as<float4>(), c->idx.as<uint32_t>(), tch, sc, descs, bd, bsum, tris,
+                                              B.tri_ranges.as<uint4>());
     if ((rc = scan_block_sums(c, bsum, b->ntchunk, &bd->ntop_pairs, &bd->overflow,
                               (uint32_t)std::min(cap_pairs, (size_t)0xffffffffu), kOvfTopPairs, &bd->req_pairs, s)))
         return rc;
-    kb_write_pairs<<<b->ntchunk, kBT, 0, s>>>(tris, tch, sc, descs, cell_off, bd, bsum, B.keys_a.as<uint32_t>(),
-                                              B.vals_a.as<uint32_t>());
+    kb_write_pairs<<<b->ntchunk, kBT, 0, s>>>(tris, tch, sc, descs, cell_off, bd, bsum, B.tri_ranges.as<uint4>(),
+                                              B.keys_a.as<uint32_t>(), B.vals_a.as<uint32_t>());
     const int passes = radix_sort_passes(key_bits);
     uint32_t* sorted_keys = (passes % 2 == 1) ? B.keys_b.as<uint32_t>() : B.keys_a.as<uint32_t>();
     if ((rc = radix_sort_pairs(c, B.keys_a.as<uint32_t>(), B.vals_a.as<uint32_t>(), B.keys_b.as<uint32_t>(),
@@ -392,13 +406,12 @@ int enqueue_build(hr_batch* b) {
     k_check_leaves<<<1, 1, 0, s>>>(bd, (uint32_t)std::min(B.cap_leaves, (size_t)0xffffffffu));
     k_tl_cell_begin<<<gcells, 256, 0, s>>>(B.leaf_cnt.as<uint32_t>(), bd, B.cells.as<uint2>());
     kb_leaf_count_pairs<<<nref_blocks, kBT, 0, s>>>(sorted_keys, B.top_refs.as<uint32_t>(), tris, descs, cell_off,
-                                                    b->nsc, bd, B.cells.as<uint2>(), bsum);
+                                                    b->nsc, bd, B.cells.as<uint2>(), bsum, B.ref_ranges.as<uint4>());
     if ((rc = scan_block_sums(c, bsum, nref_blocks, &bd->npairs, &bd->overflow,
                               (uint32_t)std::min(B.cap_leaf_pairs, (size_t)0xffffffffu), kOvfLeafPairs,
                               &bd->req_leaf_pairs, s)))
         return rc;
-    kb_leaf_write_pairs<<<nref_blocks, kBT, 0, s>>>(sorted_keys, B.top_refs.as<uint32_t>(), tris, descs, cell_off,
-                                                    b->nsc, bd, B.cells.as<uint2>(), bsum, B.lkeys_a.as<uint32_t>(),
+    kb_leaf_write_pairs<<<nref_blocks, kBT, 0, s>>>(B.ref_ranges.as<uint4>(), bd, bsum, B.lkeys_a.as<uint32_t>(),
                                                     B.lvals_a.as<uint32_t>());
     const int lpasses = radix_sort_passes(leaf_bits);
     uint32_t* leaf_keys = (lpasses % 2 == 1) ? B.lkeys_b.as<uint32_t>() : B.lkeys_a.as<uint32_t>();

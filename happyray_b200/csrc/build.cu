@@ -77,27 +77,6 @@ __global__ void k_grid_setup(GridDesc* d, float density, uint32_t cap_cells) {
 // a3: pair count, one triangle per thread; block sums for the scan (UniformGridBuildKernels.h:40-105).
 // Also writes the per-triangle vertex array (3 float4) that the later build passes and the
 // traversal read instead of gathering through the index buffer.
-// Cell ranges of up to 16-bit coordinates are kept per triangle (x: lo | hi << 16 per axis
-// in .x .y .z, pair count in .w) so that the scatter pass reads 16 bytes per triangle
-// instead of its 48-byte vertex record; a grid with an axis of more than 65,535 cells
-// keeps recomputing them from the vertices.
-__device__ __forceinline__ bool ranges_fit(const int32_t* res) {
-    return res[0] <= 65535 && res[1] <= 65535 && res[2] <= 65535;
-}
-__device__ __forceinline__ uint4 pack_range(const CRange& r, uint32_t n) {
-    uint32_t w[3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k)
-        w[k] = (uint32_t)min(max(r.lo[k], 0), 65535) | ((uint32_t)min(max(r.hi[k], 0), 65535) << 16);
-    return make_uint4(w[0], w[1], w[2], n);
-}
-__device__ __forceinline__ uint32_t unpack_range(uint4 q, CRange* r) {
-    r->lo[0] = (int32_t)(q.x & 0xFFFFu); r->hi[0] = (int32_t)(q.x >> 16);
-    r->lo[1] = (int32_t)(q.y & 0xFFFFu); r->hi[1] = (int32_t)(q.y >> 16);
-    r->lo[2] = (int32_t)(q.z & 0xFFFFu); r->hi[2] = (int32_t)(q.z >> 16);
-    return q.w;
-}
-
 __global__ __launch_bounds__(kBT) void k_count_pairs(const float4* __restrict__ v, const uint32_t* __restrict__ idx,
                                                      uint32_t ntri, const GridDesc* d, uint32_t* block_sums,
                                                      float4* __restrict__ tris, uint4* __restrict__ rng) {
@@ -216,20 +195,6 @@ __device__ __forceinline__ uint32_t ref_leaf_range(const DescRegs& g, const uint
 
 // a10: leaf pair count per top-level reference, block sums (countLeafLevelPairs,
 // TLGridBuildKernels.h:304-409)
-// Per top-level reference the count pass keeps what the scatter pass needs, 16 bytes:
-// .x = lo.x | lo.y << 8 | lo.z << 16 | lres.x << 24, .y = hi.x | hi.y << 8 | hi.z << 16 |
-// lres.y << 24 (sub-grid coordinates and resolutions are below 256), .z = the top cell's
-// first leaf, .w = the triangle.
-__device__ __forceinline__ uint4 pack_ref(const CRange& r, const uint32_t* lres, uint32_t base, uint32_t tri) {
-    uint32_t a = 0, b = 0;
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        a |= (uint32_t)min(max(r.lo[k], 0), 255) << (8 * k);
-        b |= (uint32_t)min(max(r.hi[k], 0), 255) << (8 * k);
-    }
-    return make_uint4(a | (lres[0] << 24), b | (lres[1] << 24), base, tri);
-}
-
 __global__ __launch_bounds__(kBT) void k_leaf_count_pairs(const uint32_t* __restrict__ top_keys,
                                                           const uint32_t* __restrict__ top_refs,
                                                           const float4* __restrict__ tris,

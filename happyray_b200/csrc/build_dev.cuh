@@ -177,6 +177,41 @@ __device__ __forceinline__ uint32_t leaf_range(const DescRegs& g, const uint32_t
     return cell_range(lo, hi, org, srcp, ires, r);
 }
 
+// The count passes keep each triangle's cell range, 16-bit coordinates (lo | hi << 16 per
+// axis in .x .y .z, pair count in .w), so that the scatter pass reads 16 bytes per
+// triangle instead of its 48-byte vertex record; a grid with an axis of more than 65,535
+// cells keeps recomputing them from the vertices.
+__device__ __forceinline__ bool ranges_fit(const int32_t* res) {
+    return res[0] <= 65535 && res[1] <= 65535 && res[2] <= 65535;
+}
+__device__ __forceinline__ uint4 pack_range(const CRange& r, uint32_t n) {
+    uint32_t w[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+        w[k] = (uint32_t)min(max(r.lo[k], 0), 65535) | ((uint32_t)min(max(r.hi[k], 0), 65535) << 16);
+    return make_uint4(w[0], w[1], w[2], n);
+}
+__device__ __forceinline__ uint32_t unpack_range(uint4 q, CRange* r) {
+    r->lo[0] = (int32_t)(q.x & 0xFFFFu); r->hi[0] = (int32_t)(q.x >> 16);
+    r->lo[1] = (int32_t)(q.y & 0xFFFFu); r->hi[1] = (int32_t)(q.y >> 16);
+    r->lo[2] = (int32_t)(q.z & 0xFFFFu); r->hi[2] = (int32_t)(q.z >> 16);
+    return q.w;
+}
+
+// Per top-level reference the leaf count pass keeps what the leaf scatter pass needs, 16 bytes:
+// .x = lo.x | lo.y << 8 | lo.z << 16 | lres.x << 24, .y = hi.x | hi.y << 8 | hi.z << 16 |
+// lres.y << 24 (sub-grid coordinates and resolutions are below 256), .z = the top cell's
+// first leaf, .w = the triangle.
+__device__ __forceinline__ uint4 pack_ref(const CRange& r, const uint32_t* lres, uint32_t base, uint32_t tri) {
+    uint32_t a = 0, b = 0;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        a |= (uint32_t)min(max(r.lo[k], 0), 255) << (8 * k);
+        b |= (uint32_t)min(max(r.hi[k], 0), 255) << (8 * k);
+    }
+    return make_uint4(a | (lres[0] << 24), b | (lres[1] << 24), base, tri);
+}
+
 __global__ void k_check_leaves(GridDesc* d, uint32_t cap_leaves) {
     if (d->overflow | d->error) return;   // the leaf total is meaningless after an earlier overflow
     if (d->nleaves > cap_leaves) d->overflow |= kOvfLeaves;
