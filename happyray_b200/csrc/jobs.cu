@@ -20,8 +20,11 @@ constexpr int kJobTT = 256;   // largest block of the persistent kernel
 #ifndef HR_JOB_MIN_BLOCKS
 #define HR_JOB_MIN_BLOCKS 3    // blocks of kJobTT per SM the register budget must allow (3: 80 registers)
 #endif
+#ifndef HR_JOB_PT_SMEM_STATE
+#define HR_JOB_PT_SMEM_STATE 1   // path-tracing instance: path state in shared memory
+#endif
 #ifndef HR_JOB_PT_MIN_BLOCKS
-#define HR_JOB_PT_MIN_BLOCKS HR_JOB_MIN_BLOCKS   // the same for the path-tracing instance
+#define HR_JOB_PT_MIN_BLOCKS 4   // the same for the path-tracing instance (4: 64 registers)
 #endif
 
 // position of the q-th (0-based) set bit of m; m has more than q set bits
@@ -127,7 +130,17 @@ __global__ __launch_bounds__(kJobTT, PT ? HR_JOB_PT_MIN_BLOCKS : HR_JOB_MIN_BLOC
         constexpr uint32_t kNone = 0xffffffffu;
         uint32_t cur_j = kNone, tile_local = 0, next = 32u, pend = kNone;
         bool more = true;
+#if HR_JOB_PT_SMEM_STATE
+        // the path state lives in shared memory, so the traversal has the registers to itself
+        __shared__ __align__(16) unsigned char s_lanes[sizeof(PathLane) * kJobTT];
+        PathLane& ln = reinterpret_cast<PathLane*>(s_lanes)[threadIdx.x];
+        ln.pix = 0;
+        ln.sample = 0;
+        ln.val = 0.0f;
+        ln.has = false;
+#else
         PathLane ln;
+#endif
         PtCounts n;
         while (true) {
             while (more) {

@@ -235,8 +235,11 @@ __global__ void k_ao_finish(const uint32_t* __restrict__ queue, const uint32_t* 
     }
 }
 
+#ifndef HR_PT_SMEM_STATE
+#define HR_PT_SMEM_STATE 1   // path state in shared memory (registers left to the traversal)
+#endif
 #ifndef HR_PT_MIN_BLOCKS
-#define HR_PT_MIN_BLOCKS 6   // blocks of kTT per SM the path tracer's register budget must allow (6: 80 registers)
+#define HR_PT_MIN_BLOCKS 7   // blocks of kTT per SM the path tracer's register budget must allow (7: 72 registers)
 #endif
 
 // mode 1/2: path tracing with next-event estimation (PathTracer.h:41-372 structure), one
@@ -253,7 +256,17 @@ __global__ __launch_bounds__(kTT, HR_PT_MIN_BLOCKS) void k_render_pt(Scene s, Ca
     const PtConsts k = pt_consts(g, l, bounces, albedo, eps_frac);
     const uint32_t ntiles = tile_slots(cam) >> 5;
     const uint32_t lane = threadIdx.x & 31u;
+#if HR_PT_SMEM_STATE
+    // the path state lives in shared memory, so the traversal has the registers to itself
+    __shared__ __align__(16) unsigned char s_lanes[sizeof(PathLane) * kTT];
+    PathLane& ln = reinterpret_cast<PathLane*>(s_lanes)[threadIdx.x];
+    ln.pix = 0;
+    ln.sample = 0;
+    ln.val = 0.0f;
+    ln.has = false;
+#else
     PathLane ln;
+#endif
     PtCounts n;
     uint32_t tile = 0, next = 32u;
     bool more = true;
