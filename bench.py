@@ -899,7 +899,8 @@ def main():
             dist.destroy_process_group()
         return
     peak, peak_kind = peaks()
-    names = {0: ["k_render_primary"], 1: ["k_render_pt"], 3: ["k_ao_primary", "k_ao_samples", "k_ao_finish"]}[W["mode"]]
+    ao_samples = "k_ao_samples_tl" if W["kind"] == 1 else "k_ao_samples"   # the two-level instance refills lanes
+    names = {0: ["k_render_primary"], 1: ["k_render_pt"], 3: ["k_ao_primary", ao_samples, "k_ao_finish"]}[W["mode"]]
     kbytes = {0: [b_primary + b_secondary], 1: [b_primary + b_secondary], 3: [b_primary, b_secondary, 0]}[W["mode"]]
     kmed = [statistics.median(k[j] for k in kern_ms) for j in range(len(names))] if kern_ms and kern_ms[0] else [0.0]
     top = max(range(len(kmed)), key=lambda j: kmed[j])

@@ -222,6 +222,86 @@ __global__ __launch_bounds__(kTT, HR_TRACE_MIN_BLOCKS) void k_ao_samples(Scene s
     }
 }
 
+// AO samples on a two-level grid with lanes refilled inside the traversal loop: a lane
+// whose ray is done (occluded, or out of the grid or past the radius) retires it and takes
+// the next (hit pixel, sample) item from the pool at once, so a warp keeps 32 rays in
+// flight until the pool runs dry instead of waiting for its longest ray.  Per ray the
+// generation, traversal and result are those of k_ao_samples.
+template <bool STATS>
+__global__ __launch_bounds__(kTT, HR_TRACE_MIN_BLOCKS) void k_ao_samples_tl(Scene s, Cam cam, int32_t spp, float alpha_frac,
+                                                              float alpha_abs, uint64_t seed, int32_t image_id,
+                                                              const float* __restrict__ hit_t,
+                                                              const uint32_t* __restrict__ hit_tri,
+                                                              const uint32_t* __restrict__ queue, const uint32_t* qcount,
+                                                              uint32_t* __restrict__ unocc, unsigned long long* counter,
+                                                              uint32_t* work) {
+    const G g = load_g(s.desc);
+    gate_scene(s);
+    float alpha = alpha_abs;
+    if (!(alpha > 0.0f)) {
+        const f3 dd = mk(g.bmax[0] - g.bmin[0], g.bmax[1] - g.bmin[1], g.bmax[2] - g.bmin[2]);
+        alpha = alpha_frac * sqrtf(dot(dd, dd));
+    }
+    const float off = 0.01f * alpha;
+    const f3 cpos = mk(cam.pos[0], cam.pos[1], cam.pos[2]);
+    const uint32_t nitems = *qcount * (uint32_t)spp;
+    const uint32_t lane = threadIdx.x & 31u, lt = (1u << lane) - 1u;
+    TL q;
+    Hit h;
+    h.t = alpha; h.u = 0.0f; h.v = 0.0f; h.tri = 0; h.hit = false; h.cells = 0; h.tests = 0;
+    f3 o = mk(0.0f, 0.0f, 0.0f), w = mk(1.0f, 0.0f, 0.0f);
+    uint32_t pix = 0xffffffffu, nrays = 0, ncells = 0, ntests = 0;
+    bool has = false, active = false, dry = s.ntri == 0u;
+    while (true) {
+        const uint32_t need = __ballot_sync(kFullMask, !has);
+        if (need && !dry) {   // warp-uniform
+            const int leader = __ffs(need) - 1;
+            uint32_t base = 0;
+            if ((int)lane == leader) base = atomicAdd(work, (uint32_t)__popc(need));
+            base = __shfl_sync(kFullMask, base, leader);
+            if (base + (uint32_t)__popc(need) >= nitems) dry = true;
+            const uint32_t item = base + __popc(need & lt);
+            if (!has && item < nitems) {
+                has = true;
+                const uint32_t qi = item / (uint32_t)spp, k = item % (uint32_t)spp;
+                pix = queue[qi];
+                const f3 d = primary_dir(cam, pix);
+                const float t = hit_t[pix];
+                const f3 p = mk(cpos.x + t * d.x, cpos.y + t * d.y, cpos.z + t * d.z);
+                const f3 nrm = face_normal(s, hit_tri[pix], d);
+                Pcg32 rng;
+                pcg_seed(rng, ((uint64_t)(uint32_t)image_id << 32) | pix, seed);
+                for (uint32_t j = 0; j < 2u * k; ++j) pcg_next(rng);
+                const float u1 = pcg_float(rng), u2 = pcg_float(rng);
+                w = cosine_dir(nrm, u1, u2);
+                o = mk(p.x + off * w.x, p.y + off * w.y, p.z + off * w.z);
+                h.t = alpha; h.hit = false; h.cells = 0; h.tests = 0;
+                active = tl_setup<STATS>(q, s, g, o, w, h);
+            }
+        }
+        if (!__any_sync(kFullMask, has)) break;   // the pool is dry and no ray is in flight
+        uint32_t b = 0, e = 0;
+        if (active) {
+            const uint2 lr = __ldg(s.leaves + tl_leaf(q));
+            b = lr.x; e = lr.y;
+            if (STATS) h.cells++;
+        }
+        const bool done = test_lists<kHitAny, STATS>(s, o, w, b, e, true, h);
+        if (active) active = !done && tl_advance<STATS>(q, s, g, o, w, h);
+        const bool fin = has && !active;
+        const uint32_t peers = __match_any_sync(kFullMask, fin ? pix : 0xffffffffu);
+        const uint32_t nfree = __popc(__ballot_sync(kFullMask, fin && !h.hit) & peers);
+        if (fin && nfree && (int)lane == __ffs(peers) - 1) atomicAdd(unocc + pix, nfree);
+        if (fin) {
+            nrays += 1;
+            ncells += h.cells;
+            ntests += h.tests;
+            has = false;
+        }
+    }
+    add_rays<STATS>(counter, true, nrays, ncells, ntests);
+}
+
 __global__ void k_ao_finish(const uint32_t* __restrict__ queue, const uint32_t* qcount, const uint32_t* __restrict__ unocc,
                             int32_t spp, int32_t image_id, float* __restrict__ fb) {
     const uint32_t n = *qcount;
@@ -235,6 +315,9 @@ __global__ void k_ao_finish(const uint32_t* __restrict__ queue, const uint32_t* 
     }
 }
 
+#ifndef HR_AO_REFILL
+#define HR_AO_REFILL 1   // two-level AO samples by k_ao_samples_tl (lanes refilled in the traversal loop)
+#endif
 #ifndef HR_PT_SMEM_STATE
 #define HR_PT_SMEM_STATE 1   // path state in shared memory (registers left to the traversal)
 #endif
@@ -422,8 +505,8 @@ int launch_render(hr_ctx* c, int32_t mode, int32_t image_id, float* d_fb) {
         if ((rc = ensure(c, c->hit_t, sizeof(float) * n)) || (rc = ensure(c, c->hit_tri, sizeof(uint32_t) * n)) ||
             (rc = ensure(c, c->unocc, sizeof(uint32_t) * n)) || (rc = ensure(c, c->queue, sizeof(uint32_t) * n)))
             return rc;
-        uint32_t* qcount = reinterpret_cast<uint32_t*>(ctr + 7);
-        if ((rc = cuda_check(c, cudaMemsetAsync(qcount, 0, sizeof(uint32_t), strm), "queue reset"))) return rc;
+        uint32_t* qcount = reinterpret_cast<uint32_t*>(ctr + 7);   // and the sample pool counter after it
+        if ((rc = cuda_check(c, cudaMemsetAsync(qcount, 0, 2 * sizeof(uint32_t), strm), "queue reset"))) return rc;
         const int spp = c->ip.ao_samples;
         c->launches += 3;
         mark(0);
@@ -435,10 +518,23 @@ int launch_render(hr_ctx* c, int32_t mode, int32_t image_id, float* d_fb) {
         mark(1);
         const int gs = c->num_sms * 16;
         by_kind(s.kind, st, [&](auto K, auto S) {
-            k_ao_samples<K(), S()><<<gs, kTT, 0, strm>>>(s, k, spp, c->ip.ao_radius_frac, c->ip.ao_radius_abs,
-                                                         c->ip.seed, image_id, c->hit_t.as<float>(),
-                                                         c->hit_tri.as<uint32_t>(), c->queue.as<uint32_t>(), qcount,
-                                                         c->unocc.as<uint32_t>(), ctr);
+            if (HR_AO_REFILL && K() == kTwoLevel) {
+                int nb = 0;
+                if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_ao_samples_tl<S()>, kTT, 0) != cudaSuccess ||
+                    nb < 1) {
+                    cudaGetLastError();
+                    nb = 1;
+                }
+                k_ao_samples_tl<S()><<<nb * c->num_sms, kTT, 0, strm>>>(
+                    s, k, spp, c->ip.ao_radius_frac, c->ip.ao_radius_abs, c->ip.seed, image_id, c->hit_t.as<float>(),
+                    c->hit_tri.as<uint32_t>(), c->queue.as<uint32_t>(), qcount, c->unocc.as<uint32_t>(), ctr,
+                    qcount + 1);
+            } else {
+                k_ao_samples<K(), S()><<<gs, kTT, 0, strm>>>(s, k, spp, c->ip.ao_radius_frac, c->ip.ao_radius_abs,
+                                                             c->ip.seed, image_id, c->hit_t.as<float>(),
+                                                             c->hit_tri.as<uint32_t>(), c->queue.as<uint32_t>(), qcount,
+                                                             c->unocc.as<uint32_t>(), ctr);
+            }
         });
         mark(2);
         k_ao_finish<<<c->num_sms * 4, 256, 0, strm>>>(c->queue.as<uint32_t>(), qcount, c->unocc.as<uint32_t>(), spp,

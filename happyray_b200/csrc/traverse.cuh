@@ -315,30 +315,35 @@ __device__ __forceinline__ bool tl_advance(TL& q, const Scene& s, const G& g, f3
     return tl_outer_step(q, g, h) && tl_seek<STATS>(q, s, g, o, d, h);
 }
 
+// Entry of a ray into the two-level grid (TLGridTraverser.h:79-143): clip to the grid
+// box, the top cell at the entry point, then the first non-empty top cell entered; false
+// if the ray misses the grid or leaves it (or is done) before a non-empty cell.  Per lane.
+template <bool STATS>
+__device__ __forceinline__ bool tl_setup(TL& q, const Scene& s, const G& g, f3 o, f3 d, Hit& h) {
+    q.rcp[0] = 1.0f / d.x; q.rcp[1] = 1.0f / d.y; q.rcp[2] = 1.0f / d.z;
+    float t0, t1;
+    if (!clip(g, o, q.rcp, &t0, &t1)) return false;
+    q.tentry = hmax(0.0f, t0);
+    const f3 ep = mk(o.x + q.tentry * d.x, o.y + q.tentry * d.y, o.z + q.tentry * d.z);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        float cf = floorf((comp(ep, k) - g.bmin[k]) * g.rcp[k]);
+        cf = hmin((float)g.res[k] - 1.0f, hmax(cf, 0.0f));
+        const float stp = q.rcp[k] > 0.0f ? 1.0f : 0.0f;
+        q.tmax[k] = ((cf + stp) * g.cs[k] + g.bmin[k] - comp(o, k)) * q.rcp[k];
+        q.cell[k] = f2i(cf);
+    }
+    if (!(q.cell[0] < g.res[0] && q.cell[0] > -1 && q.cell[1] < g.res[1] && q.cell[1] > -1 &&
+          q.cell[2] < g.res[2] && q.cell[2] > -1))
+        return false;
+    return tl_seek<STATS>(q, s, g, o, d, h);
+}
+
 // a15: two-level DDA, warp-synchronous
 template <int HM, bool STATS>
 __device__ void trace_tl(const Scene& s, const G& g, f3 o, f3 d, bool any, Hit& h, bool active) {
     TL q;
-    if (active) {
-        q.rcp[0] = 1.0f / d.x; q.rcp[1] = 1.0f / d.y; q.rcp[2] = 1.0f / d.z;
-        float t0, t1;
-        active = clip(g, o, q.rcp, &t0, &t1);
-        if (active) {
-            q.tentry = hmax(0.0f, t0);
-            const f3 ep = mk(o.x + q.tentry * d.x, o.y + q.tentry * d.y, o.z + q.tentry * d.z);
-#pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                float cf = floorf((comp(ep, k) - g.bmin[k]) * g.rcp[k]);
-                cf = hmin((float)g.res[k] - 1.0f, hmax(cf, 0.0f));
-                const float stp = q.rcp[k] > 0.0f ? 1.0f : 0.0f;
-                q.tmax[k] = ((cf + stp) * g.cs[k] + g.bmin[k] - comp(o, k)) * q.rcp[k];
-                q.cell[k] = f2i(cf);
-            }
-            active = q.cell[0] < g.res[0] && q.cell[0] > -1 && q.cell[1] < g.res[1] && q.cell[1] > -1 &&
-                     q.cell[2] < g.res[2] && q.cell[2] > -1;
-            if (active) active = tl_seek<STATS>(q, s, g, o, d, h);
-        }
-    }
+    if (active) active = tl_setup<STATS>(q, s, g, o, d, h);
     while (__any_sync(kFullMask, active)) {
         uint32_t b = 0, e = 0;
         if (active) {
