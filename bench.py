@@ -47,6 +47,18 @@ def peaks():
     return 6650.0, "fallback"
 
 
+def l2_read_gbs(stream=None):
+    """L2-resident read rate measured on this device by the library's probe
+    (hr_probe_l2_read: one kernel reads a 32 MiB buffer 50 times through L2).  The
+    traversal kernels' working sets live mostly in L2, so their algorithmic bytes are also
+    reported against this rate."""
+    import ctypes as C
+    from happyray_b200 import _lib
+    out = C.c_double(0.0)
+    st = _lib.load().hr_probe_l2_read(C.c_void_p(stream.cuda_stream if stream is not None else 0), C.byref(out))
+    return out.value if st == 0 else None
+
+
 def workload(name: str):
     from happyray_b200 import scenes as S
     if name == "c1":
@@ -899,6 +911,7 @@ def main():
             dist.destroy_process_group()
         return
     peak, peak_kind = peaks()
+    l2_peak = l2_read_gbs(stream)
     ao_samples = "k_ao_samples_tl" if W["kind"] == 1 else "k_ao_samples"   # the two-level instance refills lanes
     names = {0: ["k_render_primary"], 1: ["k_render_pt"], 3: ["k_ao_primary", ao_samples, "k_ao_finish"]}[W["mode"]]
     kbytes = {0: [b_primary + b_secondary], 1: [b_primary + b_secondary], 3: [b_primary, b_secondary, 0]}[W["mode"]]
@@ -929,7 +942,9 @@ def main():
         "roofline": {"bound": "hbm", "kernel": kern, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
                      "algorithmic_bytes_per_launch": b_trace, "kernel_ms": kmed[top],
-                     "render_kernels_ms": dict(zip(names, kmed))},
+                     "render_kernels_ms": dict(zip(names, kmed)),
+                     "l2": {"peak": l2_peak, "unit": "GB/s", "frac": achieved / l2_peak if l2_peak else None,
+                            "how": "L2-resident read rate of this device, measured in this run (hr_probe_l2_read)"}},
         "build_roofline": {"bound": "hbm", "achieved": b_build / (bmed * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
                            "frac": b_build / (bmed * 1e-3) / 1e9 / peak, "algorithmic_bytes": b_build},
         "gpu_launches": launches,

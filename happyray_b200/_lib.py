@@ -68,6 +68,7 @@ SIGNATURES = {
     "hr_exclusive_scan_device": (C.c_int, [P, P, C.c_uint32]),
     "hr_radix_sort_pairs_device": (C.c_int, [P, P, P, C.c_uint32, C.c_int32]),
     "hr_radix_sort_pairs_noalloc": (C.c_int, [P, P, P, C.c_uint32, C.c_int32]),
+    "hr_probe_l2_read": (C.c_int, [P, C.POINTER(C.c_double)]),
     # batched scenes
     "hr_batch_create": (C.c_int, [C.POINTER(P), C.c_int32, P]),
     "hr_batch_destroy": (None, [P]),

@@ -173,6 +173,13 @@ hr_status hr_radix_sort_pairs_device(hr_ctx *ctx, uint32_t *d_keys, uint32_t *d_
 hr_status hr_radix_sort_pairs_noalloc(void *stream, uint32_t *d_keys, uint32_t *d_values,
                                       uint32_t n, int32_t key_bits);
 
+/* Diagnostics: the L2-resident read rate of the current device in GB/s.  One kernel reads
+ * a 32 MiB buffer 50 times through L2 (ld.global.cg, bypassing L1), timed with CUDA
+ * events on `stream` (cudaStream_t, NULL = default stream).  The traversal kernels' working
+ * sets live mostly in L2; benchmarks report their algorithmic bytes against this rate as
+ * well as against the HBM copy rate.  No counterpart in the reference. */
+hr_status hr_probe_l2_read(void *stream, double *gbs);
+
 /* ---------------------------------------------------------------------------------
  * Batched scenes.  No counterpart in the reference, whose RTEngine holds one scene in
  * static globals (RTEngine.cu:91-181); it is the per-scene path above run for many

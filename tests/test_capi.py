@@ -53,3 +53,17 @@ def test_c_header_compiles_standalone(tmp_path):
     src.write_text('#include "happyray.h"\nint main(void){ hr_grid_info i; (void)i; return HR_OK; }\n')
     subprocess.run(["/usr/bin/gcc" if Path("/usr/bin/gcc").exists() else "gcc", "-std=c99", "-Wall", "-Werror",
                     "-I", str(ROOT / "include"), "-c", str(src), "-o", str(tmp_path / "t.o")], check=True)
+
+
+def test_probe_rejects_null_output(hrlib):
+    """The L2 probe checks its output pointer before touching the device."""
+    assert hrlib.hr_probe_l2_read(None, None) == 1   # HR_ERR_INVALID_ARG
+
+
+@pytest.mark.gpu
+def test_probe_l2_read_rate(hrlib):
+    """The L2-resident read rate is a plausible bandwidth (below 500 GB/s the probe is broken)."""
+    import ctypes as C
+    out = C.c_double(0.0)
+    assert hrlib.hr_probe_l2_read(None, C.byref(out)) == 0
+    assert 500.0 < out.value < 100000.0
