@@ -581,7 +581,8 @@ def hier_workload(seed: int = 0, frames: int = 8):
     """Instanced hierarchy workload: 64 objects (icospheres and heightfield tiles, 320-20480
     triangles) x 16,384 rigid instances (scales 0.01-0.05 in [0, 1]^3), 8 rigid-body frames
     (every instance shifted by a seeded offset per frame), 1920x1080 pinhole rays at the
-    instance bounds, object / instance densities 1.2 / 1.2 (RTEngine.cu:72-73)."""
+    instance bounds listed in 8x4 pixel tiles, object / instance densities 1.2 / 1.2
+    (RTEngine.cu:72-73)."""
     from happyray_b200 import scenes as S
     v, f, counts, inst = S.instanced_scene(64, 16384, seed=seed, tri_range=(320, 20480), world=1.0,
                                            scale_range=(0.01, 0.05))
@@ -607,7 +608,10 @@ def hier_workload(seed: int = 0, frames: int = 8):
     xs = ((np.arange(W) + 0.5) / W * 2 - 1) * th * W / H
     ys = (1 - (np.arange(H) + 0.5) / H * 2) * th
     d = fwd[None, None, :] + xs[None, :, None] * right[None, None, :] + ys[:, None, None] * up[None, None, :]
-    d = (d / np.linalg.norm(d, axis=2, keepdims=True)).reshape(-1, 3).astype(np.float32)
+    d = (d / np.linalg.norm(d, axis=2, keepdims=True)).astype(np.float32)
+    # the rays in 8x4 pixel tiles (as the library's camera kernels issue them), so that the
+    # 32 rays of a warp start into a small solid angle
+    d = np.ascontiguousarray(d.reshape(H // 4, 4, W // 8, 8, 3).transpose(0, 2, 1, 3, 4)).reshape(-1, 3)
     org = np.broadcast_to(pos.astype(np.float32), d.shape).copy()
     return dict(name="c6_instanced_hierarchy_64_objects_16384_instances_1080p", v=v, f=f, counts=counts,
                 frames=seq, org=org, dir=d, res=(W, H))

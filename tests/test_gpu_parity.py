@@ -171,10 +171,14 @@ def test_occluded_matches_oracle(engine, oracle, small_clusters):
     assert 0 < want.sum() < n
 
 
-def test_render_ao_bitexact(engine, oracle, small_clusters):
+@pytest.mark.parametrize("kind", [GRID_TWO_LEVEL, GRID_UNIFORM])
+def test_render_ao_bitexact(engine, oracle, small_clusters, kind):
+    """AO images bit-exact against the oracle: on a two-level grid through the kernel that
+    refills lanes inside the traversal loop, on a uniform grid through the one-ray-per-lane
+    kernel."""
     v, f = small_clusters
-    gpu_build(engine, v, f, GRID_TWO_LEVEL)
-    b = oracle_build(oracle, v, f, GRID_TWO_LEVEL)
+    gpu_build(engine, v, f, kind)
+    b = oracle_build(oracle, v, f, kind)
     cam = S.camera_at_bounds(v, (160, 120))
     set_cam(engine, cam)
     alpha = float(np.float32(0.1) * b.diag())
