@@ -916,8 +916,9 @@ def main():
         return
     peak, peak_kind = peaks()
     l2_peak = l2_read_gbs(stream)
-    ao_samples = "k_ao_samples_tl" if W["kind"] == 1 else "k_ao_samples"   # the two-level instance refills lanes
-    names = {0: ["k_render_primary"], 1: ["k_render_pt"], 3: ["k_ao_primary", ao_samples, "k_ao_finish"]}[W["mode"]]
+    tl = W["kind"] == 1   # two-level AO kernels refill lanes inside the traversal loop
+    ao = ["k_ao_primary_tl" if tl else "k_ao_primary", "k_ao_samples_tl" if tl else "k_ao_samples", "k_ao_finish"]
+    names = {0: ["k_render_primary"], 1: ["k_render_pt"], 3: ao}[W["mode"]]
     kbytes = {0: [b_primary + b_secondary], 1: [b_primary + b_secondary], 3: [b_primary, b_secondary, 0]}[W["mode"]]
     kmed = [statistics.median(k[j] for k in kern_ms) for j in range(len(names))] if kern_ms and kern_ms[0] else [0.0]
     top = max(range(len(kmed)), key=lambda j: kmed[j])

@@ -192,8 +192,8 @@ hr_status hr_create(hr_ctx** out, int32_t device, void* stream) {
     }
     for (auto& e : c->ev) cudaEventCreate(&e);
     for (auto& e : c->rev) cudaEventCreate(&e);
-    if (ensure(c, c->counters, 64)) { hr_destroy(c); return HR_ERR_OUT_OF_MEMORY; }
-    cudaMemsetAsync(c->counters.p, 0, 64, c->stream);
+    if (ensure(c, c->counters, 80)) { hr_destroy(c); return HR_ERR_OUT_OF_MEMORY; }   // 8 counter words, 2 pool words
+    cudaMemsetAsync(c->counters.p, 0, 80, c->stream);
     *out = c;
     return HR_OK;
 }

@@ -22,6 +22,12 @@
 
 #include <type_traits>
 
+#ifndef HR_AO_REFILL_MIN
+#define HR_AO_REFILL_MIN 12   // idle lanes that make k_ao_samples_tl refill
+#endif
+#ifndef HR_AO_PRIMARY_REFILL_MIN
+#define HR_AO_PRIMARY_REFILL_MIN 32   // idle lanes that make k_ao_primary_tl refill (> 32: k_ao_primary)
+#endif
 #ifndef HR_TRACE_MIN_BLOCKS
 #define HR_TRACE_MIN_BLOCKS 8   // blocks of kTT per SM the ray kernels' register budget must allow (8: 64 registers)
 #endif
@@ -222,6 +228,88 @@ __global__ __launch_bounds__(kTT, HR_TRACE_MIN_BLOCKS) void k_ao_samples(Scene s
     }
 }
 
+// AO camera rays on a two-level grid with lanes refilled inside the traversal loop: once
+// HR_AO_PRIMARY_REFILL_MIN lanes are done (their pixels shaded or queued as k_ao_primary
+// does), they take that many consecutive pixel slots of the tile order from the pool.
+template <bool STATS>
+__global__ __launch_bounds__(kTT, HR_TRACE_MIN_BLOCKS) void k_ao_primary_tl(Scene s, Cam cam, int32_t image_id,
+                                                              float* __restrict__ fb, float* __restrict__ hit_t,
+                                                              uint32_t* __restrict__ hit_tri, uint32_t* __restrict__ unocc,
+                                                              uint32_t* __restrict__ queue, uint32_t* qcount,
+                                                              unsigned long long* counter, uint32_t* work) {
+    const G g = load_g(s.desc);
+    gate_scene(s);
+    const uint32_t slots = tile_slots(cam);
+    const f3 o = mk(cam.pos[0], cam.pos[1], cam.pos[2]);
+    const uint32_t lane = threadIdx.x & 31u, lt = (1u << lane) - 1u;
+    TL q;
+    Hit h;
+    h.t = FLT_MAX; h.u = 0.0f; h.v = 0.0f; h.tri = 0; h.hit = false; h.cells = 0; h.tests = 0;
+    f3 d = mk(1.0f, 0.0f, 0.0f);
+    uint32_t pix = 0, nrays = 0, ncells = 0, ntests = 0;
+    bool has = false, valid = false, active = false, dry = false;
+    while (true) {
+        const uint32_t need = __ballot_sync(kFullMask, !has);
+        if (need && !dry && (__popc(need) >= HR_AO_PRIMARY_REFILL_MIN || need == kFullMask ||
+                             !__any_sync(kFullMask, active))) {   // warp-uniform
+            const int leader = __ffs(need) - 1;
+            uint32_t base = 0;
+            if ((int)lane == leader) base = atomicAdd(work, (uint32_t)__popc(need));
+            base = __shfl_sync(kFullMask, base, leader);
+            if (base + (uint32_t)__popc(need) >= slots) dry = true;
+            const uint32_t slot = base + __popc(need & lt);
+            if (!has && slot < slots) {
+                has = true;
+                valid = tile_pixel(cam, slot, &pix);
+                h.t = FLT_MAX; h.u = 0.0f; h.v = 0.0f; h.tri = 0; h.hit = false; h.cells = 0; h.tests = 0;
+                active = false;
+                if (valid) {
+                    d = primary_dir(cam, pix);
+                    if (s.ntri != 0u) active = tl_setup<STATS>(q, s, g, o, d, h);
+                }
+            }
+        }
+        if (!__any_sync(kFullMask, has)) break;   // the pool is dry and no ray is in flight
+        uint32_t b = 0, e = 0;
+        if (active) {
+            const uint2 lr = __ldg(s.leaves + tl_leaf(q));
+            b = lr.x; e = lr.y;
+            if (STATS) h.cells++;
+        }
+        const bool done = test_lists<kHitClosest, STATS>(s, o, d, b, e, false, h);
+        if (active) active = !done && tl_advance<STATS>(q, s, g, o, d, h);
+        const bool fin = has && !active;
+        const bool hit = fin && valid && h.hit;
+        if (hit) {
+            hit_t[pix] = h.t;
+            hit_tri[pix] = h.tri;
+            unocc[pix] = 0u;
+        } else if (fin && valid) {
+            const float val = blend(fb[3 * (size_t)pix], 1.0f, image_id);
+            fb[3 * (size_t)pix] = val;
+            fb[3 * (size_t)pix + 1] = val;
+            fb[3 * (size_t)pix + 2] = val;
+        }
+        const uint32_t m = __ballot_sync(kFullMask, hit);
+        if (m) {
+            const int leader = __ffs(m) - 1;
+            uint32_t qb = 0;
+            if ((int)lane == leader) qb = atomicAdd(qcount, (uint32_t)__popc(m));
+            qb = __shfl_sync(kFullMask, qb, leader);
+            if (hit) queue[qb + __popc(m & lt)] = pix;
+        }
+        if (fin) {
+            if (valid) {
+                nrays += 1;
+                ncells += h.cells;
+                ntests += h.tests;
+            }
+            has = false;
+        }
+    }
+    add_rays<STATS>(counter, false, nrays, ncells, ntests);
+}
+
 // AO samples on a two-level grid with lanes refilled inside the traversal loop: a lane
 // whose ray is done (occluded, or out of the grid or past the radius) retires it and takes
 // the next (hit pixel, sample) item from the pool at once, so a warp keeps 32 rays in
@@ -254,7 +342,8 @@ __global__ __launch_bounds__(kTT, HR_TRACE_MIN_BLOCKS) void k_ao_samples_tl(Scen
     bool has = false, active = false, dry = s.ntri == 0u;
     while (true) {
         const uint32_t need = __ballot_sync(kFullMask, !has);
-        if (need && !dry) {   // warp-uniform
+        if (need && !dry && (__popc(need) >= HR_AO_REFILL_MIN || need == kFullMask ||
+                             !__any_sync(kFullMask, active))) {   // warp-uniform
             const int leader = __ffs(need) - 1;
             uint32_t base = 0;
             if ((int)lane == leader) base = atomicAdd(work, (uint32_t)__popc(need));
@@ -505,15 +594,28 @@ int launch_render(hr_ctx* c, int32_t mode, int32_t image_id, float* d_fb) {
         if ((rc = ensure(c, c->hit_t, sizeof(float) * n)) || (rc = ensure(c, c->hit_tri, sizeof(uint32_t) * n)) ||
             (rc = ensure(c, c->unocc, sizeof(uint32_t) * n)) || (rc = ensure(c, c->queue, sizeof(uint32_t) * n)))
             return rc;
-        uint32_t* qcount = reinterpret_cast<uint32_t*>(ctr + 7);   // and the sample pool counter after it
-        if ((rc = cuda_check(c, cudaMemsetAsync(qcount, 0, 2 * sizeof(uint32_t), strm), "queue reset"))) return rc;
+        // word 7: the hit-pixel queue length and the sample pool; word 8: the camera-ray pool
+        uint32_t* qcount = reinterpret_cast<uint32_t*>(ctr + 7);
+        if ((rc = cuda_check(c, cudaMemsetAsync(qcount, 0, 4 * sizeof(uint32_t), strm), "queue reset"))) return rc;
         const int spp = c->ip.ao_samples;
         c->launches += 3;
         mark(0);
         by_kind(s.kind, st, [&](auto K, auto S) {
-            k_ao_primary<K(), S()><<<gb, kTT, 0, strm>>>(s, k, image_id, d_fb, c->hit_t.as<float>(),
-                                                         c->hit_tri.as<uint32_t>(), c->unocc.as<uint32_t>(),
-                                                         c->queue.as<uint32_t>(), qcount, ctr);
+            if (HR_AO_PRIMARY_REFILL_MIN <= 32 && K() == kTwoLevel) {
+                int nb = 0;
+                if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_ao_primary_tl<S()>, kTT, 0) != cudaSuccess ||
+                    nb < 1) {
+                    cudaGetLastError();
+                    nb = 1;
+                }
+                k_ao_primary_tl<S()><<<std::min(gb, nb * c->num_sms), kTT, 0, strm>>>(
+                    s, k, image_id, d_fb, c->hit_t.as<float>(), c->hit_tri.as<uint32_t>(), c->unocc.as<uint32_t>(),
+                    c->queue.as<uint32_t>(), qcount, ctr, qcount + 2);
+            } else {
+                k_ao_primary<K(), S()><<<gb, kTT, 0, strm>>>(s, k, image_id, d_fb, c->hit_t.as<float>(),
+                                                             c->hit_tri.as<uint32_t>(), c->unocc.as<uint32_t>(),
+                                                             c->queue.as<uint32_t>(), qcount, ctr);
+            }
         });
         mark(1);
         const int gs = c->num_sms * 16;

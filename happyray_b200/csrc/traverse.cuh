@@ -432,7 +432,8 @@ __device__ __forceinline__ bool tile_pixel(const Cam& c, uint32_t slot, uint32_t
 
 // Device counters (uint64 words): [0] rays, [2] cells, [3] triangle tests of the primary
 // pass; [4] rays, [5] cells, [6] tests of the secondary pass (AO samples, shadow rays);
-// word 1 holds the index check of the last upload, word 7 the AO hit-pixel queue length.
+// word 1 holds the index check of the last upload, word 7 the AO hit-pixel queue length
+// (or the path tracer's tile pool) and the AO sample pool, word 8 the AO camera-ray pool.
 template <bool STATS>
 __device__ __forceinline__ void add_rays(unsigned long long* counter, bool secondary, uint32_t rays, uint32_t cells = 0,
                                          uint32_t tests = 0) {
