@@ -249,12 +249,20 @@ int launch_wave(hr_server* S, Wave& w, std::map<uint32_t, float>& times) {
             R.pinned_out = is_pinned(R.r.out_rgb);
         }
     }
-    // job table: path-traced requests last, each group with its own tile prefix and counter
+    // job table: path-traced requests last, each group with its own tile prefix and counter.
+    // Within a group the requests with the most samples per pixel (the costliest tiles) come
+    // first, so that the warps that take the last tiles of the pool take short ones.
     Job* hj = S->h_jobs[w.slot];
     uint32_t* ht = S->h_tiles[w.slot];
     uint32_t n_main = 0, n_pt = 0;
+    std::vector<const SrvReq*> order(w.rp.begin(), w.rp.end());
+    std::stable_sort(order.begin(), order.end(), [](const SrvReq* a, const SrvReq* b) {
+        const int32_t sa = a->r.kind == HR_REQUEST_RENDER ? a->r.spp : 1;
+        const int32_t sb = b->r.kind == HR_REQUEST_RENDER ? b->r.spp : 1;
+        return sa > sb;
+    });
     for (int pass = 0; pass < 2; ++pass)
-        for (const SrvReq* rq : w.rp) {
+        for (const SrvReq* rq : order) {
             const SrvReq& R = *rq;
             const bool pt = R.r.kind == HR_REQUEST_RENDER && R.r.mode == HR_RENDER_PATH;
             if (pt != (pass == 1)) continue;
