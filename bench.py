@@ -47,6 +47,17 @@ def peaks():
     return 6650.0, "fallback"
 
 
+def profile_traffic(kernel: str, workload: str):
+    """DRAM bytes per launch of `kernel` on `workload` from its committed ncu summary
+    (profiles/<kernel>__<workload>.md, line 'dram_bytes_per_launch: N'), or None."""
+    prof = ROOT / "profiles" / f"{kernel}__{workload}.md"
+    if prof.exists():
+        for line in prof.read_text().splitlines():
+            if line.startswith("dram_bytes_per_launch:"):
+                return float(line.split(":")[1])
+    return None
+
+
 def l2_read_gbs(stream=None):
     """L2-resident read rate measured on this device by the library's probe
     (hr_probe_l2_read: one kernel reads a 32 MiB buffer 50 times through L2).  The
@@ -755,7 +766,8 @@ def run_hier(args, rank, ws, local):
             ["instance_grid_cells", "instance_boxes_tested", "instances_entered", "object_grid_cells",
              "triangle_tests"])},
         "roofline": {"bound": "hbm", "kernel": "k_hier_trace", "achieved": b_trace / (tmed * 1e-3) / 1e9,
-                     "peak": peak, "unit": "GB/s", "frac": b_trace / (tmed * 1e-3) / 1e9 / peak, "traffic": None,
+                     "peak": peak, "unit": "GB/s", "frac": b_trace / (tmed * 1e-3) / 1e9 / peak,
+                     "traffic": profile_traffic("k_hier_trace", W["name"]),
                      "peak_source": peak_kind, "algorithmic_bytes_per_launch": b_trace, "kernel_ms": tmed},
         "gpu_launches": launches,
         "e2e": e2e,
@@ -926,12 +938,7 @@ def main():
     b_trace = kbytes[top]
     tr_med = statistics.median(trace_ms)
     achieved = b_trace / (kmed[top] * 1e-3) / 1e9 if kmed[top] > 0 else 0.0
-    traffic = None
-    prof = ROOT / "profiles" / f"{kern}__{W['name']}.md"
-    if prof.exists():
-        for line in prof.read_text().splitlines():
-            if line.startswith("dram_bytes_per_launch:"):
-                traffic = float(line.split(":")[1])
+    traffic = profile_traffic(kern, W["name"])
     bmed = statistics.median(build_ms)
     line = {
         "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": ws, "steps": args.steps,
