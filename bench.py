@@ -438,7 +438,8 @@ def run_batched(args, rank, ws, local):
         "speedup_vs_plain": value / plain_value,
         "autotune": dict(tuning, seconds=tune_s) if tuning else None,
         "roofline": {"bound": "hbm", "kernel": "k_trace_jobs", "achieved": b_trace / (rmed * 1e-3) / 1e9,
-                     "peak": peak, "unit": "GB/s", "frac": b_trace / (rmed * 1e-3) / 1e9 / peak, "traffic": None,
+                     "peak": peak, "unit": "GB/s", "frac": b_trace / (rmed * 1e-3) / 1e9 / peak,
+                     "traffic": profile_traffic("k_trace_jobs", W["name"]),
                      "peak_source": peak_kind, "algorithmic_bytes_per_launch": b_trace, "kernel_ms": rmed},
         "build_roofline": {"bound": "hbm", "achieved": b_build / (bmed * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
                            "frac": b_build / (bmed * 1e-3) / 1e9 / peak, "algorithmic_bytes": b_build},
