@@ -27,6 +27,7 @@ import os
 import signal
 import statistics
 import subprocess
+import tempfile
 import sys
 import time
 from pathlib import Path
@@ -112,8 +113,7 @@ class ClockSampler:
         self.path = None
 
     def __enter__(self):
-        out = ROOT / "gpurun_out"
-        out.mkdir(exist_ok=True)
+        out = Path(tempfile.gettempdir())
         self.path = out / f"clocks_gpu{self.index}.csv"
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
