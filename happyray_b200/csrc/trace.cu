@@ -311,10 +311,12 @@ __global__ __launch_bounds__(kTT, HR_TRACE_MIN_BLOCKS) void k_ao_primary_tl(Scen
 }
 
 // AO samples on a two-level grid with lanes refilled inside the traversal loop: a lane
-// whose ray is done (occluded, or out of the grid or past the radius) retires it and takes
-// the next (hit pixel, sample) item from the pool at once, so a warp keeps 32 rays in
-// flight until the pool runs dry instead of waiting for its longest ray.  Per ray the
-// generation, traversal and result are those of k_ao_samples.
+// whose ray is done (occluded, or out of the grid or past the radius) retires it and
+// waits; once HR_AO_REFILL_MIN lanes wait (or no ray is left in flight) they take the next
+// (hit pixel, sample) items from the pool together, so a warp keeps most of its lanes
+// busy until the pool runs dry instead of waiting for its longest ray, and the divergent
+// ray set-up runs for many lanes at once.  Per ray the generation, traversal and result
+// are those of k_ao_samples.
 template <bool STATS>
 __global__ __launch_bounds__(kTT, HR_TRACE_MIN_BLOCKS) void k_ao_samples_tl(Scene s, Cam cam, int32_t spp, float alpha_frac,
                                                               float alpha_abs, uint64_t seed, int32_t image_id,
