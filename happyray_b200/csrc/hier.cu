@@ -27,6 +27,10 @@
 #include <string>
 #include <vector>
 
+#ifndef HR_HIER_WARP_POOL
+#define HR_HIER_WARP_POOL 1   // trace warps take 32 consecutive rays from a pool once all lanes are done
+#endif
+
 namespace hr {
 namespace {
 
@@ -483,9 +487,23 @@ __global__ __launch_bounds__(kTT, 8) void k_hier_trace(HierView H, const float* 
                                                        uint32_t n, int32_t* __restrict__ oinst,
                                                        int32_t* __restrict__ otri, float* __restrict__ ot,
                                                        float* __restrict__ ou, float* __restrict__ ov,
-                                                       uint8_t* __restrict__ occ, uint32_t* __restrict__ stats) {
+                                                       uint8_t* __restrict__ occ, uint32_t* __restrict__ stats,
+                                                       uint32_t* pool) {
     const GridDesc g = *H.top;
+#if HR_HIER_WARP_POOL
+    // a warp takes 32 consecutive rays from the pool once all its lanes are done, so its
+    // lanes trace neighbouring rays together (rays listed in pixel tiles stay coherent)
+    const uint32_t lane = threadIdx.x & 31u;
+    while (true) {
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(pool, 32u);
+        base = __shfl_sync(kFullMask, base, 0);
+        if (base >= n) break;
+        const uint32_t i = base + lane;
+        if (i >= n) continue;
+#else
     for (uint32_t i = blockIdx.x * kTT + threadIdx.x; i < n; i += gridDim.x * kTT) {
+#endif
         const f3 o = mk(__ldg(org + 3 * (size_t)i), __ldg(org + 3 * (size_t)i + 1), __ldg(org + 3 * (size_t)i + 2));
         const f3 d = mk(__ldg(dir + 3 * (size_t)i), __ldg(dir + 3 * (size_t)i + 1), __ldg(dir + 3 * (size_t)i + 2));
         HHit h;
@@ -526,7 +544,7 @@ struct hr_hier {
     float top_density = 1.2f, obj_density = 1.2f;
     bool objects_dirty = true, have_objects = false, have_instances = false, built = false;
     DevBuf tri_begin, enc, objs, cnt, obj_cells, prims;
-    DevBuf inst, top_desc, icnt, top_cells, inst_ids, words;   // words: [0] cells [1] pairs [2] top pairs [3] err [4] nobj [5] ninst
+    DevBuf inst, top_desc, icnt, top_cells, inst_ids, words;   // words: [0] cells [1] pairs [2] top pairs [3] err [4] nobj [5] ninst [7] ray pool
     uint32_t num_obj_cells = 0, num_pairs = 0, num_top_pairs = 0;
     GridDesc top{};
     DevBuf rays;   // host-call staging: org, dir, tmax, outputs
@@ -546,6 +564,21 @@ int grid_of(const hr_ctx* c, uint64_t n, int bt) {
     const uint64_t cap = (uint64_t)c->num_sms * 16u;
     return (int)std::max<uint64_t>(1, std::min(b, cap));
 }
+
+// blocks of the trace launch: resident blocks on every SM with the warp ray pool,
+// enough blocks for one ray per thread otherwise
+template <bool ANY, bool STATS>
+int hier_grid(hr_ctx* c, uint32_t n) {
+    const int want = grid_of(c, n, kTT);
+    if (!HR_HIER_WARP_POOL) return want;
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_hier_trace<ANY, STATS>, kTT, 0) != cudaSuccess || nb < 1) {
+        cudaGetLastError();
+        nb = 1;
+    }
+    return std::max(1, std::min(want, nb * c->num_sms));
+}
+
 
 // level two: object grids
 int build_objects(hr_hier* h) {
@@ -876,8 +909,12 @@ hr_status hr_hier_trace_rays_device(hr_hier* h, const float* org, const float* d
     if (n == 0) return HR_OK;
     DeviceGuard dg(c->device);
     c->launches += 1;
-    k_hier_trace<false, false><<<grid_of(c, n, kTT), kTT, 0, c->stream>>>(view(h), org, dir, nullptr, n, inst_id, tri_id,
-                                                                           t, u, v, nullptr, nullptr);
+    uint32_t* pool = h->words.as<uint32_t>() + 7;
+    if (cudaMemsetAsync(pool, 0, 4, c->stream) != cudaSuccess)
+        return (hr_status)cuda_check(c, cudaGetLastError(), "hier ray pool");
+    k_hier_trace<false, false><<<hier_grid<false, false>(c, n), kTT, 0, c->stream>>>(view(h), org, dir, nullptr, n,
+                                                                                    inst_id, tri_id, t, u, v, nullptr,
+                                                                                    nullptr, pool);
     return (hr_status)cuda_check(c, cudaGetLastError(), "hier trace launch");
 }
 
@@ -889,8 +926,12 @@ hr_status hr_hier_trace_stats_device(hr_hier* h, const float* org, const float* 
     if (n == 0) return HR_OK;
     DeviceGuard dg(c->device);
     c->launches += 1;
-    k_hier_trace<false, true><<<grid_of(c, n, kTT), kTT, 0, c->stream>>>(view(h), org, dir, nullptr, n, inst_id, tri_id,
-                                                                          t, u, v, nullptr, stats);
+    uint32_t* pool = h->words.as<uint32_t>() + 7;
+    if (cudaMemsetAsync(pool, 0, 4, c->stream) != cudaSuccess)
+        return (hr_status)cuda_check(c, cudaGetLastError(), "hier ray pool");
+    k_hier_trace<false, true><<<hier_grid<false, true>(c, n), kTT, 0, c->stream>>>(view(h), org, dir, nullptr, n,
+                                                                                  inst_id, tri_id, t, u, v, nullptr,
+                                                                                  stats, pool);
     return (hr_status)cuda_check(c, cudaGetLastError(), "hier trace launch");
 }
 
@@ -942,8 +983,10 @@ hr_status hr_hier_occluded(hr_hier* h, const float* org, const float* dir, const
         (rc = cuda_check(c, cudaMemcpyAsync(dtm, tmax, 4 * (size_t)n, cudaMemcpyHostToDevice, s), "rays")))
         return (hr_status)rc;
     c->launches += 1;
-    k_hier_trace<true, false><<<grid_of(c, n, kTT), kTT, 0, s>>>(view(h), dorg, ddir, dtm, n, nullptr, nullptr, nullptr,
-                                                                 nullptr, nullptr, docc, nullptr);
+    uint32_t* pool = h->words.as<uint32_t>() + 7;
+    if ((rc = cuda_check(c, cudaMemsetAsync(pool, 0, 4, s), "hier ray pool"))) return (hr_status)rc;
+    k_hier_trace<true, false><<<hier_grid<true, false>(c, n), kTT, 0, s>>>(view(h), dorg, ddir, dtm, n, nullptr, nullptr,
+                                                                          nullptr, nullptr, nullptr, docc, nullptr, pool);
     if ((rc = cuda_check(c, cudaGetLastError(), "hier occluded launch")) ||
         (rc = cuda_check(c, cudaMemcpyAsync(occluded, docc, n, cudaMemcpyDeviceToHost, s), "occluded")))
         return (hr_status)rc;
