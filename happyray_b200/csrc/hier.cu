@@ -27,6 +27,9 @@
 #include <string>
 #include <vector>
 
+#ifndef HR_HIER_MIN_BLOCKS
+#define HR_HIER_MIN_BLOCKS 8   // blocks per SM the trace kernel's register budget must allow (8: 64 registers)
+#endif
 #ifndef HR_HIER_WARP_POOL
 #define HR_HIER_WARP_POOL 1   // trace warps take 32 consecutive rays from a pool once all lanes are done
 #endif
@@ -482,7 +485,7 @@ __device__ void hier_trace(const HierView& H, const GridDesc& g, f3 o, f3 d, HHi
 }
 
 template <bool ANY, bool STATS>
-__global__ __launch_bounds__(kTT, 8) void k_hier_trace(HierView H, const float* __restrict__ org,
+__global__ __launch_bounds__(kTT, HR_HIER_MIN_BLOCKS) void k_hier_trace(HierView H, const float* __restrict__ org,
                                                        const float* __restrict__ dir, const float* __restrict__ tmax,
                                                        uint32_t n, int32_t* __restrict__ oinst,
                                                        int32_t* __restrict__ otri, float* __restrict__ ot,
