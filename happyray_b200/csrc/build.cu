@@ -257,6 +257,41 @@ int key_bits_for(size_t max_key) {
 
 }  // namespace
 
+// Everything a captured build depends on: grid kind and settings, sizes and capacities,
+// and the addresses of every buffer the build reads or writes.
+static std::vector<uint8_t> build_graph_key(const hr_ctx* c, int32_t kind, int32_t exact, float dens) {
+    const GridBuffers& B = c->g;
+    const DevBuf* bufs[] = {&B.desc, &c->tris, &B.cells, &B.keys_a, &B.tri_ranges, &B.vals_a, &B.keys_b, &B.vals_b,
+                            &B.block_sums, &B.tile_hist, &B.row_total, &B.prims, &B.top_ranges, &B.top_refs,
+                            &B.ref_ranges, &B.leaf_cnt, &B.scan_partials, &B.leaves, &B.lkeys_a, &B.lvals_a,
+                            &B.lkeys_b, &B.lvals_b, &c->verts, &c->idx, &c->counters, &c->keyframes};
+    std::vector<uint8_t> k;
+    auto put = [&](const void* p, size_t n) {
+        const uint8_t* b = static_cast<const uint8_t*>(p);
+        k.insert(k.end(), b, b + n);
+    };
+    const int32_t ints[7] = {kind, exact, c->timing ? 1 : 0, c->num_sms, c->lerp_pending ? 1 : 0, c->frame_a,
+                             c->frame_b};
+    const uint32_t sizes[2] = {c->ntri, c->nverts};
+    const float dens_all[4] = {dens, c->leaf_density, c->ug_density, c->frame_coeff};
+    const size_t caps[4] = {B.cap_cells, B.cap_pairs, B.cap_leaf_pairs, B.cap_leaves};
+    put(ints, sizeof(ints));
+    put(sizes, sizeof(sizes));
+    put(dens_all, sizeof(dens_all));
+    put(caps, sizeof(caps));
+    for (const DevBuf* b : bufs) {
+        put(&b->p, sizeof(b->p));
+        put(&b->bytes, sizeof(b->bytes));
+    }
+    return k;
+}
+
+void drop_build_graph(hr_ctx* c) {
+    if (c->build_exec) cudaGraphExecDestroy(c->build_exec);
+    c->build_exec = nullptr;
+    c->build_key.clear();
+}
+
 // Host orchestration of one build.  With wait, syncs and reports the overflow bits in
 // *ovf_out; without, only enqueues (the descriptor lands in c->desc_pinned when the stream
 // has passed the build).  Returns HR status code (0 = ok).
@@ -310,86 +345,149 @@ static int build_once(hr_ctx* c, int32_t kind, int32_t exact, uint32_t* ovf_out,
         if ((rc = ensure(c, B.prims, sizeof(uint32_t) * B.cap_leaf_pairs))) return rc;
     }
     GridDesc* d = B.desc.as<GridDesc>();
-    int ev = 0;
-    auto mark = [&]() { if (c->timing && ev < 16) cudaEventRecord(c->ev[ev++], s); };
-    mark();
-    // launches of this function (radix sort and scans count their own)
-    c->launches += 3 + (nblocks > 0 ? 3 : 0) + 2 + (kind == kTwoLevel ? 9 : 0);
-    k_desc_init<<<1, 1, 0, s>>>(d, kind, ntri, c->counters.as<uint32_t>() + 2);
-    const int gridv = std::max(1, std::min((int)((c->nverts + kBT - 1) / kBT), c->num_sms * 8));
-    if (c->lerp_pending) {
-        const float4* kf = c->keyframes.as<float4>();
-        k_lerp_bounds<<<gridv, kBT, 0, s>>>(kf + (size_t)c->frame_a * c->nverts, kf + (size_t)c->frame_b * c->nverts,
-                                            c->frame_coeff, c->verts.as<float4>(), c->nverts, d);
-    } else {
-        k_lerp_bounds<<<gridv, kBT, 0, s>>>(nullptr, nullptr, 0.0f, c->verts.as<float4>(), c->nverts, d);
+    // the whole build as one enqueue (returns an HR status)
+    auto enqueue = [&]() -> int {
+        int ev = 0;
+        auto mark = [&]() {
+            if (c->timing && ev < 16) {
+                if (c->build_capturing) cudaEventRecordWithFlags(c->ev[ev++], s, cudaEventRecordExternal);
+                else cudaEventRecord(c->ev[ev++], s);
+            }
+        };
+        mark();
+        // launches of this function (radix sort and scans count their own)
+        c->launches += 3 + (nblocks > 0 ? 3 : 0) + 2 + (kind == kTwoLevel ? 9 : 0);
+        k_desc_init<<<1, 1, 0, s>>>(d, kind, ntri, c->counters.as<uint32_t>() + 2);
+        const int gridv = std::max(1, std::min((int)((c->nverts + kBT - 1) / kBT), c->num_sms * 8));
+        if (c->lerp_pending) {
+            const float4* kf = c->keyframes.as<float4>();
+            k_lerp_bounds<<<gridv, kBT, 0, s>>>(kf + (size_t)c->frame_a * c->nverts, kf + (size_t)c->frame_b * c->nverts,
+                                                c->frame_coeff, c->verts.as<float4>(), c->nverts, d);
+        } else {
+            k_lerp_bounds<<<gridv, kBT, 0, s>>>(nullptr, nullptr, 0.0f, c->verts.as<float4>(), c->nverts, d);
+        }
+        k_grid_setup<<<1, 1, 0, s>>>(d, dens, (uint32_t)std::min(B.cap_cells, (size_t)0xffffffffu));
+        mark();
+        const float4* v = c->verts.as<float4>();
+        const uint32_t* ix = c->idx.as<uint32_t>();
+        uint32_t* bsum = B.block_sums.as<uint32_t>();
+        uint32_t* d_np = kind == kUniform ? &d->npairs : &d->ntop_pairs;
+        if (nblocks > 0) {
+            k_count_pairs<<<nblocks, kBT, 0, s>>>(v, ix, ntri, d, bsum, c->tris.as<float4>(), B.tri_ranges.as<uint4>());
+            if ((rc = scan_block_sums(c, bsum, nblocks, d_np, &d->overflow, (uint32_t)std::min(cap_pairs, (size_t)0xffffffffu),
+                                      kind == kUniform ? kOvfPairs : kOvfTopPairs, &d->req_pairs, s)))
+                return rc;
+            if (kind == kUniform && exact)
+                k_write_pairs<true><<<nblocks, kBT, 0, s>>>(c->tris.as<float4>(), ntri, d, bsum, nullptr,
+                                                            B.keys_a.as<uint32_t>(), B.vals_a.as<uint32_t>());
+            else
+                k_write_pairs<false><<<nblocks, kBT, 0, s>>>(c->tris.as<float4>(), ntri, d, bsum, B.tri_ranges.as<uint4>(),
+                                                             B.keys_a.as<uint32_t>(), B.vals_a.as<uint32_t>());
+        }
+        mark();
+        uint32_t* sorted_keys = (passes % 2 == 1) ? B.keys_b.as<uint32_t>() : B.keys_a.as<uint32_t>();
+        uint32_t* sorted_vals = kind == kUniform ? B.prims.as<uint32_t>() : B.top_refs.as<uint32_t>();
+        if ((rc = radix_sort_pairs(c, B.keys_a.as<uint32_t>(), B.vals_a.as<uint32_t>(), B.keys_b.as<uint32_t>(),
+                                   B.vals_b.as<uint32_t>(), sorted_keys, sorted_vals, d_np, cap_pairs, key_bits,
+                                   B.tile_hist.as<uint32_t>(), B.tile_hist.bytes, B.row_total.as<uint32_t>(), s)))
+            return rc;
+        mark();
+        uint2* ranges = kind == kUniform ? B.cells.as<uint2>() : B.top_ranges.as<uint2>();
+        const int gcells = std::max(1, std::min((int)((B.cap_cells + 255) / 256), c->num_sms * 16));
+        k_fill_u2<<<gcells, 256, 0, s>>>(ranges, &d->ncells, d, make_uint2(0u, 0u));
+        const int gpairs = std::max(1, std::min((int)((cap_pairs + 255) / 256), c->num_sms * 16));
+        k_cell_ranges<<<gpairs, 256, 0, s>>>(sorted_keys, d_np, &d->ncells, d, ranges);
+        mark();
+        if (kind == kTwoLevel) {
+            // leaf level, TLGridSortBuilder.h:256-410: leaf cells per top cell, scan, leaf pairs
+            // per reference in reference order, stable sort by leaf, leaf ranges
+            k_tl_cells<<<gcells, 256, 0, s>>>(ranges, d, c->leaf_density, B.leaf_cnt.as<uint32_t>(), B.cells.as<uint2>());
+            uint32_t* sp = B.scan_partials.as<uint32_t>();
+            if ((rc = exclusive_scan_u32(c, B.leaf_cnt.as<uint32_t>(), &d->ncells, B.cap_cells, &d->nleaves, sp, s)))
+                return rc;
+            k_check_leaves<<<1, 1, 0, s>>>(d, (uint32_t)std::min(B.cap_leaves, (size_t)0xffffffffu));
+            k_tl_cell_begin<<<gcells, 256, 0, s>>>(B.leaf_cnt.as<uint32_t>(), d, B.cells.as<uint2>());
+            mark();
+            uint32_t* lsum = B.block_sums.as<uint32_t>();
+            k_leaf_count_pairs<<<nref_blocks, kBT, 0, s>>>(sorted_keys, B.top_refs.as<uint32_t>(), c->tris.as<float4>(), d,
+                                                           B.cells.as<uint2>(), lsum, B.ref_ranges.as<uint4>());
+            if ((rc = scan_block_sums(c, lsum, nref_blocks, &d->npairs, &d->overflow,
+                                      (uint32_t)std::min(B.cap_leaf_pairs, (size_t)0xffffffffu), kOvfLeafPairs,
+                                      &d->req_leaf_pairs, s)))
+                return rc;
+            k_leaf_write_pairs<<<nref_blocks, kBT, 0, s>>>(B.ref_ranges.as<uint4>(), d, lsum, B.lkeys_a.as<uint32_t>(),
+                                                           B.lvals_a.as<uint32_t>());
+            mark();
+            uint32_t* leaf_keys = (leaf_passes % 2 == 1) ? B.lkeys_b.as<uint32_t>() : B.lkeys_a.as<uint32_t>();
+            if ((rc = radix_sort_pairs(c, B.lkeys_a.as<uint32_t>(), B.lvals_a.as<uint32_t>(), B.lkeys_b.as<uint32_t>(),
+                                       B.lvals_b.as<uint32_t>(), leaf_keys, B.prims.as<uint32_t>(), &d->npairs,
+                                       B.cap_leaf_pairs, leaf_bits, B.tile_hist.as<uint32_t>(), B.tile_hist.bytes,
+                                       B.row_total.as<uint32_t>(), s)))
+                return rc;
+            mark();
+            const int gleaves = std::max(1, std::min((int)((B.cap_leaves + 255) / 256), c->num_sms * 16));
+            k_fill_u2<<<gleaves, 256, 0, s>>>(B.leaves.as<uint2>(), &d->nleaves, d, make_uint2(0u, 0u));
+            const int glp = std::max(1, std::min((int)((B.cap_leaf_pairs + 255) / 256), c->num_sms * 16));
+            k_cell_ranges<<<glp, 256, 0, s>>>(leaf_keys, &d->npairs, &d->nleaves, d, B.leaves.as<uint2>());
+            mark();
+        }
+        c->nstages = ev;
+        return 0;
+    };
+    // A rebuild identical to the previous one (the same frame, sizes, buffers and
+    // settings: a static mesh rebuilt every frame) is captured once as a CUDA graph and then
+    // replayed: one launch instead of about 35, so small builds are not paced by the host's
+    // launch rate.  Builds whose key frames or frame time change go straight to the stream.
+    bool enqueued = false;
+    std::vector<uint8_t> key;
+    if (HR_BUILD_GRAPH && wait && c->build_graph_ok) key = build_graph_key(c, kind, exact, dens);
+    if (!key.empty() && (key == c->build_key || key == c->last_build_key)) {
+        if (c->build_exec && key == c->build_key) {
+            if (cudaGraphLaunch(c->build_exec, s) == cudaSuccess) {
+                c->launches += c->build_graph_launches;
+                c->nstages = c->build_graph_stages;
+                enqueued = true;
+            } else {
+                cudaGetLastError();
+                drop_build_graph(c);
+                c->build_graph_ok = false;
+            }
+        } else {
+            drop_build_graph(c);
+            cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+            if (cudaStreamIsCapturing(s, &cs) == cudaSuccess && cs == cudaStreamCaptureStatusNone &&
+                cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+                const uint64_t l0 = c->launches;
+                c->build_capturing = true;
+                const int erc = enqueue();
+                c->build_capturing = false;
+                cudaGraph_t g = nullptr;
+                const cudaError_t e = cudaStreamEndCapture(s, &g);
+                if (erc) {
+                    if (g) cudaGraphDestroy(g);
+                    cudaGetLastError();
+                    return erc;
+                }
+                if (e == cudaSuccess && g && cudaGraphInstantiate(&c->build_exec, g, 0) == cudaSuccess &&
+                    cudaGraphLaunch(c->build_exec, s) == cudaSuccess) {
+                    c->build_key = std::move(key);
+                    c->build_graph_launches = c->launches - l0;
+                    c->build_graph_stages = c->nstages;
+                    enqueued = true;
+                } else {   // not capturable here: build directly from now on
+                    cudaGetLastError();
+                    drop_build_graph(c);
+                    c->build_graph_ok = false;
+                    c->launches = l0;
+                }
+                if (g) cudaGraphDestroy(g);
+            } else {
+                cudaGetLastError();
+            }
+        }
     }
-    k_grid_setup<<<1, 1, 0, s>>>(d, dens, (uint32_t)std::min(B.cap_cells, (size_t)0xffffffffu));
-    mark();
-    const float4* v = c->verts.as<float4>();
-    const uint32_t* ix = c->idx.as<uint32_t>();
-    uint32_t* bsum = B.block_sums.as<uint32_t>();
-    uint32_t* d_np = kind == kUniform ? &d->npairs : &d->ntop_pairs;
-    if (nblocks > 0) {
-        k_count_pairs<<<nblocks, kBT, 0, s>>>(v, ix, ntri, d, bsum, c->tris.as<float4>(), B.tri_ranges.as<uint4>());
-        if ((rc = scan_block_sums(c, bsum, nblocks, d_np, &d->overflow, (uint32_t)std::min(cap_pairs, (size_t)0xffffffffu),
-                                  kind == kUniform ? kOvfPairs : kOvfTopPairs, &d->req_pairs, s)))
-            return rc;
-        if (kind == kUniform && exact)
-            k_write_pairs<true><<<nblocks, kBT, 0, s>>>(c->tris.as<float4>(), ntri, d, bsum, nullptr,
-                                                        B.keys_a.as<uint32_t>(), B.vals_a.as<uint32_t>());
-        else
-            k_write_pairs<false><<<nblocks, kBT, 0, s>>>(c->tris.as<float4>(), ntri, d, bsum, B.tri_ranges.as<uint4>(),
-                                                         B.keys_a.as<uint32_t>(), B.vals_a.as<uint32_t>());
-    }
-    mark();
-    uint32_t* sorted_keys = (passes % 2 == 1) ? B.keys_b.as<uint32_t>() : B.keys_a.as<uint32_t>();
-    uint32_t* sorted_vals = kind == kUniform ? B.prims.as<uint32_t>() : B.top_refs.as<uint32_t>();
-    if ((rc = radix_sort_pairs(c, B.keys_a.as<uint32_t>(), B.vals_a.as<uint32_t>(), B.keys_b.as<uint32_t>(),
-                               B.vals_b.as<uint32_t>(), sorted_keys, sorted_vals, d_np, cap_pairs, key_bits,
-                               B.tile_hist.as<uint32_t>(), B.tile_hist.bytes, B.row_total.as<uint32_t>(), s)))
-        return rc;
-    mark();
-    uint2* ranges = kind == kUniform ? B.cells.as<uint2>() : B.top_ranges.as<uint2>();
-    const int gcells = std::max(1, std::min((int)((B.cap_cells + 255) / 256), c->num_sms * 16));
-    k_fill_u2<<<gcells, 256, 0, s>>>(ranges, &d->ncells, d, make_uint2(0u, 0u));
-    const int gpairs = std::max(1, std::min((int)((cap_pairs + 255) / 256), c->num_sms * 16));
-    k_cell_ranges<<<gpairs, 256, 0, s>>>(sorted_keys, d_np, &d->ncells, d, ranges);
-    mark();
-    if (kind == kTwoLevel) {
-        // leaf level, TLGridSortBuilder.h:256-410: leaf cells per top cell, scan, leaf pairs
-        // per reference in reference order, stable sort by leaf, leaf ranges
-        k_tl_cells<<<gcells, 256, 0, s>>>(ranges, d, c->leaf_density, B.leaf_cnt.as<uint32_t>(), B.cells.as<uint2>());
-        uint32_t* sp = B.scan_partials.as<uint32_t>();
-        if ((rc = exclusive_scan_u32(c, B.leaf_cnt.as<uint32_t>(), &d->ncells, B.cap_cells, &d->nleaves, sp, s)))
-            return rc;
-        k_check_leaves<<<1, 1, 0, s>>>(d, (uint32_t)std::min(B.cap_leaves, (size_t)0xffffffffu));
-        k_tl_cell_begin<<<gcells, 256, 0, s>>>(B.leaf_cnt.as<uint32_t>(), d, B.cells.as<uint2>());
-        mark();
-        uint32_t* lsum = B.block_sums.as<uint32_t>();
-        k_leaf_count_pairs<<<nref_blocks, kBT, 0, s>>>(sorted_keys, B.top_refs.as<uint32_t>(), c->tris.as<float4>(), d,
-                                                       B.cells.as<uint2>(), lsum, B.ref_ranges.as<uint4>());
-        if ((rc = scan_block_sums(c, lsum, nref_blocks, &d->npairs, &d->overflow,
-                                  (uint32_t)std::min(B.cap_leaf_pairs, (size_t)0xffffffffu), kOvfLeafPairs,
-                                  &d->req_leaf_pairs, s)))
-            return rc;
-        k_leaf_write_pairs<<<nref_blocks, kBT, 0, s>>>(B.ref_ranges.as<uint4>(), d, lsum, B.lkeys_a.as<uint32_t>(),
-                                                       B.lvals_a.as<uint32_t>());
-        mark();
-        uint32_t* leaf_keys = (leaf_passes % 2 == 1) ? B.lkeys_b.as<uint32_t>() : B.lkeys_a.as<uint32_t>();
-        if ((rc = radix_sort_pairs(c, B.lkeys_a.as<uint32_t>(), B.lvals_a.as<uint32_t>(), B.lkeys_b.as<uint32_t>(),
-                                   B.lvals_b.as<uint32_t>(), leaf_keys, B.prims.as<uint32_t>(), &d->npairs,
-                                   B.cap_leaf_pairs, leaf_bits, B.tile_hist.as<uint32_t>(), B.tile_hist.bytes,
-                                   B.row_total.as<uint32_t>(), s)))
-            return rc;
-        mark();
-        const int gleaves = std::max(1, std::min((int)((B.cap_leaves + 255) / 256), c->num_sms * 16));
-        k_fill_u2<<<gleaves, 256, 0, s>>>(B.leaves.as<uint2>(), &d->nleaves, d, make_uint2(0u, 0u));
-        const int glp = std::max(1, std::min((int)((B.cap_leaf_pairs + 255) / 256), c->num_sms * 16));
-        k_cell_ranges<<<glp, 256, 0, s>>>(leaf_keys, &d->npairs, &d->nleaves, d, B.leaves.as<uint2>());
-        mark();
-    }
-    c->nstages = ev;
+    if (!enqueued && (rc = enqueue())) return rc;
+    c->last_build_key = std::move(key);
     if ((rc = cuda_check(c, cudaGetLastError(), "build launch"))) return rc;
     if (!wait) {
         if (!c->desc_pinned && cudaMallocHost((void**)&c->desc_pinned, sizeof(GridDesc)) != cudaSuccess) {
@@ -404,7 +502,7 @@ static int build_once(hr_ctx* c, int32_t kind, int32_t exact, uint32_t* ovf_out,
         return rc;
     if ((rc = cuda_check(c, cudaStreamSynchronize(s), "build"))) return rc;
     if (c->timing)
-        for (int i = 0; i + 1 < ev; ++i) cudaEventElapsedTime(&c->stage_ms[i], c->ev[i], c->ev[i + 1]);
+        for (int i = 0; i + 1 < c->nstages; ++i) cudaEventElapsedTime(&c->stage_ms[i], c->ev[i], c->ev[i + 1]);
     if (c->host_desc.error) return set_error(c, 1, "triangle index out of range of the uploaded vertices");
     *ovf_out = c->host_desc.overflow;
     return 0;

@@ -5,8 +5,13 @@
 #include <cstdint>
 #include <cstddef>
 #include <string>
+#include <vector>
 
 #include "hr_common.cuh"
+
+#ifndef HR_BUILD_GRAPH
+#define HR_BUILD_GRAPH 1   // static rebuilds replay a captured CUDA graph of the build
+#endif
 
 namespace hr {
 
@@ -96,6 +101,12 @@ struct hr_ctx {
     hr::GridDesc* desc_pinned = nullptr;   // descriptor of an asynchronous build (pinned)
     bool async_pending = false;  // an asynchronous build awaits build_async_result
     hr::DevBuf counters;         // uint64 ray counters
+    cudaGraphExec_t build_exec = nullptr;   // captured static rebuild, and what it was captured for
+    std::vector<uint8_t> build_key, last_build_key;
+    uint64_t build_graph_launches = 0;
+    int build_graph_stages = 0;
+    bool build_graph_ok = true;      // false once a capture failed: build directly
+    bool build_capturing = false;
     uint64_t launches = 0;       // kernels enqueued by this context (host-side count)
     bool collect_stats = false;  // render kernels accumulate cells visited / triangle tests
     cudaEvent_t ev[16] = {};
@@ -141,6 +152,7 @@ int build_grid(hr_ctx* c, int32_t kind, int32_t exact);
 // before is built synchronously).  Once the stream has passed it, build_async_result
 // reports whether it fit; if not, the capacities are grown and the grid must be rebuilt.
 int build_grid_async(hr_ctx* c, int32_t kind, int32_t exact);
+void drop_build_graph(hr_ctx* c);   // frees the captured rebuild (hr_destroy)
 int build_async_result(hr_ctx* c, bool* fit);
 
 // sort.cu
