@@ -37,11 +37,28 @@ __global__ void k_desc_init(GridDesc* d, int32_t kind, uint32_t ntri, const uint
     desc_init(d, kind, ntri, *bad_index_count != 0u ? 1u : 0u);
 }
 
-// a1: fused keyframe interpolation + bounds (WFObjectUploader.h:82-110).  coeff applies
-// to frame b: v = a * (1 - c) + b * c.  With a == nullptr the vertices are only reduced.
-__global__ __launch_bounds__(kBT) void k_lerp_bounds(const float4* __restrict__ a, const float4* __restrict__ b,
-                                                     float coeff, float4* __restrict__ out, uint32_t nv, GridDesc* d) {
+// The key-frame pair and weight of the next interpolating build, written in stream order
+// ahead of it so that a captured build graph replays for any frame time:
+// sel = (frame a, frame b, bits of coeff, 0).
+__global__ void k_frame_select(int4* sel, int32_t a, int32_t b, float coeff) {
+    *sel = make_int4(a, b, __float_as_int(coeff), 0);
+}
+
+// a1: fused keyframe interpolation + bounds (WFObjectUploader.h:82-110).  The frames and
+// coeff come from sel; coeff applies to frame b: v = a * (1 - c) + b * c.  With
+// kf == nullptr the vertices are only reduced.
+__global__ __launch_bounds__(kBT) void k_lerp_bounds(const float4* __restrict__ kf, const int4* __restrict__ sel,
+                                                     float4* __restrict__ out, uint32_t nv, GridDesc* d) {
     f3 lo = mk(FLT_MAX, FLT_MAX, FLT_MAX), hi = mk(-FLT_MAX, -FLT_MAX, -FLT_MAX);
+    const float4* a = nullptr;
+    const float4* b = nullptr;
+    float coeff = 0.0f;
+    if (kf) {
+        const int4 q = *sel;
+        a = kf + (size_t)q.x * nv;
+        b = kf + (size_t)q.y * nv;
+        coeff = __int_as_float(q.z);
+    }
     const float w1 = 1.0f - coeff;
     for (uint32_t i = blockIdx.x * kBT + threadIdx.x; i < nv; i += gridDim.x * kBT) {
         f3 p;
@@ -264,16 +281,16 @@ static std::vector<uint8_t> build_graph_key(const hr_ctx* c, int32_t kind, int32
     const DevBuf* bufs[] = {&B.desc, &c->tris, &B.cells, &B.keys_a, &B.tri_ranges, &B.vals_a, &B.keys_b, &B.vals_b,
                             &B.block_sums, &B.tile_hist, &B.row_total, &B.prims, &B.top_ranges, &B.top_refs,
                             &B.ref_ranges, &B.leaf_cnt, &B.scan_partials, &B.leaves, &B.lkeys_a, &B.lvals_a,
-                            &B.lkeys_b, &B.lvals_b, &c->verts, &c->idx, &c->counters, &c->keyframes};
+                            &B.lkeys_b, &B.lvals_b, &c->verts, &c->idx, &c->counters, &c->keyframes, &c->frame_sel};
     std::vector<uint8_t> k;
     auto put = [&](const void* p, size_t n) {
         const uint8_t* b = static_cast<const uint8_t*>(p);
         k.insert(k.end(), b, b + n);
     };
-    const int32_t ints[7] = {kind, exact, c->timing ? 1 : 0, c->num_sms, c->lerp_pending ? 1 : 0, c->frame_a,
-                             c->frame_b};
-    const uint32_t sizes[2] = {c->ntri, c->nverts};
-    const float dens_all[4] = {dens, c->leaf_density, c->ug_density, c->frame_coeff};
+    // the frame pair and weight are not part of it: the graph reads them from frame_sel
+    const int32_t ints[5] = {kind, exact, c->timing ? 1 : 0, c->num_sms, c->lerp_pending ? 1 : 0};
+    const uint32_t sizes[3] = {c->ntri, c->nverts, c->nkeyframes};
+    const float dens_all[3] = {dens, c->leaf_density, c->ug_density};
     const size_t caps[4] = {B.cap_cells, B.cap_pairs, B.cap_leaf_pairs, B.cap_leaves};
     put(ints, sizeof(ints));
     put(sizes, sizeof(sizes));
@@ -319,6 +336,7 @@ static int build_once(hr_ctx* c, int32_t kind, int32_t exact, uint32_t* ovf_out,
     if (kind == kTwoLevel) hist_words = std::max(hist_words, radix_tile_hist_words(B.cap_leaf_pairs, leaf_bits));
     int rc;
     if ((rc = ensure(c, B.desc, sizeof(GridDesc)))) return rc;
+    if ((rc = ensure(c, c->frame_sel, sizeof(int4)))) return rc;
     if ((rc = ensure(c, c->tris, sizeof(float4) * 3 * (size_t)ntri))) return rc;
     if ((rc = ensure(c, B.cells, sizeof(uint2) * B.cap_cells))) return rc;
     if ((rc = ensure(c, B.keys_a, sizeof(uint32_t) * cap_pairs))) return rc;
@@ -359,13 +377,8 @@ static int build_once(hr_ctx* c, int32_t kind, int32_t exact, uint32_t* ovf_out,
         c->launches += 3 + (nblocks > 0 ? 3 : 0) + 2 + (kind == kTwoLevel ? 9 : 0);
         k_desc_init<<<1, 1, 0, s>>>(d, kind, ntri, c->counters.as<uint32_t>() + 2);
         const int gridv = std::max(1, std::min((int)((c->nverts + kBT - 1) / kBT), c->num_sms * 8));
-        if (c->lerp_pending) {
-            const float4* kf = c->keyframes.as<float4>();
-            k_lerp_bounds<<<gridv, kBT, 0, s>>>(kf + (size_t)c->frame_a * c->nverts, kf + (size_t)c->frame_b * c->nverts,
-                                                c->frame_coeff, c->verts.as<float4>(), c->nverts, d);
-        } else {
-            k_lerp_bounds<<<gridv, kBT, 0, s>>>(nullptr, nullptr, 0.0f, c->verts.as<float4>(), c->nverts, d);
-        }
+        k_lerp_bounds<<<gridv, kBT, 0, s>>>(c->lerp_pending ? c->keyframes.as<float4>() : nullptr,
+                                            c->frame_sel.as<int4>(), c->verts.as<float4>(), c->nverts, d);
         k_grid_setup<<<1, 1, 0, s>>>(d, dens, (uint32_t)std::min(B.cap_cells, (size_t)0xffffffffu));
         mark();
         const float4* v = c->verts.as<float4>();
@@ -435,9 +448,14 @@ static int build_once(hr_ctx* c, int32_t kind, int32_t exact, uint32_t* ovf_out,
         return 0;
     };
     // A rebuild identical to the previous one (the same frame, sizes, buffers and
-    // settings: a static mesh rebuilt every frame) is captured once as a CUDA graph and then
+    // settings: a mesh rebuilt every frame) is captured once as a CUDA graph and then
     // replayed: one launch instead of about 35, so small builds are not paced by the host's
-    // launch rate.  Builds whose key frames or frame time change go straight to the stream.
+    // launch rate.  An animated mesh replays the same graph for every frame time: the frame
+    // pair and weight go to frame_sel first, outside the graph.
+    if (c->lerp_pending) {
+        k_frame_select<<<1, 1, 0, s>>>(c->frame_sel.as<int4>(), c->frame_a, c->frame_b, c->frame_coeff);
+        c->launches += 1;
+    }
     bool enqueued = false;
     std::vector<uint8_t> key;
     if (HR_BUILD_GRAPH && wait && c->build_graph_ok) key = build_graph_key(c, kind, exact, dens);

@@ -89,6 +89,7 @@ struct hr_ctx {
     hr::DevBuf staging;    // float4 staging of host keyframes on upload
     int32_t frame_a = 0, frame_b = 0;
     float frame_coeff = 1.0f;
+    hr::DevBuf frame_sel;  // int4 (frame a, frame b, coeff bits, 0) read by the build's lerp kernel
     bool have_frame = false;     // a frame (static or lerp request) is set
     bool lerp_pending = false;   // the next build interpolates resident keyframes
 

@@ -79,12 +79,14 @@ def test_build_uniform_clusters(engine, oracle, small_clusters):
 
 def test_keyframe_lerp_and_rebuild(engine, oracle, small_clusters):
     """Resident key frames, frame-time selection (AnimationManager.hpp:68-97) and the fused
-    device interpolation give the oracle's vertices and grid at every frame time."""
+    device interpolation give the oracle's vertices and grid at every frame time.  From the
+    third frame on, the rebuilds replay one captured build graph whose lerp kernel reads each
+    frame's pair and weight from device memory."""
     v, f = small_clusters
     frames = S.curl_keyframes(v, 6, seed=4)
     engine.set_keyframes(frames, f)
     engine.setGridDensities(0.0625, 2.0)
-    for tt, step in [(0.0, 0.0), (2.75, 0.0), (5.5, 0.0), (1.25, 1.0)]:
+    for tt, step in [(0.0, 0.0), (2.75, 0.0), (5.5, 0.0), (0.5, 0.0), (3.25, 0.0), (4.75, 0.0), (1.25, 1.0)]:
         engine.set_frame_time(tt, step)
         engine.build(GRID_TWO_LEVEL)
         k = int(tt)
