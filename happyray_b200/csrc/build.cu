@@ -27,6 +27,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstring>
 
 namespace hr {
 
@@ -452,9 +453,18 @@ static int build_once(hr_ctx* c, int32_t kind, int32_t exact, uint32_t* ovf_out,
     // replayed: one launch instead of about 35, so small builds are not paced by the host's
     // launch rate.  An animated mesh replays the same graph for every frame time: the frame
     // pair and weight go to frame_sel first, outside the graph.
+    // (only when the word does not hold this selection already: a static mesh whose frame
+    // time is set every frame launches nothing extra)
     if (c->lerp_pending) {
-        k_frame_select<<<1, 1, 0, s>>>(c->frame_sel.as<int4>(), c->frame_a, c->frame_b, c->frame_coeff);
-        c->launches += 1;
+        uint32_t cb;
+        std::memcpy(&cb, &c->frame_coeff, sizeof(cb));
+        const int32_t want[3] = {c->frame_a, c->frame_b, (int32_t)cb};
+        if (!c->frame_sel_valid || std::memcmp(want, c->frame_sel_host, sizeof(want)) != 0) {
+            k_frame_select<<<1, 1, 0, s>>>(c->frame_sel.as<int4>(), c->frame_a, c->frame_b, c->frame_coeff);
+            c->launches += 1;
+            std::memcpy(c->frame_sel_host, want, sizeof(want));
+            c->frame_sel_valid = true;
+        }
     }
     bool enqueued = false;
     std::vector<uint8_t> key;

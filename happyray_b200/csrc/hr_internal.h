@@ -90,6 +90,8 @@ struct hr_ctx {
     int32_t frame_a = 0, frame_b = 0;
     float frame_coeff = 1.0f;
     hr::DevBuf frame_sel;  // int4 (frame a, frame b, coeff bits, 0) read by the build's lerp kernel
+    int32_t frame_sel_host[3] = {0, 0, 0};   // what the last k_frame_select wrote there
+    bool frame_sel_valid = false;
     bool have_frame = false;     // a frame (static or lerp request) is set
     bool lerp_pending = false;   // the next build interpolates resident keyframes
 
