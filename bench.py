@@ -121,7 +121,7 @@ class ClockSampler:
         try:
             self.fh = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                          "--format=csv,noheader,nounits", "-lms", "20"],
                                          stdout=self.fh, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
@@ -183,15 +183,24 @@ def replica_value(units_per_rank_step: float, steps: int, total_ms: float, ws: i
     return ws * units_per_rank_step * steps / (total_ms * 1e-3) / 1e6
 
 
-def cpu_baseline(W, kind_budget_s=25.0):
-    """The oracle (CPU restatement of the reference's build and traversal) on a bounded
-    sample of the workload, all host threads: full build + a strided pixel sample, scaled."""
-    import oracle as O
-    v, f = W["v"], W["f"]
+def baseline_frame(W):
+    """The frame the CPU baseline builds and renders: key frames 0 and 1 blended half-way
+    for an animated workload, the static mesh otherwise (first frame, second frame, weight)."""
     frames = W["frames"]
-    src = frames[0] if frames is not None else v
+    if frames is not None:
+        return frames[0], frames[1], 0.5
+    return W["v"], W["v"], 1.0
+
+
+def cpu_baseline(W, kind_budget_s=25.0, keep=None):
+    """The oracle (CPU restatement of the reference's build and traversal) on a bounded
+    sample of the workload, all host threads: full build + a strided pixel sample, scaled.
+    With keep (a dict), the oracle's grid and outputs are stored there for the parity check."""
+    import oracle as O
+    f = W["f"]
+    f1, f2, coeff = baseline_frame(W)
     t0 = time.perf_counter()
-    v4, bmin, bmax = O.lerp_bounds(src, frames[1] if frames is not None else src, 0.5 if frames is not None else 1.0)
+    v4, bmin, bmax = O.lerp_bounds(f1, f2, coeff)
     if W["kind"] == 0:
         b = O.build_ug(v4, f, bmin, bmax, W["ug"], W["exact"])
     else:
@@ -203,15 +212,18 @@ def cpu_baseline(W, kind_budget_s=25.0):
     stride = 1 if W["mode"] != 1 else 2
     t1 = time.perf_counter()
     if W["mode"] == 3:
-        _, rays = O.render_ao(b, oc, W["ao"], float(np.float32(0.1) * b.diag()), 0x853c49e6748fea9b, pixel_stride=stride)
+        out, rays = O.render_ao(b, oc, W["ao"], float(np.float32(0.1) * b.diag()), 0x853c49e6748fea9b,
+                                pixel_stride=stride)
     elif W["mode"] == 1:
-        _, rays = O.render_pt(b, oc, O.make_light(), W["bounces"], 0.7, float(np.float32(1e-4) * b.diag()),
-                              0x853c49e6748fea9b, pixel_stride=stride)
+        out, rays = O.render_pt(b, oc, O.make_light(), W["bounces"], 0.7, float(np.float32(1e-4) * b.diag()),
+                                0x853c49e6748fea9b, pixel_stride=stride)
     else:
         org, d = O.primary_rays(oc)
-        O.trace(b, org[::stride], d[::stride])
+        out = O.trace(b, org[::stride], d[::stride])
         rays = org[::stride].shape[0]
     t_trace = time.perf_counter() - t1
+    if keep is not None:
+        keep.update(grid=b, out=out, stride=stride)
     sampled = len(range(0, npx, stride))
     scale = npx / sampled
     est = t_build + t_trace * scale
@@ -219,6 +231,85 @@ def cpu_baseline(W, kind_budget_s=25.0):
             "sample": f"full build ({t_build * 1e3:.0f} ms) + every {stride}th pixel ({sampled} px, "
                       f"{rays} rays, {t_trace * 1e3:.0f} ms) scaled to the full frame",
             "build_ms": t_build * 1e3}
+
+
+def gpu_parity(eng, W, keep, d_fb):
+    """The CPU baseline's frame built and rendered through the library (untimed), compared
+    with the oracle's grid and output: the number of differing entries of each (0 everywhere
+    = bit-exact)."""
+    import torch
+    f1, f2, coeff = baseline_frame(W)
+    eng.upload(f1, f2, W["f"], coeff)
+    eng.build(W["kind"], W.get("exact", True))
+    gi, cells, leaves, prims = eng.grid_download()
+    b = keep["grid"]
+
+    def ndiff(a, o):
+        a, o = np.asarray(a).reshape(-1), np.asarray(o).reshape(-1)
+        return int((a != o).sum()) if a.shape == o.shape else max(a.size, o.size)
+
+    res = {"grid_cells": ndiff(cells, b.cells), "grid_prims": ndiff(prims, b.prims)}
+    if b.leaves is not None:
+        res["grid_leaves"] = ndiff(leaves, b.leaves)
+    st = keep["stride"]
+    if W["mode"] in (1, 3):
+        eng.render_device(d_fb, 0, W["mode"])
+        eng.sync()
+        img = d_fb.view(-1, 3).cpu().numpy()
+        res["pixels_compared"] = int(img[::st].shape[0])
+        res["pixels_differing"] = ndiff(img[::st, 0], keep["out"][::st])
+    else:
+        n = W["cam"]["res_x"] * W["cam"]["res_y"]
+        outs = [torch.empty(n, dtype=dt, device=d_fb.device) for dt in (torch.int32, torch.float32, torch.float32,
+                                                                        torch.float32)]
+        eng.trace_primary_device(*outs)
+        eng.sync()
+        res["rays_compared"] = int(n)
+        res["hits_differing"] = sum(ndiff(o.cpu().numpy()[::st], k) for o, k in zip(outs, keep["out"]))
+    res["result"] = "bit-exact" if all(v == 0 for k, v in res.items() if "differing" in k or k.startswith("grid_")) \
+        else "mismatch"
+    res["checked_against"] = "oracle (CPU restatement of the reference) on the CPU baseline's frame"
+    return res
+
+
+def rebuild_2m_prepare(dev, stream):
+    """A context holding the 2,097,152-triangle key-frame mesh (16 curl-noise key frames,
+    densities 1/16 : 2), with its capacities sized and its build graph captured by three
+    untimed rebuilds."""
+    from happyray_b200 import GRID_TWO_LEVEL, Engine
+    from happyray_b200 import scenes as S
+    v, f = S.clusters(2_097_152, seed=0)
+    frames = S.curl_keyframes_torch(v, 16, amp=0.02, octaves=4, seed=0, device=f"cuda:{dev}")
+    e = Engine(dev, stream=stream.cuda_stream)
+    e.set_keyframes(frames, f)
+    e.setGridDensities(0.0625, 2.0)
+    for i in range(3):
+        e.set_frame_time(16.0 * i / 120.0, 0.0)
+        e.build(GRID_TWO_LEVEL)
+    return e, v.shape[0], f.shape[0]
+
+
+def rebuild_2m_keyframe(prep, stream, flush, frame_times=24):
+    """Two-level rebuilds of the prepared 2M-triangle key-frame mesh at `frame_times`
+    successive frame times of the 120-step cycle, each one replay of the captured build
+    graph with the key-frame interpolation fused in, L2 flushed before each.  Returns the
+    median rebuild time, its algorithmic bytes and the number of rebuilds timed."""
+    import torch
+    from happyray_b200 import GRID_TWO_LEVEL
+    e, nv, ntri = prep
+    ms = []
+    for i in range(frame_times):
+        e.set_frame_time(16.0 * ((i + 3) % 120) / 120.0, 0.0)
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        a, z = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        e.build(GRID_TWO_LEVEL)
+        z.record(stream)
+        z.synchronize()
+        ms.append(a.elapsed_time(z))
+    gi = e.grid_info()
+    return statistics.median(ms), algorithmic_build_bytes(gi, nv, ntri, lerp=True), len(ms)
 
 
 def run_reference(args, W, rank, ws):
@@ -796,6 +887,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="c4: skip the autotuner (densities 1/16, 2)")
+    ap.add_argument("--no-rebuild2m", action="store_true", help="c2: skip the 2M-triangle key-frame rebuild")
     args = ap.parse_args()
     rank, ws, local = dist_setup() if os.environ.get("WORLD_SIZE") else (0, 1, 0)
     if args.config == "c4":
@@ -877,18 +969,20 @@ def main():
     if ws > 1:
         import torch.distributed as dist
         dist.barrier()
+    prep2m = rebuild_2m_prepare(dev, stream) if args.config == "c2" and not args.no_rebuild2m else None
     evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
     l0 = eng.counters()["launches"]
     kern_ms = []
-    with ClockSampler(dev) as clk:
-        torch.cuda.synchronize()
-        for i in range(args.steps):
-            with torch.cuda.stream(stream):
-                flush.zero_()   # L2 flush between timed steps (256 MiB > 126 MB L2), outside the events
-            step(args.warmup + i, evs[i])
-            kern_ms.append(eng.render_times())
-        eng.sync()
-        torch.cuda.synchronize()
+    clk = ClockSampler(dev)
+    clk.__enter__()   # sampled over every timed region below (steps, end to end, 2M rebuild)
+    torch.cuda.synchronize()
+    for i in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()   # L2 flush between timed steps (256 MiB > 126 MB L2), outside the events
+        step(args.warmup + i, evs[i])
+        kern_ms.append(eng.render_times())
+    eng.sync()
+    torch.cuda.synchronize()
     launches = eng.counters()["launches"] - l0
     build_ms = [e[0].elapsed_time(e[1]) for e in evs]
     trace_ms = [e[1].elapsed_time(e[2]) for e in evs]
@@ -919,6 +1013,16 @@ def main():
         e2e = {"value": replica_value(rays_per_step, args.steps, et, ws), "unit": "Mrays/s",
                "h2d_bytes_per_step": int(2 * hv.nbytes + hf.nbytes), "d2h_bytes_per_step": int(hfb.nbytes),
                "ms_per_step": et / args.steps}
+    # the headline line also carries the 2M-triangle key-frame rebuild (replayed build graph)
+    rebuild2m = None
+    if prep2m is not None:
+        rb_ms, rb_bytes, rb_n = rebuild_2m_keyframe(prep2m, stream, flush)
+        prep2m[0].cleanup()
+        rb_ms = max_over_ranks(rb_ms, ws)
+        rebuild2m = {"ms": rb_ms, "frame_times": rb_n, "algorithmic_bytes": rb_bytes,
+                     "achieved_gbs": rb_bytes / (rb_ms * 1e-3) / 1e9}
+    torch.cuda.synchronize()
+    clk.__exit__(None, None, None)
 
     if rank != 0:
         eng.cleanup()
@@ -963,13 +1067,21 @@ def main():
         "gpu_launches": launches,
         "e2e": e2e,
     }
+    if rebuild2m:
+        rebuild2m["hbm_frac"] = rebuild2m["achieved_gbs"] / peak
+        line["rebuild_2M_keyframe_ms"] = rebuild2m["ms"]
+        line["rebuild_2M_keyframe"] = dict(rebuild2m, workload="c3 mesh: 2,097,152 triangles, 16 curl-noise key "
+                                           "frames, two-level 1/16 : 2, key-frame interpolation fused, one "
+                                           "replayed build graph per frame time, L2 flushed before each")
     clk_s = clk.summary()
     if clk_s:
         line["clocks"] = clk_s
     if not args.no_cpu and ws == 1:
         try:
-            line["cpu_baseline"] = cpu_baseline(W)
+            keep = {}
+            line["cpu_baseline"] = cpu_baseline(W, keep=keep)
             line["cpu_baseline"].pop("build_ms", None)
+            line["parity"] = gpu_parity(eng, W, keep, d_fb)
         except Exception as ex:   # the CPU leg is a reported baseline only
             line["cpu_baseline"] = {"error": str(ex)}
     print(json.dumps(line), flush=True)

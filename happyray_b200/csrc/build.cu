@@ -313,7 +313,7 @@ void drop_build_graph(hr_ctx* c) {
 // Host orchestration of one build.  With wait, syncs and reports the overflow bits in
 // *ovf_out; without, only enqueues (the descriptor lands in c->desc_pinned when the stream
 // has passed the build).  Returns HR status code (0 = ok).
-static int build_once(hr_ctx* c, int32_t kind, int32_t exact, uint32_t* ovf_out, bool wait) {
+static int build_once_impl(hr_ctx* c, int32_t kind, int32_t exact, uint32_t* ovf_out, bool wait) {
     cudaStream_t s = c->stream;
     GridBuffers& B = c->g;
     const uint32_t ntri = c->ntri;
@@ -460,8 +460,10 @@ static int build_once(hr_ctx* c, int32_t kind, int32_t exact, uint32_t* ovf_out,
         std::memcpy(&cb, &c->frame_coeff, sizeof(cb));
         const int32_t want[3] = {c->frame_a, c->frame_b, (int32_t)cb};
         if (!c->frame_sel_valid || std::memcmp(want, c->frame_sel_host, sizeof(want)) != 0) {
+            c->frame_sel_valid = false;
             k_frame_select<<<1, 1, 0, s>>>(c->frame_sel.as<int4>(), c->frame_a, c->frame_b, c->frame_coeff);
             c->launches += 1;
+            if ((rc = cuda_check(c, cudaGetLastError(), "frame selection"))) return rc;
             std::memcpy(c->frame_sel_host, want, sizeof(want));
             c->frame_sel_valid = true;
         }
@@ -534,6 +536,14 @@ static int build_once(hr_ctx* c, int32_t kind, int32_t exact, uint32_t* ovf_out,
     if (c->host_desc.error) return set_error(c, 1, "triangle index out of range of the uploaded vertices");
     *ovf_out = c->host_desc.overflow;
     return 0;
+}
+
+// A failed build may have stopped anywhere after the frame word's launch, so the word is
+// rewritten by the next build that interpolates.
+static int build_once(hr_ctx* c, int32_t kind, int32_t exact, uint32_t* ovf_out, bool wait) {
+    const int rc = build_once_impl(c, kind, exact, ovf_out, wait);
+    if (rc) c->frame_sel_valid = false;
+    return rc;
 }
 
 // grow what overflowed from the exact sizes the device computed

@@ -16,11 +16,16 @@
 // this lookup, so make that first call before any stream capture.
 //
 // Every call shares the one array and leaves the last call's data in it.  No part of the
-// array is accumulated into: the pair count and the digit totals are rewritten by every
-// call before they are read, and every histogram and ping-pong word a pass reads was
-// written earlier in the same call.  Two calls whose work overlaps on the GPU (two
-// streams, or two host threads) race on the array and corrupt each other's results:
-// serialise them, e.g. on one stream.
+// array is accumulated into, so nothing needs clearing: the pair count is written by
+// every call before its first pass reads it, each pass's digit-total scan rewrites the
+// totals it reads, and every histogram and ping-pong word a pass reads was written
+// earlier in the same call.  Two calls whose work overlaps on the GPU (two streams, or
+// two host threads) race on the array and corrupt each other's results: serialise them,
+// e.g. on one stream.
+//
+// The cached address belongs to the device's current context: after cudaDeviceReset the
+// module is loaded again and the array may move, so this entry point must not be used
+// across a cudaDeviceReset of a device it has already run on.
 #include "hr_internal.h"
 #include "../../include/happyray.h"
 
@@ -51,11 +56,8 @@ constexpr int kMaxDevices = 64;
 std::mutex g_mu;
 uint32_t* g_scratch[kMaxDevices] = {};
 
-// rewrites the words of the scratch that are read before being written in this call
-__global__ void k_noalloc_begin(uint32_t* scratch, uint32_t n) {
-    if (threadIdx.x == 0) scratch[kCtlOff] = n;
-    scratch[kRowOff + threadIdx.x] = 0u;
-}
+// the pair count, which the sort kernels read from device memory
+__global__ void k_noalloc_count(uint32_t* scratch, uint32_t n) { scratch[kCtlOff] = n; }
 
 // device address of the scratch on the current device (looked up once per device)
 cudaError_t scratch_address(uint32_t** out) {
@@ -93,7 +95,7 @@ extern "C" hr_status hr_radix_sort_pairs_noalloc(void* stream, uint32_t* d_keys,
     uint32_t* tk = scratch + kKeysOff;
     uint32_t* tv = scratch + kValsOff;
     uint32_t* hist = scratch + kHistOff;
-    k_noalloc_begin<<<1, 256, 0, s>>>(scratch, n);
+    k_noalloc_count<<<1, 1, 0, s>>>(scratch, n);
     const int passes = (key_bits + 7) / 8;
     cudaError_t e;
     if (passes % 2 == 0) {

@@ -168,8 +168,10 @@ hr_status hr_radix_sort_pairs_device(hr_ctx *ctx, uint32_t *d_keys, uint32_t *d_
  * d_keys / d_values (device pointers of the current device) in place on `stream`
  * (cudaStream_t, NULL = default stream).  Returns HR_ERR_INVALID_ARG if n exceeds
  * HR_NOALLOC_MAX_PAIRS or key_bits is outside 1..32.  The first call on a device looks up
- * the scratch address; make it before any stream capture.  All calls share the one
- * scratch array: calls that overlap on the GPU race, so serialise them. */
+ * the scratch address; make it before any stream capture.  The address is kept for the
+ * process, so do not use this entry point across a cudaDeviceReset of a device it has run
+ * on.  All calls share the one scratch array: calls that overlap on the GPU race, so
+ * serialise them. */
 hr_status hr_radix_sort_pairs_noalloc(void *stream, uint32_t *d_keys, uint32_t *d_values,
                                       uint32_t n, int32_t key_bits);
 

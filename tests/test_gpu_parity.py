@@ -98,6 +98,33 @@ def test_keyframe_lerp_and_rebuild(engine, oracle, small_clusters):
         assert_same_grid(engine.grid_download(), b)
 
 
+def test_replayed_rebuild_reads_new_vertices_and_recaptures_on_new_settings(engine, oracle, small_clusters):
+    """Identical consecutive builds capture the rebuild as a CUDA graph and replay it.  New
+    vertices of the same size go into the same buffers, so the next build is a replay: it
+    must read them.  Changing the densities, the grid kind or the insertion mode must not
+    replay the old graph."""
+    v, f = small_clusters
+    engine.setGridDensities(0.0625, 2.0)
+    engine.upload(v, v, f, 1.0)
+    for _ in range(3):
+        engine.build(GRID_TWO_LEVEL)
+    assert_same_grid(engine.grid_download(), oracle_build(oracle, v, f, GRID_TWO_LEVEL))
+    rng = np.random.default_rng(11)
+    for k in range(2):
+        v2 = (v + rng.normal(0, 0.002, v.shape)).astype(np.float32)
+        engine.upload(v2, v2, f, 1.0)
+        engine.build(GRID_TWO_LEVEL)
+        assert_same_grid(engine.grid_download(), oracle_build(oracle, v2, f, GRID_TWO_LEVEL))
+    for top, leaf in [(0.125, 3.0), (0.125, 3.0), (0.125, 3.0), (0.0625, 2.0)]:
+        engine.setGridDensities(top, leaf)
+        engine.build(GRID_TWO_LEVEL)
+        assert_same_grid(engine.grid_download(), oracle_build(oracle, v2, f, GRID_TWO_LEVEL, top=top, leaf=leaf))
+    engine.set_uniform_density(5.0)
+    for exact in (True, True, True, False, False, False, True):
+        engine.build(GRID_UNIFORM, exact)
+        assert_same_grid(engine.grid_download(), oracle_build(oracle, v2, f, GRID_UNIFORM, exact))
+
+
 def test_upload_coefficient(engine, oracle, small_clusters):
     v, f = small_clusters
     v2 = (v + np.random.default_rng(3).normal(0, 0.005, v.shape)).astype(np.float32)
