@@ -208,7 +208,9 @@ void hr_destroy(hr_ctx* c) {
                       &c->g.prims, &c->g.keys_a, &c->g.vals_a, &c->g.keys_b, &c->g.vals_b, &c->g.block_sums,
                       &c->g.tile_hist, &c->g.row_total, &c->g.top_ranges, &c->g.top_refs, &c->g.leaf_cnt,
                       &c->g.lkeys_a, &c->g.lvals_a, &c->g.lkeys_b, &c->g.lvals_b, &c->g.scan_partials,
-                      &c->g.tri_ranges, &c->g.ref_ranges,
+                      &c->g.tri_ranges, &c->g.ref_ranges, &c->g.cell_cnt, &c->g.cell_cur, &c->g.cell_lp,
+                      &c->g.cell_scan, &c->g.lp_scan, &c->g.tile_sums, &c->g.lp_tiles, &c->g.refs, &c->g.ctl,
+                      &c->g.bounds_part, &c->g.big_list,
                       &c->hit_t, &c->hit_tri, &c->unocc, &c->queue};
     for (DevBuf* b : bufs) free_buf(c, *b);
     cudaStreamSynchronize(c->stream);

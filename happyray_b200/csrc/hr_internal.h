@@ -61,6 +61,17 @@ struct GridBuffers {
     DevBuf scan_partials; // generic scan partial sums
     DevBuf tri_ranges;    // uint4 per triangle: its cell range (16-bit coordinates) and pair count
     DevBuf ref_ranges;    // two-level: uint4 per top-level reference: sub-cell range, first leaf, triangle
+    // per-scene build (build.cu): per-cell counters and tile-local scans, references placed
+    // by cell, control words, and the work list of the cells sorted by one CTA each
+    DevBuf cell_cnt, cell_cur, cell_lp;   // uint32 per cell: references, placement cursor, leaf pairs
+    DevBuf cell_scan;     // uint2 per cell: tile-local exclusive prefix of (references, leaves)
+    DevBuf lp_scan;       // uint32 per cell: tile-local exclusive prefix of leaf pairs
+    DevBuf tile_sums;     // uint2 per cell tile: totals, then exclusive tile offsets
+    DevBuf lp_tiles;      // uint32 per cell tile: leaf-pair totals, then offsets
+    DevBuf refs;          // uniform: uint32 per pair; two-level: uint4 per top-level reference
+    DevBuf ctl;           // build control words (tickets, work counters)
+    DevBuf bounds_part;   // per block of the first kernel: its encoded bounds
+    DevBuf big_list;      // cells sorted by one CTA each
     size_t cap_cells = 0, cap_pairs = 0, cap_top_pairs = 0, cap_leaves = 0, cap_leaf_pairs = 0;
     // largest sizes seen by a completed build: the capacities (which size the count, scan
     // and sort launches) follow them with headroom instead of the first estimates
