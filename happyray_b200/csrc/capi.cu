@@ -52,6 +52,51 @@ int ensure(hr_ctx* c, DevBuf& b, size_t bytes) {
     return 0;
 }
 
+int make_light_set(LightSet* out, uint32_t n, const float* corners, const float* e1, const float* e2,
+                   const float* normals, const float* emissions) {
+    if (n < 1 || n > (uint32_t)kMaxLights || !corners || !e1 || !e2 || !emissions) return 1;
+    std::memset(out, 0, sizeof(LightSet));
+    out->count = n;
+    float run = 0.0f;
+    for (uint32_t k = 0; k < n; ++k) {
+        LightQ& q = out->q[k];
+        for (int i = 0; i < 3; ++i) { q.c[i] = corners[3 * k + i]; q.e1[i] = e1[3 * k + i]; q.e2[i] = e2[3 * k + i]; }
+        q.nc[0] = q.e1[1] * q.e2[2] - q.e1[2] * q.e2[1];
+        q.nc[1] = q.e1[2] * q.e2[0] - q.e1[0] * q.e2[2];
+        q.nc[2] = q.e1[0] * q.e2[1] - q.e1[1] * q.e2[0];
+        const float nn = q.nc[0] * q.nc[0] + q.nc[1] * q.nc[1] + q.nc[2] * q.nc[2];
+        if (!(nn > 0.0f) || !(emissions[k] >= 0.0f)) return 1;
+        q.inv_nn = 1.0f / nn;
+        q.area = sqrtf(nn);
+        q.emission = emissions[k];
+        if (normals) {
+            for (int i = 0; i < 3; ++i) q.n[i] = normals[3 * k + i];
+        } else {   // the side of e2 x e1 = -nc
+            const float inv = 1.0f / q.area;
+            for (int i = 0; i < 3; ++i) q.n[i] = -q.nc[i] * inv;
+        }
+        run = run + q.area * q.emission;
+        out->cdf[k] = run;
+    }
+    return 0;
+}
+
+int set_lights(hr_ctx* c, uint32_t n, const float* corners, const float* e1, const float* e2, const float* normals,
+               const float* emissions) {
+    LightSet ls;
+    if (make_light_set(&ls, n, corners, e1, e2, normals, emissions))
+        return set_error(c, HR_ERR_INVALID_ARG, "set_lights: %u lights (1..%d, non-degenerate, emission >= 0)", n,
+                         kMaxLights);
+    int rc;
+    if ((rc = ensure(c, c->lights_dev, sizeof(LightSet)))) return rc;
+    // stream order: renders enqueued before this call still read the previous collection
+    c->lights = ls;
+    if ((rc = cuda_check(c, cudaMemcpyAsync(c->lights_dev.p, &c->lights, sizeof(LightSet), cudaMemcpyHostToDevice,
+                                            c->stream), "light upload")))
+        return rc;
+    return cuda_check(c, cudaStreamSynchronize(c->stream), "light upload");
+}
+
 // Camera::init (Camera.h:40-64), evaluated on the host in binary32
 void camera_init(Camera* c, const float pos[3], const float fwd[3], const float up[3], float fov, int w, int h) {
     auto norm = [](float v[3]) {
@@ -194,6 +239,11 @@ hr_status hr_create(hr_ctx** out, int32_t device, void* stream) {
     for (auto& e : c->rev) cudaEventCreate(&e);
     if (ensure(c, c->counters, 80)) { hr_destroy(c); return HR_ERR_OUT_OF_MEMORY; }   // 8 counter words, 2 pool words
     cudaMemsetAsync(c->counters.p, 0, 80, c->stream);
+    {   // default light: a 0.2 x 0.2 quad at z = 1 centred over (0.5, 0.5), emitting along -z
+        const float corner[3] = {0.4f, 0.4f, 1.0f}, e1[3] = {0.2f, 0.0f, 0.0f}, e2[3] = {0.0f, 0.2f, 0.0f};
+        const float em = 20.0f;
+        if (set_lights(c, 1, corner, e1, e2, nullptr, &em)) { hr_destroy(c); return HR_ERR_OUT_OF_MEMORY; }
+    }
     *out = c;
     return HR_OK;
 }
@@ -208,9 +258,8 @@ void hr_destroy(hr_ctx* c) {
                       &c->g.prims, &c->g.keys_a, &c->g.vals_a, &c->g.keys_b, &c->g.vals_b, &c->g.block_sums,
                       &c->g.tile_hist, &c->g.row_total, &c->g.top_ranges, &c->g.top_refs, &c->g.leaf_cnt,
                       &c->g.lkeys_a, &c->g.lvals_a, &c->g.lkeys_b, &c->g.lvals_b, &c->g.scan_partials,
-                      &c->g.tri_ranges, &c->g.ref_ranges, &c->g.cell_cnt, &c->g.cell_cur, &c->g.cell_lp,
-                      &c->g.cell_scan, &c->g.lp_scan, &c->g.tile_sums, &c->g.lp_tiles, &c->g.refs, &c->g.ctl,
-                      &c->g.bounds_part, &c->g.big_list,
+                      &c->g.tri_ranges, &c->g.ref_ranges, &c->g.cell_pb, &c->g.cell_pe, &c->g.ctl,
+                      &c->g.big_list, &c->g.seg_words, &c->lights_dev,
                       &c->hit_t, &c->hit_tri, &c->unocc, &c->queue};
     for (DevBuf* b : bufs) free_buf(c, *b);
     cudaStreamSynchronize(c->stream);
@@ -382,9 +431,15 @@ hr_status hr_set_camera(hr_ctx* c, const float pos[3], const float orient[3], co
 
 hr_status hr_set_light(hr_ctx* c, const float corner[3], const float e1[3], const float e2[3], float emission) {
     if (bad(c) || !corner || !e1 || !e2) return HR_ERR_INVALID_ARG;
-    for (int k = 0; k < 3; ++k) { c->light.corner[k] = corner[k]; c->light.e1[k] = e1[k]; c->light.e2[k] = e2[k]; }
-    c->light.emission = emission;
-    return HR_OK;
+    DeviceGuard dg(c->device);
+    return (hr_status)set_lights(c, 1, corner, e1, e2, nullptr, &emission);
+}
+
+hr_status hr_set_lights(hr_ctx* c, uint32_t n, const float* corners, const float* edge1s, const float* edge2s,
+                        const float* normals, const float* emissions) {
+    if (bad(c)) return HR_ERR_INVALID_ARG;
+    DeviceGuard dg(c->device);
+    return (hr_status)set_lights(c, n, corners, edge1s, edge2s, normals, emissions);
 }
 
 hr_status hr_set_integrator(hr_ctx* c, int32_t ao_samples, float ao_radius, int32_t pt_bounces, float albedo,

@@ -47,6 +47,25 @@ struct GridDesc {
     uint32_t pad1;
 };
 
+// Area lights of the path tracer (AreaLightSource, LightSource.hpp:38-95): parallelogram
+// c + s e1 + t e2 (s, t in [0, 1]) emitting radiance `emission` towards the side of its unit
+// normal n, with the values formed once: nc = e1 x e2, inv_nn = 1 / |nc|^2, area = |nc|.
+// A collection (AreaLightSourceCollection, LightSource.hpp:102-198) picks light k for a
+// sample with probability w_k / W, w_k = area_k * emission_k, from the inclusive running
+// sum cdf of the weights; it is built on the host (make_light_set) and read by the kernels
+// from device memory.
+constexpr int kMaxLights = 64;
+struct LightQ {
+    float c[3], e1[3], e2[3], n[3], nc[3];
+    float inv_nn, area, emission;
+};
+struct LightSet {
+    uint32_t count;
+    uint32_t pad[3];
+    float cdf[kMaxLights];
+    LightQ q[kMaxLights];
+};
+
 __host__ __device__ __forceinline__ float hmin(float a, float b) { return (a != a) ? b : ((b < a) ? b : a); }
 __host__ __device__ __forceinline__ float hmax(float a, float b) { return (a != a) ? b : ((b > a) ? b : a); }
 __device__ __forceinline__ int32_t f2i(float x) { return __float2int_rz(x); }  // saturating, NaN -> 0

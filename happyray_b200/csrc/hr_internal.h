@@ -27,12 +27,6 @@ struct Camera {
     int32_t w = 0, h = 0;
 };
 
-struct Light {
-    float corner[3] = {0.4f, 0.4f, 1.0f};
-    float e1[3] = {0.2f, 0.0f, 0.0f};
-    float e2[3] = {0.0f, 0.2f, 0.0f};
-    float emission = 20.0f;
-};
 
 struct IntegratorParams {
     int32_t ao_samples = 8;
@@ -61,17 +55,12 @@ struct GridBuffers {
     DevBuf scan_partials; // generic scan partial sums
     DevBuf tri_ranges;    // uint4 per triangle: its cell range (16-bit coordinates) and pair count
     DevBuf ref_ranges;    // two-level: uint4 per top-level reference: sub-cell range, first leaf, triangle
-    // per-scene build (build.cu): per-cell counters and tile-local scans, references placed
-    // by cell, control words, and the work list of the cells sorted by one CTA each
-    DevBuf cell_cnt, cell_cur, cell_lp;   // uint32 per cell: references, placement cursor, leaf pairs
-    DevBuf cell_scan;     // uint2 per cell: tile-local exclusive prefix of (references, leaves)
-    DevBuf lp_scan;       // uint32 per cell: tile-local exclusive prefix of leaf pairs
-    DevBuf tile_sums;     // uint2 per cell tile: totals, then exclusive tile offsets
-    DevBuf lp_tiles;      // uint32 per cell tile: leaf-pair totals, then offsets
-    DevBuf refs;          // uniform: uint32 per pair; two-level: uint4 per top-level reference
-    DevBuf ctl;           // build control words (tickets, work counters)
-    DevBuf bounds_part;   // per block of the first kernel: its encoded bounds
-    DevBuf big_list;      // cells sorted by one CTA each
+    // per-scene leaf stage (build.cu): each top cell's segment of leaf pairs, the cells
+    // sorted by one CTA each, and the global scratch of segments too large for shared memory
+    DevBuf cell_pb, cell_pe;   // uint32 per top cell: its leaf pairs [pb, pe)
+    DevBuf ctl;           // build control words (work list length and counter)
+    DevBuf big_list;      // top cells sorted by one CTA each
+    DevBuf seg_words;     // 2 x 64-bit words per leaf pair
     size_t cap_cells = 0, cap_pairs = 0, cap_top_pairs = 0, cap_leaves = 0, cap_leaf_pairs = 0;
     // largest sizes seen by a completed build: the capacities (which size the count, scan
     // and sort launches) follow them with headroom instead of the first estimates
@@ -131,7 +120,8 @@ struct hr_ctx {
     // camera / integrators
     hr::Camera cam;
     bool have_camera = false;
-    hr::Light light;
+    hr::LightSet lights;         // host copy of the light collection (default: one 0.2 x 0.2 quad at z = 1)
+    hr::DevBuf lights_dev;       // its device copy, read by the path tracer
     hr::IntegratorParams ip;
     hr::DevBuf fb;               // float3 framebuffer (device)
     hr::DevBuf out_id, out_t, out_u, out_v, ray_in;  // ray-query staging
@@ -150,6 +140,14 @@ int cuda_check(hr_ctx* c, cudaError_t e, const char* what);
 int ensure(hr_ctx* c, DevBuf& b, size_t bytes);
 // xyz (3 floats per vertex, device) -> float4 with w = 0
 void expand_xyz(const float* xyz, float4* out, size_t n, int grid, cudaStream_t s);
+// Builds a light collection of n lights (LightSource.hpp:38-198) in binary32 on the host:
+// corners, edges and normals are xyz triples; normals may be null (then n = unit e2 x e1).
+// Returns 0, or 1 when n is outside 1..kMaxLights or a light is degenerate.
+int make_light_set(LightSet* out, uint32_t n, const float* corners, const float* e1, const float* e2,
+                   const float* normals, const float* emissions);
+// Makes `n` lights the context's collection (host and device copies).
+int set_lights(hr_ctx* c, uint32_t n, const float* corners, const float* e1, const float* e2, const float* normals,
+               const float* emissions);
 // Camera::init (Camera.h:40-64) in binary32 on the host
 void camera_init(Camera* c, const float pos[3], const float fwd[3], const float up[3], float fov, int w, int h);
 
@@ -210,8 +208,7 @@ struct Job {
     float* out_v;
     float cam_pos[3], cam_tl[3], cam_sx[3], cam_sy[3];
     int32_t w, h;                    // render jobs: image size; ray jobs: w = ray count
-    float light_c[3], light_e1[3], light_e2[3];
-    float light_emission;
+    const LightSet* lights;          // path jobs: the light collection (device memory)
     uint32_t ntri;
     int32_t kind;                    // kTwoLevel
     int32_t mode;                    // kJob*

@@ -550,10 +550,19 @@ hr_status hr_scene_upload(hr_ctx* ctx, const hr_scene* sc) {
     if (sc->has_camera && sc->w > 0 && sc->h > 0 &&
         (st = hr_set_camera(ctx, sc->pos, sc->orient, sc->up, sc->fov, sc->w, sc->h)) != HR_OK)
         return st;
-    if (!sc->lights.empty()) {
-        const hr_scene::QuadLight& L = sc->lights[0];
-        const float em = (L.intensity[0] + L.intensity[1] + L.intensity[2]) / 3.0f;
-        if ((st = hr_set_light(ctx, L.position, L.edge1, L.edge2, em)) != HR_OK) return st;
+    if (!sc->lights.empty()) {   // every light, emission = mean intensity (scalar radiance)
+        const size_t n = std::min(sc->lights.size(), (size_t)64);
+        std::vector<float> pos(3 * n), e1(3 * n), e2(3 * n), nrm(3 * n), em(n);
+        for (size_t k = 0; k < n; ++k) {
+            const hr_scene::QuadLight& L = sc->lights[k];
+            for (int i = 0; i < 3; ++i) {
+                pos[3 * k + i] = L.position[i]; e1[3 * k + i] = L.edge1[i]; e2[3 * k + i] = L.edge2[i];
+                nrm[3 * k + i] = L.normal[i];
+            }
+            em[k] = (L.intensity[0] + L.intensity[1] + L.intensity[2]) / 3.0f;
+        }
+        if ((st = hr_set_lights(ctx, (uint32_t)n, pos.data(), e1.data(), e2.data(), nrm.data(), em.data())) != HR_OK)
+            return st;
     }
     return hr_set_frame_time(ctx, 0.0f, 0.0f);
 }

@@ -92,10 +92,7 @@ __device__ __forceinline__ void load_tile_ctx(TileCtx& T, const Job* __restrict_
     T.alpha = alpha;
     T.off = 0.01f * alpha;
     if (J->mode == kJobPath) {
-        LightP l;
-        for (int q = 0; q < 3; ++q) { l.c[q] = J->light_c[q]; l.e1[q] = J->light_e1[q]; l.e2[q] = J->light_e2[q]; }
-        l.emission = J->light_emission;
-        T.pk = pt_consts(T.g, l, J->bounces, J->albedo, J->eps_frac);
+        T.pk = pt_consts(T.g, J->lights, J->bounces, J->albedo, J->eps_frac);
     }
 }
 

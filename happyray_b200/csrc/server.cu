@@ -188,10 +188,7 @@ void fill_render_job(Job& J, const SrvScene& X, const SrvReq& R) {
     J.eps_frac = c->ip.ray_eps_frac;
     J.bounces = c->ip.pt_bounces;
     J.albedo = c->ip.albedo;
-    for (int q = 0; q < 3; ++q) {
-        J.light_c[q] = c->light.corner[q]; J.light_e1[q] = c->light.e1[q]; J.light_e2[q] = c->light.e2[q];
-    }
-    J.light_emission = c->light.emission;
+    J.lights = c->lights_dev.as<LightSet>();
     if (R.r.kind == HR_REQUEST_RAYS) {
         float* base = static_cast<float*>(R.dbuf);
         const size_t n = R.r.num_rays;

@@ -421,13 +421,13 @@ __global__ void k_ao_finish(const uint32_t* __restrict__ queue, const uint32_t* 
 // path ends takes the next pixel at once (path_refill / path_step / path_retire), so lanes
 // do not idle through the bounces of their warp's longest path.
 template <int KIND, bool STATS>
-__global__ __launch_bounds__(kTT, HR_PT_MIN_BLOCKS) void k_render_pt(Scene s, Cam cam, LightP l, int32_t bounces,
+__global__ __launch_bounds__(kTT, HR_PT_MIN_BLOCKS) void k_render_pt(Scene s, Cam cam, const LightSet* __restrict__ ls, int32_t bounces,
                                                                   float albedo, float eps_frac, uint64_t seed,
                                                                   int32_t image_id, float* __restrict__ fb,
                                                                   unsigned long long* counter, uint32_t* work) {
     const G g = load_g(s.desc);
     gate_scene(s);
-    const PtConsts k = pt_consts(g, l, bounces, albedo, eps_frac);
+    const PtConsts k = pt_consts(g, ls, bounces, albedo, eps_frac);
     const uint32_t ntiles = tile_slots(cam) >> 5;
     const uint32_t lane = threadIdx.x & 31u;
 #if HR_PT_SMEM_STATE
@@ -569,9 +569,7 @@ int launch_render(hr_ctx* c, int32_t mode, int32_t image_id, float* d_fb) {
         break;
     case 1:
     case 2: {
-        LightP l;
-        for (int i = 0; i < 3; ++i) { l.c[i] = c->light.corner[i]; l.e1[i] = c->light.e1[i]; l.e2[i] = c->light.e2[i]; }
-        l.emission = c->light.emission;
+        const LightSet* l = c->lights_dev.as<LightSet>();
         uint32_t* work = reinterpret_cast<uint32_t*>(ctr + 7);
         int rc;
         if ((rc = cuda_check(c, cudaMemsetAsync(work, 0, sizeof(uint32_t), strm), "tile counter reset"))) return rc;

@@ -384,12 +384,6 @@ struct Cam {
     int32_t w, h;
 };
 
-// quad area light: corner, two edges, emitted radiance (LightSource.hpp:38-203)
-struct LightP {
-    float c[3], e1[3], e2[3];
-    float emission;
-};
-
 // pixel-centre ray, normalised (Camera.h:66-69 getDirection)
 __device__ __forceinline__ f3 primary_dir(const Cam& c, uint32_t pix) {
     const float px = (float)(pix % (uint32_t)c.w) + 0.5f;
@@ -458,27 +452,50 @@ __device__ __forceinline__ void add_rays(unsigned long long* counter, bool secon
 // warp-uniform bound of a 1-D grid-stride loop over n items
 __device__ __forceinline__ uint32_t round32(uint32_t n) { return (n + 31u) & ~31u; }
 
-// constants of the path tracer for one grid and light
+// constants of the path tracer for one grid and light collection
 struct PtConsts {
-    f3 lc, le1, le2;
-    float emission, larea, a_pi, albedo, ray_eps;
+    const LightSet* ls;   // device memory
+    uint32_t nlights;
+    float a_pi, albedo, ray_eps;
     int32_t bounces;
 };
-__device__ __forceinline__ PtConsts pt_consts(const G& g, const LightP& l, int32_t bounces, float albedo,
+__device__ __forceinline__ PtConsts pt_consts(const G& g, const LightSet* ls, int32_t bounces, float albedo,
                                               float eps_frac) {
     PtConsts k;
     const f3 dd = mk(g.bmax[0] - g.bmin[0], g.bmax[1] - g.bmin[1], g.bmax[2] - g.bmin[2]);
     k.ray_eps = eps_frac * sqrtf(dot(dd, dd));
-    k.lc = mk(l.c[0], l.c[1], l.c[2]);
-    k.le1 = mk(l.e1[0], l.e1[1], l.e1[2]);
-    k.le2 = mk(l.e2[0], l.e2[1], l.e2[2]);
-    const f3 lcr = cross(k.le1, k.le2);
-    k.larea = sqrtf(dot(lcr, lcr));
+    k.ls = ls;
+    k.nlights = __ldg(&ls->count);
     k.a_pi = albedo * 0.318309886f;
     k.albedo = albedo;
-    k.emission = l.emission;
     k.bounces = bounces;
     return k;
+}
+
+__device__ __forceinline__ f3 ldf3(const float* p) { return mk(__ldg(p), __ldg(p + 1), __ldg(p + 2)); }
+
+// distance along (o, d) to the emitting side of light q, or -1 when the ray misses it
+__device__ __forceinline__ float light_hit(const LightQ* q, f3 o, f3 d) {
+    const f3 n = ldf3(q->n);
+    const float den = dot(d, n);
+    if (!(den < 0.0f)) return -1.0f;
+    const f3 c = ldf3(q->c);
+    const float tl = dot(sub(c, o), n) / den;
+    const f3 r = sub(mk(o.x + tl * d.x, o.y + tl * d.y, o.z + tl * d.z), c);
+    const f3 nc = ldf3(q->nc);
+    const float inv_nn = __ldg(&q->inv_nn);
+    const float a = dot(cross(r, ldf3(q->e2)), nc) * inv_nn;
+    const float b = dot(cross(ldf3(q->e1), r), nc) * inv_nn;
+    return (a >= 0.0f && a <= 1.0f && b >= 0.0f && b <= 1.0f) ? tl : -1.0f;
+}
+
+// AreaLightSourceCollection::getLight (LightSource.hpp:114-126): the first light whose
+// normalised running weight exceeds u, else the last
+__device__ __forceinline__ uint32_t light_pick(const LightSet* ls, uint32_t n, float u) {
+    const float total = __ldg(&ls->cdf[n - 1]);
+    for (uint32_t i = 0; i + 1 < n; ++i)
+        if (u < __ldg(&ls->cdf[i]) / total) return i;
+    return n - 1;
 }
 
 struct PtCounts {
@@ -544,29 +561,41 @@ __device__ __forceinline__ bool path_step(const Scene& s, const G& g, const PtCo
     n.rays += 1;
     n.cells += h.cells;
     n.tests += h.tests;
-    if (p.bounce == 0 && p.d.z > 0.0f) {
-        const float tl = (k.lc.z - p.o.z) / p.d.z;
-        const float px = p.o.x + tl * p.d.x, py = p.o.y + tl * p.d.y;
-        const float fx = (px - k.lc.x) / k.le1.x, fy = (py - k.lc.y) / k.le2.y;
-        if (tl > kIsectEps && tl < h.t && fx >= 0.0f && fx <= 1.0f && fy >= 0.0f && fy <= 1.0f) {
-            p.L = p.L + k.emission;
+    if (p.bounce == 0) {
+        // camera ray against the emitters: the nearest one in front of the hit ends the path
+        float best = h.t;
+        int32_t lit = -1;
+        for (uint32_t j = 0; j < k.nlights; ++j) {
+            const float tl = light_hit(&k.ls->q[j], p.o, p.d);
+            if (tl > kIsectEps && tl < best) { best = tl; lit = (int32_t)j; }
+        }
+        if (lit >= 0) {
+            p.L = p.L + __ldg(&k.ls->q[lit].emission);
             return false;
         }
     }
     if (!h.hit) return false;
     const f3 q = mk(p.o.x + h.t * p.d.x, p.o.y + h.t * p.d.y, p.o.z + h.t * p.d.z);
     const f3 nrm = face_normal(s, h.tri, p.d);
+    // next-event estimation: one light of the collection (by weight when there are several;
+    // its radiance divided by the probability of picking it), one point on it
+    uint32_t li = 0;
+    if (k.nlights > 1) li = light_pick(k.ls, k.nlights, pcg_float(p.rng));
+    const LightQ* lq = &k.ls->q[li];
+    const f3 lc = ldf3(lq->c), le1 = ldf3(lq->e1), le2 = ldf3(lq->e2);
     const float u1 = pcg_float(p.rng), u2 = pcg_float(p.rng);
-    const f3 lp = mk(k.lc.x + u1 * k.le1.x + u2 * k.le2.x, k.lc.y + u1 * k.le1.y + u2 * k.le2.y,
-                     k.lc.z + u1 * k.le1.z + u2 * k.le2.z);
+    const f3 lp = mk(lc.x + u1 * le1.x + u2 * le2.x, lc.y + u1 * le1.y + u2 * le2.y, lc.z + u1 * le1.z + u2 * le2.z);
     f3 wi = sub(lp, q);
     const float dist2 = dot(wi, wi);
     const float dist = sqrtf(dist2);
     wi = mulf(wi, 1.0f / dist);
     const float cos_s = dot(nrm, wi);
-    const float cos_l = wi.z;
+    const float cos_l = -dot(ldf3(lq->n), wi);
     const bool shadow = cos_s > 0.0f && cos_l > 0.0f;
-    if (shadow) p.c = p.beta * k.a_pi * k.emission * cos_s * cos_l * k.larea / dist2;
+    if (shadow) {
+        p.c = p.beta * k.a_pi * __ldg(&lq->emission) * cos_s * cos_l * __ldg(&lq->area) / dist2;
+        if (k.nlights > 1) p.c = p.c * (__ldg(&k.ls->cdf[k.nlights - 1]) / (__ldg(&lq->area) * __ldg(&lq->emission)));
+    }
     p.beta = p.beta * k.albedo;
     const float u3 = pcg_float(p.rng), u4 = pcg_float(p.rng);
     const f3 nd = cosine_dir(nrm, u3, u4);

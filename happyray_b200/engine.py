@@ -161,8 +161,21 @@ class Engine:
                   "hr_set_camera")
         self.res = (res_x, res_y)
 
-    def setLights(self, corner, edge1, edge2, emission: float):
-        self._chk(self.L.hr_set_light(self.ctx, _f3(corner), _f3(edge1), _f3(edge2), emission), "hr_set_light")
+    def setLights(self, corner, edge1, edge2, emission, normals=None):
+        """One light (corner, edge1, edge2: xyz; emission: float), or a collection: arrays of
+        shape (n, 3) and n emissions, optional (n, 3) unit normals (RTEngine::setLights)."""
+        c = np.asarray(corner, np.float32)
+        if c.ndim == 1 and normals is None:
+            self._chk(self.L.hr_set_light(self.ctx, _f3(corner), _f3(edge1), _f3(edge2), float(emission)),
+                      "hr_set_light")
+            return
+        c = np.ascontiguousarray(c.reshape(-1, 3))
+        e1 = np.ascontiguousarray(np.asarray(edge1, np.float32).reshape(-1, 3))
+        e2 = np.ascontiguousarray(np.asarray(edge2, np.float32).reshape(-1, 3))
+        em = np.ascontiguousarray(np.asarray(emission, np.float32).reshape(-1))
+        nr = None if normals is None else np.ascontiguousarray(np.asarray(normals, np.float32).reshape(-1, 3))
+        self._chk(self.L.hr_set_lights(self.ctx, c.shape[0], _ptr(c), _ptr(e1), _ptr(e2), _ptr(nr), _ptr(em)),
+                  "hr_set_lights")
 
     def set_integrator(self, ao_samples=8, ao_radius=-0.1, pt_bounces=4, albedo=0.7, seed=0x853c49e6748fea9b):
         self._chk(self.L.hr_set_integrator(self.ctx, ao_samples, ao_radius, pt_bounces, albedo, seed),

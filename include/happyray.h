@@ -105,9 +105,22 @@ hr_status hr_download_vertices(hr_ctx *ctx, float *xyzw);
 /* RTEngine::setCamera (RTEngine.h:49-55, Camera.h:40-64) */
 hr_status hr_set_camera(hr_ctx *ctx, const float position[3], const float orientation[3],
                         const float up[3], float fov_deg, int32_t res_x, int32_t res_y);
-/* RTEngine::setLights (RTEngine.h:57): one quad light, corner + edges, emits along -z */
+/* RTEngine::setLights (RTEngine.h:57, RTEngine.cu:393-396) for one light: a parallelogram
+ * corner + s * edge1 + t * edge2 (s, t in [0, 1]) emitting radiance `emission` towards the
+ * side of edge2 x edge1 (-z for edges along +x and +y).  Replaces the collection. */
 hr_status hr_set_light(hr_ctx *ctx, const float corner[3], const float edge1[3],
                        const float edge2[3], float emission);
+/* RTEngine::setLights with an AreaLightSourceCollection (LightSource.hpp:102-198): n lights
+ * (1..64), corner / edge / normal xyz triples and one scalar radiance each (host arrays).
+ * normals may be NULL (then each light emits towards its edge2 x edge1); a given normal is
+ * used as is (unit length, the emitting side).  The path tracer picks a light per
+ * next-event sample with probability area * emission / total, by the collection's
+ * inclusive running sum of those weights (getLight, LightSource.hpp:114-126, CDF built by
+ * InclusiveSum, Scan.cu:81-100), and divides its contribution by that probability.
+ * Takes effect for renders enqueued after it returns.  HR_ERR_INVALID_ARG for n outside
+ * 1..64, a degenerate light or a negative emission. */
+hr_status hr_set_lights(hr_ctx *ctx, uint32_t n, const float *corners, const float *edge1s,
+                        const float *edge2s, const float *normals, const float *emissions);
 /* Integrator parameters: AO samples per hit and radius (fraction of the bounds diagonal
  * if ao_radius < 0, absolute otherwise), PT extension rays, Lambertian albedo, seed. */
 hr_status hr_set_integrator(hr_ctx *ctx, int32_t ao_samples, float ao_radius,
@@ -383,7 +396,8 @@ const uint32_t *hr_scene_indices(const hr_scene *scene);
 hr_status hr_scene_get_light(const hr_scene *scene, uint32_t light, float position[3], float edge1[3],
                              float edge2[3], float normal[3], float intensity[3]);
 /* hr_set_keyframes with the scene's frames; its camera (hr_set_camera) if it has one; its
- * first light (hr_set_light: corner = position, emission = mean intensity) if any. */
+ * lights (hr_set_lights: corner = position, the file's normal, emission = mean intensity;
+ * the first 64) if any. */
 hr_status hr_scene_upload(hr_ctx *ctx, const hr_scene *scene);
 
 hr_status hr_rays_file_count(const char *path, uint32_t *num_rays);

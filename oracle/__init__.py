@@ -55,7 +55,7 @@ class Camera(C.Structure):
 
 class Light(C.Structure):
     _fields_ = [("corner", C.c_float * 3), ("e1", C.c_float * 3), ("e2", C.c_float * 3),
-                ("emission", C.c_float)]
+                ("normal", C.c_float * 3), ("emission", C.c_float)]
 
 
 def build():
@@ -92,7 +92,7 @@ def lib():
                 "orc_trace_primary": (None, [C.POINTER(Scene), C.POINTER(Camera), P, P, P, P, P]),
                 "orc_occluded": (None, [C.POINTER(Scene), P, P, P, U32, P]),
                 "orc_render_ao": (None, [C.POINTER(Scene), C.POINTER(Camera), I32, F, U64, I32, P, U32, P]),
-                "orc_render_pt": (None, [C.POINTER(Scene), C.POINTER(Camera), C.POINTER(Light), I32, F, F, U64, I32, P, U32, P]),
+                "orc_render_pt": (None, [C.POINTER(Scene), C.POINTER(Camera), C.POINTER(Light), I32, I32, F, F, U64, I32, P, U32, P]),
                 "orc_brute_f64": (None, [P, P, U32, P, P, U32, P, P, P, P, P]),
                 "orc_sincos2pi": (None, [F, C.POINTER(F), C.POINTER(F)]),
                 "orc_pcg32_first_floats": (F, [U64, U64, I32, P]),
@@ -284,22 +284,27 @@ def render_ao(b: Built, cam: Camera, spp: int, alpha: float, seed: int, image_id
     return fb, int(counts[0])
 
 
-def render_pt(b: Built, cam: Camera, light: Light, bounces: int, albedo: float, ray_eps: float, seed: int,
+def render_pt(b: Built, cam: Camera, light, bounces: int, albedo: float, ray_eps: float, seed: int,
               image_id: int = 0, fb=None, pixel_stride: int = 1):
+    """Path-traced frame; `light` is one Light or a sequence of them (a light collection)."""
+    lights = [light] if isinstance(light, Light) else list(light)
+    arr = (Light * len(lights))(*lights)
     n = cam.w * cam.h
     fb = np.zeros(n, np.float32) if fb is None else np.ascontiguousarray(fb, np.float32)
     counts = np.zeros(1, np.uint64)
     s = b.scene()
-    lib().orc_render_pt(C.byref(s), C.byref(cam), C.byref(light), bounces, albedo, ray_eps, seed, image_id,
+    lib().orc_render_pt(C.byref(s), C.byref(cam), arr, len(lights), bounces, albedo, ray_eps, seed, image_id,
                         _p(fb), pixel_stride, _p(counts))
     return fb, int(counts[0])
 
 
-def make_light(corner=(0.4, 0.4, 1.0), e1=(0.2, 0.0, 0.0), e2=(0.0, 0.2, 0.0), emission=20.0) -> Light:
+def make_light(corner=(0.4, 0.4, 1.0), e1=(0.2, 0.0, 0.0), e2=(0.0, 0.2, 0.0), emission=20.0,
+               normal=(0.0, 0.0, -1.0)) -> Light:
     l = Light()
     l.corner = _f3(corner)
     l.e1 = _f3(e1)
     l.e2 = _f3(e2)
+    l.normal = _f3(normal)
     l.emission = emission
     return l
 

@@ -815,15 +815,58 @@ void orc_render_ao(const orc_scene *s, const orc_camera *c, int32_t spp, float a
 /* a20: path tracing with next-event estimation towards one quad light (PathTracer.h
  * pathTrace 41-372 / tracePath 374-747 structure, configured as a fixed number of
  * extension rays, Lambertian albedo, no Russian roulette). */
-void orc_render_pt(const orc_scene *s, const orc_camera *c, const orc_light *l,
+/* A light of the collection with the values the path tracer forms once: the edge cross
+ * product nc, 1 / |nc|^2 (for the parallelogram coordinates), area |nc|, sampling weight
+ * area * emission.  cdf: inclusive running sum of the weights (LightSource.hpp:185-190). */
+typedef struct { f3 c, e1, e2, nrm, nc; float inv_nn, emission, area, w; } light_q;
+
+static void lights_prep(const orc_light *l, int32_t n, light_q *q, float *cdf) {
+    float run = 0.0f;
+    for (int32_t k = 0; k < n; ++k) {
+        q[k].c = ld3(l[k].corner);
+        q[k].e1 = ld3(l[k].e1);
+        q[k].e2 = ld3(l[k].e2);
+        q[k].nrm = ld3(l[k].normal);
+        q[k].nc = cross(q[k].e1, q[k].e2);
+        const float nn = dot(q[k].nc, q[k].nc);
+        q[k].inv_nn = 1.0f / nn;
+        q[k].area = sqrtf(nn);
+        q[k].emission = l[k].emission;
+        q[k].w = q[k].area * q[k].emission;
+        run = run + q[k].w;
+        cdf[k] = run;
+    }
+}
+
+/* AreaLightSourceCollection::getLight (LightSource.hpp:114-126): the first light whose
+ * normalised running weight exceeds u, else the last */
+static inline int32_t light_pick(const float *cdf, int32_t n, float u) {
+    for (int32_t i = 0; i < n - 1; ++i)
+        if (u < cdf[i] / cdf[n - 1]) return i;
+    return n - 1;
+}
+
+/* distance along (o, d) to the emitting side of parallelogram light q, or -1 */
+static inline float light_hit(const light_q *q, f3 o, f3 d) {
+    const float den = dot(d, q->nrm);
+    if (!(den < 0.0f)) return -1.0f;
+    const float tl = dot(sub(q->c, o), q->nrm) / den;
+    const f3 r = sub(mk(o.x + tl * d.x, o.y + tl * d.y, o.z + tl * d.z), q->c);
+    const float a = dot(cross(r, q->e2), q->nc) * q->inv_nn;
+    const float b = dot(cross(q->e1, r), q->nc) * q->inv_nn;
+    return (a >= 0.0f && a <= 1.0f && b >= 0.0f && b <= 1.0f) ? tl : -1.0f;
+}
+
+void orc_render_pt(const orc_scene *s, const orc_camera *c, const orc_light *l, int32_t nlights,
                    int32_t bounces, float albedo, float ray_eps, uint64_t seed,
                    int32_t image_id, float *fb, uint32_t pixel_stride, uint64_t *counts) {
     uint32_t n = (uint32_t)c->w * (uint32_t)c->h;
     if (pixel_stride == 0) pixel_stride = 1;
+    if (nlights < 1 || nlights > ORC_MAX_LIGHTS) return;
     uint64_t rays = 0;
-    const f3 lc = ld3(l->corner), le1 = ld3(l->e1), le2 = ld3(l->e2);
-    const f3 lcr = cross(le1, le2);
-    const float larea = sqrtf(dot(lcr, lcr));
+    light_q lq[ORC_MAX_LIGHTS];
+    float cdf[ORC_MAX_LIGHTS];
+    lights_prep(l, nlights, lq, cdf);
     const float a_pi = albedo * 0.318309886f;
 #pragma omp parallel for schedule(dynamic, 64) reduction(+ : rays)
     for (long long ii = 0; ii < (long long)n; ii += pixel_stride) {
@@ -837,34 +880,49 @@ void orc_render_pt(const orc_scene *s, const orc_camera *c, const orc_light *l,
             hitrec h;
             trace_one(s, o, d, FLT_MAX, 0, &h);
             rays += 1;
-            if (bounce == 0 && d.z > 0.0f) {
-                /* camera ray against the emitter (plane z = corner.z, facing -z) */
-                float tl = (lc.z - o.z) / d.z;
-                float px = o.x + tl * d.x, py = o.y + tl * d.y;
-                float fx = (px - lc.x) / le1.x, fy = (py - lc.y) / le2.y;
-                if (tl > ORC_ISECT_EPS && tl < h.t && fx >= 0.0f && fx <= 1.0f && fy >= 0.0f && fy <= 1.0f) {
-                    L = L + l->emission;
+            if (bounce == 0) {
+                /* camera ray against the emitters: the nearest one in front of the hit ends the path */
+                float best = h.t;
+                int32_t hit_light = -1;
+                for (int32_t k = 0; k < nlights; ++k) {
+                    const float tl = light_hit(&lq[k], o, d);
+                    if (tl > ORC_ISECT_EPS && tl < best) { best = tl; hit_light = k; }
+                }
+                if (hit_light >= 0) {
+                    L = L + lq[hit_light].emission;
                     break;
                 }
             }
             if (!h.hit) break;
             f3 p = mk(o.x + h.t * d.x, o.y + h.t * d.y, o.z + h.t * d.z);
             f3 nrm = face_normal(s, h.tri, d);
-            /* next-event estimation */
+            /* next-event estimation: one light of the collection (by weight when there are
+             * several; its radiance divided by the probability of picking it), one point on it */
+            int32_t k = 0;
+            float scale = 1.0f;
+            if (nlights > 1) {
+                k = light_pick(cdf, nlights, pcg32_float(&rng));
+                scale = cdf[nlights - 1] / lq[k].w;
+            }
+            const light_q *q = &lq[k];
             float u1 = pcg32_float(&rng), u2 = pcg32_float(&rng);
-            f3 lp = mk(lc.x + u1 * le1.x + u2 * le2.x, lc.y + u1 * le1.y + u2 * le2.y,
-                       lc.z + u1 * le1.z + u2 * le2.z);
+            f3 lp = mk(q->c.x + u1 * q->e1.x + u2 * q->e2.x, q->c.y + u1 * q->e1.y + u2 * q->e2.y,
+                       q->c.z + u1 * q->e1.z + u2 * q->e2.z);
             f3 wi = sub(lp, p);
             float dist2 = dot(wi, wi);
             float dist = sqrtf(dist2);
             wi = mulf(wi, 1.0f / dist);
-            float cos_s = dot(nrm, wi), cos_l = wi.z;
+            float cos_s = dot(nrm, wi), cos_l = -dot(q->nrm, wi);
             if (cos_s > 0.0f && cos_l > 0.0f) {
                 f3 so = mk(p.x + ray_eps * wi.x, p.y + ray_eps * wi.y, p.z + ray_eps * wi.z);
                 hitrec hs;
                 trace_one(s, so, wi, dist - ray_eps, 1, &hs);
                 rays += 1;
-                if (!hs.hit) L = L + beta * a_pi * l->emission * cos_s * cos_l * larea / dist2;
+                if (!hs.hit) {
+                    float cl = beta * a_pi * q->emission * cos_s * cos_l * q->area / dist2;
+                    if (nlights > 1) cl = cl * scale;
+                    L = L + cl;
+                }
             }
             /* Lambertian bounce: f * cos / pdf = albedo */
             beta = beta * albedo;

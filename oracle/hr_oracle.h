@@ -62,9 +62,14 @@ typedef struct {
     int32_t w, h;
 } orc_camera;
 
-/* Area light for the path tracer: corner + two edges, emits towards -z. */
+/* Area lights for the path tracer (AreaLightSource, LightSource.hpp:38-95): a parallelogram
+ * corner + s*e1 + t*e2 (s, t in [0, 1]) emitting radiance `emission` towards the side its
+ * unit normal points to.  A collection of lights (AreaLightSourceCollection,
+ * LightSource.hpp:102-198) picks light k for a sample with probability w_k / W, w_k =
+ * area_k * emission_k, from the inclusive running sum of the weights. */
+#define ORC_MAX_LIGHTS 64
 typedef struct {
-    float corner[3], e1[3], e2[3];
+    float corner[3], e1[3], e2[3], normal[3];
     float emission;
 } orc_light;
 
@@ -111,7 +116,7 @@ void orc_render_ao(const orc_scene *s, const orc_camera *c, int32_t spp, float a
                    uint64_t seed, int32_t image_id, float *fb, uint32_t pixel_stride,
                    uint64_t *counts);
 /* PT: scalar radiance per pixel, `bounces` extension rays, NEE per hit. */
-void orc_render_pt(const orc_scene *s, const orc_camera *c, const orc_light *l,
+void orc_render_pt(const orc_scene *s, const orc_camera *c, const orc_light *l, int32_t nlights,
                    int32_t bounces, float albedo, float ray_eps, uint64_t seed,
                    int32_t image_id, float *fb, uint32_t pixel_stride, uint64_t *counts);
 

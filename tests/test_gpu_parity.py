@@ -244,6 +244,48 @@ def test_render_pt_bitexact(engine, oracle, small_clusters):
     assert img.max() > 0
 
 
+def test_render_pt_light_collection_bitexact(engine, oracle, small_clusters):
+    """Two lights through hr_set_lights: a ceiling quad and a wall quad facing +y, picked per
+    next-event sample by their weights (area x emission) from the running sum, each
+    contribution divided by its probability; the camera sees the emitters directly too."""
+    v, f = small_clusters
+    gpu_build(engine, v, f, GRID_TWO_LEVEL)
+    b = oracle_build(oracle, v, f, GRID_TWO_LEVEL)
+    cam = S.camera_at_bounds(v, (128, 96))
+    set_cam(engine, cam)
+    corners = np.array([[0.4, 0.4, 1.0], [0.1, -0.3, 0.2]], np.float32)
+    e1 = np.array([[0.2, 0.0, 0.0], [0.6, 0.0, 0.0]], np.float32)
+    e2 = np.array([[0.0, 0.2, 0.0], [0.0, 0.0, 0.5]], np.float32)
+    normals = np.array([[0.0, 0.0, -1.0], [0.0, 1.0, 0.0]], np.float32)
+    em = np.array([20.0, 6.0], np.float32)
+    engine.setLights(corners, e1, e2, em, normals=normals)
+    seed = 4242
+    engine.set_integrator(pt_bounces=4, albedo=0.7, seed=seed)
+    engine.ray_count(reset=True)
+    fb = engine.renderFrame(None, 0, RENDER_PATH)
+    rays = engine.ray_count(reset=True)
+    eps = float(np.float32(1e-4) * b.diag())
+    lights = [oracle.make_light(corners[k], e1[k], e2[k], float(em[k]), normals[k]) for k in range(2)]
+    img, orays = oracle.render_pt(b, ocam(oracle, cam), lights, 4, 0.7, eps, seed)
+    assert np.array_equal(fb[:, 0], img)
+    assert rays == orays
+    # the same collection with a single light equals hr_set_light
+    engine.setLights(corners[:1], e1[:1], e2[:1], em[:1], normals=normals[:1])
+    one = engine.renderFrame(None, 0, RENDER_PATH)
+    engine.setLights(corners[0], e1[0], e2[0], float(em[0]))
+    assert np.array_equal(engine.renderFrame(None, 0, RENDER_PATH), one)
+    from happyray_b200 import HRError
+    for n in (0, 65):
+        c = np.tile(corners[:1], (max(n, 1), 1))
+        a, bb = np.tile(e1[:1], (max(n, 1), 1)), np.tile(e2[:1], (max(n, 1), 1))
+        st = engine.L.hr_set_lights(engine.ctx, n, c.ctypes.data, a.ctypes.data, bb.ctypes.data, None,
+                                    np.ones(max(n, 1), np.float32).ctypes.data)
+        assert st == 1   # HR_ERR_INVALID_ARG
+    with pytest.raises(HRError):   # degenerate: zero-area quad
+        engine.setLights(corners, e1, np.zeros_like(e2), em)
+    engine.setLights((0.4, 0.4, 1.0), (0.2, 0, 0), (0, 0.2, 0), 20.0)
+
+
 def test_render_primary_mode0(engine, oracle, c1_scene):
     v, f = c1_scene
     gpu_build(engine, v, f, GRID_UNIFORM)
@@ -366,7 +408,10 @@ def test_scene_file_upload_renders_like_arrays(engine, tmp_path):
     (tmp_path / "camera.cfg").write_text(
         "position %r %r %r\norientation %r %r %r\nup 0 0 1\nresX 64\nresY 48\nFOV 60\n"
         % tuple(float(x) for x in list(cam["position"]) + list(cam["orientation"])))
-    (tmp_path / "light.cfg").write_text("position 0.4 0.4 1\nintensity 20 20 20\nedge1 0.2 0 0\nedge2 0 0.2 0\n")
+    # a ceiling light: without its normal line the light would face edge1 x edge2 = +z, away
+    # from the scene (LightSourceLoader.cpp:90-93)
+    (tmp_path / "light.cfg").write_text("position 0.4 0.4 1\nnormal 0 0 -1\nintensity 20 20 20\n"
+                                        "edge1 0.2 0 0\nedge2 0 0.2 0\n")
     (tmp_path / "scene.cfg").write_text("frame prefix = fr\nframe suffix = .obj\nnumber of frames = 3\n"
                                         "camera = camera.cfg\nlight = light.cfg\n")
     assert engine.upload_scene(str(tmp_path / "scene.cfg")) == (64, 48)
