@@ -179,6 +179,33 @@ __device__ __forceinline__ void sincos2pi(float u, float* s, float* c) {
     }
 }
 
+// Natural logarithm of a positive normal float: x = m * 2^e with m in [sqrt(1/2), sqrt(2)),
+// ln m = 2 atanh(s), s = (m - 1) / (m + 1), from the series 2 (s + s^3/3 + ... + s^11/11)
+// (|s| <= 0.1716, truncation error < 1e-10), plus e ln 2.  The same binary32 operations on
+// the host and the device.
+__host__ __device__ __forceinline__ float log_series(float x) {
+    uint32_t b;
+#ifdef __CUDA_ARCH__
+    b = __float_as_uint(x);
+#else
+    __builtin_memcpy(&b, &x, 4);
+#endif
+    int32_t e = (int32_t)((b >> 23) & 0xFFu) - 127;
+    b = (b & 0x7FFFFFu) | 0x3F800000u;
+    float m;
+#ifdef __CUDA_ARCH__
+    m = __uint_as_float(b);
+#else
+    __builtin_memcpy(&m, &b, 4);
+#endif
+    if (m > 1.41421356f) { m = m * 0.5f; e += 1; }
+    const float sv = (m - 1.0f) / (m + 1.0f);
+    const float s2 = sv * sv;
+    const float lm = sv * (2.0f + s2 * (0.666666667f + s2 * (0.4f + s2 * (0.285714286f + s2 * (0.222222222f +
+                     s2 * 0.181818182f)))));
+    return lm + (float)e * 0.693147181f;
+}
+
 // Orthonormal basis, Duff et al., JCGT 6(1) 2017
 __device__ __forceinline__ void onb(f3 n, f3* t, f3* b) {
     float sg = copysignf(1.0f, n.z);

@@ -1,7 +1,7 @@
 // jobs.cu -- persistent rendering of many jobs in one launch (batched and served forms).
 //
 // A job is one grid (two-level), a camera or a list of rays, an integrator and an output:
-//   kJobPrimary  camera rays, barycentric shading (SimpleIntegrator.h:41-126)
+//   kJobPrimary  camera rays (mode 0 pixel samplers), simpleShade (SimpleIntegrator.h:41-126)
 //   kJobAO       camera rays + spp AO samples per hit (AOIntegrator.h:234-351)
 //   kJobPath     spp paths per pixel (PathTracer.h:41-372 structure), progressive blend
 //   kJobRays     closest hit of a ray list (SimpleRayTraverser.h:168-261 query form)
@@ -203,7 +203,8 @@ __global__ __launch_bounds__(kJobTT, PT ? HR_JOB_PT_MIN_BLOCKS : HR_JOB_MIN_BLOC
             valid = x < cw && y < chh;
             pix = valid ? y * cw + x : 0u;
             o = mk(T.cam.pos[0], T.cam.pos[1], T.cam.pos[2]);
-            d = valid ? primary_dir(T.cam, pix) : mk(1.0f, 0.0f, 0.0f);
+            d = !valid ? mk(1.0f, 0.0f, 0.0f)
+                       : (T.mode == kJobPrimary ? primary_sample_dir(T.cam, pix, T.image_id, T.seed) : primary_dir(T.cam, pix));
         }
         Hit h;
         trace_one<kTwoLevel, false, false>(T.s, T.g, o, d, FLT_MAX, h, valid);
@@ -221,15 +222,11 @@ __global__ __launch_bounds__(kJobTT, PT ? HR_JOB_PT_MIN_BLOCKS : HR_JOB_MIN_BLOC
         float* fb = T.fb + 3 * (size_t)pix;
         if (T.mode != kJobAO) {
             if (valid) {
-                float r = 0.15f, gg = 0.2f, b = 0.3f;
-                if (h.hit) {
-                    const f3 nrm = face_normal(T.s, h.tri, d);
-                    const float cs = fabsf(dot(nrm, d));
-                    r = (1.0f - h.u - h.v) * cs; gg = h.u * cs; b = h.v * cs;
-                }
-                fb[0] = blend(fb[0], r, T.image_id);
-                fb[1] = blend(fb[1], gg, T.image_id);
-                fb[2] = blend(fb[2], b, T.image_id);
+                float rgb[3];
+                simple_shade(T.s, h.hit, h.tri, o, d, rgb);
+                fb[0] = blend(fb[0], rgb[0], T.image_id);
+                fb[1] = blend(fb[1], rgb[1], T.image_id);
+                fb[2] = blend(fb[2], rgb[2], T.image_id);
             }
             __syncwarp();
             continue;

@@ -109,8 +109,8 @@ __global__ __launch_bounds__(kTT, HR_TRACE_MIN_BLOCKS) void k_occluded(Scene s, 
 
 // mode 0: primary rays with barycentric false colour (SimpleIntegrator.h:41-126)
 template <int KIND, bool STATS>
-__global__ __launch_bounds__(kTT, HR_TRACE_MIN_BLOCKS) void k_render_primary(Scene s, Cam cam, int32_t image_id, float* __restrict__ fb,
-                                                        unsigned long long* counter) {
+__global__ __launch_bounds__(kTT, HR_TRACE_MIN_BLOCKS) void k_render_primary(Scene s, Cam cam, int32_t image_id, uint64_t seed,
+                                                        float* __restrict__ fb, unsigned long long* counter) {
     const G g = load_g(s.desc);
     gate_scene(s);
     const uint32_t slots = tile_slots(cam);
@@ -118,19 +118,15 @@ __global__ __launch_bounds__(kTT, HR_TRACE_MIN_BLOCKS) void k_render_primary(Sce
     for (uint32_t slot = blockIdx.x * kTT + threadIdx.x; slot < slots; slot += gridDim.x * kTT) {
         uint32_t i;
         const bool valid = tile_pixel(cam, slot, &i);
-        const f3 d = valid ? primary_dir(cam, i) : mk(1.0f, 0.0f, 0.0f);
+        const f3 d = valid ? primary_sample_dir(cam, i, image_id, seed) : mk(1.0f, 0.0f, 0.0f);
         Hit h;
         trace_one<KIND, false, STATS>(s, g, o, d, FLT_MAX, h, valid);
         if (valid) {
-            float r = 0.15f, gg = 0.2f, b = 0.3f;
-            if (h.hit) {
-                const f3 nrm = face_normal(s, h.tri, d);
-                const float cs = fabsf(dot(nrm, d));
-                r = (1.0f - h.u - h.v) * cs; gg = h.u * cs; b = h.v * cs;
-            }
-            fb[3 * (size_t)i] = blend(fb[3 * (size_t)i], r, image_id);
-            fb[3 * (size_t)i + 1] = blend(fb[3 * (size_t)i + 1], gg, image_id);
-            fb[3 * (size_t)i + 2] = blend(fb[3 * (size_t)i + 2], b, image_id);
+            float rgb[3];
+            simple_shade(s, h.hit, h.tri, o, d, rgb);
+            fb[3 * (size_t)i] = blend(fb[3 * (size_t)i], rgb[0], image_id);
+            fb[3 * (size_t)i + 1] = blend(fb[3 * (size_t)i + 1], rgb[1], image_id);
+            fb[3 * (size_t)i + 2] = blend(fb[3 * (size_t)i + 2], rgb[2], image_id);
         }
         add_rays<STATS>(counter, false, valid ? 1u : 0u, h.cells, h.tests);
     }
@@ -563,7 +559,7 @@ int launch_render(hr_ctx* c, int32_t mode, int32_t image_id, float* d_fb) {
     case 0:
         c->launches += 1;
         mark(0);
-        by_kind(s.kind, st, [&](auto K, auto S) { k_render_primary<K(), S()><<<gb, kTT, 0, strm>>>(s, k, image_id, d_fb, ctr); });
+        by_kind(s.kind, st, [&](auto K, auto S) { k_render_primary<K(), S()><<<gb, kTT, 0, strm>>>(s, k, image_id, c->ip.seed, d_fb, ctr); });
         mark(1);
         c->nrender_ev = 2;
         break;

@@ -395,6 +395,61 @@ __device__ __forceinline__ f3 primary_dir(const Cam& c, uint32_t pix) {
     return normalize(d);
 }
 
+// Camera ray of render mode 0 for progressive image `image_id` (RTEngine.cu:409-424):
+// images 0-3 take the 2 x 2 regular in-pixel pattern (RegularPixelSampler<2,2>,
+// Camera.h:75-98), later ones a Gaussian offset around the pixel's corner
+// (GaussianPixelSampler, Camera.h:116-132) from two PCG32 draws keyed by (image, pixel,
+// seed); normalised.
+__device__ __forceinline__ f3 primary_sample_dir(const Cam& c, uint32_t pix, int32_t image_id, uint64_t seed) {
+    float ox, oy;
+    if (image_id < 4) {
+        const float tmp = (float)(image_id % 4) / 2.0f;
+        oy = (truncf(tmp) + 0.5f) / 2.0f;
+        ox = tmp - truncf(tmp) + 0.5f / 2.0f;
+    } else {
+        Pcg32 r;
+        pcg_seed(r, ((uint64_t)(uint32_t)image_id << 32) | pix, seed);
+        const float u1 = pcg_float(r), u2 = pcg_float(r);
+        const float rad = 0.5f * sqrtf(-log_series(1.0f - u1));
+        float sn, cs;
+        sincos2pi(u2, &sn, &cs);
+        ox = rad * cs;
+        oy = rad * sn;
+    }
+    const float px = (float)(pix % (uint32_t)c.w) + ox;
+    const float py = (float)(pix / (uint32_t)c.w) + oy;
+    f3 d;
+    d.x = c.tl[0] + px * c.sx[0] + py * c.sy[0];
+    d.y = c.tl[1] + px * c.sx[1] + py * c.sy[1];
+    d.z = c.tl[2] + px * c.sx[2] + py * c.sy[2];
+    return normalize(d);
+}
+
+// simpleShade (SimpleIntegrator.h:41-126) of a hit: weights u = |(v1 - o) x (v2 - o)| / |N|,
+// v = |(v2 - o) x (v0 - o)| / |N| (N the triangle's edge cross product, o the ray origin) as
+// the colour (u, v, 1 - u - v), times |cos| between the unit normal and the unit direction;
+// background (0.15, 0.2, 0.3) on a miss.
+__device__ __forceinline__ void simple_shade(const Scene& s, bool hit, uint32_t tri, f3 o, f3 d, float* rgb) {
+    if (!hit) {
+        rgb[0] = 0.15f; rgb[1] = 0.2f; rgb[2] = 0.3f;
+        return;
+    }
+    f3 p[3];
+    tri_fetch(s.tris, tri, p);
+    const f3 nr = cross(sub(p[1], p[0]), sub(p[2], p[0]));
+    const f3 a0 = sub(p[0], o), a1 = sub(p[1], o), a2 = sub(p[2], o);
+    const f3 n0 = cross(a1, a2), n1 = cross(a2, a0);
+    const float inv = 1.0f / sqrtf(dot(nr, nr));
+    const float u = sqrtf(dot(n0, n0)) * inv;
+    const float v = sqrtf(dot(n1, n1)) * inv;
+    const f3 nrm = normalize(nr);
+    const f3 dn = normalize(d);
+    const float cs = fmaxf(0.0f, fabsf(dot(mk(-nrm.x, -nrm.y, -nrm.z), dn)));
+    rgb[0] = u * cs;
+    rgb[1] = v * cs;
+    rgb[2] = (1.0f - u - v) * cs;
+}
+
 __device__ __forceinline__ f3 face_normal(const Scene& s, uint32_t tri, f3 d) {
     f3 p[3];
     tri_fetch(s.tris, tri, p);

@@ -92,6 +92,8 @@ def lib():
                 "orc_trace_primary": (None, [C.POINTER(Scene), C.POINTER(Camera), P, P, P, P, P]),
                 "orc_occluded": (None, [C.POINTER(Scene), P, P, P, U32, P]),
                 "orc_render_ao": (None, [C.POINTER(Scene), C.POINTER(Camera), I32, F, U64, I32, P, U32, P]),
+                "orc_render_primary": (None, [C.POINTER(Scene), C.POINTER(Camera), I32, U64, P]),
+                "orc_log_series": (F, [F]),
                 "orc_render_pt": (None, [C.POINTER(Scene), C.POINTER(Camera), C.POINTER(Light), I32, I32, F, F, U64, I32, P, U32, P]),
                 "orc_brute_f64": (None, [P, P, U32, P, P, U32, P, P, P, P, P]),
                 "orc_sincos2pi": (None, [F, C.POINTER(F), C.POINTER(F)]),
@@ -282,6 +284,19 @@ def render_ao(b: Built, cam: Camera, spp: int, alpha: float, seed: int, image_id
     s = b.scene()
     lib().orc_render_ao(C.byref(s), C.byref(cam), spp, alpha, seed, image_id, _p(fb), pixel_stride, _p(counts))
     return fb, int(counts[0])
+
+
+def render_primary(b: Built, cam: Camera, image_id: int, seed: int, fb=None):
+    """Render mode 0 (pixel samplers + simpleShade), blended into fb (pixels x 3 floats)."""
+    n = cam.w * cam.h
+    fb = np.zeros((n, 3), np.float32) if fb is None else np.ascontiguousarray(fb, np.float32).reshape(n, 3)
+    s = b.scene()
+    lib().orc_render_primary(C.byref(s), C.byref(cam), image_id, seed, _p(fb))
+    return fb
+
+
+def log_series(x: float) -> float:
+    return float(lib().orc_log_series(x))
 
 
 def render_pt(b: Built, cam: Camera, light, bounces: int, albedo: float, ray_eps: float, seed: int,

@@ -774,6 +774,89 @@ static inline void blend(float *fb, size_t i, float val, int32_t image_id) {
 
 /* a19: ambient occlusion, AOIntegrator.h:234-351 and RayGenerators.h:286-342 with the
  * configured sample count, AO radius and PCG32 stream keyed by (image, pixel, seed). */
+/* natural logarithm of a positive normal float (atanh series of m in [sqrt(1/2), sqrt(2))),
+ * the same binary32 operations as the library's */
+static inline float log_series(float x) {
+    uint32_t b;
+    memcpy(&b, &x, 4);
+    int32_t e = (int32_t)((b >> 23) & 0xFFu) - 127;
+    b = (b & 0x7FFFFFu) | 0x3F800000u;
+    float m;
+    memcpy(&m, &b, 4);
+    if (m > 1.41421356f) { m = m * 0.5f; e += 1; }
+    const float sv = (m - 1.0f) / (m + 1.0f);
+    const float s2 = sv * sv;
+    const float lm = sv * (2.0f + s2 * (0.666666667f + s2 * (0.4f + s2 * (0.285714286f + s2 * (0.222222222f +
+                     s2 * 0.181818182f)))));
+    return lm + (float)e * 0.693147181f;
+}
+
+float orc_log_series(float x) { return log_series(x); }
+
+/* camera ray of render mode 0 for progressive image image_id (RTEngine.cu:409-424): the
+ * 2 x 2 regular in-pixel pattern for images 0-3 (RegularPixelSampler<2,2>, Camera.h:75-98),
+ * a Gaussian offset around the pixel corner for later ones (GaussianPixelSampler,
+ * Camera.h:116-132) from two PCG32 draws keyed by (image, pixel, seed); normalised */
+static inline f3 primary_sample_dir(const orc_camera *c, uint32_t pix, int32_t image_id, uint64_t seed) {
+    float ox, oy;
+    if (image_id < 4) {
+        const float tmp = (float)(image_id % 4) / 2.0f;
+        oy = (truncf(tmp) + 0.5f) / 2.0f;
+        ox = tmp - truncf(tmp) + 0.5f / 2.0f;
+    } else {
+        pcg32 r;
+        pcg32_seed(&r, ((uint64_t)(uint32_t)image_id << 32) | pix, seed);
+        const float u1 = pcg32_float(&r), u2 = pcg32_float(&r);
+        const float rad = 0.5f * sqrtf(-log_series(1.0f - u1));
+        float sn, cs;
+        orc_sincos2pi(u2, &sn, &cs);
+        ox = rad * cs;
+        oy = rad * sn;
+    }
+    const float px = (float)(pix % (uint32_t)c->w) + ox;
+    const float py = (float)(pix / (uint32_t)c->w) + oy;
+    f3 d;
+    d.x = c->top_left[0] + px * c->step_x[0] + py * c->step_y[0];
+    d.y = c->top_left[1] + px * c->step_x[1] + py * c->step_y[1];
+    d.z = c->top_left[2] + px * c->step_x[2] + py * c->step_y[2];
+    return normalize(d);
+}
+
+/* render mode 0: simpleShade (SimpleIntegrator.h:41-126) of the closest hit, weights from
+ * the ray origin's cross products, progressive blend of the 3 channels into fb (3 floats
+ * per pixel) */
+void orc_render_primary(const orc_scene *s, const orc_camera *c, int32_t image_id, uint64_t seed, float *fb) {
+    const uint32_t n = (uint32_t)c->w * (uint32_t)c->h;
+    const f3 o = ld3(c->pos);
+    const float nw = 1.0f / (float)(image_id + 1);
+    const float ow = 1.0f - nw;
+#pragma omp parallel for schedule(dynamic, 256)
+    for (long long ii = 0; ii < (long long)n; ++ii) {
+        const uint32_t pix = (uint32_t)ii;
+        const f3 d = primary_sample_dir(c, pix, image_id, seed);
+        hitrec h;
+        trace_one(s, o, d, FLT_MAX, 0, &h);
+        float rgb[3] = {0.15f, 0.2f, 0.3f};
+        if (h.hit) {
+            const f3 p0 = vtx(s->v4, s->idx[3 * (size_t)h.tri]), p1 = vtx(s->v4, s->idx[3 * (size_t)h.tri + 1]),
+                     p2 = vtx(s->v4, s->idx[3 * (size_t)h.tri + 2]);
+            const f3 nr = cross(sub(p1, p0), sub(p2, p0));
+            const f3 a0 = sub(p0, o), a1 = sub(p1, o), a2 = sub(p2, o);
+            const f3 n0 = cross(a1, a2), n1 = cross(a2, a0);
+            const float inv = 1.0f / sqrtf(dot(nr, nr));
+            const float u = sqrtf(dot(n0, n0)) * inv;
+            const float v = sqrtf(dot(n1, n1)) * inv;
+            const f3 nrm = normalize(nr);
+            const f3 dn = normalize(d);
+            const float cs = fmaxf(0.0f, fabsf(dot(mk(-nrm.x, -nrm.y, -nrm.z), dn)));
+            rgb[0] = u * cs;
+            rgb[1] = v * cs;
+            rgb[2] = (1.0f - u - v) * cs;
+        }
+        for (int k = 0; k < 3; ++k) fb[3 * (size_t)pix + k] = fb[3 * (size_t)pix + k] * ow + rgb[k] * nw;
+    }
+}
+
 void orc_render_ao(const orc_scene *s, const orc_camera *c, int32_t spp, float alpha,
                    uint64_t seed, int32_t image_id, float *fb, uint32_t pixel_stride,
                    uint64_t *counts) {

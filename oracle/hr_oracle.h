@@ -116,6 +116,10 @@ void orc_render_ao(const orc_scene *s, const orc_camera *c, int32_t spp, float a
                    uint64_t seed, int32_t image_id, float *fb, uint32_t pixel_stride,
                    uint64_t *counts);
 /* PT: scalar radiance per pixel, `bounces` extension rays, NEE per hit. */
+/* render mode 0 (RTEngine.cu:409-424): regular 2 x 2 / Gaussian pixel samples, simpleShade
+ * (SimpleIntegrator.h:41-126), progressive blend into fb (3 floats per pixel) */
+void orc_render_primary(const orc_scene *s, const orc_camera *c, int32_t image_id, uint64_t seed, float *fb);
+float orc_log_series(float x);
 void orc_render_pt(const orc_scene *s, const orc_camera *c, const orc_light *l, int32_t nlights,
                    int32_t bounces, float albedo, float ray_eps, uint64_t seed,
                    int32_t image_id, float *fb, uint32_t pixel_stride, uint64_t *counts);

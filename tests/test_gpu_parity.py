@@ -286,21 +286,25 @@ def test_render_pt_light_collection_bitexact(engine, oracle, small_clusters):
     engine.setLights((0.4, 0.4, 1.0), (0.2, 0, 0), (0, 0.2, 0), 20.0)
 
 
-def test_render_primary_mode0(engine, oracle, c1_scene):
+@pytest.mark.parametrize("kind", [GRID_UNIFORM, GRID_TWO_LEVEL])
+def test_render_primary_mode0(engine, oracle, c1_scene, kind):
+    """Render mode 0 bit-exact against the oracle's simpleShade (SimpleIntegrator.h:41-126)
+    over six progressive images: 0-3 take the 2 x 2 regular in-pixel pattern, 4 and 5 the
+    Gaussian pixel sampler (RTEngine.cu:409-424)."""
     v, f = c1_scene
-    gpu_build(engine, v, f, GRID_UNIFORM)
-    cam = S.camera_c1((64, 64))
+    gpu_build(engine, v, f, kind)
+    b = oracle_build(oracle, v, f, kind)
+    cam = S.camera_c1((64, 48))
     set_cam(engine, cam)
-    fb = engine.renderFrame(None, 0, RENDER_PRIMARY)
-    b = oracle_build(oracle, v, f, GRID_UNIFORM)
-    hid, t, u, vv = oracle.trace_primary(b, ocam(oracle, cam))
-    miss = hid < 0
-    assert np.allclose(fb[miss], [0.15, 0.2, 0.3])
-    hit = ~miss
-    # barycentric false colour: (w0, w1, w2) * |cos|
-    s = fb[hit].sum(1)
-    assert np.all(s <= 1.0 + 1e-6) and np.all(s >= 0)
-    assert np.allclose(fb[hit, 1] / np.maximum(s, 1e-12), u[hit] / np.maximum(u[hit] + vv[hit] + (1 - u[hit] - vv[hit]), 1e-12), atol=1e-4)
+    seed = 777
+    engine.set_integrator(seed=seed)
+    fb, want = None, None
+    for im in range(6):
+        fb = engine.renderFrame(fb, im, RENDER_PRIMARY)
+        want = oracle.render_primary(b, ocam(oracle, cam), im, seed, want)
+        assert np.array_equal(fb, want), f"image {im}"
+    miss = np.all(want == np.array([0.15, 0.2, 0.3], np.float32), axis=1)
+    assert 0 < miss.sum() < miss.size
 
 
 def test_radix_sort_and_scan_device(engine):

@@ -33,6 +33,15 @@ def test_sincos2pi_accuracy(oracle):
     assert err < 5e-7
 
 
+def test_log_series_accuracy(oracle):
+    """The Gaussian pixel sampler's logarithm (atanh series) against math.log over the
+    range it is used on, 1 - u for u in [0, 1): absolute error below 1e-6."""
+    xs = np.concatenate([np.float32(2.0) ** -np.arange(0, 25),
+                         np.random.default_rng(5).uniform(2.0 ** -24, 1.0, 4000).astype(np.float32)])
+    err = max(abs(oracle.log_series(float(x)) - math.log(float(x))) for x in xs)
+    assert err < 1e-6
+
+
 def test_pow_third_close_to_cube_root(oracle):
     for x in [1e-6, 0.37, 1.0, 27.0, 1234.5, 5.0 * 32768 / 0.2, 3.3e7]:
         y = oracle.pow_third(x)
