@@ -33,12 +33,9 @@ namespace hr {
 
 namespace {
 
-// ctl: the build's control words, whose work-list length and counter restart at zero
-__global__ void k_desc_init(GridDesc* d, int32_t kind, uint32_t ntri, const uint32_t* bad_index_count, uint32_t* ctl) {
+__global__ void k_desc_init(GridDesc* d, int32_t kind, uint32_t ntri, const uint32_t* bad_index_count) {
     // the error flag is set by the index check of the last upload
     desc_init(d, kind, ntri, *bad_index_count != 0u ? 1u : 0u);
-    ctl[0] = 0u;   // kBigCount
-    ctl[1] = 0u;   // kBigNext
 }
 
 // The key-frame pair and weight of the next interpolating build, written in stream order
@@ -240,15 +237,10 @@ __global__ __launch_bounds__(kBT) void k_leaf_count_pairs(const uint32_t* __rest
 }
 
 // a11: leaf pairs in reference order at each reference's scan offset; key = first leaf of
-// the top cell + local sub-cell index (writeLeafLevelKeysAndValues, TLGridBuildKernels.h:536-663).
-// The references are sorted by (top cell, triangle), so each top cell's leaf pairs form one
-// segment [cell_pb, cell_pe) in ascending triangle order; the first and last reference of a
-// cell record the segment's ends.
+// the top cell + local sub-cell index (writeLeafLevelKeysAndValues, TLGridBuildKernels.h:536-663)
 __global__ __launch_bounds__(kBT) void k_leaf_write_pairs(const uint4* __restrict__ refrng, const GridDesc* d,
                                                           const uint32_t* block_sums, uint32_t* __restrict__ keys,
-                                                          uint32_t* __restrict__ vals,
-                                                          const uint32_t* __restrict__ top_keys,
-                                                          uint32_t* __restrict__ cell_pb, uint32_t* __restrict__ cell_pe) {
+                                                          uint32_t* __restrict__ vals) {
     if (d->overflow | d->error) return;
     const uint32_t i = blockIdx.x * kBT + threadIdx.x;
     uint32_t n = 0, tri = 0, base = 0, lres[2] = {1u, 1u};
@@ -271,203 +263,7 @@ __global__ __launch_bounds__(kBT) void k_leaf_write_pairs(const uint4* __restric
     PairRun run;
     if (n) run = {base + (uint32_t)r.lo[0] + (uint32_t)r.lo[1] * lres[0] + (uint32_t)r.lo[2] * lres[0] * lres[1],
                   (uint32_t)(r.hi[0] - r.lo[0]), (uint32_t)(r.hi[1] - r.lo[1]), lres[0], lres[0] * lres[1], tri};
-    const uint32_t at = block_write_runs<kBT>(n, run, block_sums[blockIdx.x], keys, vals);
-    const uint32_t nref = d->ntop_pairs;
-    if (i < nref) {
-        const uint32_t cell = __ldg(top_keys + i);
-        if (i == 0 || __ldg(top_keys + i - 1) != cell) cell_pb[cell] = at;
-        if (i + 1 == nref || __ldg(top_keys + i + 1) != cell) cell_pe[cell] = at + n;
-    }
-}
-
-// Build control words in device memory: the big-cell list length and its work counter,
-// reset by k_desc_init at the start of every build.
-enum : int { kBigCount = 0, kBigNext = 1, kCtlWords = 16 };
-
-constexpr int kSegT = 512;                       // threads of the per-segment CTA kernel
-constexpr int kSegW = kSegT / 32;
-constexpr int kSegIpt = 8;
-constexpr uint32_t kSegChunk = kSegT * kSegIpt;  // items ranked per chunk
-constexpr uint32_t kSegCap = 24576;              // items a segment sorts in shared memory
-constexpr int kSegPosBits = 17;                  // position of an item in its segment
-constexpr size_t kSegDynSmem = sizeof(uint32_t) * 2 * kSegCap;
-
-// a13 for the common cases, one thread per top cell (prepareLeafCellRanges,
-// TLGridBuildKernels.h:750-834): an empty cell's single leaf is empty; a cell with one
-// leaf holds its whole segment, already in ascending triangle order.  Cells with more
-// leaves are listed for k_leaf_cells_big.
-__global__ void k_leaf_cells(const GridDesc* d, const uint2* __restrict__ top_ranges, const uint2* __restrict__ cells,
-                             const uint32_t* __restrict__ cell_pb, const uint32_t* __restrict__ cell_pe,
-                             const uint32_t* __restrict__ vals, uint2* __restrict__ leaves,
-                             uint32_t* __restrict__ prims, uint32_t* ctl, uint32_t* __restrict__ big_list) {
-    if (d->overflow | d->error) return;
-    const uint32_t C = d->ncells;
-    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < C; c += gridDim.x * blockDim.x) {
-        const uint2 tr = top_ranges[c];
-        const uint2 cw = cells[c];
-        const uint32_t y = cw.y;
-        const uint32_t nl = (y & 0xFFu) * ((y >> 8) & 0xFFu) * ((y >> 16) & 0xFFu);
-        if (tr.y == tr.x) {
-            leaves[cw.x] = make_uint2(0u, 0u);
-        } else if (nl == 1u) {
-            const uint32_t pb = cell_pb[c], pe = cell_pe[c];
-            leaves[cw.x] = pe > pb ? make_uint2(pb, pe) : make_uint2(0u, 0u);
-            for (uint32_t i = pb; i < pe; ++i) prims[i] = __ldg(vals + i);
-        } else {
-            big_list[atomicAdd(ctl + kBigCount, 1u)] = c;
-        }
-    }
-}
-
-struct SegSmem {
-    uint32_t cur[256];            // digit counts, then running digit cursors
-    uint32_t whist[kSegW][256];   // per warp and digit: count, then output base
-    uint32_t item;
-};
-
-// Stable LSD radix sort by one CTA of the n words at a (b: the other half of the
-// ping-pong; shared memory, or global scratch for large segments) on the bits [shift, shift + 8 * passes) in 8-bit digits.  Each pass counts
-// the digits, then ranks chunks of kSegChunk words in order: within a warp by match_any,
-// across warps by per-warp digit counts.  Returns the buffer holding the result.
-template <class Wd>
-__device__ Wd* cta_smem_radix(Wd* a, Wd* b, uint32_t n, int shift, int passes, SegSmem& sm) {
-    const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
-    const uint32_t lt = (1u << lane) - 1u;
-    for (int p = 0; p < passes; ++p) {
-        const Wd* src = (p & 1) ? b : a;
-        Wd* dst = (p & 1) ? a : b;
-        const int sh = shift + 8 * p;
-        for (uint32_t i = threadIdx.x; i < 256; i += kSegT) sm.cur[i] = 0u;
-        __syncthreads();
-        for (uint32_t base = 0; base < n; base += kSegT) {
-            const uint32_t i = base + threadIdx.x;
-            const uint32_t dg = i < n ? (uint32_t)(src[i] >> sh) & 255u : 256u;
-            const uint32_t peers = __match_any_sync(kFullMask, dg);
-            if (dg < 256u && lane == (uint32_t)(__ffs(peers) - 1)) atomicAdd(&sm.cur[dg], (uint32_t)__popc(peers));
-        }
-        __syncthreads();
-        if (w == 0) {   // exclusive scan of the 256 digit counts, 8 per lane
-            uint32_t x[8], s = 0;
-#pragma unroll
-            for (int k = 0; k < 8; ++k) { x[k] = sm.cur[lane * 8 + k]; s += x[k]; }
-            uint32_t inc = s;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const uint32_t y = __shfl_up_sync(kFullMask, inc, o);
-                if ((int)lane >= o) inc += y;
-            }
-            uint32_t run = inc - s;
-#pragma unroll
-            for (int k = 0; k < 8; ++k) { sm.cur[lane * 8 + k] = run; run += x[k]; }
-        }
-        __syncthreads();
-        for (uint32_t base = 0; base < n; base += kSegChunk) {
-            for (uint32_t i = threadIdx.x; i < kSegW * 256; i += kSegT) (&sm.whist[0][0])[i] = 0u;
-            __syncthreads();
-            Wd key[kSegIpt];
-            uint32_t dig[kSegIpt], rank[kSegIpt];
-#pragma unroll
-            for (int r = 0; r < kSegIpt; ++r) {
-                const uint32_t i = base + (w * kSegIpt + r) * 32 + lane;
-                key[r] = i < n ? src[i] : (Wd)0;
-                dig[r] = i < n ? (uint32_t)(key[r] >> sh) & 255u : 256u;
-            }
-#pragma unroll
-            for (int r = 0; r < kSegIpt; ++r) {
-                const uint32_t peers = __match_any_sync(kFullMask, dig[r]);
-                const uint32_t leader = (uint32_t)(__ffs(peers) - 1);
-                uint32_t bb = 0;
-                if (dig[r] < 256u && lane == leader) {
-                    bb = sm.whist[w][dig[r]];
-                    sm.whist[w][dig[r]] = bb + (uint32_t)__popc(peers);
-                }
-                bb = __shfl_sync(kFullMask, bb, (int)leader);
-                rank[r] = bb + (uint32_t)__popc(peers & lt);
-                __syncwarp();
-            }
-            __syncthreads();
-            for (uint32_t dd = threadIdx.x; dd < 256; dd += kSegT) {
-                uint32_t run = sm.cur[dd];
-                for (uint32_t ww = 0; ww < kSegW; ++ww) {
-                    const uint32_t t = sm.whist[ww][dd];
-                    sm.whist[ww][dd] = run;
-                    run += t;
-                }
-                sm.cur[dd] = run;
-            }
-            __syncthreads();
-#pragma unroll
-            for (int r = 0; r < kSegIpt; ++r)
-                if (dig[r] < 256u) dst[sm.whist[w][dig[r]] + rank[r]] = key[r];
-            __syncthreads();
-        }
-    }
-    return (passes & 1) ? b : a;
-}
-
-__device__ __forceinline__ int bit_width(uint32_t x) { return x ? 32 - __clz(x) : 0; }
-
-// a11-a13 for top cells with more than one leaf: one CTA per listed cell, taken from a work
-// counter.  The cell's segment of leaf pairs is in ascending triangle order; it is sorted
-// stably by local leaf index: the words (leaf << 17 | position in the segment) are
-// radix-sorted on their leaf bits in shared memory, the leaf ranges follow from the sorted
-// words and each list takes its triangles from the positions.  A segment of more than
-// kSegCap pairs or a cell of more than 2^15 leaves sorts 64-bit words (leaf << 32 |
-// position) the same way in global scratch (g64: 2 words per leaf pair).
-__global__ __launch_bounds__(kSegT, 1) void k_leaf_cells_big(const GridDesc* d, const uint2* __restrict__ cells,
-                                                             const uint32_t* __restrict__ cell_pb,
-                                                             const uint32_t* __restrict__ cell_pe,
-                                                             const uint32_t* __restrict__ keys,
-                                                             const uint32_t* __restrict__ vals,
-                                                             uint2* __restrict__ leaves, uint32_t* __restrict__ prims,
-                                                             uint32_t* ctl, const uint32_t* __restrict__ big_list,
-                                                             unsigned long long* g64) {
-    if (d->overflow | d->error) return;
-    __shared__ SegSmem sm;
-    extern __shared__ uint32_t s_buf[];
-    const uint32_t nbig = ctl[kBigCount];
-    const uint32_t npairs = d->npairs;
-    for (;;) {
-        if (threadIdx.x == 0) sm.item = atomicAdd(ctl + kBigNext, 1u);
-        __syncthreads();
-        const uint32_t item = sm.item;
-        __syncthreads();
-        if (item >= nbig) return;
-        const uint32_t c = big_list[item];
-        const uint2 cw = cells[c];
-        const uint32_t lb = cw.x, y = cw.y;
-        const uint32_t nl = (y & 0xFFu) * ((y >> 8) & 0xFFu) * ((y >> 16) & 0xFFu);
-        const uint32_t pb = cell_pb[c], P = cell_pe[c] - pb;
-        const int lbits = bit_width(nl - 1u);
-        for (uint32_t l = threadIdx.x; l < nl; l += kSegT) leaves[lb + l] = make_uint2(0u, 0u);
-        if (P <= kSegCap && lbits <= 32 - kSegPosBits) {
-            for (uint32_t i = threadIdx.x; i < P; i += kSegT)
-                s_buf[i] = ((__ldg(keys + pb + i) - lb) << kSegPosBits) | i;
-            __syncthreads();
-            const uint32_t* sw = cta_smem_radix(s_buf, s_buf + kSegCap, P, kSegPosBits, (lbits + 7) / 8, sm);
-            for (uint32_t s = threadIdx.x; s < P; s += kSegT) {
-                const uint32_t wv = sw[s], l = wv >> kSegPosBits;
-                prims[pb + s] = __ldg(vals + pb + (wv & ((1u << kSegPosBits) - 1u)));
-                if (s == 0 || (sw[s - 1] >> kSegPosBits) != l) leaves[lb + l].x = pb + s;
-                if (s + 1 == P || (sw[s + 1] >> kSegPosBits) != l) leaves[lb + l].y = pb + s + 1;
-            }
-        } else {
-            unsigned long long* a = g64 + pb;
-            unsigned long long* b = g64 + npairs + pb;
-            for (uint32_t i = threadIdx.x; i < P; i += kSegT)
-                a[i] = ((unsigned long long)(__ldg(keys + pb + i) - lb) << 32) | i;
-            __syncthreads();
-            const unsigned long long* sw = cta_smem_radix(a, b, P, 32, (lbits + 7) / 8, sm);
-            for (uint32_t s = threadIdx.x; s < P; s += kSegT) {
-                const unsigned long long wv = sw[s];
-                const uint32_t l = (uint32_t)(wv >> 32);
-                prims[pb + s] = __ldg(vals + pb + (uint32_t)wv);
-                if (s == 0 || (uint32_t)(sw[s - 1] >> 32) != l) leaves[lb + l].x = pb + s;
-                if (s + 1 == P || (uint32_t)(sw[s + 1] >> 32) != l) leaves[lb + l].y = pb + s + 1;
-            }
-        }
-        __syncthreads();
-    }
+    block_write_runs<kBT>(n, run, block_sums[blockIdx.x], keys, vals);
 }
 
 int key_bits_for(size_t max_key) {
@@ -486,8 +282,7 @@ static std::vector<uint8_t> build_graph_key(const hr_ctx* c, int32_t kind, int32
     const DevBuf* bufs[] = {&B.desc, &c->tris, &B.cells, &B.keys_a, &B.tri_ranges, &B.vals_a, &B.keys_b, &B.vals_b,
                             &B.block_sums, &B.tile_hist, &B.row_total, &B.prims, &B.top_ranges, &B.top_refs,
                             &B.ref_ranges, &B.leaf_cnt, &B.scan_partials, &B.leaves, &B.lkeys_a, &B.lvals_a,
-                            &B.cell_pb, &B.cell_pe, &B.ctl, &B.big_list, &B.seg_words, &c->verts, &c->idx,
-                            &c->counters, &c->keyframes, &c->frame_sel};
+                            &B.lkeys_b, &B.lvals_b, &c->verts, &c->idx, &c->counters, &c->keyframes, &c->frame_sel};
     std::vector<uint8_t> k;
     auto put = [&](const void* p, size_t n) {
         const uint8_t* b = static_cast<const uint8_t*>(p);
@@ -535,8 +330,11 @@ static int build_once_impl(hr_ctx* c, int32_t kind, int32_t exact, uint32_t* ovf
     const uint32_t nblocks = (ntri + kBT - 1) / kBT;
     const int key_bits = key_bits_for(B.cap_cells);
     const int passes = radix_sort_passes(key_bits);
+    const int leaf_bits = key_bits_for(B.cap_leaves);
+    const int leaf_passes = radix_sort_passes(leaf_bits);
     const uint32_t nref_blocks = (uint32_t)((cap_pairs + kBT - 1) / kBT);   // per top-level reference
     size_t hist_words = radix_tile_hist_words(cap_pairs, key_bits);
+    if (kind == kTwoLevel) hist_words = std::max(hist_words, radix_tile_hist_words(B.cap_leaf_pairs, leaf_bits));
     int rc;
     if ((rc = ensure(c, B.desc, sizeof(GridDesc)))) return rc;
     if ((rc = ensure(c, c->frame_sel, sizeof(int4)))) return rc;
@@ -550,7 +348,6 @@ static int build_once_impl(hr_ctx* c, int32_t kind, int32_t exact, uint32_t* ovf
     if ((rc = ensure(c, B.block_sums, sizeof(uint32_t) * (std::max(nblocks, nref_blocks) + 1)))) return rc;
     if ((rc = ensure(c, B.tile_hist, sizeof(uint32_t) * hist_words))) return rc;
     if ((rc = ensure(c, B.row_total, sizeof(uint32_t) * kRadixRowWords))) return rc;
-    if (!B.ctl.p && (rc = ensure(c, B.ctl, sizeof(uint32_t) * kCtlWords))) return rc;
     if (kind == kUniform) {
         if ((rc = ensure(c, B.prims, sizeof(uint32_t) * cap_pairs))) return rc;
     } else {
@@ -562,19 +359,9 @@ static int build_once_impl(hr_ctx* c, int32_t kind, int32_t exact, uint32_t* ovf
         if ((rc = ensure(c, B.leaves, sizeof(uint2) * B.cap_leaves))) return rc;
         if ((rc = ensure(c, B.lkeys_a, sizeof(uint32_t) * B.cap_leaf_pairs))) return rc;
         if ((rc = ensure(c, B.lvals_a, sizeof(uint32_t) * B.cap_leaf_pairs))) return rc;
+        if ((rc = ensure(c, B.lkeys_b, sizeof(uint32_t) * B.cap_leaf_pairs))) return rc;
+        if ((rc = ensure(c, B.lvals_b, sizeof(uint32_t) * B.cap_leaf_pairs))) return rc;
         if ((rc = ensure(c, B.prims, sizeof(uint32_t) * B.cap_leaf_pairs))) return rc;
-        if ((rc = ensure(c, B.cell_pb, sizeof(uint32_t) * B.cap_cells))) return rc;
-        if ((rc = ensure(c, B.cell_pe, sizeof(uint32_t) * B.cap_cells))) return rc;
-        if ((rc = ensure(c, B.big_list, sizeof(uint32_t) * B.cap_cells))) return rc;
-        if ((rc = ensure(c, B.seg_words, sizeof(unsigned long long) * 2 * B.cap_leaf_pairs))) return rc;
-        static bool attr_set[64] = {};   // per device, once per process
-        const int dv = c->device & 63;
-        if (!attr_set[dv]) {
-            if ((rc = cuda_check(c, cudaFuncSetAttribute(k_leaf_cells_big, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                         (int)kSegDynSmem), "leaf kernel shared memory")))
-                return rc;
-            attr_set[dv] = true;
-        }
     }
     GridDesc* d = B.desc.as<GridDesc>();
     // the whole build as one enqueue (returns an HR status)
@@ -588,8 +375,8 @@ static int build_once_impl(hr_ctx* c, int32_t kind, int32_t exact, uint32_t* ovf
         };
         mark();
         // launches of this function (radix sort and scans count their own)
-        c->launches += 3 + (nblocks > 0 ? 3 : 0) + 2 + (kind == kTwoLevel ? 6 : 0);
-        k_desc_init<<<1, 1, 0, s>>>(d, kind, ntri, c->counters.as<uint32_t>() + 2, B.ctl.as<uint32_t>());
+        c->launches += 3 + (nblocks > 0 ? 3 : 0) + 2 + (kind == kTwoLevel ? 9 : 0);
+        k_desc_init<<<1, 1, 0, s>>>(d, kind, ntri, c->counters.as<uint32_t>() + 2);
         const int gridv = std::max(1, std::min((int)((c->nverts + kBT - 1) / kBT), c->num_sms * 8));
         k_lerp_bounds<<<gridv, kBT, 0, s>>>(c->lerp_pending ? c->keyframes.as<float4>() : nullptr,
                                             c->frame_sel.as<int4>(), c->verts.as<float4>(), c->nverts, d);
@@ -643,18 +430,19 @@ static int build_once_impl(hr_ctx* c, int32_t kind, int32_t exact, uint32_t* ovf
                                       &d->req_leaf_pairs, s)))
                 return rc;
             k_leaf_write_pairs<<<nref_blocks, kBT, 0, s>>>(B.ref_ranges.as<uint4>(), d, lsum, B.lkeys_a.as<uint32_t>(),
-                                                           B.lvals_a.as<uint32_t>(), sorted_keys, B.cell_pb.as<uint32_t>(),
-                                                           B.cell_pe.as<uint32_t>());
+                                                           B.lvals_a.as<uint32_t>());
             mark();
-            // a12-a13: each top cell's segment sorted stably by leaf where it lies
-            c->launches += 2;
-            k_leaf_cells<<<gcells, 256, 0, s>>>(d, ranges, B.cells.as<uint2>(), B.cell_pb.as<uint32_t>(),
-                                                B.cell_pe.as<uint32_t>(), B.lvals_a.as<uint32_t>(), B.leaves.as<uint2>(),
-                                                B.prims.as<uint32_t>(), B.ctl.as<uint32_t>(), B.big_list.as<uint32_t>());
-            k_leaf_cells_big<<<c->num_sms, kSegT, kSegDynSmem, s>>>(
-                d, B.cells.as<uint2>(), B.cell_pb.as<uint32_t>(), B.cell_pe.as<uint32_t>(), B.lkeys_a.as<uint32_t>(),
-                B.lvals_a.as<uint32_t>(), B.leaves.as<uint2>(), B.prims.as<uint32_t>(), B.ctl.as<uint32_t>(),
-                B.big_list.as<uint32_t>(), B.seg_words.as<unsigned long long>());
+            uint32_t* leaf_keys = (leaf_passes % 2 == 1) ? B.lkeys_b.as<uint32_t>() : B.lkeys_a.as<uint32_t>();
+            if ((rc = radix_sort_pairs(c, B.lkeys_a.as<uint32_t>(), B.lvals_a.as<uint32_t>(), B.lkeys_b.as<uint32_t>(),
+                                       B.lvals_b.as<uint32_t>(), leaf_keys, B.prims.as<uint32_t>(), &d->npairs,
+                                       B.cap_leaf_pairs, leaf_bits, B.tile_hist.as<uint32_t>(), B.tile_hist.bytes,
+                                       B.row_total.as<uint32_t>(), s)))
+                return rc;
+            mark();
+            const int gleaves = std::max(1, std::min((int)((B.cap_leaves + 255) / 256), c->num_sms * 16));
+            k_fill_u2<<<gleaves, 256, 0, s>>>(B.leaves.as<uint2>(), &d->nleaves, d, make_uint2(0u, 0u));
+            const int glp = std::max(1, std::min((int)((B.cap_leaf_pairs + 255) / 256), c->num_sms * 16));
+            k_cell_ranges<<<glp, 256, 0, s>>>(leaf_keys, &d->npairs, &d->nleaves, d, B.leaves.as<uint2>());
             mark();
         }
         c->nstages = ev;

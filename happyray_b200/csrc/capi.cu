@@ -258,8 +258,7 @@ void hr_destroy(hr_ctx* c) {
                       &c->g.prims, &c->g.keys_a, &c->g.vals_a, &c->g.keys_b, &c->g.vals_b, &c->g.block_sums,
                       &c->g.tile_hist, &c->g.row_total, &c->g.top_ranges, &c->g.top_refs, &c->g.leaf_cnt,
                       &c->g.lkeys_a, &c->g.lvals_a, &c->g.lkeys_b, &c->g.lvals_b, &c->g.scan_partials,
-                      &c->g.tri_ranges, &c->g.ref_ranges, &c->g.cell_pb, &c->g.cell_pe, &c->g.ctl,
-                      &c->g.big_list, &c->g.seg_words, &c->lights_dev,
+                      &c->g.tri_ranges, &c->g.ref_ranges, &c->lights_dev,
                       &c->hit_t, &c->hit_tri, &c->unocc, &c->queue};
     for (DevBuf* b : bufs) free_buf(c, *b);
     cudaStreamSynchronize(c->stream);

@@ -66,15 +66,14 @@ struct PairRun { uint32_t key0, ex, ey, sx, sxy, val; };
 // from out0, and pair j of the block is stored by thread j mod NT, so a run of thousands of
 // cells costs its block a few strides instead of one thread a serial loop, and consecutive
 // threads store consecutive slots.  n is this thread's run length, run is read when n > 0.
-// Every thread of the block calls it; it returns where this thread's run starts (from out0).
+// Every thread of the block calls it.
 template <int NT>
-__device__ __forceinline__ uint32_t block_write_runs(uint32_t n, const PairRun& run, uint32_t out0,
-                                                     uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+__device__ __forceinline__ void block_write_runs(uint32_t n, const PairRun& run, uint32_t out0,
+                                                 uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
     __shared__ uint32_t s_off[NT];
     __shared__ PairRun s_run[NT];
     uint32_t tot;
-    const uint32_t mine = block_excl_scan<uint32_t, NT>(n, &tot);
-    s_off[threadIdx.x] = mine;
+    s_off[threadIdx.x] = block_excl_scan<uint32_t, NT>(n, &tot);
     if (n) s_run[threadIdx.x] = run;
     __syncthreads();
     for (uint32_t j = threadIdx.x; j < tot; j += NT) {
@@ -89,7 +88,6 @@ __device__ __forceinline__ uint32_t block_write_runs(uint32_t n, const PairRun& 
         keys[out0 + j] = key;
         vals[out0 + j] = q.val;
     }
-    return out0 + mine;
 }
 
 

@@ -55,12 +55,6 @@ struct GridBuffers {
     DevBuf scan_partials; // generic scan partial sums
     DevBuf tri_ranges;    // uint4 per triangle: its cell range (16-bit coordinates) and pair count
     DevBuf ref_ranges;    // two-level: uint4 per top-level reference: sub-cell range, first leaf, triangle
-    // per-scene leaf stage (build.cu): each top cell's segment of leaf pairs, the cells
-    // sorted by one CTA each, and the global scratch of segments too large for shared memory
-    DevBuf cell_pb, cell_pe;   // uint32 per top cell: its leaf pairs [pb, pe)
-    DevBuf ctl;           // build control words (work list length and counter)
-    DevBuf big_list;      // top cells sorted by one CTA each
-    DevBuf seg_words;     // 2 x 64-bit words per leaf pair
     size_t cap_cells = 0, cap_pairs = 0, cap_top_pairs = 0, cap_leaves = 0, cap_leaf_pairs = 0;
     // largest sizes seen by a completed build: the capacities (which size the count, scan
     // and sort launches) follow them with headroom instead of the first estimates
