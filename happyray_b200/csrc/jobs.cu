@@ -211,6 +211,7 @@ __global__ __launch_bounds__(kJobTT, PT ? HR_JOB_PT_MIN_BLOCKS : HR_JOB_MIN_BLOC
         add_rays<false>(counter, false, valid ? 1u : 0u);
         if (rays) {
             if (valid) {
+                if (h.hit) refine_uv(T.s, h.tri, o, d, &h.u, &h.v);
                 T.out_id[pix] = h.hit ? (int32_t)h.tri : -1;
                 T.out_t[pix] = h.hit ? h.t : FLT_MAX;
                 T.out_u[pix] = h.u;

@@ -54,6 +54,7 @@ __global__ __launch_bounds__(kTT, HR_TRACE_MIN_BLOCKS) void k_trace_rays(Scene s
         Hit h;
         trace_one<KIND, false, STATS>(s, g, o, d, FLT_MAX, h, valid);
         if (valid) {
+            if (h.hit) refine_uv(s, h.tri, o, d, &h.u, &h.v);
             oid[i] = h.hit ? (int32_t)h.tri : -1;
             ot[i] = h.hit ? h.t : FLT_MAX;
             ou[i] = h.u;
@@ -75,8 +76,10 @@ __global__ __launch_bounds__(kTT, HR_TRACE_MIN_BLOCKS) void k_trace_primary(Scen
         uint32_t i;
         const bool valid = tile_pixel(cam, slot, &i);
         Hit h;
-        trace_one<KIND, false, STATS>(s, g, o, valid ? primary_dir(cam, i) : mk(1.0f, 0.0f, 0.0f), FLT_MAX, h, valid);
+        const f3 d = valid ? primary_dir(cam, i) : mk(1.0f, 0.0f, 0.0f);
+        trace_one<KIND, false, STATS>(s, g, o, d, FLT_MAX, h, valid);
         if (valid) {
+            if (h.hit) refine_uv(s, h.tri, o, d, &h.u, &h.v);
             oid[i] = h.hit ? (int32_t)h.tri : -1;
             ot[i] = h.hit ? h.t : FLT_MAX;
             ou[i] = h.u;

@@ -78,6 +78,28 @@ __device__ __forceinline__ bool mt_test(const Scene& s, uint32_t tri, f3 o, f3 d
     return u >= 0.0f && v >= 0.0f && u + v <= 1.0f && t > kIsectEps && t < tbest;
 }
 
+// Barycentric weights (u, v) of the hit of ray (o, d) on triangle tri, reported by the ray
+// queries: Moller-Trumbore evaluated in binary64 from the binary32 inputs, once per ray.
+// The traversal's binary32 weights carry up to ~6e-5 absolute error when the origin is far
+// from a small triangle (the differences of nearly equal products); in binary64 the
+// result is within a rounding of the exact weights of the same inputs.
+__device__ __forceinline__ void refine_uv(const Scene& s, uint32_t tri, f3 o, f3 d, float* ou, float* ov) {
+    f3 p[3];
+    tri_fetch(s.tris, tri, p);
+    const double ax = p[0].x, ay = p[0].y, az = p[0].z;
+    const double e1x = (double)p[1].x - ax, e1y = (double)p[1].y - ay, e1z = (double)p[1].z - az;
+    const double e2x = (double)p[2].x - ax, e2y = (double)p[2].y - ay, e2z = (double)p[2].z - az;
+    const double dx = d.x, dy = d.y, dz = d.z;
+    const double px = dy * e2z - dz * e2y, py = dz * e2x - dx * e2z, pz = dx * e2y - dy * e2x;
+    const double det = e1x * px + e1y * py + e1z * pz;
+    const double sx = (double)o.x - ax, sy = (double)o.y - ay, sz = (double)o.z - az;
+    const double u = (sx * px + sy * py + sz * pz) / det;
+    const double qx = sy * e1z - sz * e1y, qy = sz * e1x - sx * e1z, qz = sx * e1y - sy * e1x;
+    const double v = (qx * dx + qy * dy + qz * dz) / det;
+    *ou = (float)u;
+    *ov = (float)v;
+}
+
 // hit modes of a traversal: closest hit, any hit, or per lane (the lane's `any` argument)
 constexpr int kHitClosest = 0, kHitAny = 1, kHitMixed = 2;
 

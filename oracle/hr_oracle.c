@@ -646,6 +646,25 @@ static inline void trace_one(const orc_scene *s, f3 o, f3 d, float tmax, int any
     else trace_tl(s, o, d, anyhit, h);
 }
 
+/* (u, v) of the hit of ray (o, d) on triangle tri reported by the ray queries:
+ * Moller-Trumbore in binary64 from the binary32 inputs, in the library's operation order */
+static inline void refine_uv(const orc_scene *s, uint32_t tri, f3 o, f3 d, float *ou, float *ov) {
+    const f3 p0 = vtx(s->v4, s->idx[3 * (size_t)tri]), p1 = vtx(s->v4, s->idx[3 * (size_t)tri + 1]),
+             p2 = vtx(s->v4, s->idx[3 * (size_t)tri + 2]);
+    const double ax = p0.x, ay = p0.y, az = p0.z;
+    const double e1x = (double)p1.x - ax, e1y = (double)p1.y - ay, e1z = (double)p1.z - az;
+    const double e2x = (double)p2.x - ax, e2y = (double)p2.y - ay, e2z = (double)p2.z - az;
+    const double dx = d.x, dy = d.y, dz = d.z;
+    const double px = dy * e2z - dz * e2y, py = dz * e2x - dx * e2z, pz = dx * e2y - dy * e2x;
+    const double det = e1x * px + e1y * py + e1z * pz;
+    const double sx = (double)o.x - ax, sy = (double)o.y - ay, sz = (double)o.z - az;
+    const double u = (sx * px + sy * py + sz * pz) / det;
+    const double qx = sy * e1z - sz * e1y, qy = sz * e1x - sx * e1z, qz = sx * e1y - sy * e1x;
+    const double v = (qx * dx + qy * dy + qz * dz) / det;
+    *ou = (float)u;
+    *ov = (float)v;
+}
+
 void orc_trace(const orc_scene *s, const float *org, const float *dir, uint32_t n,
                int32_t *id, float *t, float *u, float *v, uint32_t *stats) {
 #pragma omp parallel for schedule(dynamic, 256)
@@ -653,6 +672,7 @@ void orc_trace(const orc_scene *s, const float *org, const float *dir, uint32_t 
         size_t i = (size_t)ii;
         hitrec h;
         trace_one(s, ld3(org + 3 * i), ld3(dir + 3 * i), FLT_MAX, 0, &h);
+        if (h.hit) refine_uv(s, h.tri, ld3(org + 3 * i), ld3(dir + 3 * i), &h.u, &h.v);
         id[i] = h.hit ? (int32_t)h.tri : -1;
         t[i] = h.hit ? h.t : FLT_MAX;
         u[i] = h.u; v[i] = h.v;
@@ -668,7 +688,9 @@ void orc_trace_primary(const orc_scene *s, const orc_camera *c, int32_t *id,
     for (long long ii = 0; ii < (long long)n; ++ii) {
         size_t i = (size_t)ii;
         hitrec h;
-        trace_one(s, o, primary_dir(c, (uint32_t)i), FLT_MAX, 0, &h);
+        const f3 d = primary_dir(c, (uint32_t)i);
+        trace_one(s, o, d, FLT_MAX, 0, &h);
+        if (h.hit) refine_uv(s, h.tri, o, d, &h.u, &h.v);
         id[i] = h.hit ? (int32_t)h.tri : -1;
         t[i] = h.hit ? h.t : FLT_MAX;
         u[i] = h.u; v[i] = h.v;
@@ -895,9 +917,6 @@ void orc_render_ao(const orc_scene *s, const orc_camera *c, int32_t spp, float a
     if (counts) counts[0] += rays;
 }
 
-/* a20: path tracing with next-event estimation towards one quad light (PathTracer.h
- * pathTrace 41-372 / tracePath 374-747 structure, configured as a fixed number of
- * extension rays, Lambertian albedo, no Russian roulette). */
 /* A light of the collection with the values the path tracer forms once: the edge cross
  * product nc, 1 / |nc|^2 (for the parallelogram coordinates), area |nc|, sampling weight
  * area * emission.  cdf: inclusive running sum of the weights (LightSource.hpp:185-190). */
@@ -940,6 +959,9 @@ static inline float light_hit(const light_q *q, f3 o, f3 d) {
     return (a >= 0.0f && a <= 1.0f && b >= 0.0f && b <= 1.0f) ? tl : -1.0f;
 }
 
+/* a20: path tracing with next-event estimation towards a light collection (PathTracer.h
+ * pathTrace 41-372 / tracePath 374-747 structure, configured as a fixed number of
+ * extension rays, Lambertian albedo, no Russian roulette). */
 void orc_render_pt(const orc_scene *s, const orc_camera *c, const orc_light *l, int32_t nlights,
                    int32_t bounces, float albedo, float ray_eps, uint64_t seed,
                    int32_t image_id, float *fb, uint32_t pixel_stride, uint64_t *counts) {

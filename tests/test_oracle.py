@@ -210,12 +210,15 @@ def test_tl_build_invariants(oracle, small_clusters):
 
 def compare_fp64(oracle, v4, f, org, d, hid, t, u, v, tol=1e-5):
     """Ids equal to the FP64 brute force except at flagged ties / edges / grazing hits;
-    t within `tol` relative; hit point from (u, v) within `tol` relative to its magnitude."""
+    t and the barycentric weights u, v within `tol` relative; and the hit point from (u, v)
+    within `tol` relative to its magnitude."""
     bid, bt, bu, bv, fl = oracle.brute_f64(v4, f, org, d)
     unflagged = fl == 0
     assert np.array_equal(hid[unflagged], bid[unflagged])
     m = unflagged & (bid >= 0)
     assert np.all(np.abs(t[m] - bt[m]) <= tol * bt[m])
+    assert np.all(np.abs(u[m] - bu[m]) <= tol * np.abs(bu[m]) + 1e-30)
+    assert np.all(np.abs(v[m] - bv[m]) <= tol * np.abs(bv[m]) + 1e-30)
     tri = v4[f[bid[m]]][:, :, :3].astype(np.float64)
     e1, e2 = tri[:, 1] - tri[:, 0], tri[:, 2] - tri[:, 0]
     dp = (u[m] - bu[m])[:, None] * e1 + (v[m] - bv[m])[:, None] * e2
