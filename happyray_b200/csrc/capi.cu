@@ -528,6 +528,14 @@ hr_status hr_trace_primary_device(hr_ctx* c, int32_t* id, float* t, float* u, fl
     return (hr_status)launch_trace_primary(c, id, t, u, v, stats);
 }
 
+hr_status hr_render_rays_device(hr_ctx* c, const float* org, const float* dir, uint32_t n, int32_t image_id,
+                                float* fb) {
+    if (bad(c) || (n && (!org || !dir || !fb)) || image_id < 0) return HR_ERR_INVALID_ARG;
+    if (!c->built) return (hr_status)set_error(c, HR_ERR_NOT_READY, "render_rays: build a grid first");
+    DeviceGuard dg(c->device);
+    return (hr_status)launch_render_rays(c, org, dir, n, image_id, fb);
+}
+
 hr_status hr_occluded_device(hr_ctx* c, const float* org, const float* dir, const float* tmax, uint32_t n, uint8_t* occ) {
     if (bad(c) || (n && (!org || !dir || !tmax || !occ))) return HR_ERR_INVALID_ARG;
     if (!c->built) return (hr_status)set_error(c, HR_ERR_NOT_READY, "occluded: build a grid first");

@@ -229,5 +229,6 @@ int launch_trace_primary(hr_ctx* c, int32_t* id, float* t, float* u, float* v, u
 int launch_render(hr_ctx* c, int32_t mode, int32_t image_id, float* d_fb);
 int launch_occluded(hr_ctx* c, const float* org, const float* dir, const float* tmax, uint32_t n,
                     uint8_t* occluded);
+int launch_render_rays(hr_ctx* c, const float* org, const float* dir, uint32_t n, int32_t image_id, float* fb);
 
 }  // namespace hr

@@ -89,6 +89,35 @@ __global__ __launch_bounds__(kTT, HR_TRACE_MIN_BLOCKS) void k_trace_primary(Scen
     }
 }
 
+// the ray-file form of render mode 0 (SimpleRayTraverser::integrate,
+// SimpleRayTraverser.h:166-180): ray i traced (closest hit) and shaded by simpleShade into
+// pixel i, progressive blend
+template <int KIND>
+__global__ __launch_bounds__(kTT, HR_TRACE_MIN_BLOCKS) void k_render_rays(Scene s, const float* __restrict__ org,
+                                                                     const float* __restrict__ dir, uint32_t n,
+                                                                     int32_t image_id, float* __restrict__ fb,
+                                                                     unsigned long long* counter) {
+    const G g = load_g(s.desc);
+    gate_scene(s);
+    const uint32_t nl = round32(n);
+    for (uint32_t i = blockIdx.x * kTT + threadIdx.x; i < nl; i += gridDim.x * kTT) {
+        const bool valid = i < n;
+        f3 o = mk(0.0f, 0.0f, 0.0f), d = mk(1.0f, 0.0f, 0.0f);
+        if (valid) {
+            o = mk(__ldg(org + 3 * (size_t)i), __ldg(org + 3 * (size_t)i + 1), __ldg(org + 3 * (size_t)i + 2));
+            d = mk(__ldg(dir + 3 * (size_t)i), __ldg(dir + 3 * (size_t)i + 1), __ldg(dir + 3 * (size_t)i + 2));
+        }
+        Hit h;
+        trace_one<KIND, false, false>(s, g, o, d, FLT_MAX, h, valid);
+        if (valid) {
+            float rgb[3];
+            simple_shade(s, h.hit, h.tri, o, d, rgb);
+            for (int k = 0; k < 3; ++k) fb[3 * (size_t)i + k] = blend(fb[3 * (size_t)i + k], rgb[k], image_id);
+        }
+        add_rays<false>(counter, false, valid ? 1u : 0u);
+    }
+}
+
 template <int KIND>
 __global__ __launch_bounds__(kTT, HR_TRACE_MIN_BLOCKS) void k_occluded(Scene s, const float* __restrict__ org, const float* __restrict__ dir,
                                                   const float* __restrict__ tmax, uint32_t n, uint8_t* __restrict__ occ) {
@@ -537,6 +566,17 @@ int launch_trace_primary(hr_ctx* c, int32_t* id, float* t, float* u, float* v, u
         k_trace_primary<K(), S()><<<gb, kTT, 0, c->stream>>>(s, k, id, t, u, v, stats);
     });
     return cuda_check(c, cudaGetLastError(), "trace_primary launch");
+}
+
+int launch_render_rays(hr_ctx* c, const float* org, const float* dir, uint32_t n, int32_t image_id, float* fb) {
+    if (n == 0) return 0;
+    c->launches += 1;
+    const Scene s = make_scene(c);
+    unsigned long long* ctr = c->counters.as<unsigned long long>();
+    by_kind(s.kind, false, [&](auto K, auto) {
+        k_render_rays<K()><<<grid_for(c, n), kTT, 0, c->stream>>>(s, org, dir, n, image_id, fb, ctr);
+    });
+    return cuda_check(c, cudaGetLastError(), "render_rays launch");
 }
 
 int launch_occluded(hr_ctx* c, const float* org, const float* dir, const float* tmax, uint32_t n, uint8_t* occ) {

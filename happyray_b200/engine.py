@@ -223,6 +223,11 @@ class Engine:
         self._chk(self.L.hr_trace_primary_device(self.ctx, _ptr(d_id), _ptr(d_t), _ptr(d_u), _ptr(d_v),
                                                  _ptr(d_stats)), "hr_trace_primary_device")
 
+    def render_rays_device(self, d_org, d_dir, n, image_id, d_fb):
+        """Ray-file form of renderFrame mode 0: ray i shaded into pixel i (device buffers)."""
+        self._chk(self.L.hr_render_rays_device(self.ctx, _ptr(d_org), _ptr(d_dir), n, image_id, _ptr(d_fb)),
+                  "hr_render_rays_device")
+
     def occluded_device(self, d_org, d_dir, d_tmax, n, d_occ):
         self._chk(self.L.hr_occluded_device(self.ctx, _ptr(d_org), _ptr(d_dir), _ptr(d_tmax), n, _ptr(d_occ)),
                   "hr_occluded_device")

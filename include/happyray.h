@@ -141,6 +141,12 @@ hr_status hr_trace_rays_device(hr_ctx *ctx, const float *d_org, const float *d_d
 /* Camera rays of the current camera (RegularPrimaryRayGenerator, RayGenerators.h:40-69). */
 hr_status hr_trace_primary_device(hr_ctx *ctx, int32_t *d_id, float *d_t, float *d_u, float *d_v,
                                   uint32_t *d_stats);
+/* The ray-file form of RTEngine::renderFrame mode 0 (RTEngine.cu:410-414,
+ * SimpleRayTraverser.h:166-180): ray i (xyz origin and direction triples, device) is traced
+ * and shaded as a mode-0 camera ray (simpleShade) into pixel i of the float3 frame buffer
+ * (device, n pixels), blended with weight 1 / (image_id + 1). */
+hr_status hr_render_rays_device(hr_ctx *ctx, const float *d_org, const float *d_dir, uint32_t n,
+                                int32_t image_id, float *d_framebuffer_rgb);
 /* Any-hit within (1e-4, tmax[i]) per ray (shadow / AO traversal, UGridTraverser.h:68-74). */
 hr_status hr_occluded_device(hr_ctx *ctx, const float *d_org, const float *d_dir,
                              const float *d_tmax, uint32_t n, uint8_t *d_occluded);

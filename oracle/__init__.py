@@ -94,6 +94,7 @@ def lib():
                 "orc_render_ao": (None, [C.POINTER(Scene), C.POINTER(Camera), I32, F, U64, I32, P, U32, P]),
                 "orc_render_primary": (None, [C.POINTER(Scene), C.POINTER(Camera), I32, U64, P]),
                 "orc_log_series": (F, [F]),
+                "orc_render_rays": (None, [C.POINTER(Scene), P, P, U32, I32, P]),
                 "orc_render_pt": (None, [C.POINTER(Scene), C.POINTER(Camera), C.POINTER(Light), I32, I32, F, F, U64, I32, P, U32, P]),
                 "orc_brute_f64": (None, [P, P, U32, P, P, U32, P, P, P, P, P]),
                 "orc_sincos2pi": (None, [F, C.POINTER(F), C.POINTER(F)]),
@@ -292,6 +293,17 @@ def render_primary(b: Built, cam: Camera, image_id: int, seed: int, fb=None):
     fb = np.zeros((n, 3), np.float32) if fb is None else np.ascontiguousarray(fb, np.float32).reshape(n, 3)
     s = b.scene()
     lib().orc_render_primary(C.byref(s), C.byref(cam), image_id, seed, _p(fb))
+    return fb
+
+
+def render_rays(b: Built, org, dirs, image_id: int = 0, fb=None):
+    """Ray-file form of render mode 0: ray i traced and shaded into pixel i (n x 3 floats)."""
+    org = np.ascontiguousarray(org, np.float32)
+    dirs = np.ascontiguousarray(dirs, np.float32)
+    n = org.shape[0]
+    fb = np.zeros((n, 3), np.float32) if fb is None else np.ascontiguousarray(fb, np.float32).reshape(n, 3)
+    s = b.scene()
+    lib().orc_render_rays(C.byref(s), _p(org), _p(dirs), n, image_id, _p(fb))
     return fb
 
 

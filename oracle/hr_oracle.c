@@ -844,9 +844,29 @@ static inline f3 primary_sample_dir(const orc_camera *c, uint32_t pix, int32_t i
     return normalize(d);
 }
 
-/* render mode 0: simpleShade (SimpleIntegrator.h:41-126) of the closest hit, weights from
- * the ray origin's cross products, progressive blend of the 3 channels into fb (3 floats
- * per pixel) */
+/* simpleShade (SimpleIntegrator.h:41-126) of a closest hit: weights from the ray origin's
+ * cross products, colour (u, v, 1 - u - v) times |cos|; background on a miss */
+static inline void simple_shade(const orc_scene *s, const hitrec *h, f3 o, f3 d, float *rgb) {
+    rgb[0] = 0.15f; rgb[1] = 0.2f; rgb[2] = 0.3f;
+    if (!h->hit) return;
+    const f3 p0 = vtx(s->v4, s->idx[3 * (size_t)h->tri]), p1 = vtx(s->v4, s->idx[3 * (size_t)h->tri + 1]),
+             p2 = vtx(s->v4, s->idx[3 * (size_t)h->tri + 2]);
+    const f3 nr = cross(sub(p1, p0), sub(p2, p0));
+    const f3 a0 = sub(p0, o), a1 = sub(p1, o), a2 = sub(p2, o);
+    const f3 n0 = cross(a1, a2), n1 = cross(a2, a0);
+    const float inv = 1.0f / sqrtf(dot(nr, nr));
+    const float u = sqrtf(dot(n0, n0)) * inv;
+    const float v = sqrtf(dot(n1, n1)) * inv;
+    const f3 nrm = normalize(nr);
+    const f3 dn = normalize(d);
+    const float cs = fmaxf(0.0f, fabsf(dot(mk(-nrm.x, -nrm.y, -nrm.z), dn)));
+    rgb[0] = u * cs;
+    rgb[1] = v * cs;
+    rgb[2] = (1.0f - u - v) * cs;
+}
+
+/* render mode 0: camera rays of the mode-0 samplers, simpleShade, progressive blend of the
+ * 3 channels into fb (3 floats per pixel) */
 void orc_render_primary(const orc_scene *s, const orc_camera *c, int32_t image_id, uint64_t seed, float *fb) {
     const uint32_t n = (uint32_t)c->w * (uint32_t)c->h;
     const f3 o = ld3(c->pos);
@@ -858,24 +878,26 @@ void orc_render_primary(const orc_scene *s, const orc_camera *c, int32_t image_i
         const f3 d = primary_sample_dir(c, pix, image_id, seed);
         hitrec h;
         trace_one(s, o, d, FLT_MAX, 0, &h);
-        float rgb[3] = {0.15f, 0.2f, 0.3f};
-        if (h.hit) {
-            const f3 p0 = vtx(s->v4, s->idx[3 * (size_t)h.tri]), p1 = vtx(s->v4, s->idx[3 * (size_t)h.tri + 1]),
-                     p2 = vtx(s->v4, s->idx[3 * (size_t)h.tri + 2]);
-            const f3 nr = cross(sub(p1, p0), sub(p2, p0));
-            const f3 a0 = sub(p0, o), a1 = sub(p1, o), a2 = sub(p2, o);
-            const f3 n0 = cross(a1, a2), n1 = cross(a2, a0);
-            const float inv = 1.0f / sqrtf(dot(nr, nr));
-            const float u = sqrtf(dot(n0, n0)) * inv;
-            const float v = sqrtf(dot(n1, n1)) * inv;
-            const f3 nrm = normalize(nr);
-            const f3 dn = normalize(d);
-            const float cs = fmaxf(0.0f, fabsf(dot(mk(-nrm.x, -nrm.y, -nrm.z), dn)));
-            rgb[0] = u * cs;
-            rgb[1] = v * cs;
-            rgb[2] = (1.0f - u - v) * cs;
-        }
+        float rgb[3];
+        simple_shade(s, &h, o, d, rgb);
         for (int k = 0; k < 3; ++k) fb[3 * (size_t)pix + k] = fb[3 * (size_t)pix + k] * ow + rgb[k] * nw;
+    }
+}
+
+/* the ray-file form of render mode 0 (SimpleRayTraverser.h:166-180): ray i shaded into pixel i */
+void orc_render_rays(const orc_scene *s, const float *org, const float *dir, uint32_t n, int32_t image_id,
+                     float *fb) {
+    const float nw = 1.0f / (float)(image_id + 1);
+    const float ow = 1.0f - nw;
+#pragma omp parallel for schedule(dynamic, 256)
+    for (long long ii = 0; ii < (long long)n; ++ii) {
+        const size_t i = (size_t)ii;
+        const f3 o = ld3(org + 3 * i), d = ld3(dir + 3 * i);
+        hitrec h;
+        trace_one(s, o, d, FLT_MAX, 0, &h);
+        float rgb[3];
+        simple_shade(s, &h, o, d, rgb);
+        for (int k = 0; k < 3; ++k) fb[3 * i + k] = fb[3 * i + k] * ow + rgb[k] * nw;
     }
 }
 

@@ -120,6 +120,9 @@ void orc_render_ao(const orc_scene *s, const orc_camera *c, int32_t spp, float a
  * (SimpleIntegrator.h:41-126), progressive blend into fb (3 floats per pixel) */
 void orc_render_primary(const orc_scene *s, const orc_camera *c, int32_t image_id, uint64_t seed, float *fb);
 float orc_log_series(float x);
+/* the ray-file form of render mode 0 (SimpleRayTraverser.h:166-180): ray i shaded into pixel i */
+void orc_render_rays(const orc_scene *s, const float *org, const float *dir, uint32_t n, int32_t image_id,
+                     float *fb);
 void orc_render_pt(const orc_scene *s, const orc_camera *c, const orc_light *l, int32_t nlights,
                    int32_t bounces, float albedo, float ray_eps, uint64_t seed,
                    int32_t image_id, float *fb, uint32_t pixel_stride, uint64_t *counts);

@@ -307,6 +307,29 @@ def test_render_primary_mode0(engine, oracle, c1_scene, kind):
     assert 0 < miss.sum() < miss.size
 
 
+def test_render_rays_ray_file_mode(engine, oracle, small_clusters):
+    """The ray-file form of render mode 0 (hr_render_rays_device): ray i traced and shaded by
+    simpleShade into pixel i, bit-exact against the oracle, over two progressive images."""
+    import torch
+    v, f = small_clusters
+    gpu_build(engine, v, f, GRID_TWO_LEVEL)
+    b = oracle_build(oracle, v, f, GRID_TWO_LEVEL)
+    rng = np.random.default_rng(12)
+    n = 4000
+    org = rng.uniform(v.min(0), v.max(0), (n, 3)).astype(np.float32)
+    dirs = rng.normal(size=(n, 3)).astype(np.float32)
+    d_org, d_dir = torch.from_numpy(org).cuda(), torch.from_numpy(dirs).cuda()
+    d_fb = torch.zeros((n, 3), dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+    want = None
+    for im in range(2):
+        engine.render_rays_device(d_org, d_dir, n, im, d_fb)
+        engine.sync()
+        want = oracle.render_rays(b, org, dirs, im, want)
+        assert np.array_equal(d_fb.cpu().numpy(), want)
+    assert 0 < (want[:, 0] == 0.15).sum() < n
+
+
 def test_radix_sort_and_scan_device(engine):
     import torch
     rng = np.random.default_rng(7)
