@@ -647,6 +647,20 @@ def run_served(args, rank, ws, local):
         served = serve_run(pool, reqs, BATCHED, budget)
         serial = serve_run(pool, reqs, SERIAL, budget)
         plain = serve_run(pool, reqs, PLAIN, budget)
+        # latency of continuous batching at loads the server sustains: the same request mix
+        # arriving at 50% and 80% of the request rate the server just completed at 2000 req/s
+        capacity_rps = served["completed_per_s"]
+        at_load = []
+        if not args.no_load_sweep:
+            for frac in (0.5, 0.8):
+                rate = frac * capacity_rps
+                n_l = max(50, min(n_req, int(rate * args.load_seconds)))
+                lreqs = served_requests(pool, n_l, rate, seed=1)
+                r = serve_run(pool, lreqs, BATCHED, budget)
+                at_load.append({"offered_fraction_of_capacity": frac, "arrival_rate_rps": rate, "requests": n_l,
+                                "p50_ms": r["p50_ms"], "p99_ms": r["p99_ms"], "mean_ms": r["mean_ms"],
+                                "mrays_s": r["mrays_s"], "completed_per_s": r["completed_per_s"],
+                                "waves": r["waves"]})
     if rank != 0:
         return
     line = {
@@ -666,6 +680,8 @@ def run_served(args, rank, ws, local):
         "speedup_vs_plain": served["mrays_s"] / plain["mrays_s"],
         "speedup_vs_serial_resident": served["mrays_s"] / serial["mrays_s"],
         "p50_ms": served["p50_ms"], "p99_ms": served["p99_ms"],
+        "capacity_rps": capacity_rps,
+        "latency_at_sustained_load": at_load,
         "timing": "wall clock from each request's submission to its completion (results in pinned host memory); "
                   "throughput = rays / (last completion - first submission)",
         "scene_generation_s": gen_s,
@@ -888,6 +904,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="c4: skip the autotuner (densities 1/16, 2)")
     ap.add_argument("--no-rebuild2m", action="store_true", help="c2: skip the 2M-triangle key-frame rebuild")
+    ap.add_argument("--no-load-sweep", action="store_true", help="c5: skip the latency runs at sustained loads")
+    ap.add_argument("--load-seconds", type=float, default=6.0, help="c5: arrival span of each sustained-load run")
     args = ap.parse_args()
     rank, ws, local = dist_setup() if os.environ.get("WORLD_SIZE") else (0, 1, 0)
     if args.config == "c4":
