@@ -101,6 +101,8 @@ SIGNATURES = {
     "hr_server_drain": (C.c_int, [P, C.c_int32]),
     "hr_server_request_info": (C.c_int, [P, C.c_uint64, P]),
     "hr_server_get_stats": (C.c_int, [P, P]),
+    "hr_server_set_watchdog": (C.c_int, [P, C.c_int32]),
+    "hr_server_inject_stall": (C.c_int, [P, C.c_uint32, C.c_int32]),
     # scene input, ray files, images
     "hr_scene_load": (C.c_int, [C.c_char_p, C.c_int32, C.POINTER(P)]),
     "hr_scene_load_obj": (C.c_int, [C.c_char_p, C.c_int32, C.POINTER(P)]),
@@ -196,7 +198,7 @@ class ServerStats(C.Structure):
     """hr_server_stats"""
     _fields_ = [("completed", C.c_uint64), ("failed", C.c_uint64), ("waves", C.c_uint64), ("rebuilds", C.c_uint64),
                 ("rays", C.c_uint64), ("resident_bytes", C.c_uint64), ("peak_inflight_bytes", C.c_uint64),
-                ("launches", C.c_uint64), ("trace_ms", C.c_double)]
+                ("launches", C.c_uint64), ("trace_ms", C.c_double), ("watchdog_trips", C.c_uint64)]
 
 
 _lock = threading.Lock()

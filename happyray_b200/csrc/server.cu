@@ -95,6 +95,9 @@ struct Wave {
     cudaEvent_t done = nullptr;
     int slot = 0;
     uint32_t index = 0;
+    uint64_t launched_ns = 0;        // host time of the launch (watchdog)
+    int32_t stall_ms = 0;            // injected: treated as unfinished this long after the launch
+    bool timed_out = false;          // the watchdog failed its requests; its buffers are held until it ends
 };
 
 constexpr int kSlots = 2;
@@ -141,6 +144,10 @@ struct hr_server {
     int blocks_main = 0, blocks_pt = 0;
     uint32_t waves = 0;
     uint64_t completed = 0, failed = 0, rebuilds = 0, host_rays = 0;
+    int32_t watchdog_ms = 0;         // 0: no watchdog
+    uint64_t watchdog_trips = 0;     // waves the watchdog declared stuck
+    uint32_t inject_waves = 0;       // test hook: the next waves are held back ...
+    int32_t inject_ms = 0;           // ... this long after their launch, on the host only
     std::string err;                 // last error (caller-visible)
 };
 
@@ -330,7 +337,9 @@ std::vector<uint64_t> retire_wave(hr_server* S, Wave& w) {
     }
     for (size_t i = 0; i < w.rp.size(); ++i) {
         SrvReq& R = *w.rp[i];
-        if (S->scenes[R.r.scene]->bad_gens.count(R.gen)) {
+        if (w.timed_out) {
+            // the caller was answered with a timeout: nothing is copied to its buffers
+        } else if (S->scenes[R.r.scene]->bad_gens.count(R.gen)) {
             redo.push_back(w.reqs[i]);
         } else if (!R.pinned_out) {
             if (R.r.kind == HR_REQUEST_RAYS) {
@@ -452,10 +461,33 @@ void worker_main(hr_server* S) {
             S->cv_done.notify_all();
             continue;
         }
-        // retire finished waves in launch order
+        // retire finished waves in launch order; the watchdog answers the requests of a wave
+        // still unfinished watchdog_ms after its launch with HR_ERR_TIMEOUT at once (its GPU
+        // work cannot be recalled: its buffers stay held until it ends, and later waves on
+        // the same stream wait behind it)
         bool retired = false;
+        const uint64_t tnow = now_ns();
+        auto finished = [&](Wave& w, cudaError_t* qq) {
+            *qq = cudaEventQuery(w.done);
+            if (*qq == cudaErrorNotReady) return false;
+            return !(w.stall_ms > 0 && tnow - w.launched_ns < (uint64_t)w.stall_ms * 1000000ull);
+        };
+        if (S->watchdog_ms > 0) {
+            for (Wave& w : S->inflight) {
+                cudaError_t qq;
+                if (w.timed_out || tnow - w.launched_ns < (uint64_t)S->watchdog_ms * 1000000ull || finished(w, &qq))
+                    continue;
+                w.timed_out = true;
+                S->watchdog_trips += 1;
+                set_error(S->c, HR_ERR_TIMEOUT, "wave %u unfinished after %d ms: its requests failed", w.index,
+                          S->watchdog_ms);
+                for (SrvReq* rq : w.rp)
+                    if (rq->status == 1) fail_req(S, *rq, HR_ERR_TIMEOUT);
+                retired = true;
+            }
+        }
         cudaError_t q;
-        while (!S->inflight.empty() && (q = cudaEventQuery(S->inflight.front().done)) != cudaErrorNotReady) {
+        while (!S->inflight.empty() && finished(S->inflight.front(), &q)) {
             Wave w = std::move(S->inflight.front());
             S->inflight.pop_front();
             if (q != cudaSuccess) {
@@ -463,7 +495,7 @@ void worker_main(hr_server* S) {
                 set_error(S->c, HR_ERR_DEVICE, "wave %u: %s", w.index, cudaGetErrorString(q));
                 for (SrvReq* rq : w.rp) {
                     S->inflight_bytes -= rq->bytes;
-                    fail_req(S, *rq, HR_ERR_DEVICE);
+                    if (rq->status == 1) fail_req(S, *rq, HR_ERR_DEVICE);
                 }
                 S->slot_busy[w.slot] = false;
                 retired = true;
@@ -476,6 +508,7 @@ void worker_main(hr_server* S) {
             for (size_t i = w.rp.size(); i-- > 0;) {
                 SrvReq& R = *w.rp[i];
                 S->inflight_bytes -= R.bytes;
+                if (w.timed_out) continue;   // answered by the watchdog
                 if (std::find(redo.begin(), redo.end(), w.reqs[i]) != redo.end()) {
                     R.status = 0;
                     S->queue.push_front(w.reqs[i]);
@@ -516,6 +549,11 @@ void worker_main(hr_server* S) {
             if (!w.reqs.empty()) {
                 w.index = S->waves++;
                 w.done = S->wave_ev[w.slot];
+                w.launched_ns = now_ns();
+                if (S->inject_waves > 0) {
+                    S->inject_waves -= 1;
+                    w.stall_ms = S->inject_ms;
+                }
                 S->slot_busy[w.slot] = true;
                 S->inflight_bytes += used;
                 S->peak_inflight = std::max(S->peak_inflight, S->inflight_bytes);
@@ -801,6 +839,23 @@ hr_status hr_server_get_stats(hr_server* S, hr_server_stats* st) {
     st->peak_inflight_bytes = S->peak_inflight;
     st->launches = launches;
     st->trace_ms = S->trace_ms;
+    st->watchdog_trips = S->watchdog_trips;
+    return HR_OK;
+}
+
+hr_status hr_server_set_watchdog(hr_server* S, int32_t timeout_ms) {
+    if (!valid_server(S) || timeout_ms < 0) return HR_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> g(S->m);
+    S->watchdog_ms = timeout_ms;
+    S->cv_work.notify_all();
+    return HR_OK;
+}
+
+hr_status hr_server_inject_stall(hr_server* S, uint32_t waves, int32_t stall_ms) {
+    if (!valid_server(S) || stall_ms < 0) return HR_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> g(S->m);
+    S->inject_waves = waves;
+    S->inject_ms = stall_ms;
     return HR_OK;
 }
 

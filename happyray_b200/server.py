@@ -125,6 +125,15 @@ class Server:
     def drain(self, timeout_ms: int = -1):
         self._chk(self.L.hr_server_drain(self.s, timeout_ms), "drain")
 
+    def set_watchdog(self, timeout_ms: int):
+        """Requests of a wave still unfinished timeout_ms after its launch fail with
+        HR_ERR_TIMEOUT (0: off)."""
+        self._chk(self.L.hr_server_set_watchdog(self.s, int(timeout_ms)), "set_watchdog")
+
+    def inject_stall(self, waves: int, stall_ms: int):
+        """Test hook: the next `waves` waves are held back stall_ms on the host."""
+        self._chk(self.L.hr_server_inject_stall(self.s, int(waves), int(stall_ms)), "inject_stall")
+
     def stats(self) -> dict:
         st = ServerStats()
         self._chk(self.L.hr_server_get_stats(self.s, C.byref(st)), "stats")

@@ -331,6 +331,7 @@ typedef struct hr_server_stats {
     uint64_t peak_inflight_bytes; /* request buffers */
     uint64_t launches;
     double trace_ms;              /* device time of the waves' traversal launches (batched) */
+    uint64_t watchdog_trips;      /* waves the watchdog declared stuck */
 } hr_server_stats;
 
 hr_status hr_server_create(hr_server **out, int32_t device, uint64_t hbm_budget_bytes, int32_t mode);
@@ -353,6 +354,17 @@ hr_status hr_server_wait(hr_server *server, uint64_t request_id, int32_t timeout
 hr_status hr_server_drain(hr_server *server, int32_t timeout_ms);
 hr_status hr_server_request_info(hr_server *server, uint64_t request_id, hr_request_info *info);
 hr_status hr_server_get_stats(hr_server *server, hr_server_stats *stats);
+/* Watchdog (batched mode; no counterpart in the reference): a wave whose GPU work has not
+ * finished timeout_ms after its launch is declared stuck and its requests fail at once
+ * with HR_ERR_TIMEOUT, so that callers waiting on them are answered; the server keeps
+ * admitting and launching.  GPU work cannot be recalled: a stuck wave's device buffers stay
+ * held until it ends, later waves on the server's stream wait behind it, and its requests'
+ * output buffers may still be written until then -- hr_server_drain returns only after
+ * that.  0 turns the watchdog off (the default). */
+hr_status hr_server_set_watchdog(hr_server *server, int32_t timeout_ms);
+/* Test hook for the watchdog: the worker treats each of the next `waves` waves as
+ * unfinished until stall_ms after its launch.  Host side only: the GPU work is untouched. */
+hr_status hr_server_inject_stall(hr_server *server, uint32_t waves, int32_t stall_ms);
 
 /* ---------------------------------------------------------------------------------
  * Scene input, ray files and images (host side; no GPU needed).

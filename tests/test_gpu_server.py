@@ -188,3 +188,25 @@ def test_invalid_requests(hrlib, pool):
             srv.submit_render(0, 99.0, RENDER_AO, 1, cam, SEED)      # beyond the key frames
         with pytest.raises(HRError):
             srv.submit_render(0, 0.0, RENDER_AO, 0, cam, SEED)       # no samples
+
+
+def test_watchdog_answers_a_stuck_wave_and_keeps_serving(hrlib, pool):
+    """A wave whose GPU work has not finished within the watchdog's limit is declared stuck
+    and its requests fail with HR_ERR_TIMEOUT instead of leaving their callers waiting; the
+    server keeps serving.  The stuck wave is made on the host (the worker holds it back:
+    hr_server_inject_stall), no GPU work is stalled."""
+    cam = S.camera_at_bounds(pool[0][0][0], (24, 24))
+    with make_server(pool, BATCHED) as srv:
+        ref = srv.submit_render(0, 1.0, RENDER_AO, 2, cam, SEED).wait(30_000)
+        srv.set_watchdog(150)
+        srv.inject_stall(1, 1500)
+        stuck = srv.submit_render(1, 0.5, RENDER_AO, 2, cam, SEED)
+        with pytest.raises(HRError) as ei:
+            stuck.wait(30_000)
+        assert ei.value.status == 5   # HR_ERR_TIMEOUT
+        assert srv.stats()["watchdog_trips"] == 1
+        # later requests are served (after the held-back wave ends), with the same results
+        again = srv.submit_render(0, 1.0, RENDER_AO, 2, cam, SEED).wait(30_000)
+        assert same(again, ref)
+        srv.drain(30_000)
+        assert srv.stats()["watchdog_trips"] == 1
