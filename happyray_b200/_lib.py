@@ -53,6 +53,8 @@ SIGNATURES = {
     "hr_set_camera": (C.c_int, [P, P, P, P, C.c_float, C.c_int32, C.c_int32]),
     "hr_set_light": (C.c_int, [P, P, P, P, C.c_float]),
     "hr_set_lights": (C.c_int, [P, C.c_uint32, P, P, P, P, P]),
+    "hr_set_normals": (C.c_int, [P, P, C.c_uint32, P]),
+    "hr_set_materials": (C.c_int, [P, P, C.c_uint32, P]),
     "hr_render_rays_device": (C.c_int, [P, P, P, C.c_uint32, C.c_int32, P]),
     "hr_set_integrator": (C.c_int, [P, C.c_int32, C.c_float, C.c_int32, C.c_float, C.c_uint64]),
     "hr_render": (C.c_int, [P, C.c_int32, C.c_int32, P]),

@@ -11,6 +11,7 @@
 #include <cstdio>
 #include <cstring>
 #include <new>
+#include <vector>
 
 namespace hr {
 
@@ -258,7 +259,7 @@ void hr_destroy(hr_ctx* c) {
                       &c->g.prims, &c->g.keys_a, &c->g.vals_a, &c->g.keys_b, &c->g.vals_b, &c->g.block_sums,
                       &c->g.tile_hist, &c->g.row_total, &c->g.top_ranges, &c->g.top_refs, &c->g.leaf_cnt,
                       &c->g.lkeys_a, &c->g.lvals_a, &c->g.lkeys_b, &c->g.lvals_b, &c->g.scan_partials,
-                      &c->g.tri_ranges, &c->g.ref_ranges, &c->lights_dev,
+                      &c->g.tri_ranges, &c->g.ref_ranges, &c->lights_dev, &c->tri_nrm, &c->tri_alb,
                       &c->hit_t, &c->hit_tri, &c->unocc, &c->queue};
     for (DevBuf* b : bufs) free_buf(c, *b);
     cudaStreamSynchronize(c->stream);
@@ -439,6 +440,55 @@ hr_status hr_set_lights(hr_ctx* c, uint32_t n, const float* corners, const float
     if (bad(c)) return HR_ERR_INVALID_ARG;
     DeviceGuard dg(c->device);
     return (hr_status)set_lights(c, n, corners, edge1s, edge2s, normals, emissions);
+}
+
+hr_status hr_set_normals(hr_ctx* c, const float* normals, uint32_t num_normals, const uint32_t* tri_normal_idx) {
+    if (bad(c)) return HR_ERR_INVALID_ARG;
+    if (!normals || !tri_normal_idx || num_normals == 0) {
+        c->nrm_ntri = 0;
+        return HR_OK;
+    }
+    if (c->ntri == 0) return (hr_status)set_error(c, HR_ERR_NOT_READY, "set_normals: upload the mesh first");
+    DeviceGuard dg(c->device);
+    std::vector<float> g((size_t)c->ntri * 12);
+    for (size_t i = 0; i < 3 * (size_t)c->ntri; ++i) {
+        const uint32_t k = tri_normal_idx[i];
+        if (k >= num_normals) return (hr_status)set_error(c, HR_ERR_INVALID_ARG, "set_normals: index %u of %u", k, num_normals);
+        g[4 * i] = normals[3 * (size_t)k]; g[4 * i + 1] = normals[3 * (size_t)k + 1];
+        g[4 * i + 2] = normals[3 * (size_t)k + 2]; g[4 * i + 3] = 0.0f;
+    }
+    int rc;
+    if ((rc = ensure(c, c->tri_nrm, g.size() * sizeof(float)))) return (hr_status)rc;
+    if ((rc = cuda_check(c, cudaMemcpyAsync(c->tri_nrm.p, g.data(), g.size() * sizeof(float), cudaMemcpyHostToDevice,
+                                            c->stream), "normal upload")) ||
+        (rc = cuda_check(c, cudaStreamSynchronize(c->stream), "normal upload")))
+        return (hr_status)rc;
+    c->nrm_ntri = c->ntri;
+    return HR_OK;
+}
+
+hr_status hr_set_materials(hr_ctx* c, const float* albedo, uint32_t num_materials, const uint32_t* tri_material) {
+    if (bad(c)) return HR_ERR_INVALID_ARG;
+    if (!albedo || !tri_material || num_materials == 0) {
+        c->alb_ntri = 0;
+        return HR_OK;
+    }
+    if (c->ntri == 0) return (hr_status)set_error(c, HR_ERR_NOT_READY, "set_materials: upload the mesh first");
+    DeviceGuard dg(c->device);
+    std::vector<float> g(c->ntri);
+    for (size_t i = 0; i < c->ntri; ++i) {
+        const uint32_t k = tri_material[i];
+        if (k >= num_materials) return (hr_status)set_error(c, HR_ERR_INVALID_ARG, "set_materials: index %u of %u", k, num_materials);
+        g[i] = albedo[k];
+    }
+    int rc;
+    if ((rc = ensure(c, c->tri_alb, g.size() * sizeof(float)))) return (hr_status)rc;
+    if ((rc = cuda_check(c, cudaMemcpyAsync(c->tri_alb.p, g.data(), g.size() * sizeof(float), cudaMemcpyHostToDevice,
+                                            c->stream), "material upload")) ||
+        (rc = cuda_check(c, cudaStreamSynchronize(c->stream), "material upload")))
+        return (hr_status)rc;
+    c->alb_ntri = c->ntri;
+    return HR_OK;
 }
 
 hr_status hr_set_integrator(hr_ctx* c, int32_t ao_samples, float ao_radius, int32_t pt_bounces, float albedo,

@@ -116,6 +116,9 @@ struct hr_ctx {
     bool have_camera = false;
     hr::LightSet lights;         // host copy of the light collection (default: one 0.2 x 0.2 quad at z = 1)
     hr::DevBuf lights_dev;       // its device copy, read by the path tracer
+    hr::DevBuf tri_nrm;          // 3 vertex normals (float4) per triangle, for the path tracer
+    hr::DevBuf tri_alb;          // diffuse albedo per triangle, for the path tracer
+    uint32_t nrm_ntri = 0, alb_ntri = 0;   // triangle count they were given for (0: none)
     hr::IntegratorParams ip;
     hr::DevBuf fb;               // float3 framebuffer (device)
     hr::DevBuf out_id, out_t, out_u, out_v, ray_in;  // ray-query staging

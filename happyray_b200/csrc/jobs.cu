@@ -70,6 +70,8 @@ __device__ __forceinline__ void load_tile_ctx(TileCtx& T, const Job* __restrict_
     const GridDesc* st = J->status ? J->status : J->desc;
     T.s.ntri = (__ldg(&st->overflow) | __ldg(&st->error)) ? 0u : J->ntri;
     T.s.kind = J->kind;
+    T.s.nrm3 = nullptr;   // served scenes shade with geometric normals and the job's albedo
+    T.s.alb = nullptr;
     T.g = load_g(J->desc);
     for (int q = 0; q < 3; ++q) {
         T.cam.pos[q] = J->cam_pos[q]; T.cam.tl[q] = J->cam_tl[q];

@@ -504,6 +504,9 @@ Scene make_scene(hr_ctx* c) {
     s.desc = c->g.desc.as<GridDesc>();
     s.ntri = c->ntri;
     s.kind = c->built_kind;
+    // shading normals and materials given for the current mesh
+    s.nrm3 = c->nrm_ntri && c->nrm_ntri == c->ntri ? c->tri_nrm.as<float4>() : nullptr;
+    s.alb = c->alb_ntri && c->alb_ntri == c->ntri ? c->tri_alb.as<float>() : nullptr;
     return s;
 }
 

@@ -30,6 +30,8 @@ struct Scene {
     const GridDesc* desc;
     uint32_t ntri;
     int32_t kind;
+    const float4* __restrict__ nrm3 = nullptr;   // path tracer: 3 vertex normals per triangle, or none
+    const float* __restrict__ alb = nullptr;     // path tracer: diffuse albedo per triangle, or none
 };
 
 struct G {
@@ -480,6 +482,28 @@ __device__ __forceinline__ f3 face_normal(const Scene& s, uint32_t tri, f3 d) {
     return n;
 }
 
+// Shading normal of a path tracer hit (PathTracer.h:111-136): the triangle's vertex normals
+// blended with the weights simpleShade forms from the ray origin (u of vertex 0, v of
+// vertex 1, 1 - u - v of vertex 2), normalised, and turned to face the ray as the
+// geometric normal is.
+__device__ __forceinline__ f3 shading_normal(const Scene& s, uint32_t tri, f3 o, f3 d) {
+    f3 p[3];
+    tri_fetch(s.tris, tri, p);
+    const f3 nr = cross(sub(p[1], p[0]), sub(p[2], p[0]));
+    const f3 a0 = sub(p[0], o), a1 = sub(p[1], o), a2 = sub(p[2], o);
+    const f3 n0 = cross(a1, a2), n1 = cross(a2, a0);
+    const float inv = 1.0f / sqrtf(dot(nr, nr));
+    const float u = sqrtf(dot(n0, n0)) * inv;
+    const float v = sqrtf(dot(n1, n1)) * inv;
+    const float w = 1.0f - u - v;
+    const float4* q = s.nrm3 + 3 * (size_t)tri;
+    const float4 m0 = __ldg(q), m1 = __ldg(q + 1), m2 = __ldg(q + 2);
+    f3 n = mk(u * m0.x + v * m1.x + w * m2.x, u * m0.y + v * m1.y + w * m2.y, u * m0.z + v * m1.z + w * m2.z);
+    n = normalize(n);
+    if (dot(n, d) > 0.0f) n = mk(-n.x, -n.y, -n.z);
+    return n;
+}
+
 __device__ __forceinline__ float blend(float old, float val, int32_t image_id) {
     const float nw = 1.0f / (float)(image_id + 1);
     const float ow = 1.0f - nw;
@@ -653,7 +677,10 @@ __device__ __forceinline__ bool path_step(const Scene& s, const G& g, const PtCo
     }
     if (!h.hit) return false;
     const f3 q = mk(p.o.x + h.t * p.d.x, p.o.y + h.t * p.d.y, p.o.z + h.t * p.d.z);
-    const f3 nrm = face_normal(s, h.tri, p.d);
+    f3 nrm = face_normal(s, h.tri, p.d);
+    if (s.nrm3) nrm = shading_normal(s, h.tri, p.o, p.d);
+    const float alb = s.alb ? __ldg(s.alb + h.tri) : k.albedo;
+    const float a_pi = s.alb ? alb * 0.318309886f : k.a_pi;
     // next-event estimation: one light of the collection (by weight when there are several;
     // its radiance divided by the probability of picking it), one point on it
     uint32_t li = 0;
@@ -670,10 +697,10 @@ __device__ __forceinline__ bool path_step(const Scene& s, const G& g, const PtCo
     const float cos_l = -dot(ldf3(lq->n), wi);
     const bool shadow = cos_s > 0.0f && cos_l > 0.0f;
     if (shadow) {
-        p.c = p.beta * k.a_pi * __ldg(&lq->emission) * cos_s * cos_l * __ldg(&lq->area) / dist2;
+        p.c = p.beta * a_pi * __ldg(&lq->emission) * cos_s * cos_l * __ldg(&lq->area) / dist2;
         if (k.nlights > 1) p.c = p.c * (__ldg(&k.ls->cdf[k.nlights - 1]) / (__ldg(&lq->area) * __ldg(&lq->emission)));
     }
-    p.beta = p.beta * k.albedo;
+    p.beta = p.beta * alb;
     const float u3 = pcg_float(p.rng), u4 = pcg_float(p.rng);
     const f3 nd = cosine_dir(nrm, u3, u4);
     const f3 no = mk(q.x + k.ray_eps * nd.x, q.y + k.ray_eps * nd.y, q.z + k.ray_eps * nd.z);

@@ -177,6 +177,24 @@ class Engine:
         self._chk(self.L.hr_set_lights(self.ctx, c.shape[0], _ptr(c), _ptr(e1), _ptr(e2), _ptr(nr), _ptr(em)),
                   "hr_set_lights")
 
+    def set_normals(self, normals_xyz=None, tri_normal_idx=None):
+        """Shading normals for the path tracer (None removes them)."""
+        if normals_xyz is None:
+            self._chk(self.L.hr_set_normals(self.ctx, None, 0, None), "hr_set_normals")
+            return
+        n = np.ascontiguousarray(normals_xyz, np.float32).reshape(-1, 3)
+        ix = np.ascontiguousarray(tri_normal_idx, np.uint32).reshape(-1, 3)
+        self._chk(self.L.hr_set_normals(self.ctx, _ptr(n), n.shape[0], _ptr(ix)), "hr_set_normals")
+
+    def set_materials(self, albedo=None, tri_material=None):
+        """Per-triangle diffuse albedo table and indices for the path tracer (None removes them)."""
+        if albedo is None:
+            self._chk(self.L.hr_set_materials(self.ctx, None, 0, None), "hr_set_materials")
+            return
+        a = np.ascontiguousarray(albedo, np.float32).reshape(-1)
+        ix = np.ascontiguousarray(tri_material, np.uint32).reshape(-1)
+        self._chk(self.L.hr_set_materials(self.ctx, _ptr(a), a.shape[0], _ptr(ix)), "hr_set_materials")
+
     def set_integrator(self, ao_samples=8, ao_radius=-0.1, pt_bounces=4, albedo=0.7, seed=0x853c49e6748fea9b):
         self._chk(self.L.hr_set_integrator(self.ctx, ao_samples, ao_radius, pt_bounces, albedo, seed),
                   "hr_set_integrator")

@@ -121,6 +121,21 @@ hr_status hr_set_light(hr_ctx *ctx, const float corner[3], const float edge1[3],
  * 1..64, a degenerate light or a negative emission. */
 hr_status hr_set_lights(hr_ctx *ctx, uint32_t n, const float *corners, const float *edge1s,
                         const float *edge2s, const float *normals, const float *emissions);
+/* Shading normals of the mesh for the path tracer (WFObject normals and the faces' normal
+ * indices, WFObject.hpp:96-106; RTEngine::upload's uploadObjFrameNormalData,
+ * RTEngine.cu:205-209): num_normals xyz triples and 3 normal indices per triangle of the
+ * current mesh (host).  At a hit the path tracer shades with the vertex normals blended as
+ * PathTracer.h:111-136 does (weights of simpleShade), normalised, facing the ray.  Null
+ * arguments remove them (geometric normals); a new mesh upload with another triangle count
+ * drops them. */
+hr_status hr_set_normals(hr_ctx *ctx, const float *normals_xyz, uint32_t num_normals,
+                         const uint32_t *tri_normal_idx);
+/* Per-triangle materials for the path tracer (the per-triangle PhongMaterial array,
+ * RTEngine.cu:211, PathTracer.h:138): a table of num_materials diffuse albedos (scalar: the
+ * path tracer's radiance is grey) and one material index per triangle of the current mesh
+ * (host).  Null arguments remove them (hr_set_integrator's albedo for every triangle). */
+hr_status hr_set_materials(hr_ctx *ctx, const float *albedo, uint32_t num_materials,
+                           const uint32_t *tri_material);
 /* Integrator parameters: AO samples per hit and radius (fraction of the bounds diagonal
  * if ao_radius < 0, absolute otherwise), PT extension rays, Lambertian albedo, seed. */
 hr_status hr_set_integrator(hr_ctx *ctx, int32_t ao_samples, float ao_radius,

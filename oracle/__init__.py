@@ -30,7 +30,8 @@ class Grid(C.Structure):
 
 class Scene(C.Structure):
     _fields_ = [("v4", C.c_void_p), ("idx", C.c_void_p), ("ntri", C.c_uint32), ("kind", C.c_int32),
-                ("g", Grid), ("cells", C.c_void_p), ("leaves", C.c_void_p), ("prims", C.c_void_p)]
+                ("g", Grid), ("cells", C.c_void_p), ("leaves", C.c_void_p), ("prims", C.c_void_p),
+                ("nrm3", C.c_void_p), ("alb", C.c_void_p)]
 
 
 class Obj(C.Structure):
@@ -169,8 +170,19 @@ class Built:
         s.cells = _p(self.cells)
         s.leaves = _p(self.leaves) if self.leaves is not None else None
         s.prims = _p(self.prims)
+        nrm3 = getattr(self, "nrm3", None)
+        alb = getattr(self, "alb", None)
+        s.nrm3 = _p(nrm3) if nrm3 is not None else None
+        s.alb = _p(alb) if alb is not None else None
         self._scene = s
         return s
+
+    def set_shading(self, normals_xyz=None, tri_normal_idx=None, albedo=None, tri_material=None):
+        """Path-tracer shading normals (gathered to 3 per triangle) and per-triangle albedo."""
+        self.nrm3 = None if normals_xyz is None else np.ascontiguousarray(
+            np.asarray(normals_xyz, np.float32).reshape(-1, 3)[np.asarray(tri_normal_idx).reshape(-1, 3)])
+        self.alb = None if albedo is None else np.ascontiguousarray(
+            np.asarray(albedo, np.float32)[np.asarray(tri_material).reshape(-1)])
 
     def diag(self) -> np.float32:
         d = np.array(self.grid.bmax, np.float32) - np.array(self.grid.bmin, np.float32)

@@ -939,6 +939,25 @@ void orc_render_ao(const orc_scene *s, const orc_camera *c, int32_t spp, float a
     if (counts) counts[0] += rays;
 }
 
+/* shading normal of a path tracer hit (PathTracer.h:111-136): vertex normals blended with the
+ * simpleShade weights from the ray origin, normalised, turned to face the ray */
+static inline f3 shading_normal(const orc_scene *s, uint32_t tri, f3 o, f3 d) {
+    const f3 p0 = vtx(s->v4, s->idx[3 * (size_t)tri]), p1 = vtx(s->v4, s->idx[3 * (size_t)tri + 1]),
+             p2 = vtx(s->v4, s->idx[3 * (size_t)tri + 2]);
+    const f3 nr = cross(sub(p1, p0), sub(p2, p0));
+    const f3 a0 = sub(p0, o), a1 = sub(p1, o), a2 = sub(p2, o);
+    const f3 n0 = cross(a1, a2), n1 = cross(a2, a0);
+    const float inv = 1.0f / sqrtf(dot(nr, nr));
+    const float u = sqrtf(dot(n0, n0)) * inv;
+    const float v = sqrtf(dot(n1, n1)) * inv;
+    const float w = 1.0f - u - v;
+    const float *m = s->nrm3 + 9 * (size_t)tri;
+    f3 n = mk(u * m[0] + v * m[3] + w * m[6], u * m[1] + v * m[4] + w * m[7], u * m[2] + v * m[5] + w * m[8]);
+    n = normalize(n);
+    if (dot(n, d) > 0.0f) n = mk(-n.x, -n.y, -n.z);
+    return n;
+}
+
 /* A light of the collection with the values the path tracer forms once: the edge cross
  * product nc, 1 / |nc|^2 (for the parallelogram coordinates), area |nc|, sampling weight
  * area * emission.  cdf: inclusive running sum of the weights (LightSource.hpp:185-190). */
@@ -1023,6 +1042,9 @@ void orc_render_pt(const orc_scene *s, const orc_camera *c, const orc_light *l, 
             if (!h.hit) break;
             f3 p = mk(o.x + h.t * d.x, o.y + h.t * d.y, o.z + h.t * d.z);
             f3 nrm = face_normal(s, h.tri, d);
+            if (s->nrm3) nrm = shading_normal(s, h.tri, o, d);
+            const float alb = s->alb ? s->alb[h.tri] : albedo;
+            const float hit_a_pi = s->alb ? alb * 0.318309886f : a_pi;
             /* next-event estimation: one light of the collection (by weight when there are
              * several; its radiance divided by the probability of picking it), one point on it */
             int32_t k = 0;
@@ -1046,13 +1068,13 @@ void orc_render_pt(const orc_scene *s, const orc_camera *c, const orc_light *l, 
                 trace_one(s, so, wi, dist - ray_eps, 1, &hs);
                 rays += 1;
                 if (!hs.hit) {
-                    float cl = beta * a_pi * q->emission * cos_s * cos_l * q->area / dist2;
+                    float cl = beta * hit_a_pi * q->emission * cos_s * cos_l * q->area / dist2;
                     if (nlights > 1) cl = cl * scale;
                     L = L + cl;
                 }
             }
             /* Lambertian bounce: f * cos / pdf = albedo */
-            beta = beta * albedo;
+            beta = beta * alb;
             float u3 = pcg32_float(&rng), u4 = pcg32_float(&rng);
             d = cosine_dir(nrm, u3, u4);
             o = mk(p.x + ray_eps * d.x, p.y + ray_eps * d.y, p.z + ray_eps * d.z);

@@ -55,6 +55,8 @@ typedef struct {
     const uint32_t *cells;   /* UG: uint2 cell ranges; TL: packed top cells */
     const uint32_t *leaves;  /* TL: uint2 leaf ranges */
     const uint32_t *prims;   /* primitive (triangle id) lists */
+    const float    *nrm3;    /* path tracer: 9 floats (3 vertex normals) per triangle, or NULL */
+    const float    *alb;     /* path tracer: diffuse albedo per triangle, or NULL */
 } orc_scene;
 
 typedef struct {

@@ -286,6 +286,42 @@ def test_render_pt_light_collection_bitexact(engine, oracle, small_clusters):
     engine.setLights((0.4, 0.4, 1.0), (0.2, 0, 0), (0, 0.2, 0), 20.0)
 
 
+def test_render_pt_shading_normals_and_materials_bitexact(engine, oracle, small_clusters):
+    """Path tracing with per-vertex shading normals (area-weighted vertex normals of the
+    mesh, blended at a hit as PathTracer.h:111-136) and a per-triangle albedo table,
+    bit-exact against the oracle; removing them gives back the plain images."""
+    v, f = small_clusters
+    gpu_build(engine, v, f, GRID_TWO_LEVEL)
+    b = oracle_build(oracle, v, f, GRID_TWO_LEVEL)
+    cam = S.camera_at_bounds(v, (96, 72))
+    set_cam(engine, cam)
+    fn = np.cross(v[f[:, 1]] - v[f[:, 0]], v[f[:, 2]] - v[f[:, 0]]).astype(np.float64)
+    vn = np.zeros(v.shape, np.float64)
+    for k in range(3):
+        np.add.at(vn, f[:, k], fn)
+    vn = (vn / np.maximum(np.linalg.norm(vn, axis=1, keepdims=True), 1e-30)).astype(np.float32)
+    albedo = np.array([0.3, 0.7, 0.9], np.float32)
+    tri_mat = (np.arange(f.shape[0]) % 3).astype(np.uint32)
+    seed = 31
+    engine.set_integrator(pt_bounces=4, albedo=0.7, seed=seed)
+    engine.setLights((0.4, 0.4, 1.0), (0.2, 0, 0), (0, 0.2, 0), 20.0)
+    plain = engine.renderFrame(None, 0, RENDER_PATH)
+    engine.set_normals(vn, f)
+    engine.set_materials(albedo, tri_mat)
+    fb = engine.renderFrame(None, 0, RENDER_PATH)
+    b.set_shading(vn, f, albedo, tri_mat)
+    eps = float(np.float32(1e-4) * b.diag())
+    img, _ = oracle.render_pt(b, ocam(oracle, cam), oracle.make_light(), 4, 0.7, eps, seed)
+    assert np.array_equal(fb[:, 0], img)
+    assert not np.array_equal(fb, plain)
+    engine.set_normals(None)
+    engine.set_materials(None)
+    assert np.array_equal(engine.renderFrame(None, 0, RENDER_PATH), plain)
+    from happyray_b200 import HRError
+    with pytest.raises(HRError):
+        engine.set_materials(albedo, np.full(f.shape[0], 3, np.uint32))   # index out of the table
+
+
 @pytest.mark.parametrize("kind", [GRID_UNIFORM, GRID_TWO_LEVEL])
 def test_render_primary_mode0(engine, oracle, c1_scene, kind):
     """Render mode 0 bit-exact against the oracle's simpleShade (SimpleIntegrator.h:41-126)
