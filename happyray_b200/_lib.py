@@ -113,6 +113,10 @@ SIGNATURES = {
     "hr_scene_get_info": (C.c_int, [P, P]),
     "hr_scene_keyframes": (P, [P]),
     "hr_scene_indices": (P, [P]),
+    "hr_scene_normals": (P, [P]),
+    "hr_scene_normal_indices": (P, [P]),
+    "hr_scene_material_albedo": (P, [P]),
+    "hr_scene_triangle_materials": (P, [P]),
     "hr_scene_get_light": (C.c_int, [P, C.c_uint32, P, P, P, P, P]),
     "hr_scene_upload": (C.c_int, [P, P]),
     "hr_rays_file_count": (C.c_int, [C.c_char_p, C.POINTER(C.c_uint32)]),
@@ -178,7 +182,8 @@ class SceneInfo(C.Structure):
     _fields_ = [("num_vertices", C.c_uint32), ("num_triangles", C.c_uint32), ("num_keyframes", C.c_uint32),
                 ("frame_step", C.c_float), ("has_camera", C.c_int32), ("cam_position", C.c_float * 3),
                 ("cam_orientation", C.c_float * 3), ("cam_up", C.c_float * 3), ("cam_fov_deg", C.c_float),
-                ("width", C.c_int32), ("height", C.c_int32), ("num_lights", C.c_uint32)]
+                ("width", C.c_int32), ("height", C.c_int32), ("num_lights", C.c_uint32),
+                ("num_normals", C.c_uint32), ("num_materials", C.c_uint32)]
 
 
 class Request(C.Structure):

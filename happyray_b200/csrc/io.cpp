@@ -44,6 +44,10 @@ struct hr_scene {
     int32_t w = 0, h = 0;
     struct QuadLight { float position[3], normal[3], intensity[3], edge1[3], edge2[3]; };
     std::vector<QuadLight> lights;
+    std::vector<float> normals;     // shading normals, M x 3 (empty: the file had none)
+    std::vector<uint32_t> nidx;     // N x 3 normal indices, with normals
+    std::vector<float> albedo;      // material table (empty: no usemtl / mtllib)
+    std::vector<uint32_t> tri_mat;  // N material indices, with albedo
 };
 
 namespace {
@@ -79,9 +83,37 @@ struct ObjChunk {
     std::vector<float> v;
     std::vector<int64_t> face;       // triangle corners: > 0 global 1-based, < 0 relative
     std::vector<uint32_t> face_vcount;   // local vertex count when the corner was read
+    std::vector<float> n;            // vn triples
+    // normal index per triangle corner (0: none, else as `face`), kept only once a corner
+    // of this chunk named one; shorter than `face` means "none" for the corners past it
+    std::vector<int64_t> fnorm;
+    std::vector<uint32_t> face_ncount;   // local normal count when the corner was read
+    std::vector<std::pair<size_t, std::string>> usemtl;   // (triangles before it, name)
+    std::vector<std::string> mtllib;
     size_t first_line = 0;
     std::string err;
 };
+
+// what an OBJ file holds besides positions and triangles
+struct ObjExtras {
+    std::vector<float> normals;          // the file's vn, then one geometric normal per face lacking one
+    std::vector<uint32_t> nidx;          // 3 per triangle; empty when the file has no vn
+    std::vector<std::string> mat_names;  // "Default" first, then in order of first usemtl
+    std::vector<float> albedo;           // per material
+    std::vector<uint32_t> tri_mat;       // per triangle; empty when the file names no material
+};
+
+inline bool starts_with_ci(const char* s, const char* e, const char* w) {
+    for (; *w; ++w, ++s)
+        if (s >= e || std::tolower((unsigned char)*s) != *w) return false;
+    return true;
+}
+
+std::string trimmed(const char* s, const char* e) {
+    while (s < e && (*s == ' ' || *s == '\t')) ++s;
+    while (e > s && (e[-1] == ' ' || e[-1] == '\t' || e[-1] == '\r')) --e;
+    return std::string(s, e);
+}
 
 inline const char* skip_ws(const char* s, const char* e) {
     while (s < e && (*s == ' ' || *s == '\t' || *s == '\r')) ++s;
@@ -98,9 +130,10 @@ bool obj_line(const char* s, const char* e, ObjChunk& c, size_t line) {
     if (s >= e) return true;
     const char k = (char)std::tolower((unsigned char)s[0]);
     if (k == 'v') {
-        if (s + 1 < e && (s[1] == ' ' || s[1] == '\t')) {
-            // position: exactly three numbers (WFObjectReader.cpp:354-386)
-            const char* p = s + 1;
+        const bool is_n = s + 2 < e && (s[1] == 'n' || s[1] == 'N') && (s[2] == ' ' || s[2] == '\t');
+        if ((s + 1 < e && (s[1] == ' ' || s[1] == '\t')) || is_n) {
+            // position or normal: exactly three numbers (WFObjectReader.cpp:354-386)
+            const char* p = s + (is_n ? 2 : 1);
             float xyz[3];
             int n = 0;
             std::string tmp(p, e);
@@ -121,15 +154,16 @@ bool obj_line(const char* s, const char* e, ObjChunk& c, size_t line) {
                 c.err = "line " + std::to_string(line) + ": a vertex needs three numbers";
                 return false;
             }
-            c.v.insert(c.v.end(), xyz, xyz + 3);
+            (is_n ? c.n : c.v).insert((is_n ? c.n : c.v).end(), xyz, xyz + 3);
         }
-        return true;   // vn, vt: not needed by the hot path
+        return true;   // vt: not needed by the hot path
     }
     // 'f' (or "fo") and, as in the reference, 'l': three or more corners make triangles
     if ((k == 'f' || k == 'l') && s + 1 < e && (s[1] == ' ' || s[1] == '\t' || s[1] == 'o' || s[1] == 'O')) {
         std::string tmp(s + (s[1] == 'o' || s[1] == 'O' ? 2 : 1), e);
         const char* q = tmp.c_str();
-        std::vector<int64_t> poly;
+        std::vector<int64_t> poly, pnorm;
+        bool any_n = false;
         for (;;) {
             while (*q == ' ' || *q == '\t') ++q;
             if (!*q) break;
@@ -140,22 +174,101 @@ bool obj_line(const char* s, const char* e, ObjChunk& c, size_t line) {
                 return false;
             }
             q = end;
-            // skip the texture / normal indices of this corner
-            while (*q == '/' || (*q >= '0' && *q <= '9') || *q == '-') ++q;
+            // v, v/t, v//n or v/t/n (WFObjectReader.cpp:411-470): the texture index is skipped
+            long long ni = 0;
+            if (*q == '/') {
+                ++q;
+                if (*q != '/') {
+                    std::strtoll(q, &end, 10);
+                    if (end == q) {
+                        c.err = "line " + std::to_string(line) + ": bad face index";
+                        return false;
+                    }
+                    q = end;
+                }
+                if (*q == '/') {
+                    ++q;
+                    ni = std::strtoll(q, &end, 10);
+                    if (end == q || ni == 0) {
+                        c.err = "line " + std::to_string(line) + ": bad normal index";
+                        return false;
+                    }
+                    q = end;
+                }
+            }
             poly.push_back(vi);
+            pnorm.push_back(ni);
+            any_n |= ni != 0;
         }
         if (poly.size() < 3) return true;   // points and lines are not triangles
-        const uint32_t vc = (uint32_t)(c.v.size() / 3);
+        const uint32_t vc = (uint32_t)(c.v.size() / 3), ncnt = (uint32_t)(c.n.size() / 3);
+        if (any_n) {   // align the normal-index arrays with the corners before this face
+            c.fnorm.resize(c.face.size(), 0);
+            c.face_ncount.resize(c.face.size(), 0);
+        }
         for (size_t i = 1; i + 1 < poly.size(); ++i) {   // fan from the first corner
-            const int64_t tri[3] = {poly[0], poly[i], poly[i + 1]};
+            const size_t cs[3] = {0, i, i + 1};
             for (int t = 0; t < 3; ++t) {
-                c.face.push_back(tri[t]);
+                c.face.push_back(poly[cs[t]]);
                 c.face_vcount.push_back(vc);
+                if (any_n) {
+                    c.fnorm.push_back(pnorm[cs[t]]);
+                    c.face_ncount.push_back(ncnt);
+                }
             }
         }
         return true;
     }
-    return true;   // o, g, s, p, usemtl, mtllib and anything else: skipped
+    // materials (WFObjectReader.cpp:541-565): usemtl selects one for the faces after it,
+    // mtllib names a .mtl file read once the OBJ is parsed
+    if (starts_with_ci(s, e, "usemtl") && s + 6 < e && (s[6] == ' ' || s[6] == '\t')) {
+        const std::string name = trimmed(s + 6, e);
+        if (!name.empty()) c.usemtl.emplace_back(c.face.size() / 3, name);
+        return true;
+    }
+    if (starts_with_ci(s, e, "mtllib") && s + 6 < e && (s[6] == ' ' || s[6] == '\t')) {
+        const std::string name = trimmed(s + 6, e);
+        if (!name.empty()) c.mtllib.push_back(name);
+        return true;
+    }
+    return true;   // o, g, s, p and anything else: skipped
+}
+
+// A .mtl file (readMtlLib, WFObjectReader.cpp:135-258): "newmtl name" selects a material the
+// OBJ named (an unknown name leaves the selection as it was, as the reference does), "Kd r g
+// b" sets its diffuse colour.  The path tracer's albedo is the grey of the reference's
+// normalised reflectance (setupPhongCoefficients, WFObjectReader.cpp:49-57: min(Kd, 0.99)
+// per channel; the 1/pi of its BRDF is applied by the tracer): the mean of the three.
+hr_status read_mtl(const std::string& path, const std::vector<std::string>& names, std::vector<float>& albedo) {
+    std::ifstream in(path, std::ios::binary);
+    if (!in) return io_error(HR_ERR_INVALID_ARG, "cannot read .mtl file %s", path.c_str());
+    std::string line;
+    long cur = -1;
+    while (std::getline(in, line)) {
+        const size_t hash = line.find('#');
+        if (hash != std::string::npos) line.resize(hash);
+        const char* s = skip_ws(line.data(), line.data() + line.size());
+        const char* e = line.data() + line.size();
+        if (starts_with_ci(s, e, "newmtl")) {
+            const std::string name = trimmed(s + 6, e);
+            const auto it = std::find(names.begin(), names.end(), name);
+            if (it != names.end()) cur = (long)(it - names.begin());
+        } else if (starts_with_ci(s, e, "kd") && cur >= 0) {
+            std::string tmp(s + 2, e);
+            const char* q = tmp.c_str();
+            float kd[3];
+            int n = 0;
+            for (; n < 3; ++n) {
+                char* end;
+                kd[n] = std::strtof(q, &end);
+                if (end == q) break;
+                q = end;
+            }
+            if (n == 3)
+                albedo[(size_t)cur] = (std::min(kd[0], 0.99f) + std::min(kd[1], 0.99f) + std::min(kd[2], 0.99f)) / 3.0f;
+        }
+    }
+    return HR_OK;
 }
 
 void obj_parse_chunk(const char* b, const char* e, ObjChunk& c) {
@@ -169,7 +282,109 @@ void obj_parse_chunk(const char* b, const char* e, ObjChunk& c) {
     }
 }
 
-hr_status read_obj(const std::string& path, int threads, std::vector<float>& v, std::vector<uint32_t>& idx) {
+std::string dir_of(const std::string& p);
+
+constexpr uint32_t kNoNormal = 0xffffffffu;
+
+// every triangle with a corner lacking a normal index gets one appended normal, its
+// normalised edge1 x edge2, for those corners (WFObjectReader.cpp:602-614)
+bool fill_geometric_normals(std::vector<float>& normals, std::vector<uint32_t>& nidx, const float* v,
+                            const std::vector<uint32_t>& idx) {
+    const size_t nt = idx.size() / 3;
+    for (size_t t = 0; t < nt; ++t) {
+        uint32_t* ni = &nidx[3 * t];
+        if (ni[0] != kNoNormal && ni[1] != kNoNormal && ni[2] != kNoNormal) continue;
+        const float* a = &v[3 * (size_t)idx[3 * t]];
+        const float* b = &v[3 * (size_t)idx[3 * t + 1]];
+        const float* d = &v[3 * (size_t)idx[3 * t + 2]];
+        const float e1[3] = {b[0] - a[0], b[1] - a[1], b[2] - a[2]};
+        const float e2[3] = {d[0] - a[0], d[1] - a[1], d[2] - a[2]};
+        float n[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]};
+        const float len = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+        for (int k = 0; k < 3; ++k) n[k] = len > 0.0f ? n[k] / len : 0.0f;
+        const size_t at = normals.size() / 3;
+        if (at >= kNoNormal) return false;
+        normals.insert(normals.end(), n, n + 3);
+        for (int k = 0; k < 3; ++k)
+            if (ni[k] == kNoNormal) ni[k] = (uint32_t)at;
+    }
+    return true;
+}
+
+// Normals and materials of a parsed OBJ (WFObjectReader.cpp:583-640).  With any vn in the
+// file, every face lacking a normal index at some corner gets one appended geometric normal
+// (normalised edge1 x edge2 of its vertices) for those corners; a file without vn keeps no
+// normals (the tracer's geometric normal).  Materials: "Default" (diffuse 0.6774,
+// WFObjectReader.cpp:277-283) at index 0, then each usemtl name in order of first use; the
+// file's mtllib files, relative to its directory, fill in their Kd.
+hr_status obj_extras(const std::string& path, const std::vector<ObjChunk>& ch, const std::vector<float>& v,
+                     const std::vector<uint32_t>& idx, ObjExtras& ex) {
+    ex = ObjExtras();
+    const size_t nt = idx.size() / 3;
+    size_t nn = 0;
+    for (const auto& c : ch) nn += c.n.size() / 3;
+    if (nn > 0xffffffffull) return io_error(HR_ERR_INVALID_ARG, "%s: too many normals", path.c_str());
+    if (nn > 0) {
+        ex.normals.reserve(3 * nn);
+        ex.nidx.assign(3 * nt, kNoNormal);
+        uint64_t noff = 0;
+        size_t corner = 0;
+        for (const auto& c : ch) {
+            ex.normals.insert(ex.normals.end(), c.n.begin(), c.n.end());
+            for (size_t i = 0; i < c.fnorm.size(); ++i) {
+                const int64_t f = c.fnorm[i];
+                if (f == 0) continue;
+                const int64_t g = f > 0 ? f - 1 : (int64_t)(noff + c.face_ncount[i]) + f;
+                if (g < 0 || (uint64_t)g >= nn)
+                    return io_error(HR_ERR_INVALID_ARG, "%s: normal index %lld out of range of %zu normals",
+                                    path.c_str(), (long long)f, nn);
+                ex.nidx[corner + i] = (uint32_t)g;
+            }
+            corner += c.face.size();
+            noff += c.n.size() / 3;
+        }
+        if (!fill_geometric_normals(ex.normals, ex.nidx, v.data(), idx))
+            return io_error(HR_ERR_INVALID_ARG, "%s: too many normals", path.c_str());
+    }
+    bool any_mat = false;
+    for (const auto& c : ch) any_mat |= !c.usemtl.empty() || !c.mtllib.empty();
+    if (!any_mat) return HR_OK;
+    ex.mat_names.push_back("Default");
+    ex.albedo.push_back(0.6774f);
+    ex.tri_mat.assign(nt, 0);
+    uint32_t cur = 0;
+    size_t tri0 = 0;
+    for (const auto& c : ch) {
+        const size_t ntc = c.face.size() / 3;
+        size_t at = 0;
+        for (size_t u = 0; u <= c.usemtl.size(); ++u) {
+            const size_t upto = u < c.usemtl.size() ? c.usemtl[u].first : ntc;
+            std::fill(ex.tri_mat.begin() + (tri0 + at), ex.tri_mat.begin() + (tri0 + upto), cur);
+            at = upto;
+            if (u == c.usemtl.size()) break;
+            const std::string& name = c.usemtl[u].second;
+            const auto it = std::find(ex.mat_names.begin(), ex.mat_names.end(), name);
+            if (it != ex.mat_names.end()) {
+                cur = (uint32_t)(it - ex.mat_names.begin());
+            } else {   // a new material: the reference's Material(name) has diffuse 0
+                cur = (uint32_t)ex.mat_names.size();
+                ex.mat_names.push_back(name);
+                ex.albedo.push_back(0.0f);
+            }
+        }
+        tri0 += ntc;
+    }
+    const std::string dir = dir_of(path);
+    for (const auto& c : ch)
+        for (const auto& lib : c.mtllib) {
+            const hr_status st = read_mtl(lib[0] == '/' ? lib : dir + lib, ex.mat_names, ex.albedo);
+            if (st != HR_OK) return st;
+        }
+    return HR_OK;
+}
+
+hr_status read_obj(const std::string& path, int threads, std::vector<float>& v, std::vector<uint32_t>& idx,
+                   ObjExtras* ex = nullptr) {
     std::string text;
     if (!read_file(path, text)) return io_error(HR_ERR_INVALID_ARG, "cannot read %s", path.c_str());
     if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
@@ -216,7 +431,7 @@ hr_status read_obj(const std::string& path, int threads, std::vector<float>& v, 
         }
         voff += c.v.size() / 3;
     }
-    return HR_OK;
+    return ex ? obj_extras(path, ch, v, idx, *ex) : HR_OK;
 }
 
 // ---------------------------------------------------------------------------------
@@ -330,6 +545,66 @@ std::string frame_name(const std::string& prefix, const std::string& suffix, uin
     return prefix + id + suffix;
 }
 
+// the normals and materials of one more OBJ file of a static scene, whose triangles follow
+// tri_before earlier ones: normal indices move past the earlier normals, materials merge
+// by name; triangles of files without them get sentinels (normals) or "Default"
+hr_status append_extras(ObjExtras& acc, ObjExtras& ex, size_t tri_before, size_t tri_count) {
+    if (!ex.normals.empty() || !acc.normals.empty()) {
+        acc.nidx.resize(3 * tri_before, kNoNormal);
+        if (ex.normals.empty()) {
+            acc.nidx.resize(3 * (tri_before + tri_count), kNoNormal);
+        } else {
+            const size_t off = acc.normals.size() / 3;
+            if (off + ex.normals.size() / 3 >= kNoNormal) return io_error(HR_ERR_INVALID_ARG, "too many normals");
+            acc.normals.insert(acc.normals.end(), ex.normals.begin(), ex.normals.end());
+            for (uint32_t x : ex.nidx) acc.nidx.push_back((uint32_t)(x + off));
+        }
+    }
+    if (!ex.tri_mat.empty() || !acc.tri_mat.empty()) {
+        if (acc.mat_names.empty()) {
+            acc.mat_names.push_back("Default");
+            acc.albedo.push_back(0.6774f);
+        }
+        acc.tri_mat.resize(tri_before, 0);
+        if (ex.tri_mat.empty()) {
+            acc.tri_mat.resize(tri_before + tri_count, 0);
+        } else {
+            std::vector<uint32_t> remap(ex.mat_names.size());
+            for (size_t m = 0; m < ex.mat_names.size(); ++m) {
+                const auto it = std::find(acc.mat_names.begin(), acc.mat_names.end(), ex.mat_names[m]);
+                if (it != acc.mat_names.end()) {
+                    remap[m] = (uint32_t)(it - acc.mat_names.begin());
+                } else {
+                    remap[m] = (uint32_t)acc.mat_names.size();
+                    acc.mat_names.push_back(ex.mat_names[m]);
+                    acc.albedo.push_back(ex.albedo[m]);
+                }
+            }
+            for (uint32_t x : ex.tri_mat) acc.tri_mat.push_back(remap[x]);
+        }
+    }
+    return HR_OK;
+}
+
+// the scene keeps the normals of `ns` (the first key frame's) and the materials of `ms`
+hr_status take_extras(hr_scene& sc, ObjExtras& ns, ObjExtras& ms) {
+    if (!ns.normals.empty()) {
+        if (ns.nidx.size() != 3 * (size_t)sc.nt)
+            return io_error(HR_ERR_INVALID_ARG, "the first key frame's normal indices do not match the triangles");
+        if (!fill_geometric_normals(ns.normals, ns.nidx, sc.kf.data(), sc.idx))
+            return io_error(HR_ERR_INVALID_ARG, "too many normals");
+        sc.normals.swap(ns.normals);
+        sc.nidx.swap(ns.nidx);
+    }
+    if (!ms.tri_mat.empty()) {
+        if (ms.tri_mat.size() != sc.nt)
+            return io_error(HR_ERR_INVALID_ARG, "the material list does not match the triangles");
+        sc.albedo.swap(ms.albedo);
+        sc.tri_mat.swap(ms.tri_mat);
+    }
+    return HR_OK;
+}
+
 hr_status finish_scene(hr_scene& sc, std::vector<std::vector<float>>& frames, std::vector<uint32_t>& idx) {
     if (frames.empty()) return io_error(HR_ERR_INVALID_ARG, "the scene has no geometry");
     const size_t nv3 = frames[0].size();
@@ -436,8 +711,10 @@ hr_status hr_scene_load_obj(const char* path, int32_t threads, hr_scene** out) {
     if (!sc) return HR_ERR_OUT_OF_MEMORY;
     std::vector<std::vector<float>> frames(1);
     std::vector<uint32_t> idx;
-    hr_status st = read_obj(path, threads, frames[0], idx);
+    ObjExtras ex;
+    hr_status st = read_obj(path, threads, frames[0], idx, &ex);
     if (st == HR_OK) st = finish_scene(*sc, frames, idx);
+    if (st == HR_OK) st = take_extras(*sc, ex, ex);
     if (st != HR_OK) { delete sc; return st; }
     *out = sc;
     return HR_OK;
@@ -477,12 +754,16 @@ hr_status hr_scene_load(const char* cfg, int32_t threads, hr_scene** out) {
     if (!sc) return HR_ERR_OUT_OF_MEMORY;
     std::vector<std::vector<float>> frames;
     std::vector<uint32_t> idx;
+    ObjExtras first, last;
     hr_status st = HR_OK;
     if (nframes > 0 && (!prefix.empty() || !suffix.empty())) {
-        // key frames (AnimationManager::read): the last frame's triangles are kept
+        // key frames (AnimationManager::read): the last frame's triangles and materials are
+        // kept, the first frame's normals (RTEngine::upload takes the normals of its first
+        // frame, RTEngine.cu:205-209; WFObjectUploader.h:121-250)
         for (uint32_t k = 0; k < nframes && st == HR_OK; ++k) {
             std::vector<float> v;
-            st = read_obj(resolve(frame_name(prefix, suffix, k, nframes), base), threads, v, idx);
+            st = read_obj(resolve(frame_name(prefix, suffix, k, nframes), base), threads, v, idx,
+                          k == 0 ? &first : &last);
             frames.push_back(std::move(v));
         }
     } else {
@@ -491,15 +772,19 @@ hr_status hr_scene_load(const char* cfg, int32_t threads, hr_scene** out) {
         for (size_t i = 0; i < objs.size() && st == HR_OK; ++i) {
             std::vector<float> v;
             std::vector<uint32_t> fi;
-            st = read_obj(resolve(objs[i], base), threads, v, fi);
+            ObjExtras ex;
+            st = read_obj(resolve(objs[i], base), threads, v, fi, &ex);
+            if (st == HR_OK) st = append_extras(first, ex, (uint32_t)(idx.size() / 3), (uint32_t)(fi.size() / 3));
             const uint32_t off = (uint32_t)(frames[0].size() / 3);
             for (uint32_t& x : fi) x += off;
             frames[0].insert(frames[0].end(), v.begin(), v.end());
             idx.insert(idx.end(), fi.begin(), fi.end());
         }
+        nframes = 1;
     }
     sc->frame_step = step;
     if (st == HR_OK) st = finish_scene(*sc, frames, idx);
+    if (st == HR_OK) st = take_extras(*sc, first, nframes > 1 ? last : first);
     if (st == HR_OK && !camera.empty()) st = read_camera(resolve(camera, base), *sc);
     if (st == HR_OK && !light.empty() && file_exists(resolve(light, base))) st = read_lights(resolve(light, base), *sc);
     if (st != HR_OK) { delete sc; return st; }
@@ -523,11 +808,23 @@ hr_status hr_scene_get_info(const hr_scene* sc, hr_scene_info* info) {
     info->width = sc->w;
     info->height = sc->h;
     info->num_lights = (uint32_t)sc->lights.size();
+    info->num_normals = (uint32_t)(sc->normals.size() / 3);
+    info->num_materials = (uint32_t)sc->albedo.size();
     return HR_OK;
 }
 
 const float* hr_scene_keyframes(const hr_scene* sc) { return sc ? sc->kf.data() : nullptr; }
 const uint32_t* hr_scene_indices(const hr_scene* sc) { return sc ? sc->idx.data() : nullptr; }
+const float* hr_scene_normals(const hr_scene* sc) { return sc && !sc->normals.empty() ? sc->normals.data() : nullptr; }
+const uint32_t* hr_scene_normal_indices(const hr_scene* sc) {
+    return sc && !sc->normals.empty() ? sc->nidx.data() : nullptr;
+}
+const float* hr_scene_material_albedo(const hr_scene* sc) {
+    return sc && !sc->albedo.empty() ? sc->albedo.data() : nullptr;
+}
+const uint32_t* hr_scene_triangle_materials(const hr_scene* sc) {
+    return sc && !sc->albedo.empty() ? sc->tri_mat.data() : nullptr;
+}
 
 hr_status hr_scene_get_light(const hr_scene* sc, uint32_t i, float pos[3], float e1[3], float e2[3], float n[3],
                              float inten[3]) {
@@ -564,6 +861,14 @@ hr_status hr_scene_upload(hr_ctx* ctx, const hr_scene* sc) {
         if ((st = hr_set_lights(ctx, (uint32_t)n, pos.data(), e1.data(), e2.data(), nrm.data(), em.data())) != HR_OK)
             return st;
     }
+    // the mesh's shading normals and materials, or none (a scene without them must not
+    // keep an earlier scene's)
+    st = sc->normals.empty() ? hr_set_normals(ctx, nullptr, 0, nullptr)
+                             : hr_set_normals(ctx, sc->normals.data(), (uint32_t)(sc->normals.size() / 3), sc->nidx.data());
+    if (st != HR_OK) return st;
+    st = sc->albedo.empty() ? hr_set_materials(ctx, nullptr, 0, nullptr)
+                            : hr_set_materials(ctx, sc->albedo.data(), (uint32_t)sc->albedo.size(), sc->tri_mat.data());
+    if (st != HR_OK) return st;
     return hr_set_frame_time(ctx, 0.0f, 0.0f);
 }
 

@@ -95,9 +95,10 @@ class Engine:
 
     # -- RTEngine::setGridDensities / buildAccStruct -----------------------------
     def upload_scene(self, path: str, threads: int = 0):
-        """Load a scene.cfg (or one .obj) and make it current: key frames, camera and first
-        light (hr_scene_load / hr_scene_upload; CUDAApplication.cu:63-71 reads the same
-        files at start-up).  Returns the camera resolution, or None without a camera."""
+        """Load a scene.cfg (or one .obj) and make it current: key frames, camera, lights,
+        the OBJ's shading normals and materials (hr_scene_load / hr_scene_upload;
+        CUDAApplication.cu:63-71 reads the same files at start-up).  Returns the camera
+        resolution, or None without a camera."""
         h = C.c_void_p()
         fn = self.L.hr_scene_load_obj if str(path).lower().endswith(".obj") else self.L.hr_scene_load
         st = fn(str(path).encode(), threads, C.byref(h))

@@ -37,12 +37,17 @@ class QuadLight:
 
 @dataclass
 class Scene:
-    """Key frames (K, V, 3) float32, triangles (N, 3) uint32, camera, lights, frame step."""
+    """Key frames (K, V, 3) float32, triangles (N, 3) uint32, camera, lights, frame step, and
+    the OBJ's shading normals and materials when it has them."""
     keyframes: np.ndarray
     faces: np.ndarray
     frame_step: float = 0.0
     camera: Optional[dict] = None
     lights: List[QuadLight] = field(default_factory=list)
+    normals: Optional[np.ndarray] = None          # (M, 3) float32 shading normals
+    normal_idx: Optional[np.ndarray] = None       # (N, 3) uint32, with normals
+    albedo: Optional[np.ndarray] = None           # (K,) float32 material table
+    materials: Optional[np.ndarray] = None        # (N,) uint32 material per triangle, with albedo
 
 
 def _load(fn, path: str, threads: int) -> Scene:
@@ -65,7 +70,16 @@ def _load(fn, path: str, threads: int) -> Scene:
             a = [(C.c_float * 3)() for _ in range(5)]
             _chk(L.hr_scene_get_light(h, i, *a), "light")
             lights.append(QuadLight(*[np.array(x, np.float32) for x in a]))
-        return Scene(kf, fa, float(info.frame_step), cam, lights)
+        nrm = nid = alb = mat = None
+        if info.num_normals and n:
+            nrm = np.ctypeslib.as_array((C.c_float * (3 * info.num_normals)).from_address(L.hr_scene_normals(h)))
+            nrm = nrm.reshape(-1, 3).copy()
+            nid = np.ctypeslib.as_array((C.c_uint32 * (n * 3)).from_address(L.hr_scene_normal_indices(h)))
+            nid = nid.reshape(n, 3).copy()
+        if info.num_materials and n:
+            alb = np.ctypeslib.as_array((C.c_float * info.num_materials).from_address(L.hr_scene_material_albedo(h))).copy()
+            mat = np.ctypeslib.as_array((C.c_uint32 * n).from_address(L.hr_scene_triangle_materials(h))).copy()
+        return Scene(kf, fa, float(info.frame_step), cam, lights, nrm, nid, alb, mat)
     finally:
         L.hr_scene_free(h)
 

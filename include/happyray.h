@@ -409,6 +409,8 @@ typedef struct hr_scene_info {
     float cam_fov_deg;
     int32_t width, height;
     uint32_t num_lights;
+    uint32_t num_normals;    /* shading normals (0: the OBJ had no vn) */
+    uint32_t num_materials;  /* material table incl. "Default" (0: no usemtl / mtllib) */
 } hr_scene_info;
 
 #define HR_IMAGE_PNG 0
@@ -428,9 +430,22 @@ const float *hr_scene_keyframes(const hr_scene *scene);
 const uint32_t *hr_scene_indices(const hr_scene *scene);
 hr_status hr_scene_get_light(const hr_scene *scene, uint32_t light, float position[3], float edge1[3],
                              float edge2[3], float normal[3], float intensity[3]);
+/* The OBJ's shading normals (num_normals x 3 floats: its vn, then one geometric normal per
+ * face that lacks a normal index, as WFObjectReader.cpp:583-614) and num_triangles x 3
+ * normal indices; null when num_normals is 0.  Key-frame scenes keep the first frame's
+ * (RTEngine::upload's normals come from its first frame, RTEngine.cu:205-209). */
+const float *hr_scene_normals(const hr_scene *scene);
+const uint32_t *hr_scene_normal_indices(const hr_scene *scene);
+/* The material table (num_materials diffuse albedos: "Default" 0.6774 first, then each
+ * usemtl name in order of first use, its .mtl Kd as mean(min(Kd, 0.99)),
+ * WFObjectReader.cpp:49-57, 135-258) and num_triangles material indices; null when
+ * num_materials is 0.  Key-frame scenes keep the last frame's. */
+const float *hr_scene_material_albedo(const hr_scene *scene);
+const uint32_t *hr_scene_triangle_materials(const hr_scene *scene);
 /* hr_set_keyframes with the scene's frames; its camera (hr_set_camera) if it has one; its
  * lights (hr_set_lights: corner = position, the file's normal, emission = mean intensity;
- * the first 64) if any. */
+ * the first 64) if any; its shading normals (hr_set_normals) and materials
+ * (hr_set_materials), or none of either. */
 hr_status hr_scene_upload(hr_ctx *ctx, const hr_scene *scene);
 
 hr_status hr_rays_file_count(const char *path, uint32_t *num_rays);

@@ -492,6 +492,51 @@ def test_scene_file_upload_renders_like_arrays(engine, tmp_path):
     assert np.array_equal(outs[0][0], outs[1][0]) and np.array_equal(outs[0][1], outs[1][1])
 
 
+def test_obj_normals_materials_upload_like_arrays(engine, tmp_path):
+    """An OBJ with vn, usemtl and a .mtl, uploaded from the file, path-traces the same image
+    as its arrays given through set_normals / set_materials; a plain OBJ uploaded after it
+    drops them again."""
+    from happyray_b200 import sceneio
+    from tests.test_io import write_obj
+    v, f = S.clusters(6_000, seed=8)
+    rng = np.random.default_rng(8)
+    vn = rng.normal(size=v.shape).astype(np.float32)
+    vn /= np.linalg.norm(vn, axis=1, keepdims=True)
+    (tmp_path / "m.mtl").write_text("newmtl a\nKd 0.2 0.3 0.4\nnewmtl b\nKd 0.9 0.9 0.6\n")
+    with open(tmp_path / "s.obj", "w") as fh:
+        fh.write("mtllib m.mtl\n")
+        fh.writelines("v %.9g %.9g %.9g\n" % tuple(p) for p in v)
+        fh.writelines("vn %.9g %.9g %.9g\n" % tuple(p) for p in vn)
+        for i, t in enumerate(f):
+            if i % 500 == 0:
+                fh.write("usemtl %s\n" % "ab"[(i // 500) % 2])
+            fh.write("f %d//%d %d//%d %d//%d\n" % (t[0] + 1, t[0] + 1, t[1] + 1, t[1] + 1, t[2] + 1, t[2] + 1))
+    sc = sceneio.load_obj(str(tmp_path / "s.obj"))
+    cam = S.camera_at_bounds(v, (64, 48))
+
+    def frame():
+        engine.set_frame_time(0.0, 0.0)
+        engine.setGridDensities(0.0625, 2.0)
+        engine.build(GRID_TWO_LEVEL)
+        engine.setCamera(cam["position"], cam["orientation"], cam["up"], cam["fov"], 64, 48)
+        engine.setLights((0.4, 0.4, 1.0), (0.2, 0, 0), (0, 0.2, 0), 20.0)
+        engine.set_integrator(pt_bounces=3, albedo=0.7, seed=12)
+        return engine.renderFrame(None, 0, RENDER_PATH)
+
+    engine.upload_scene(str(tmp_path / "s.obj"))
+    from_file = frame()
+    engine.set_keyframes(sc.keyframes, sc.faces)
+    engine.set_normals(sc.normals, sc.normal_idx)
+    engine.set_materials(sc.albedo, sc.materials)
+    assert np.array_equal(from_file, frame())
+    write_obj(tmp_path / "plain.obj", v, f)
+    engine.upload_scene(str(tmp_path / "plain.obj"))
+    plain = frame()
+    assert not np.array_equal(plain, from_file)
+    engine.set_keyframes(sc.keyframes, sc.faces)
+    assert np.array_equal(plain, frame())
+
+
 def test_ray_query_files(engine, oracle, small_clusters, tmp_path):
     """.rays in, hits out: the ids and t of the oracle's closest hits."""
     from happyray_b200 import sceneio
