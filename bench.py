@@ -14,6 +14,10 @@ render launch in a CUDA graph, against the per-scene path on the same scenes) an
 (64 resident animated scenes served under Poisson arrivals, continuous batching against
 the serial per-scene path; p50/p99 latency).
 
+c2 and c3 lines also carry `fast_arith`: the same steps through libhappyray_b200_fast.so
+(traversal kernels with FMA contraction and approximate division, IEEE grid build), its
+Mrays/s and its image on the CPU baseline's frame against the oracle's.
+
 Multi-GPU (torchrun): independent replicas, one per GPU (the path has no exchange step).
 `--impl reference` times the CPU restatement of the reference's build + traversal
 (oracle/, all host threads) on the same workload.
@@ -892,6 +896,87 @@ def run_hier(args, rank, ws, local):
     h.close()
 
 
+def configure(eng, W, frames):
+    """The workload's mesh, grid settings, camera, integrator and light on an Engine."""
+    cam = W["cam"]
+    eng.set_keyframes(frames, W["f"])
+    if W["kind"] == 0:
+        eng.set_uniform_density(W["ug"])
+    else:
+        eng.setGridDensities(W["top"], W["leaf"])
+    eng.setCamera(cam["position"], cam["orientation"], cam["up"], cam["fov"], cam["res_x"], cam["res_y"])
+    if W["mode"] == 3:
+        eng.set_integrator(ao_samples=W["ao"], ao_radius=-0.1)
+    elif W["mode"] == 1:
+        eng.set_integrator(pt_bounces=W["bounces"], albedo=0.7)
+        eng.setLights((0.4, 0.4, 1.0), (0.2, 0.0, 0.0), (0.0, 0.2, 0.0), 20.0)
+
+
+def fast_arith_leg(args, W, dev, stream, frames, flush, times_fn, keep, ieee_value):
+    """The same frames through libhappyray_b200_fast.so (traversal kernels with FMA
+    contraction and approximate division; the grid build is the IEEE one), timed like the
+    main steps, and its output on the CPU baseline's frame compared with the oracle's."""
+    import torch
+    from happyray_b200 import Engine, _lib
+    fe = Engine(dev, stream=stream.cuda_stream, lib=_lib.load_fast())
+    try:
+        configure(fe, W, frames)
+        npx = W["cam"]["res_x"] * W["cam"]["res_y"]
+        fb = torch.zeros(npx * 3, dtype=torch.float32, device=f"cuda:{dev}")
+
+        def step(i, evs=None):
+            fe.set_frame_time(times_fn(i), 0.0)
+            if evs:
+                evs[0].record(stream)
+            fe.build(W["kind"], W.get("exact", True))
+            fe.render_device(fb, 0, W["mode"])
+            if evs:
+                evs[1].record(stream)
+
+        fe.set_stats(True)
+        fe.counters(reset=True)
+        step(0)
+        fe.sync()
+        rays = fe.counters(reset=True)["rays"]
+        fe.set_stats(False)
+        for i in range(args.warmup):
+            step(i)
+        fe.sync()
+        evs = [[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(args.steps)]
+        for i in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+            step(args.warmup + i, evs[i])
+        fe.sync()
+        torch.cuda.synchronize()
+        ms = sum(e[0].elapsed_time(e[1]) for e in evs)
+        value = rays * args.steps / (ms * 1e-3) / 1e6
+        out = {"library": "libhappyray_b200_fast.so", "value": value, "unit": "Mrays/s",
+               "ms_per_step": ms / args.steps, "vs_ieee_build": value / ieee_value if ieee_value else None,
+               "rays_per_step": rays}
+        if keep and W["mode"] in (1, 3):
+            f1, f2, coeff = baseline_frame(W)
+            fe.upload(f1, f2, W["f"], coeff)
+            fe.build(W["kind"], W.get("exact", True))
+            gi, cells, leaves, prims = fe.grid_download()
+            b = keep["grid"]
+            grid_equal = bool(np.array_equal(cells, b.cells) and np.array_equal(prims, b.prims) and
+                              (b.leaves is None or np.array_equal(leaves, b.leaves)))
+            fe.render_device(fb, 0, W["mode"])
+            fe.sync()
+            st = keep["stride"]
+            img = fb.view(-1, 3).cpu().numpy()[::st, 0].astype(np.float64)
+            ref = np.asarray(keep["out"])[::st].astype(np.float64)
+            d = np.abs(img - ref)
+            out["vs_oracle"] = {"grid_bit_exact": grid_equal, "pixels_compared": int(d.size),
+                                "pixels_differing": int((d > 0).sum()), "max_abs_diff": float(d.max()),
+                                "rmse": float(np.sqrt((d * d).mean())),
+                                "image_range": [float(ref.min()), float(ref.max())]}
+        return out
+    finally:
+        fe.cleanup()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -904,6 +989,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="c4: skip the autotuner (densities 1/16, 2)")
     ap.add_argument("--no-rebuild2m", action="store_true", help="c2: skip the 2M-triangle key-frame rebuild")
+    ap.add_argument("--no-fast", action="store_true", help="c2/c3: skip the fast-arithmetic build's leg")
     ap.add_argument("--no-load-sweep", action="store_true", help="c5: skip the latency runs at sustained loads")
     ap.add_argument("--load-seconds", type=float, default=6.0, help="c5: arrival span of each sustained-load run")
     args = ap.parse_args()
@@ -933,17 +1019,7 @@ def main():
     frames = W["frames"]
     if frames is None:
         frames = v[None]
-    eng.set_keyframes(frames, f)
-    if W["kind"] == 0:
-        eng.set_uniform_density(W["ug"])
-    else:
-        eng.setGridDensities(W["top"], W["leaf"])
-    eng.setCamera(cam["position"], cam["orientation"], cam["up"], cam["fov"], cam["res_x"], cam["res_y"])
-    if W["mode"] == 3:
-        eng.set_integrator(ao_samples=W["ao"], ao_radius=-0.1)
-    elif W["mode"] == 1:
-        eng.set_integrator(pt_bounces=W["bounces"], albedo=0.7)
-        eng.setLights((0.4, 0.4, 1.0), (0.2, 0.0, 0.0), (0.0, 0.2, 0.0), 20.0)
+    configure(eng, W, frames)
     npx = cam["res_x"] * cam["res_y"]
     d_fb = torch.zeros(npx * 3, dtype=torch.float32, device=f"cuda:{dev}")
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{dev}")
@@ -1102,6 +1178,12 @@ def main():
             line["parity"] = gpu_parity(eng, W, keep, d_fb)
         except Exception as ex:   # the CPU leg is a reported baseline only
             line["cpu_baseline"] = {"error": str(ex)}
+    if W["mode"] in (1, 3) and ws == 1 and not args.no_fast:
+        try:
+            line["fast_arith"] = fast_arith_leg(args, W, dev, stream, frames, flush, frame_time,
+                                                keep if not args.no_cpu and "grid" in keep else None, value)
+        except Exception as ex:   # an extra measurement; the line above stands without it
+            line["fast_arith"] = {"error": str(ex)}
     print(json.dumps(line), flush=True)
     eng.cleanup()
     if ws > 1:

@@ -6,11 +6,16 @@ cannot be loaded, every call raises HRError -- there is no CPU fallback.
 from __future__ import annotations
 
 import ctypes as C
+import os
 import threading
 from pathlib import Path
 
 PKG = Path(__file__).resolve().parent
-LIB_PATH = PKG / "libhappyray_b200.so"
+IEEE_LIB_PATH = PKG / "libhappyray_b200.so"
+FAST_LIB_PATH = PKG / "libhappyray_b200_fast.so"
+# HAPPYRAY_B200_ARITH=fast selects the fast-arithmetic build (results within the ray
+# queries' floating-point tolerance instead of bit-exact); the default is the IEEE build
+LIB_PATH = FAST_LIB_PATH if os.environ.get("HAPPYRAY_B200_ARITH", "").lower() == "fast" else IEEE_LIB_PATH
 
 HR_OK = 0
 STATUS = {0: "HR_OK", 1: "HR_ERR_INVALID_ARG", 2: "HR_ERR_OUT_OF_MEMORY", 3: "HR_ERR_CAPACITY_RETRY",
@@ -209,16 +214,17 @@ class ServerStats(C.Structure):
 
 
 _lock = threading.Lock()
-_lib = None
+_libs = {}
 
 
 def load(path: Path | None = None):
-    """Load the CUDA library (raises HRError if it is missing: no fallback)."""
-    global _lib
+    """Load a CUDA library: `path`, else the build HAPPYRAY_B200_ARITH selects (raises
+    HRError if it is missing: no fallback).  Each library is loaded once, with its own
+    symbols (RTLD_LOCAL), so the IEEE and the fast build can be used side by side."""
+    p = Path(path).resolve() if path else LIB_PATH
     with _lock:
-        if _lib is not None:
-            return _lib
-        p = Path(path) if path else LIB_PATH
+        if p in _libs:
+            return _libs[p]
         if not p.exists():
             raise HRError(4, f"{p} is missing; build it with happyray_b200.build.build()")
         L = C.CDLL(str(p))
@@ -226,14 +232,19 @@ def load(path: Path | None = None):
             fn = getattr(L, name)
             fn.restype = res
             fn.argtypes = args
-        _lib = L
+        _libs[p] = L
         return L
 
 
-def check(ctx, status: int, what: str = ""):
+def load_fast():
+    """The fast-arithmetic build (libhappyray_b200_fast.so)."""
+    return load(FAST_LIB_PATH)
+
+
+def check(ctx, status: int, what: str = "", lib=None):
     if status != HR_OK:
         msg = ""
         if ctx:
-            m = load().hr_last_error(ctx)
+            m = (lib or load()).hr_last_error(ctx)
             msg = m.decode() if m else ""
         raise HRError(status, f"{what}: {msg}" if what else msg)

@@ -122,16 +122,19 @@ __global__ __launch_bounds__(1024) void kb_setup(const BScene* __restrict__ sc, 
     }
 }
 
-// a3 per scene chunk: pair count + the per-triangle vertex array
+// a3 per scene chunk: pair count + the per-triangle vertex array; also clears the per-top-cell
+// reference counts kb_write_pairs accumulates, and adds the chunk's pairs to its scene's
+// top-level pair count
 __global__ __launch_bounds__(kBT) void kb_count_pairs(const float4* __restrict__ v, const uint32_t* __restrict__ idx,
                                                       const uint2* __restrict__ tchunk, const BScene* __restrict__ sc,
-                                                      const GridDesc* __restrict__ descs, const GridDesc* bd,
+                                                      GridDesc* __restrict__ descs, const GridDesc* bd,
                                                       uint32_t* block_sums, float4* __restrict__ tris,
-                                                      uint4* __restrict__ rng) {
+                                                      uint4* __restrict__ rng, uint32_t* __restrict__ cell_count) {
     if (bd->overflow | bd->error) {
         if (threadIdx.x == 0) block_sums[blockIdx.x] = 0u;
         return;
     }
+    for (uint32_t c = blockIdx.x * kBT + threadIdx.x; c < bd->ncells; c += gridDim.x * kBT) cell_count[c] = 0u;
     const uint2 ch = tchunk[blockIdx.x];
     const uint32_t end = sc[ch.x].tri_off + sc[ch.x].ntri;
     const DescRegs g = load_desc(descs + ch.x);
@@ -151,7 +154,10 @@ __global__ __launch_bounds__(kBT) void kb_count_pairs(const float4* __restrict__
     }
     uint32_t tot;
     block_excl_scan<uint32_t, kBT>(n, &tot);
-    if (threadIdx.x == 0) block_sums[blockIdx.x] = tot;
+    if (threadIdx.x == 0) {
+        block_sums[blockIdx.x] = tot;
+        if (tot) atomicAdd(&descs[ch.x].ntop_pairs, tot);
+    }
 }
 
 // a5 per scene chunk: key = the scene's first top cell + local cell key, value = global
@@ -160,7 +166,8 @@ __global__ __launch_bounds__(kBT) void kb_write_pairs(const float4* __restrict__
                                                       const BScene* __restrict__ sc, const GridDesc* __restrict__ descs,
                                                       const uint32_t* __restrict__ cell_off, const GridDesc* bd,
                                                       const uint32_t* block_sums, const uint4* __restrict__ rng,
-                                                      uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+                                                      uint32_t* __restrict__ keys, uint32_t* __restrict__ vals,
+                                                      uint32_t* __restrict__ cell_count) {
     if (bd->overflow | bd->error) return;
     const uint2 ch = tchunk[blockIdx.x];
     const uint32_t end = sc[ch.x].tri_off + sc[ch.x].ntri;
@@ -183,11 +190,12 @@ __global__ __launch_bounds__(kBT) void kb_write_pairs(const float4* __restrict__
     PairRun run;
     if (n) run = {base + (uint32_t)r.lo[0] + (uint32_t)r.lo[1] * rx + (uint32_t)r.lo[2] * rxy,
                   (uint32_t)(r.hi[0] - r.lo[0]), (uint32_t)(r.hi[1] - r.lo[1]), rx, rxy, t};
-    block_write_runs<kBT>(n, run, block_sums[blockIdx.x], keys, vals);
+    block_write_runs<kBT>(n, run, block_sums[blockIdx.x], keys, vals, cell_count);
 }
 
-// a8 per global top cell, with the cell's scene found by binary search
-__global__ void kb_tl_cells(const uint2* __restrict__ top_ranges, const BScene* __restrict__ sc,
+// a8 per global top cell, with the cell's scene found by binary search; leaf_cnt holds the
+// cell's reference count on entry and its leaf count on return
+__global__ void kb_tl_cells(const BScene* __restrict__ sc,
                             const GridDesc* __restrict__ descs, const uint32_t* __restrict__ cell_off, uint32_t nsc,
                             const GridDesc* bd, uint32_t* __restrict__ leaf_cnt, uint2* __restrict__ top_cells) {
     if (bd->overflow | bd->error) return;
@@ -195,8 +203,7 @@ __global__ void kb_tl_cells(const uint2* __restrict__ top_ranges, const BScene* 
     for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < C; c += gridDim.x * blockDim.x) {
         const uint32_t s = find_segment(cell_off, nsc, c);
         const DescRegs g = load_desc(descs + s);
-        const uint2 rg = top_ranges[c];
-        const uint32_t refs = rg.y - rg.x;
+        const uint32_t refs = leaf_cnt[c];
         const LeafGeom lg = leaf_geom(g, refs, sc[s].leaf);
         uint32_t y = (lg.res[0] & 0xFFu) | ((lg.res[1] & 0xFFu) << 8) | ((lg.res[2] & 0xFFu) << 16);
         if (lg.leaf) y |= kLeafMask;
@@ -331,20 +338,15 @@ int batch_alloc(hr_batch* b) {
     hr_ctx* c = b->c;
     GridBuffers& B = c->g;
     const size_t cap_pairs = B.cap_pairs;
-    const int key_bits = std::max(1, (int)std::ceil(std::log2((double)B.cap_cells + 1.0)));
     const int leaf_bits = std::max(1, (int)std::ceil(std::log2((double)B.cap_leaves + 1.0)));
-    size_t hist = std::max(radix_tile_hist_words(cap_pairs, key_bits), radix_tile_hist_words(B.cap_leaf_pairs, leaf_bits));
+    size_t hist = radix_tile_hist_words(B.cap_leaf_pairs, leaf_bits);
     const size_t nref_blocks = (cap_pairs + kBT - 1) / kBT;
     int rc;
     if ((rc = ensure(c, B.cells, sizeof(uint2) * B.cap_cells))) return rc;
-    if ((rc = ensure(c, B.top_ranges, sizeof(uint2) * B.cap_cells))) return rc;
     if ((rc = ensure(c, B.leaf_cnt, sizeof(uint32_t) * B.cap_cells))) return rc;
     if ((rc = ensure(c, B.scan_partials, sizeof(uint32_t) * (scan_partials_words(B.cap_cells) + 2)))) return rc;
     if ((rc = ensure(c, B.keys_a, sizeof(uint32_t) * cap_pairs))) return rc;
     if ((rc = ensure(c, B.vals_a, sizeof(uint32_t) * cap_pairs))) return rc;
-    if ((rc = ensure(c, B.keys_b, sizeof(uint32_t) * cap_pairs))) return rc;
-    if ((rc = ensure(c, B.vals_b, sizeof(uint32_t) * cap_pairs))) return rc;
-    if ((rc = ensure(c, B.top_refs, sizeof(uint32_t) * cap_pairs))) return rc;
     if ((rc = ensure(c, B.ref_ranges, sizeof(uint4) * cap_pairs))) return rc;
     if ((rc = ensure(c, B.tri_ranges, sizeof(uint4) * std::max<size_t>(b->ntri, 1)))) return rc;
     if ((rc = ensure(c, B.block_sums, sizeof(uint32_t) * (std::max((size_t)b->ntchunk, nref_blocks) + 1)))) return rc;
@@ -365,7 +367,6 @@ int enqueue_build(hr_batch* b) {
     cudaStream_t s = c->stream;
     GridBuffers& B = c->g;
     const size_t cap_pairs = B.cap_pairs;
-    const int key_bits = std::max(1, (int)std::ceil(std::log2((double)B.cap_cells + 1.0)));
     const int leaf_bits = std::max(1, (int)std::ceil(std::log2((double)B.cap_leaves + 1.0)));
     const uint32_t nref_blocks = (uint32_t)((cap_pairs + kBT - 1) / kBT);
     GridDesc* descs = dev<GridDesc>(b->d_descs);
@@ -376,36 +377,27 @@ int enqueue_build(hr_batch* b) {
     float4* tris = c->tris.as<float4>();
     uint32_t* bsum = B.block_sums.as<uint32_t>();
     int rc;
-    c->launches += 16;   // this function's kernels, both block-sum scans included
+    c->launches += 14;   // this function's kernels, both block-sum scans included
     kb_init<<<(b->nsc + 255) / 256, 256, 0, s>>>(sc, b->nsc, descs, bd, b->ntri, dev<uint32_t>(b->d_bad));
     kb_bounds<<<b->nvchunk, kBT, 0, s>>>(c->verts.as<float4>(), dev<uint2>(b->d_vchunk), sc, descs);
     kb_setup<<<1, 1024, 0, s>>>(sc, b->nsc, descs, cell_off, bd, (uint32_t)std::min(B.cap_cells, (size_t)0xffffffffu));
+    // the top-level pairs stay in triangle order (as the per-scene build: the leaf level needs
+    // only each top cell's reference count, counted as they are written)
     kb_count_pairs<<<b->ntchunk, kBT, 0, s>>>(c->verts.as<float4>(), c->idx.as<uint32_t>(), tch, sc, descs, bd, bsum, tris,
-                                              B.tri_ranges.as<uint4>());
+                                              B.tri_ranges.as<uint4>(), B.leaf_cnt.as<uint32_t>());
     if ((rc = scan_block_sums(c, bsum, b->ntchunk, &bd->ntop_pairs, &bd->overflow,
                               (uint32_t)std::min(cap_pairs, (size_t)0xffffffffu), kOvfTopPairs, &bd->req_pairs, s)))
         return rc;
     kb_write_pairs<<<b->ntchunk, kBT, 0, s>>>(tris, tch, sc, descs, cell_off, bd, bsum, B.tri_ranges.as<uint4>(),
-                                              B.keys_a.as<uint32_t>(), B.vals_a.as<uint32_t>());
-    const int passes = radix_sort_passes(key_bits);
-    uint32_t* sorted_keys = (passes % 2 == 1) ? B.keys_b.as<uint32_t>() : B.keys_a.as<uint32_t>();
-    if ((rc = radix_sort_pairs(c, B.keys_a.as<uint32_t>(), B.vals_a.as<uint32_t>(), B.keys_b.as<uint32_t>(),
-                               B.vals_b.as<uint32_t>(), sorted_keys, B.top_refs.as<uint32_t>(), &bd->ntop_pairs,
-                               cap_pairs, key_bits, B.tile_hist.as<uint32_t>(), B.tile_hist.bytes, B.row_total.as<uint32_t>(), s)))
-        return rc;
-    uint2* ranges = B.top_ranges.as<uint2>();
+                                              B.keys_a.as<uint32_t>(), B.vals_a.as<uint32_t>(), B.leaf_cnt.as<uint32_t>());
     const int gcells = std::max(1, std::min((int)((B.cap_cells + 255) / 256), c->num_sms * 16));
-    k_fill_u2<<<gcells, 256, 0, s>>>(ranges, &bd->ncells, bd, make_uint2(0u, 0u));
-    const int gpairs = std::max(1, std::min((int)((cap_pairs + 255) / 256), c->num_sms * 16));
-    k_cell_ranges<<<gpairs, 256, 0, s>>>(sorted_keys, &bd->ntop_pairs, &bd->ncells, bd, ranges);
-    kb_tl_cells<<<gcells, 256, 0, s>>>(ranges, sc, descs, cell_off, b->nsc, bd, B.leaf_cnt.as<uint32_t>(),
-                                       B.cells.as<uint2>());
+    kb_tl_cells<<<gcells, 256, 0, s>>>(sc, descs, cell_off, b->nsc, bd, B.leaf_cnt.as<uint32_t>(), B.cells.as<uint2>());
     if ((rc = exclusive_scan_u32(c, B.leaf_cnt.as<uint32_t>(), &bd->ncells, B.cap_cells, &bd->nleaves,
                                  B.scan_partials.as<uint32_t>(), s)))
         return rc;
     k_check_leaves<<<1, 1, 0, s>>>(bd, (uint32_t)std::min(B.cap_leaves, (size_t)0xffffffffu));
     k_tl_cell_begin<<<gcells, 256, 0, s>>>(B.leaf_cnt.as<uint32_t>(), bd, B.cells.as<uint2>());
-    kb_leaf_count_pairs<<<nref_blocks, kBT, 0, s>>>(sorted_keys, B.top_refs.as<uint32_t>(), tris, descs, cell_off,
+    kb_leaf_count_pairs<<<nref_blocks, kBT, 0, s>>>(B.keys_a.as<uint32_t>(), B.vals_a.as<uint32_t>(), tris, descs, cell_off,
                                                     b->nsc, bd, B.cells.as<uint2>(), bsum, B.ref_ranges.as<uint4>());
     if ((rc = scan_block_sums(c, bsum, nref_blocks, &bd->npairs, &bd->overflow,
                               (uint32_t)std::min(B.cap_leaf_pairs, (size_t)0xffffffffu), kOvfLeafPairs,
@@ -957,16 +949,7 @@ hr_status hr_batch_grid_info(hr_batch* b, uint32_t scene, hr_grid_info* info) {
     info->num_cells = co[1] - co[0];
     info->num_leaves = leaf_end - first.x;
     info->num_pairs = pmax > pmin ? pmax - pmin : 0u;
-    // top-level references of the scene: the sum of its cells' ranges
-    std::vector<uint2> tr(info->num_cells);
-    if (!tr.empty()) {
-        rc = cuda_check(c, cudaMemcpy(tr.data(), c->g.top_ranges.as<uint2>() + co[0], tr.size() * sizeof(uint2),
-                                      cudaMemcpyDeviceToHost), "top ranges");
-        if (rc) return (hr_status)rc;
-    }
-    uint32_t ntop = 0;
-    for (const uint2& r : tr) ntop += r.y - r.x;
-    info->num_top_pairs = ntop;
+    info->num_top_pairs = d.ntop_pairs;   // counted per scene by kb_count_pairs
     return HR_OK;
 }
 

@@ -95,14 +95,19 @@ __global__ void k_grid_setup(GridDesc* d, float density, uint32_t cap_cells) {
 // a3: pair count, one triangle per thread; block sums for the scan (UniformGridBuildKernels.h:40-105).
 // Also writes the per-triangle vertex array (3 float4) that the later build passes and the
 // traversal read instead of gathering through the index buffer.
+// With cell_count (two-level), the kernel's threads also clear the per-top-cell reference
+// counts that k_write_pairs accumulates.
 __global__ __launch_bounds__(kBT) void k_count_pairs(const float4* __restrict__ v, const uint32_t* __restrict__ idx,
                                                      uint32_t ntri, const GridDesc* d, uint32_t* block_sums,
-                                                     float4* __restrict__ tris, uint4* __restrict__ rng) {
+                                                     float4* __restrict__ tris, uint4* __restrict__ rng,
+                                                     uint32_t* __restrict__ cell_count) {
     if (d->overflow | d->error) {
         if (threadIdx.x == 0) block_sums[blockIdx.x] = 0u;
         return;
     }
     const DescRegs g = load_desc(d);
+    if (cell_count)
+        for (uint32_t c = blockIdx.x * kBT + threadIdx.x; c < g.ncells; c += gridDim.x * kBT) cell_count[c] = 0u;
     const uint32_t t = blockIdx.x * kBT + threadIdx.x;
     uint32_t n = 0;
     if (t < ntri) {
@@ -124,10 +129,13 @@ __global__ __launch_bounds__(kBT) void k_count_pairs(const float4* __restrict__ 
 
 // a5: pair scatter at the triangle's exclusive-scan offset.  Keys are x + y*rx + z*rx*ry;
 // with EXACT a cell rejected by the SAT test gets key = ncells (sorted last, skipped).
+// With cell_count, every pair's cell is also counted there (the two-level build needs the
+// number of references per top cell, not their sorted order).
 template <bool EXACT>
 __global__ __launch_bounds__(kBT) void k_write_pairs(const float4* __restrict__ tris, uint32_t ntri, const GridDesc* d,
                                                      const uint32_t* block_sums, const uint4* __restrict__ rng,
-                                                     uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+                                                     uint32_t* __restrict__ keys, uint32_t* __restrict__ vals,
+                                                     uint32_t* __restrict__ cell_count) {
     if (d->overflow | d->error) return;
     const DescRegs g = load_desc(d);
     const uint32_t t = blockIdx.x * kBT + threadIdx.x;
@@ -148,7 +156,7 @@ __global__ __launch_bounds__(kBT) void k_write_pairs(const float4* __restrict__ 
         PairRun run;
         if (n) run = {(uint32_t)r.lo[0] + (uint32_t)r.lo[1] * rx + (uint32_t)r.lo[2] * rxy,
                       (uint32_t)(r.hi[0] - r.lo[0]), (uint32_t)(r.hi[1] - r.lo[1]), rx, rxy, t};
-        block_write_runs<kBT>(n, run, block_sums[blockIdx.x], keys, vals);
+        block_write_runs<kBT>(n, run, block_sums[blockIdx.x], keys, vals, cell_count);
         return;
     }
     uint32_t tot;
@@ -179,13 +187,14 @@ __global__ __launch_bounds__(kBT) void k_write_pairs(const float4* __restrict__ 
 
 // a8: per top cell: leaf resolution, flags, leaf-cell count (countLeafLevelCells,
 // TLGridBuildKernels.h:45-122); packed y of TwoLevelGridCell (TwoLevelGrid.h:38-161)
-__global__ void k_tl_cells(const uint2* __restrict__ top_ranges, const GridDesc* d, float leaf_density,
-                           uint32_t* __restrict__ leaf_cnt, uint2* __restrict__ top_cells) {
+// leaf_cnt holds each top cell's reference count on entry (k_write_pairs) and its leaf
+// count on return.
+__global__ void k_tl_cells(const GridDesc* d, float leaf_density, uint32_t* __restrict__ leaf_cnt,
+                           uint2* __restrict__ top_cells) {
     if (d->overflow | d->error) return;
     const DescRegs g = load_desc(d);
     for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < g.ncells; c += gridDim.x * blockDim.x) {
-        const uint2 rg = top_ranges[c];
-        const uint32_t refs = rg.y - rg.x;
+        const uint32_t refs = leaf_cnt[c];
         const LeafGeom lg = leaf_geom(g, refs, leaf_density);
         uint32_t y = (lg.res[0] & 0xFFu) | ((lg.res[1] & 0xFFu) << 8) | ((lg.res[2] & 0xFFu) << 16);
         if (lg.leaf) y |= kLeafMask;
@@ -195,7 +204,8 @@ __global__ void k_tl_cells(const uint2* __restrict__ top_ranges, const GridDesc*
     }
 }
 
-// sub-cell range of top-level reference i: its top cell (sorted key), triangle, cell sub-grid
+// sub-cell range of top-level reference i (pairs in triangle order): its top cell, triangle,
+// cell sub-grid
 __device__ __forceinline__ uint32_t ref_leaf_range(const DescRegs& g, const uint32_t* __restrict__ top_keys,
                                                    const uint32_t* __restrict__ top_refs,
                                                    const float4* __restrict__ tris,
@@ -212,7 +222,8 @@ __device__ __forceinline__ uint32_t ref_leaf_range(const DescRegs& g, const uint
 }
 
 // a10: leaf pair count per top-level reference, block sums (countLeafLevelPairs,
-// TLGridBuildKernels.h:304-409)
+// TLGridBuildKernels.h:304-409); the references are the top-level pairs as written, in
+// triangle order
 __global__ __launch_bounds__(kBT) void k_leaf_count_pairs(const uint32_t* __restrict__ top_keys,
                                                           const uint32_t* __restrict__ top_refs,
                                                           const float4* __restrict__ tris,
@@ -280,7 +291,7 @@ int key_bits_for(size_t max_key) {
 static std::vector<uint8_t> build_graph_key(const hr_ctx* c, int32_t kind, int32_t exact, float dens) {
     const GridBuffers& B = c->g;
     const DevBuf* bufs[] = {&B.desc, &c->tris, &B.cells, &B.keys_a, &B.tri_ranges, &B.vals_a, &B.keys_b, &B.vals_b,
-                            &B.block_sums, &B.tile_hist, &B.row_total, &B.prims, &B.top_ranges, &B.top_refs,
+                            &B.block_sums, &B.tile_hist, &B.row_total, &B.prims,
                             &B.ref_ranges, &B.leaf_cnt, &B.scan_partials, &B.leaves, &B.lkeys_a, &B.lvals_a,
                             &B.lkeys_b, &B.lvals_b, &c->verts, &c->idx, &c->counters, &c->keyframes, &c->frame_sel};
     std::vector<uint8_t> k;
@@ -333,8 +344,8 @@ static int build_once_impl(hr_ctx* c, int32_t kind, int32_t exact, uint32_t* ovf
     const int leaf_bits = key_bits_for(B.cap_leaves);
     const int leaf_passes = radix_sort_passes(leaf_bits);
     const uint32_t nref_blocks = (uint32_t)((cap_pairs + kBT - 1) / kBT);   // per top-level reference
-    size_t hist_words = radix_tile_hist_words(cap_pairs, key_bits);
-    if (kind == kTwoLevel) hist_words = std::max(hist_words, radix_tile_hist_words(B.cap_leaf_pairs, leaf_bits));
+    const size_t hist_words = kind == kUniform ? radix_tile_hist_words(cap_pairs, key_bits)
+                                               : radix_tile_hist_words(B.cap_leaf_pairs, leaf_bits);
     int rc;
     if ((rc = ensure(c, B.desc, sizeof(GridDesc)))) return rc;
     if ((rc = ensure(c, c->frame_sel, sizeof(int4)))) return rc;
@@ -343,16 +354,14 @@ static int build_once_impl(hr_ctx* c, int32_t kind, int32_t exact, uint32_t* ovf
     if ((rc = ensure(c, B.keys_a, sizeof(uint32_t) * cap_pairs))) return rc;
     if ((rc = ensure(c, B.tri_ranges, sizeof(uint4) * (size_t)ntri))) return rc;
     if ((rc = ensure(c, B.vals_a, sizeof(uint32_t) * cap_pairs))) return rc;
-    if ((rc = ensure(c, B.keys_b, sizeof(uint32_t) * cap_pairs))) return rc;
-    if ((rc = ensure(c, B.vals_b, sizeof(uint32_t) * cap_pairs))) return rc;
     if ((rc = ensure(c, B.block_sums, sizeof(uint32_t) * (std::max(nblocks, nref_blocks) + 1)))) return rc;
     if ((rc = ensure(c, B.tile_hist, sizeof(uint32_t) * hist_words))) return rc;
     if ((rc = ensure(c, B.row_total, sizeof(uint32_t) * kRadixRowWords))) return rc;
-    if (kind == kUniform) {
+    if (kind == kUniform) {   // the sort's second buffers (the two-level top level is not sorted)
+        if ((rc = ensure(c, B.keys_b, sizeof(uint32_t) * cap_pairs))) return rc;
+        if ((rc = ensure(c, B.vals_b, sizeof(uint32_t) * cap_pairs))) return rc;
         if ((rc = ensure(c, B.prims, sizeof(uint32_t) * cap_pairs))) return rc;
     } else {
-        if ((rc = ensure(c, B.top_ranges, sizeof(uint2) * B.cap_cells))) return rc;
-        if ((rc = ensure(c, B.top_refs, sizeof(uint32_t) * cap_pairs))) return rc;
         if ((rc = ensure(c, B.ref_ranges, sizeof(uint4) * cap_pairs))) return rc;
         if ((rc = ensure(c, B.leaf_cnt, sizeof(uint32_t) * B.cap_cells))) return rc;
         if ((rc = ensure(c, B.scan_partials, sizeof(uint32_t) * (scan_partials_words(B.cap_cells) + 2)))) return rc;
@@ -375,7 +384,7 @@ static int build_once_impl(hr_ctx* c, int32_t kind, int32_t exact, uint32_t* ovf
         };
         mark();
         // launches of this function (radix sort and scans count their own)
-        c->launches += 3 + (nblocks > 0 ? 3 : 0) + 2 + (kind == kTwoLevel ? 9 : 0);
+        c->launches += 3 + (nblocks > 0 ? 3 : 0) + (kind == kTwoLevel ? 9 : 2);
         k_desc_init<<<1, 1, 0, s>>>(d, kind, ntri, c->counters.as<uint32_t>() + 2);
         const int gridv = std::max(1, std::min((int)((c->nverts + kBT - 1) / kBT), c->num_sms * 8));
         k_lerp_bounds<<<gridv, kBT, 0, s>>>(c->lerp_pending ? c->keyframes.as<float4>() : nullptr,
@@ -386,36 +395,44 @@ static int build_once_impl(hr_ctx* c, int32_t kind, int32_t exact, uint32_t* ovf
         const uint32_t* ix = c->idx.as<uint32_t>();
         uint32_t* bsum = B.block_sums.as<uint32_t>();
         uint32_t* d_np = kind == kUniform ? &d->npairs : &d->ntop_pairs;
+        // two-level: the references per top cell are counted as the pairs are written
+        uint32_t* cell_count = kind == kTwoLevel ? B.leaf_cnt.as<uint32_t>() : nullptr;
         if (nblocks > 0) {
-            k_count_pairs<<<nblocks, kBT, 0, s>>>(v, ix, ntri, d, bsum, c->tris.as<float4>(), B.tri_ranges.as<uint4>());
+            k_count_pairs<<<nblocks, kBT, 0, s>>>(v, ix, ntri, d, bsum, c->tris.as<float4>(), B.tri_ranges.as<uint4>(),
+                                                  cell_count);
             if ((rc = scan_block_sums(c, bsum, nblocks, d_np, &d->overflow, (uint32_t)std::min(cap_pairs, (size_t)0xffffffffu),
                                       kind == kUniform ? kOvfPairs : kOvfTopPairs, &d->req_pairs, s)))
                 return rc;
             if (kind == kUniform && exact)
                 k_write_pairs<true><<<nblocks, kBT, 0, s>>>(c->tris.as<float4>(), ntri, d, bsum, nullptr,
-                                                            B.keys_a.as<uint32_t>(), B.vals_a.as<uint32_t>());
+                                                            B.keys_a.as<uint32_t>(), B.vals_a.as<uint32_t>(), nullptr);
             else
                 k_write_pairs<false><<<nblocks, kBT, 0, s>>>(c->tris.as<float4>(), ntri, d, bsum, B.tri_ranges.as<uint4>(),
-                                                             B.keys_a.as<uint32_t>(), B.vals_a.as<uint32_t>());
+                                                             B.keys_a.as<uint32_t>(), B.vals_a.as<uint32_t>(), cell_count);
         }
         mark();
-        uint32_t* sorted_keys = (passes % 2 == 1) ? B.keys_b.as<uint32_t>() : B.keys_a.as<uint32_t>();
-        uint32_t* sorted_vals = kind == kUniform ? B.prims.as<uint32_t>() : B.top_refs.as<uint32_t>();
-        if ((rc = radix_sort_pairs(c, B.keys_a.as<uint32_t>(), B.vals_a.as<uint32_t>(), B.keys_b.as<uint32_t>(),
-                                   B.vals_b.as<uint32_t>(), sorted_keys, sorted_vals, d_np, cap_pairs, key_bits,
-                                   B.tile_hist.as<uint32_t>(), B.tile_hist.bytes, B.row_total.as<uint32_t>(), s)))
-            return rc;
-        mark();
-        uint2* ranges = kind == kUniform ? B.cells.as<uint2>() : B.top_ranges.as<uint2>();
         const int gcells = std::max(1, std::min((int)((B.cap_cells + 255) / 256), c->num_sms * 16));
-        k_fill_u2<<<gcells, 256, 0, s>>>(ranges, &d->ncells, d, make_uint2(0u, 0u));
-        const int gpairs = std::max(1, std::min((int)((cap_pairs + 255) / 256), c->num_sms * 16));
-        k_cell_ranges<<<gpairs, 256, 0, s>>>(sorted_keys, d_np, &d->ncells, d, ranges);
-        mark();
-        if (kind == kTwoLevel) {
-            // leaf level, TLGridSortBuilder.h:256-410: leaf cells per top cell, scan, leaf pairs
-            // per reference in reference order, stable sort by leaf, leaf ranges
-            k_tl_cells<<<gcells, 256, 0, s>>>(ranges, d, c->leaf_density, B.leaf_cnt.as<uint32_t>(), B.cells.as<uint2>());
+        if (kind == kUniform) {
+            // a6-a7: pairs sorted by cell, cell ranges
+            uint32_t* sorted_keys = (passes % 2 == 1) ? B.keys_b.as<uint32_t>() : B.keys_a.as<uint32_t>();
+            if ((rc = radix_sort_pairs(c, B.keys_a.as<uint32_t>(), B.vals_a.as<uint32_t>(), B.keys_b.as<uint32_t>(),
+                                       B.vals_b.as<uint32_t>(), sorted_keys, B.prims.as<uint32_t>(), d_np, cap_pairs,
+                                       key_bits, B.tile_hist.as<uint32_t>(), B.tile_hist.bytes,
+                                       B.row_total.as<uint32_t>(), s)))
+                return rc;
+            mark();
+            k_fill_u2<<<gcells, 256, 0, s>>>(B.cells.as<uint2>(), &d->ncells, d, make_uint2(0u, 0u));
+            const int gpairs = std::max(1, std::min((int)((cap_pairs + 255) / 256), c->num_sms * 16));
+            k_cell_ranges<<<gpairs, 256, 0, s>>>(sorted_keys, d_np, &d->ncells, d, B.cells.as<uint2>());
+            mark();
+        } else {
+            // Leaf level, TLGridSortBuilder.h:256-410: leaf cells per top cell, scan, leaf pairs
+            // per top-level reference, stable sort by leaf, leaf ranges.  The reference sorts
+            // the top-level pairs by cell first; here they stay in triangle order: the leaf
+            // level needs only each top cell's reference count (counted as they were written),
+            // and the one stable sort by global leaf index then orders every leaf's list by
+            // triangle exactly as the two sorts would.
+            k_tl_cells<<<gcells, 256, 0, s>>>(d, c->leaf_density, B.leaf_cnt.as<uint32_t>(), B.cells.as<uint2>());
             uint32_t* sp = B.scan_partials.as<uint32_t>();
             if ((rc = exclusive_scan_u32(c, B.leaf_cnt.as<uint32_t>(), &d->ncells, B.cap_cells, &d->nleaves, sp, s)))
                 return rc;
@@ -423,8 +440,9 @@ static int build_once_impl(hr_ctx* c, int32_t kind, int32_t exact, uint32_t* ovf
             k_tl_cell_begin<<<gcells, 256, 0, s>>>(B.leaf_cnt.as<uint32_t>(), d, B.cells.as<uint2>());
             mark();
             uint32_t* lsum = B.block_sums.as<uint32_t>();
-            k_leaf_count_pairs<<<nref_blocks, kBT, 0, s>>>(sorted_keys, B.top_refs.as<uint32_t>(), c->tris.as<float4>(), d,
-                                                           B.cells.as<uint2>(), lsum, B.ref_ranges.as<uint4>());
+            k_leaf_count_pairs<<<nref_blocks, kBT, 0, s>>>(B.keys_a.as<uint32_t>(), B.vals_a.as<uint32_t>(),
+                                                           c->tris.as<float4>(), d, B.cells.as<uint2>(), lsum,
+                                                           B.ref_ranges.as<uint4>());
             if ((rc = scan_block_sums(c, lsum, nref_blocks, &d->npairs, &d->overflow,
                                       (uint32_t)std::min(B.cap_leaf_pairs, (size_t)0xffffffffu), kOvfLeafPairs,
                                       &d->req_leaf_pairs, s)))

@@ -67,26 +67,40 @@ struct PairRun { uint32_t key0, ex, ey, sx, sxy, val; };
 // cells costs its block a few strides instead of one thread a serial loop, and consecutive
 // threads store consecutive slots.  n is this thread's run length, run is read when n > 0.
 // Every thread of the block calls it.
+// With `counts`, also adds every written key to counts[key] (a histogram of the keys; the
+// lanes of a warp holding the same key add once, so a crowded cell costs few atomics).
 template <int NT>
 __device__ __forceinline__ void block_write_runs(uint32_t n, const PairRun& run, uint32_t out0,
-                                                 uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+                                                 uint32_t* __restrict__ keys, uint32_t* __restrict__ vals,
+                                                 uint32_t* __restrict__ counts = nullptr) {
     __shared__ uint32_t s_off[NT];
     __shared__ PairRun s_run[NT];
     uint32_t tot;
     s_off[threadIdx.x] = block_excl_scan<uint32_t, NT>(n, &tot);
     if (n) s_run[threadIdx.x] = run;
     __syncthreads();
-    for (uint32_t j = threadIdx.x; j < tot; j += NT) {
-        const int k = block_owner<NT>(s_off, j);
-        const PairRun q = s_run[k];
-        const uint32_t l = j - s_off[k];
-        uint32_t key = q.key0;
-        if (l) {
-            const uint32_t a = l / q.ex, z = a / q.ey;
-            key += (l - a * q.ex) + (a - z * q.ey) * q.sx + z * q.sxy;
+    const uint32_t lane = threadIdx.x & 31u;
+    // warp-uniform trip count, so that the whole warp meets the match below
+    for (uint32_t j0 = threadIdx.x - lane; j0 < tot; j0 += NT) {
+        const uint32_t j = j0 + lane;
+        const bool valid = j < tot;
+        uint32_t key = 0xffffffffu;
+        if (valid) {
+            const int k = block_owner<NT>(s_off, j);
+            const PairRun q = s_run[k];
+            const uint32_t l = j - s_off[k];
+            key = q.key0;
+            if (l) {
+                const uint32_t a = l / q.ex, z = a / q.ey;
+                key += (l - a * q.ex) + (a - z * q.ey) * q.sx + z * q.sxy;
+            }
+            keys[out0 + j] = key;
+            vals[out0 + j] = q.val;
         }
-        keys[out0 + j] = key;
-        vals[out0 + j] = q.val;
+        if (counts) {
+            const uint32_t peers = __match_any_sync(0xffffffffu, key);
+            if (valid && lane == (uint32_t)(__ffs(peers) - 1)) atomicAdd(counts + key, (uint32_t)__popc(peers));
+        }
     }
 }
 

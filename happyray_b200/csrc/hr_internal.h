@@ -48,9 +48,7 @@ struct GridBuffers {
     DevBuf block_sums;    // per-block counts of the pair-count pass
     DevBuf tile_hist;     // radix tile histograms
     DevBuf row_total;     // radix digit totals
-    DevBuf top_ranges;    // two-level: uint2 per top cell
-    DevBuf top_refs;      // two-level: sorted top-level values
-    DevBuf leaf_cnt;      // two-level: leaf cells per top cell, scanned in place to the first leaf
+    DevBuf leaf_cnt;      // two-level: references, then leaf cells per top cell, scanned in place to the first leaf
     DevBuf lkeys_a, lvals_a, lkeys_b, lvals_b;   // two-level: leaf pair ping-pong
     DevBuf scan_partials; // generic scan partial sums
     DevBuf tri_ranges;    // uint4 per triangle: its cell range (16-bit coordinates) and pair count

@@ -36,8 +36,8 @@ def _f3(x):
 class Engine:
     """One GPU context (hr_ctx).  `stream` is a cudaStream_t handle (int) or None."""
 
-    def __init__(self, device: int = 0, stream: Optional[int] = None):
-        self.L = _lib.load()
+    def __init__(self, device: int = 0, stream: Optional[int] = None, lib=None):
+        self.L = lib or _lib.load()
         ctx = C.c_void_p()
         st = self.L.hr_create(C.byref(ctx), device, C.c_void_p(stream) if stream else None)
         if st != 0:
@@ -72,7 +72,7 @@ class Engine:
         self.cleanup()
 
     def _chk(self, st, what):
-        check(self.ctx, st, what)
+        check(self.ctx, st, what, self.L)
 
     # -- RTEngine::upload(frame1, frame2, coeff) ---------------------------------
     def upload(self, frame1_xyz, frame2_xyz, tri_idx, coeff: float = 1.0):

@@ -32,6 +32,22 @@ def test_library_exports_every_declared_symbol(hrlib):
         assert hasattr(hrlib, s)
 
 
+def test_fast_library_exports_the_same_symbols(hrlib):
+    """libhappyray_b200_fast.so (the fast-arithmetic traversal) is a drop-in for the IEEE
+    library: the same exported hr_* symbols."""
+    from happyray_b200 import _lib
+    from happyray_b200 import build as B
+    if not B.OUT_FAST.exists():
+        B.build(fast=True)
+
+    def exported(p):
+        out = subprocess.run(["nm", "-D", "--defined-only", str(p)], capture_output=True, text=True, check=True).stdout
+        return set(re.findall(r"\bT (hr_[a-z0-9_]+)", out))
+
+    assert exported(_lib.FAST_LIB_PATH) == exported(_lib.IEEE_LIB_PATH)
+    assert set(declared_symbols()) <= exported(_lib.FAST_LIB_PATH)
+
+
 def test_binding_matches_header():
     from happyray_b200 import _lib
     assert sorted(_lib.SIGNATURES) == declared_symbols()
