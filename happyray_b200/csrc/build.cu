@@ -138,7 +138,8 @@ __global__ __launch_bounds__(kBT) void k_write_pairs(const float4* __restrict__ 
                                                      uint32_t* __restrict__ cell_count) {
     if (d->overflow | d->error) return;
     const DescRegs g = load_desc(d);
-    const uint32_t t = blockIdx.x * kBT + threadIdx.x;
+    const uint32_t bx = gridDim.x - 1u - blockIdx.x;   // last block first (see k_leaf_write_pairs)
+    const uint32_t t = bx * kBT + threadIdx.x;
     uint32_t n = 0;
     f3 p[3], lo, hi;
     CRange r;
@@ -156,11 +157,11 @@ __global__ __launch_bounds__(kBT) void k_write_pairs(const float4* __restrict__ 
         PairRun run;
         if (n) run = {(uint32_t)r.lo[0] + (uint32_t)r.lo[1] * rx + (uint32_t)r.lo[2] * rxy,
                       (uint32_t)(r.hi[0] - r.lo[0]), (uint32_t)(r.hi[1] - r.lo[1]), rx, rxy, t};
-        block_write_runs<kBT>(n, run, block_sums[blockIdx.x], keys, vals, cell_count);
+        block_write_runs<kBT>(n, run, block_sums[bx], keys, vals, cell_count);
         return;
     }
     uint32_t tot;
-    uint32_t slot = block_excl_scan<uint32_t, kBT>(n, &tot) + block_sums[blockIdx.x];
+    uint32_t slot = block_excl_scan<uint32_t, kBT>(n, &tot) + block_sums[bx];
     if (n == 0) return;
     const f3 nrm = normalize(cross(sub(p[1], p[0]), sub(p[2], p[0])));
     const f3 h = mulf(g.cs, 0.505f);
@@ -248,12 +249,16 @@ __global__ __launch_bounds__(kBT) void k_leaf_count_pairs(const uint32_t* __rest
 }
 
 // a11: leaf pairs in reference order at each reference's scan offset; key = first leaf of
-// the top cell + local sub-cell index (writeLeafLevelKeysAndValues, TLGridBuildKernels.h:536-663)
+// the top cell + local sub-cell index (writeLeafLevelKeysAndValues, TLGridBuildKernels.h:536-663).
+// Blocks take the references from the end first: a block's work is its pair count, and a
+// mesh's large triangles (a ground plane over thousands of cells) tend to sit at one end of
+// it; launched last, their long blocks would run alone at the end of the kernel.
 __global__ __launch_bounds__(kBT) void k_leaf_write_pairs(const uint4* __restrict__ refrng, const GridDesc* d,
                                                           const uint32_t* block_sums, uint32_t* __restrict__ keys,
                                                           uint32_t* __restrict__ vals) {
     if (d->overflow | d->error) return;
-    const uint32_t i = blockIdx.x * kBT + threadIdx.x;
+    const uint32_t bx = gridDim.x - 1u - blockIdx.x;
+    const uint32_t i = bx * kBT + threadIdx.x;
     uint32_t n = 0, tri = 0, base = 0, lres[2] = {1u, 1u};
     CRange r;
     if (i < d->ntop_pairs) {   // the sub-cell range k_leaf_count_pairs found
@@ -274,7 +279,7 @@ __global__ __launch_bounds__(kBT) void k_leaf_write_pairs(const uint4* __restric
     PairRun run;
     if (n) run = {base + (uint32_t)r.lo[0] + (uint32_t)r.lo[1] * lres[0] + (uint32_t)r.lo[2] * lres[0] * lres[1],
                   (uint32_t)(r.hi[0] - r.lo[0]), (uint32_t)(r.hi[1] - r.lo[1]), lres[0], lres[0] * lres[1], tri};
-    block_write_runs<kBT>(n, run, block_sums[blockIdx.x], keys, vals);
+    block_write_runs<kBT>(n, run, block_sums[bx], keys, vals);
 }
 
 int key_bits_for(size_t max_key) {
