@@ -197,19 +197,29 @@ __global__ __launch_bounds__(kBT) void kb_write_pairs(const float4* __restrict__
 // cell's reference count on entry and its leaf count on return
 __global__ void kb_tl_cells(const BScene* __restrict__ sc,
                             const GridDesc* __restrict__ descs, const uint32_t* __restrict__ cell_off, uint32_t nsc,
-                            const GridDesc* bd, uint32_t* __restrict__ leaf_cnt, uint2* __restrict__ top_cells) {
+                            const GridDesc* bd, uint32_t* __restrict__ leaf_cnt, uint2* __restrict__ top_cells,
+                            uint32_t* __restrict__ occ) {
     if (bd->overflow | bd->error) return;
     const uint32_t C = bd->ncells;
-    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < C; c += gridDim.x * blockDim.x) {
-        const uint32_t s = find_segment(cell_off, nsc, c);
-        const DescRegs g = load_desc(descs + s);
-        const uint32_t refs = leaf_cnt[c];
-        const LeafGeom lg = leaf_geom(g, refs, sc[s].leaf);
-        uint32_t y = (lg.res[0] & 0xFFu) | ((lg.res[1] & 0xFFu) << 8) | ((lg.res[2] & 0xFFu) << 16);
-        if (lg.leaf) y |= kLeafMask;
-        if (refs != 0) y |= kNotEmptyMask;
-        top_cells[c].y = y;
-        leaf_cnt[c] = lg.res[0] * lg.res[1] * lg.res[2];
+    const uint32_t lane = threadIdx.x & 31u;
+    // warp-uniform trip count: the 32 cells of a pass share one occupancy word (global cell bits)
+    for (uint32_t c0 = blockIdx.x * blockDim.x + threadIdx.x - lane; c0 < C; c0 += gridDim.x * blockDim.x) {
+        const uint32_t c = c0 + lane;
+        bool full = false;
+        if (c < C) {
+            const uint32_t s = find_segment(cell_off, nsc, c);
+            const DescRegs g = load_desc(descs + s);
+            const uint32_t refs = leaf_cnt[c];
+            const LeafGeom lg = leaf_geom(g, refs, sc[s].leaf);
+            uint32_t y = (lg.res[0] & 0xFFu) | ((lg.res[1] & 0xFFu) << 8) | ((lg.res[2] & 0xFFu) << 16);
+            if (lg.leaf) y |= kLeafMask;
+            if (refs != 0) y |= kNotEmptyMask;
+            top_cells[c].y = y;
+            leaf_cnt[c] = lg.res[0] * lg.res[1] * lg.res[2];
+            full = refs != 0;
+        }
+        const uint32_t word = __ballot_sync(0xffffffffu, full);
+        if (lane == 0) occ[c0 >> 5] = word;
     }
 }
 
@@ -344,6 +354,7 @@ int batch_alloc(hr_batch* b) {
     int rc;
     if ((rc = ensure(c, B.cells, sizeof(uint2) * B.cap_cells))) return rc;
     if ((rc = ensure(c, B.leaf_cnt, sizeof(uint32_t) * B.cap_cells))) return rc;
+    if ((rc = ensure(c, B.occ, sizeof(uint32_t) * (B.cap_cells / 32 + 1)))) return rc;
     if ((rc = ensure(c, B.scan_partials, sizeof(uint32_t) * (scan_partials_words(B.cap_cells) + 2)))) return rc;
     if ((rc = ensure(c, B.keys_a, sizeof(uint32_t) * cap_pairs))) return rc;
     if ((rc = ensure(c, B.vals_a, sizeof(uint32_t) * cap_pairs))) return rc;
@@ -391,7 +402,8 @@ int enqueue_build(hr_batch* b) {
     kb_write_pairs<<<b->ntchunk, kBT, 0, s>>>(tris, tch, sc, descs, cell_off, bd, bsum, B.tri_ranges.as<uint4>(),
                                               B.keys_a.as<uint32_t>(), B.vals_a.as<uint32_t>(), B.leaf_cnt.as<uint32_t>());
     const int gcells = std::max(1, std::min((int)((B.cap_cells + 255) / 256), c->num_sms * 16));
-    kb_tl_cells<<<gcells, 256, 0, s>>>(sc, descs, cell_off, b->nsc, bd, B.leaf_cnt.as<uint32_t>(), B.cells.as<uint2>());
+    kb_tl_cells<<<gcells, 256, 0, s>>>(sc, descs, cell_off, b->nsc, bd, B.leaf_cnt.as<uint32_t>(), B.cells.as<uint2>(),
+                                       B.occ.as<uint32_t>());
     if ((rc = exclusive_scan_u32(c, B.leaf_cnt.as<uint32_t>(), &bd->ncells, B.cap_cells, &bd->nleaves,
                                  B.scan_partials.as<uint32_t>(), s)))
         return rc;
@@ -443,6 +455,7 @@ int upload_jobs(hr_batch* b, int32_t image_id) {
         J.prims = c->g.prims.as<uint32_t>();
         J.desc = dev<GridDesc>(b->d_descs) + i;
         J.cells_offset = dev<uint32_t>(b->d_cell_off) + i;
+        J.occ = c->g.occ.as<uint32_t>();
         J.status = dev<GridDesc>(b->d_bdesc);   // overflow and error bits of the whole batch build
         J.fb = dev<float>(b->d_fb) + 3 * b->px_off[i];
         const Camera& k = b->cams[i];

@@ -190,18 +190,29 @@ __global__ __launch_bounds__(kBT) void k_write_pairs(const float4* __restrict__ 
 // TLGridBuildKernels.h:45-122); packed y of TwoLevelGridCell (TwoLevelGrid.h:38-161)
 // leaf_cnt holds each top cell's reference count on entry (k_write_pairs) and its leaf
 // count on return.
+// occ gets one bit per top cell (set: the cell has references), a word per warp pass.
+// Launched with a block size that is a multiple of 32.
 __global__ void k_tl_cells(const GridDesc* d, float leaf_density, uint32_t* __restrict__ leaf_cnt,
-                           uint2* __restrict__ top_cells) {
+                           uint2* __restrict__ top_cells, uint32_t* __restrict__ occ) {
     if (d->overflow | d->error) return;
     const DescRegs g = load_desc(d);
-    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < g.ncells; c += gridDim.x * blockDim.x) {
-        const uint32_t refs = leaf_cnt[c];
-        const LeafGeom lg = leaf_geom(g, refs, leaf_density);
-        uint32_t y = (lg.res[0] & 0xFFu) | ((lg.res[1] & 0xFFu) << 8) | ((lg.res[2] & 0xFFu) << 16);
-        if (lg.leaf) y |= kLeafMask;
-        if (refs != 0) y |= kNotEmptyMask;
-        top_cells[c].y = y;
-        leaf_cnt[c] = lg.res[0] * lg.res[1] * lg.res[2];
+    const uint32_t lane = threadIdx.x & 31u;
+    // warp-uniform trip count: the 32 cells of a pass share one occupancy word
+    for (uint32_t c0 = blockIdx.x * blockDim.x + threadIdx.x - lane; c0 < g.ncells; c0 += gridDim.x * blockDim.x) {
+        const uint32_t c = c0 + lane;
+        bool full = false;
+        if (c < g.ncells) {
+            const uint32_t refs = leaf_cnt[c];
+            const LeafGeom lg = leaf_geom(g, refs, leaf_density);
+            uint32_t y = (lg.res[0] & 0xFFu) | ((lg.res[1] & 0xFFu) << 8) | ((lg.res[2] & 0xFFu) << 16);
+            if (lg.leaf) y |= kLeafMask;
+            if (refs != 0) y |= kNotEmptyMask;
+            top_cells[c].y = y;
+            leaf_cnt[c] = lg.res[0] * lg.res[1] * lg.res[2];
+            full = refs != 0;
+        }
+        const uint32_t word = __ballot_sync(0xffffffffu, full);
+        if (lane == 0) occ[c0 >> 5] = word;
     }
 }
 
@@ -297,7 +308,7 @@ static std::vector<uint8_t> build_graph_key(const hr_ctx* c, int32_t kind, int32
     const GridBuffers& B = c->g;
     const DevBuf* bufs[] = {&B.desc, &c->tris, &B.cells, &B.keys_a, &B.tri_ranges, &B.vals_a, &B.keys_b, &B.vals_b,
                             &B.block_sums, &B.tile_hist, &B.row_total, &B.prims,
-                            &B.ref_ranges, &B.leaf_cnt, &B.scan_partials, &B.leaves, &B.lkeys_a, &B.lvals_a,
+                            &B.ref_ranges, &B.leaf_cnt, &B.occ, &B.scan_partials, &B.leaves, &B.lkeys_a, &B.lvals_a,
                             &B.lkeys_b, &B.lvals_b, &c->verts, &c->idx, &c->counters, &c->keyframes, &c->frame_sel};
     std::vector<uint8_t> k;
     auto put = [&](const void* p, size_t n) {
@@ -369,6 +380,7 @@ static int build_once_impl(hr_ctx* c, int32_t kind, int32_t exact, uint32_t* ovf
     } else {
         if ((rc = ensure(c, B.ref_ranges, sizeof(uint4) * cap_pairs))) return rc;
         if ((rc = ensure(c, B.leaf_cnt, sizeof(uint32_t) * B.cap_cells))) return rc;
+        if ((rc = ensure(c, B.occ, sizeof(uint32_t) * (B.cap_cells / 32 + 1)))) return rc;
         if ((rc = ensure(c, B.scan_partials, sizeof(uint32_t) * (scan_partials_words(B.cap_cells) + 2)))) return rc;
         if ((rc = ensure(c, B.leaves, sizeof(uint2) * B.cap_leaves))) return rc;
         if ((rc = ensure(c, B.lkeys_a, sizeof(uint32_t) * B.cap_leaf_pairs))) return rc;
@@ -437,7 +449,8 @@ static int build_once_impl(hr_ctx* c, int32_t kind, int32_t exact, uint32_t* ovf
             // level needs only each top cell's reference count (counted as they were written),
             // and the one stable sort by global leaf index then orders every leaf's list by
             // triangle exactly as the two sorts would.
-            k_tl_cells<<<gcells, 256, 0, s>>>(d, c->leaf_density, B.leaf_cnt.as<uint32_t>(), B.cells.as<uint2>());
+            k_tl_cells<<<gcells, 256, 0, s>>>(d, c->leaf_density, B.leaf_cnt.as<uint32_t>(), B.cells.as<uint2>(),
+                                              B.occ.as<uint32_t>());
             uint32_t* sp = B.scan_partials.as<uint32_t>();
             if ((rc = exclusive_scan_u32(c, B.leaf_cnt.as<uint32_t>(), &d->ncells, B.cap_cells, &d->nleaves, sp, s)))
                 return rc;

@@ -257,7 +257,7 @@ void hr_destroy(hr_ctx* c) {
     DevBuf* bufs[] = {&c->verts, &c->idx, &c->tris, &c->keyframes, &c->frame_sel, &c->staging, &c->counters, &c->fb, &c->out_id,
                       &c->out_t, &c->out_u, &c->out_v, &c->ray_in, &c->g.desc, &c->g.cells, &c->g.leaves,
                       &c->g.prims, &c->g.keys_a, &c->g.vals_a, &c->g.keys_b, &c->g.vals_b, &c->g.block_sums,
-                      &c->g.tile_hist, &c->g.row_total, &c->g.leaf_cnt,
+                      &c->g.tile_hist, &c->g.row_total, &c->g.leaf_cnt, &c->g.occ,
                       &c->g.lkeys_a, &c->g.lvals_a, &c->g.lkeys_b, &c->g.lvals_b, &c->g.scan_partials,
                       &c->g.tri_ranges, &c->g.ref_ranges, &c->lights_dev, &c->tri_nrm, &c->tri_alb,
                       &c->hit_t, &c->hit_tri, &c->unocc, &c->queue};

@@ -49,6 +49,7 @@ struct GridBuffers {
     DevBuf tile_hist;     // radix tile histograms
     DevBuf row_total;     // radix digit totals
     DevBuf leaf_cnt;      // two-level: references, then leaf cells per top cell, scanned in place to the first leaf
+    DevBuf occ;           // two-level: one bit per top cell, set when the cell holds references
     DevBuf lkeys_a, lvals_a, lkeys_b, lvals_b;   // two-level: leaf pair ping-pong
     DevBuf scan_partials; // generic scan partial sums
     DevBuf tri_ranges;    // uint4 per triangle: its cell range (16-bit coordinates) and pair count
@@ -193,6 +194,7 @@ struct Job {
     const uint32_t* prims;
     const GridDesc* desc;
     const uint32_t* cells_offset;    // nullable: added to cells (grids of one batch share arrays)
+    const uint32_t* occ;             // nullable: top-cell occupancy bits, indexed like cells before the offset
     const GridDesc* status;          // nullable (then desc): a grid whose build overflowed or failed is not traced
     float* fb;                       // render jobs: float RGB per pixel
     const float* org;                // ray jobs: 3 floats per ray

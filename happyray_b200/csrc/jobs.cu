@@ -61,7 +61,10 @@ struct TileCtx {
 
 __device__ __forceinline__ void load_tile_ctx(TileCtx& T, const Job* __restrict__ J) {
     T.s.tris = J->tris;
-    T.s.cells = J->cells + (J->cells_offset ? __ldg(J->cells_offset) : 0u);
+    const uint32_t coff = J->cells_offset ? __ldg(J->cells_offset) : 0u;
+    T.s.cells = J->cells + coff;
+    T.s.occ = J->occ;
+    T.s.occ_bit0 = coff;
     T.s.leaves = J->leaves;
     T.s.prims = J->prims;
     T.s.desc = J->desc;

@@ -53,7 +53,7 @@ size_t ctx_bytes(const hr_ctx* c) {
     const DevBuf* b[] = {&c->verts, &c->idx, &c->tris, &c->keyframes, &c->staging, &c->counters, &c->fb,
                          &c->out_id, &c->out_t, &c->out_u, &c->out_v, &c->ray_in, &c->g.desc, &c->g.cells,
                          &c->g.leaves, &c->g.prims, &c->g.keys_a, &c->g.vals_a, &c->g.keys_b, &c->g.vals_b,
-                         &c->g.block_sums, &c->g.tile_hist, &c->g.row_total, &c->g.leaf_cnt, &c->g.lkeys_a, &c->g.lvals_a, &c->g.lkeys_b, &c->g.lvals_b,
+                         &c->g.block_sums, &c->g.tile_hist, &c->g.row_total, &c->g.leaf_cnt, &c->g.occ, &c->g.lkeys_a, &c->g.lvals_a, &c->g.lkeys_b, &c->g.lvals_b,
                          &c->g.scan_partials, &c->g.tri_ranges, &c->g.ref_ranges, &c->hit_t, &c->hit_tri,
                          &c->unocc, &c->queue};
     size_t s = 0;
@@ -184,6 +184,7 @@ void fill_render_job(Job& J, const SrvScene& X, const SrvReq& R) {
     const hr_ctx* c = X.ctx;
     J.tris = c->tris.as<float4>();
     J.cells = c->g.cells.as<uint2>();
+    J.occ = c->g.occ.as<uint32_t>();
     J.leaves = c->g.leaves.as<uint2>();
     J.prims = c->g.prims.as<uint32_t>();
     J.desc = c->g.desc.as<GridDesc>();

@@ -507,6 +507,8 @@ Scene make_scene(hr_ctx* c) {
     // shading normals and materials given for the current mesh
     s.nrm3 = c->nrm_ntri && c->nrm_ntri == c->ntri ? c->tri_nrm.as<float4>() : nullptr;
     s.alb = c->alb_ntri && c->alb_ntri == c->ntri ? c->tri_alb.as<float>() : nullptr;
+    s.occ = c->built_kind == kTwoLevel ? c->g.occ.as<uint32_t>() : nullptr;
+    s.occ_bit0 = 0;
     return s;
 }
 

@@ -32,6 +32,11 @@ struct Scene {
     int32_t kind;
     const float4* __restrict__ nrm3 = nullptr;   // path tracer: 3 vertex normals per triangle, or none
     const float* __restrict__ alb = nullptr;     // path tracer: diffuse albedo per triangle, or none
+    // two-level: one bit per top cell, set for a cell with references (bit occ_bit0 + c for
+    // cell c), or none; 64 times smaller than the cell records, so an empty cell costs a
+    // cached bit instead of a cell-record load
+    const uint32_t* __restrict__ occ = nullptr;
+    uint32_t occ_bit0 = 0;
 };
 
 struct G {
@@ -307,16 +312,26 @@ __device__ __forceinline__ bool tl_outer_step(TL& q, const G& g, const Hit& h) {
 }
 
 // From the current top cell, walk to the first non-empty one and enter it; false if the
-// ray leaves the grid (or is done) first.
-template <bool STATS>
+// ray leaves the grid (or is done) first.  OCC: test each cell's occupancy bit first and
+// load the cell record only for a cell with references (long incoherent rays, which cross
+// mostly empty cells whose records would miss in L1: the path tracer).
+template <bool STATS, bool OCC = false>
 __device__ __forceinline__ bool tl_seek(TL& q, const Scene& s, const G& g, f3 o, f3 d, Hit& h) {
     const uint32_t rx = (uint32_t)g.res[0], rxy = (uint32_t)g.res[0] * (uint32_t)g.res[1];
     while (true) {
-        const uint2 tc = __ldg(s.cells + ((uint32_t)q.cell[0] + (uint32_t)q.cell[1] * rx + (uint32_t)q.cell[2] * rxy));
+        const uint32_t c = (uint32_t)q.cell[0] + (uint32_t)q.cell[1] * rx + (uint32_t)q.cell[2] * rxy;
         if (STATS) h.cells++;
-        if (tc.y & kNotEmptyMask) {
-            tl_enter(q, g, o, d, tc);
-            return true;
+        bool full = true;
+        if (OCC && s.occ) {
+            const uint32_t bit = s.occ_bit0 + c;
+            full = ((__ldg(s.occ + (bit >> 5)) >> (bit & 31u)) & 1u) != 0u;
+        }
+        if (full) {
+            const uint2 tc = __ldg(s.cells + c);
+            if (tc.y & kNotEmptyMask) {
+                tl_enter(q, g, o, d, tc);
+                return true;
+            }
         }
         if (!tl_outer_step(q, g, h)) return false;
     }
@@ -329,20 +344,20 @@ __device__ __forceinline__ uint32_t tl_leaf(const TL& q) {
 
 // Inner step (TLGridTraverser.h:225-290): stop when the hit lies before the leaf's exit,
 // else step; leaving the sub-grid continues in the top grid.  False when the ray is done.
-template <bool STATS>
+template <bool STATS, bool OCC = false>
 __device__ __forceinline__ bool tl_advance(TL& q, const Scene& s, const G& g, f3 o, f3 d, Hit& h) {
     const int32_t lres[3] = {(int32_t)q.lres[0], (int32_t)q.lres[1], (int32_t)q.lres[2]};
     float tk;
     const bool inside = dda_step(q.tm2, q.c2, q.rcp, q.scs, lres, &tk);
     if (h.t < tk) return false;
     if (inside) return true;
-    return tl_outer_step(q, g, h) && tl_seek<STATS>(q, s, g, o, d, h);
+    return tl_outer_step(q, g, h) && tl_seek<STATS, OCC>(q, s, g, o, d, h);
 }
 
 // Entry of a ray into the two-level grid (TLGridTraverser.h:79-143): clip to the grid
 // box, the top cell at the entry point, then the first non-empty top cell entered; false
 // if the ray misses the grid or leaves it (or is done) before a non-empty cell.  Per lane.
-template <bool STATS>
+template <bool STATS, bool OCC = false>
 __device__ __forceinline__ bool tl_setup(TL& q, const Scene& s, const G& g, f3 o, f3 d, Hit& h) {
     q.rcp[0] = 1.0f / d.x; q.rcp[1] = 1.0f / d.y; q.rcp[2] = 1.0f / d.z;
     float t0, t1;
@@ -360,14 +375,14 @@ __device__ __forceinline__ bool tl_setup(TL& q, const Scene& s, const G& g, f3 o
     if (!(q.cell[0] < g.res[0] && q.cell[0] > -1 && q.cell[1] < g.res[1] && q.cell[1] > -1 &&
           q.cell[2] < g.res[2] && q.cell[2] > -1))
         return false;
-    return tl_seek<STATS>(q, s, g, o, d, h);
+    return tl_seek<STATS, OCC>(q, s, g, o, d, h);
 }
 
 // a15: two-level DDA, warp-synchronous
-template <int HM, bool STATS>
+template <int HM, bool STATS, bool OCC = false>
 __device__ void trace_tl(const Scene& s, const G& g, f3 o, f3 d, bool any, Hit& h, bool active) {
     TL q;
-    if (active) active = tl_setup<STATS>(q, s, g, o, d, h);
+    if (active) active = tl_setup<STATS, OCC>(q, s, g, o, d, h);
     while (__any_sync(kFullMask, active)) {
         uint32_t b = 0, e = 0;
         if (active) {
@@ -376,7 +391,7 @@ __device__ void trace_tl(const Scene& s, const G& g, f3 o, f3 d, bool any, Hit& 
             if (STATS) h.cells++;
         }
         const bool done = test_lists<HM, STATS>(s, o, d, b, e, any, h);
-        if (active) active = !done && tl_advance<STATS>(q, s, g, o, d, h);
+        if (active) active = !done && tl_advance<STATS, OCC>(q, s, g, o, d, h);
     }
 }
 
@@ -400,7 +415,7 @@ __device__ __forceinline__ void trace_mixed(const Scene& s, const G& g, f3 o, f3
     h.t = tmax; h.u = 0.0f; h.v = 0.0f; h.tri = 0; h.hit = false; h.cells = 0; h.tests = 0;
     if (s.ntri == 0) return;
     if (KIND == kUniform) trace_ug<kHitMixed, STATS>(s, g, o, d, any, h, active);
-    else trace_tl<kHitMixed, STATS>(s, g, o, d, any, h, active);
+    else trace_tl<kHitMixed, STATS, true>(s, g, o, d, any, h, active);   // path rays: occupancy bits
 }
 
 struct Cam {
