@@ -395,6 +395,98 @@ __device__ void trace_tl(const Scene& s, const G& g, f3 o, f3 d, bool any, Hit& 
     }
 }
 
+// Paced two-level traversal, for path and shadow rays.  A lane walking empty top cells
+// takes at most K of them per warp step (and per call below), so one long walk does not
+// hold back the other lanes' leaf steps and list tests; each lane's own sequence of cells
+// and tests is unchanged, so the results are those of the unbounded walk.  Lane state: 0
+// done, 1 in a leaf, 2 walking empty top cells.  (Camera, AO and query rays keep the
+// unbounded walk of trace_tl: paced, they measured slower.)
+#ifndef HR_PT_SEEK_STEPS
+#define HR_PT_SEEK_STEPS 1   // path and shadow rays: empty top cells per warp step (0: unbounded)
+#endif
+
+// tl_seek with at most K steps over empty top cells: 1 entered a non-empty cell, 0 done
+// (left the grid, or the hit lies before the next cell), 2 stopped at a top cell not yet
+// looked at (the next call starts there).
+template <bool STATS, bool OCC, int K>
+__device__ __forceinline__ int tl_seek_n(TL& q, const Scene& s, const G& g, f3 o, f3 d, Hit& h) {
+    const uint32_t rx = (uint32_t)g.res[0], rxy = (uint32_t)g.res[0] * (uint32_t)g.res[1];
+    for (int i = 0;; ++i) {
+        const uint32_t c = (uint32_t)q.cell[0] + (uint32_t)q.cell[1] * rx + (uint32_t)q.cell[2] * rxy;
+        if (STATS) h.cells++;
+        bool full = true;
+        if (OCC && s.occ) {
+            const uint32_t bit = s.occ_bit0 + c;
+            full = ((__ldg(s.occ + (bit >> 5)) >> (bit & 31u)) & 1u) != 0u;
+        }
+        if (full) {
+            const uint2 tc = __ldg(s.cells + c);
+            if (tc.y & kNotEmptyMask) {
+                tl_enter(q, g, o, d, tc);
+                return 1;
+            }
+        }
+        if (!tl_outer_step(q, g, h)) return 0;
+        if (i + 1 >= K) return 2;
+    }
+}
+
+// tl_setup, paced: the lane state after entering the grid
+template <bool STATS, bool OCC, int K>
+__device__ __forceinline__ int tl_setup_n(TL& q, const Scene& s, const G& g, f3 o, f3 d, Hit& h) {
+    q.rcp[0] = 1.0f / d.x; q.rcp[1] = 1.0f / d.y; q.rcp[2] = 1.0f / d.z;
+    float t0, t1;
+    if (!clip(g, o, q.rcp, &t0, &t1)) return 0;
+    q.tentry = hmax(0.0f, t0);
+    const f3 ep = mk(o.x + q.tentry * d.x, o.y + q.tentry * d.y, o.z + q.tentry * d.z);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        float cf = floorf((comp(ep, k) - g.bmin[k]) * g.rcp[k]);
+        cf = hmin((float)g.res[k] - 1.0f, hmax(cf, 0.0f));
+        const float stp = q.rcp[k] > 0.0f ? 1.0f : 0.0f;
+        q.tmax[k] = ((cf + stp) * g.cs[k] + g.bmin[k] - comp(o, k)) * q.rcp[k];
+        q.cell[k] = f2i(cf);
+    }
+    if (!(q.cell[0] < g.res[0] && q.cell[0] > -1 && q.cell[1] < g.res[1] && q.cell[1] > -1 &&
+          q.cell[2] < g.res[2] && q.cell[2] > -1))
+        return 0;
+    return tl_seek_n<STATS, OCC, K>(q, s, g, o, d, h);
+}
+
+// The lane state after a warp step: a lane in a leaf (st 1) whose list test ended the ray
+// (done) stops, else steps to the next leaf (tl_advance); a walking lane (st 2) walks on.
+template <bool STATS, bool OCC, int K>
+__device__ __forceinline__ int tl_next(TL& q, const Scene& s, const G& g, f3 o, f3 d, Hit& h, int st, bool done) {
+    if (st == 1) {
+        if (done) return 0;
+        const int32_t lres[3] = {(int32_t)q.lres[0], (int32_t)q.lres[1], (int32_t)q.lres[2]};
+        float tk;
+        const bool inside = dda_step(q.tm2, q.c2, q.rcp, q.scs, lres, &tk);
+        if (h.t < tk) return 0;
+        if (inside) return 1;
+        return tl_outer_step(q, g, h) ? tl_seek_n<STATS, OCC, K>(q, s, g, o, d, h) : 0;
+    }
+    if (st == 2) return tl_seek_n<STATS, OCC, K>(q, s, g, o, d, h);
+    return 0;
+}
+
+// a15, paced (trace_tl's results)
+template <int HM, bool STATS, bool OCC, int K>
+__device__ void trace_tl_paced(const Scene& s, const G& g, f3 o, f3 d, bool any, Hit& h, bool active) {
+    TL q;
+    int st = active ? tl_setup_n<STATS, OCC, K>(q, s, g, o, d, h) : 0;
+    while (__any_sync(kFullMask, st != 0)) {
+        uint32_t b = 0, e = 0;
+        if (st == 1) {
+            const uint2 lr = __ldg(s.leaves + tl_leaf(q));
+            b = lr.x; e = lr.y;
+            if (STATS) h.cells++;
+        }
+        const bool done = test_lists<HM, STATS>(s, o, d, b, e, any, h);
+        st = tl_next<STATS, OCC, K>(q, s, g, o, d, h, st, done);
+    }
+}
+
 // Closest hit (ANY = false) or any hit within (1e-4, tmax) on a grid of kind KIND
 // (kUniform or kTwoLevel).  The kind is a template argument so that a kernel holds the
 // registers of one traversal only.  Warp-synchronous.
@@ -415,7 +507,9 @@ __device__ __forceinline__ void trace_mixed(const Scene& s, const G& g, f3 o, f3
     h.t = tmax; h.u = 0.0f; h.v = 0.0f; h.tri = 0; h.hit = false; h.cells = 0; h.tests = 0;
     if (s.ntri == 0) return;
     if (KIND == kUniform) trace_ug<kHitMixed, STATS>(s, g, o, d, any, h, active);
-    else trace_tl<kHitMixed, STATS, true>(s, g, o, d, any, h, active);   // path rays: occupancy bits
+    // path rays: occupancy bits
+    else if constexpr (HR_PT_SEEK_STEPS > 0) trace_tl_paced<kHitMixed, STATS, true, HR_PT_SEEK_STEPS>(s, g, o, d, any, h, active);
+    else trace_tl<kHitMixed, STATS, true>(s, g, o, d, any, h, active);
 }
 
 struct Cam {
