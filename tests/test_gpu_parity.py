@@ -416,6 +416,38 @@ def test_edge_cases(engine, oracle):
     assert hid[0] == -1
 
 
+@pytest.mark.parametrize("kind", [GRID_UNIFORM, GRID_TWO_LEVEL])
+def test_axis_parallel_and_cell_boundary_rays(engine, oracle, small_clusters, kind):
+    """Rays with zero direction components (infinite reciprocals), origins exactly on cell
+    planes, origins outside the grid and rays grazing the grid box: ids, t, u, v equal to
+    the oracle's, bit for bit."""
+    v, f = small_clusters
+    gpu_build(engine, v, f, kind)
+    b = oracle_build(oracle, v, f, kind)
+    gi = engine.grid_info()
+    lo, hi, cs = (np.asarray(gi[k], np.float32) for k in ("bounds_min", "bounds_max", "cell_size"))
+    rng = np.random.default_rng(11)
+    dirs = [(1, 0, 0), (-1, 0, 0), (0, 1, 0), (0, -1, 0), (0, 0, 1), (0, 0, -1),
+            (1, 1, 0), (0, -1, 1), (1, 0, -1), (1, 1, 1), (-1, 1, -1)]
+    org, d = [], []
+    for dv in dirs:
+        dv = np.asarray(dv, np.float32) / np.float32(np.linalg.norm(dv))
+        n = 400
+        cells = rng.integers(0, np.asarray(gi["res"]), (n, 3))
+        o = lo + cells.astype(np.float32) * cs                                 # cell corners
+        o[: n // 2] += rng.uniform(0, 1, (n // 2, 3)).astype(np.float32) * cs  # ... and interiors
+        o[n // 4: n // 2, 0] = lo[0] - 0.25                                    # outside the box
+        o[-20:] = np.where(dv > 0, lo, np.where(dv < 0, hi, o[-20:]))          # on the box faces
+        org.append(o.astype(np.float32))
+        d.append(np.repeat(dv[None], n, 0))
+    org, d = np.concatenate(org), np.concatenate(d)
+    hid, t, u, vv = engine.trace_rays(org, d)
+    ohid, ot, ou, ov = oracle.trace(b, org, d)
+    assert np.array_equal(hid, ohid) and np.array_equal(t, ot)
+    assert np.array_equal(u, ou) and np.array_equal(vv, ov)
+    assert (hid >= 0).sum() > 100
+
+
 def test_empty_mesh(engine):
     from happyray_b200 import HRError
     v = np.zeros((3, 3), np.float32)
