@@ -1090,6 +1090,7 @@ def main():
         hv = torch.from_numpy(np.ascontiguousarray(frames[0])).pin_memory().numpy()
         hf = torch.from_numpy(f.view(np.int32)).pin_memory().numpy().view(np.uint32)
         hfb = torch.zeros((npx, 3), dtype=torch.float32).pin_memory().numpy()
+        # one frame at a time: upload, build, render into the host frame buffer, wait
         e_ms = []
         for i in range(args.warmup + args.steps):
             with torch.cuda.stream(stream):
@@ -1103,10 +1104,48 @@ def main():
             b.synchronize()
             if i >= args.warmup:
                 e_ms.append(a.elapsed_time(b))
-        et = max_over_ranks(sum(e_ms), ws)
+        et_serial = max_over_ranks(sum(e_ms), ws)
+        # two frames in flight: frame i on context i % 2 (own stream, own device and pinned
+        # frame buffers), so one frame's readback and the next one's upload overlap the other
+        # context's build and render; every frame still uploads its inputs and reads back
+        # its image, inside one timed region around all frames
+        stream2 = torch.cuda.Stream(device=dev)
+        eng2 = Engine(dev, stream=stream2.cuda_stream)
+        configure(eng2, W, frames)
+        engs, strs = [eng, eng2], [stream, stream2]
+        d_fbs = [d_fb, torch.zeros_like(d_fb)]
+        h_fbs = [torch.zeros(npx * 3, dtype=torch.float32).pin_memory() for _ in range(2)]
+
+        def frame(i):
+            k = i % 2
+            with torch.cuda.stream(strs[k]):
+                flush.zero_()
+            engs[k].upload(hv, hv, hf, 1.0)
+            engs[k].build(W["kind"], W.get("exact", True))
+            engs[k].render_device(d_fbs[k], 0, W["mode"])
+            with torch.cuda.stream(strs[k]):
+                h_fbs[k].copy_(d_fbs[k], non_blocking=True)
+
+        for i in range(args.warmup):
+            frame(i)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        stream2.wait_event(a)
+        for i in range(args.steps):
+            frame(args.warmup + i)
+        stream.wait_stream(stream2)
+        b.record(stream)
+        b.synchronize()
+        et = max_over_ranks(a.elapsed_time(b), ws)
+        eng2.cleanup()
         e2e = {"value": replica_value(rays_per_step, args.steps, et, ws), "unit": "Mrays/s",
                "h2d_bytes_per_step": int(2 * hv.nbytes + hf.nbytes), "d2h_bytes_per_step": int(hfb.nbytes),
-               "ms_per_step": et / args.steps}
+               "ms_per_step": et / args.steps,
+               "how": "public C-ABI (hr_upload, hr_build, hr_render_device, then a pinned readback), two frames in "
+                      "flight on two contexts; L2 flushed before every frame inside the timed region",
+               "one_frame_at_a_time": {"value": replica_value(rays_per_step, args.steps, et_serial, ws),
+                                       "ms_per_step": et_serial / args.steps}}
     # the headline line also carries the 2M-triangle key-frame rebuild (replayed build graph)
     rebuild2m = None
     if prep2m is not None:
