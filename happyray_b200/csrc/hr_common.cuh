@@ -159,6 +159,35 @@ __device__ __forceinline__ void pcg_seed(Pcg32& r, uint64_t initstate, uint64_t 
 }
 __device__ __forceinline__ float pcg_float(Pcg32& r) { return (float)(pcg_next(r) >> 8) * (1.0f / 16777216.0f); }
 
+// Advancing a PCG32 state n steps: the LCG's closed form state * a^n + inc * (1 + a + ... +
+// a^(n-1)) (mod 2^64), so a pixel's AO sample k reaches its draws 2k and 2k + 1 in one
+// multiply-add instead of 2k steps (the same state as stepping: integer arithmetic).
+__host__ __device__ constexpr uint64_t pcg_pow(uint32_t n) {
+    uint64_t a = 1u;
+    for (uint32_t i = 0; i < n; ++i) a *= 6364136223846793005ULL;
+    return a;
+}
+__host__ __device__ constexpr uint64_t pcg_geo(uint32_t n) {
+    uint64_t g = 0u, a = 1u;
+    for (uint32_t i = 0; i < n; ++i) { g += a; a *= 6364136223846793005ULL; }
+    return g;
+}
+constexpr int kPcgJumps = 16;   // even step counts 0, 2, ..., 30 (AO samples 0..15)
+__constant__ const uint64_t kPcgJumpA[kPcgJumps] = {
+    pcg_pow(0), pcg_pow(2), pcg_pow(4), pcg_pow(6), pcg_pow(8), pcg_pow(10), pcg_pow(12), pcg_pow(14),
+    pcg_pow(16), pcg_pow(18), pcg_pow(20), pcg_pow(22), pcg_pow(24), pcg_pow(26), pcg_pow(28), pcg_pow(30)};
+__constant__ const uint64_t kPcgJumpG[kPcgJumps] = {
+    pcg_geo(0), pcg_geo(2), pcg_geo(4), pcg_geo(6), pcg_geo(8), pcg_geo(10), pcg_geo(12), pcg_geo(14),
+    pcg_geo(16), pcg_geo(18), pcg_geo(20), pcg_geo(22), pcg_geo(24), pcg_geo(26), pcg_geo(28), pcg_geo(30)};
+// skip the 2k draws of AO samples 0..k-1
+__device__ __forceinline__ void pcg_skip_pairs(Pcg32& r, uint32_t k) {
+    if (k < (uint32_t)kPcgJumps) {
+        r.state = r.state * kPcgJumpA[k] + r.inc * kPcgJumpG[k];
+    } else {
+        for (uint32_t j = 0; j < 2u * k; ++j) pcg_next(r);
+    }
+}
+
 // sin/cos of 2*pi*u, u in [0,1): exact quadrant reduction + Maclaurin series of sin (to
 // x^13) and cos (to x^14) on [0, pi/2) in Horner form; truncation error < 7e-10.
 __device__ __forceinline__ void sincos2pi(float u, float* s, float* c) {

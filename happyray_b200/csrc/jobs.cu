@@ -268,7 +268,7 @@ __global__ __launch_bounds__(kJobTT, PT ? HR_JOB_PT_MIN_BLOCKS : HR_JOB_MIN_BLOC
                 const uint32_t src = nth_set_bit(m, q);
                 Pcg32 rng;
                 pcg_seed(rng, ((uint64_t)(uint32_t)T.image_id << 32) | T.pix[src], T.seed);
-                for (uint32_t i = 0; i < 2u * k; ++i) pcg_next(rng);
+                pcg_skip_pairs(rng, k);
                 const float u1 = pcg_float(rng), u2 = pcg_float(rng);
                 w = cosine_dir(mk(T.nx[src], T.ny[src], T.nz[src]), u1, u2);
                 const float off = T.off;

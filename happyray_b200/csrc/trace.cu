@@ -241,7 +241,7 @@ __global__ __launch_bounds__(kTT, HR_TRACE_MIN_BLOCKS) void k_ao_samples(Scene s
             const f3 nrm = face_normal(s, hit_tri[pix], d);
             Pcg32 rng;
             pcg_seed(rng, ((uint64_t)(uint32_t)image_id << 32) | pix, seed);
-            for (uint32_t j = 0; j < 2u * k; ++j) pcg_next(rng);
+            pcg_skip_pairs(rng, k);
             const float u1 = pcg_float(rng), u2 = pcg_float(rng);
             w = cosine_dir(nrm, u1, u2);
             ao = mk(p.x + off * w.x, p.y + off * w.y, p.z + off * w.z);
@@ -390,7 +390,7 @@ __global__ __launch_bounds__(kTT, HR_TRACE_MIN_BLOCKS) void k_ao_samples_tl(Scen
                 const f3 nrm = face_normal(s, hit_tri[pix], d);
                 Pcg32 rng;
                 pcg_seed(rng, ((uint64_t)(uint32_t)image_id << 32) | pix, seed);
-                for (uint32_t j = 0; j < 2u * k; ++j) pcg_next(rng);
+                pcg_skip_pairs(rng, k);
                 const float u1 = pcg_float(rng), u2 = pcg_float(rng);
                 w = cosine_dir(nrm, u1, u2);
                 o = mk(p.x + off * w.x, p.y + off * w.y, p.z + off * w.z);
