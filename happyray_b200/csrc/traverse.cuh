@@ -404,6 +404,9 @@ __device__ void trace_tl(const Scene& s, const G& g, f3 o, f3 d, bool any, Hit& 
 #ifndef HR_PT_SEEK_STEPS
 #define HR_PT_SEEK_STEPS 1   // path and shadow rays: empty top cells per warp step (0: unbounded)
 #endif
+#ifndef HR_PT_LEAF_STEPS
+#define HR_PT_LEAF_STEPS 4   // path and shadow rays: leaves stepped per warp step while they are empty
+#endif
 
 // tl_seek with at most K steps over empty top cells: 1 entered a non-empty cell, 0 done
 // (left the grid, or the hit lies before the next cell), 2 stopped at a top cell not yet
@@ -460,11 +463,17 @@ __device__ __forceinline__ int tl_next(TL& q, const Scene& s, const G& g, f3 o, 
     if (st == 1) {
         if (done) return 0;
         const int32_t lres[3] = {(int32_t)q.lres[0], (int32_t)q.lres[1], (int32_t)q.lres[2]};
-        float tk;
-        const bool inside = dda_step(q.tm2, q.c2, q.rcp, q.scs, lres, &tk);
-        if (h.t < tk) return 0;
-        if (inside) return 1;
-        return tl_outer_step(q, g, h) ? tl_seek_n<STATS, OCC, K>(q, s, g, o, d, h) : 0;
+        for (int j = 1;; ++j) {
+            float tk;
+            const bool inside = dda_step(q.tm2, q.c2, q.rcp, q.scs, lres, &tk);
+            if (h.t < tk) return 0;
+            if (!inside) return tl_outer_step(q, g, h) ? tl_seek_n<STATS, OCC, K>(q, s, g, o, d, h) : 0;
+            if (j >= HR_PT_LEAF_STEPS) return 1;
+            // an empty leaf has no list to test: step over it within this warp step
+            const uint2 lr = __ldg(s.leaves + tl_leaf(q));
+            if (lr.y > lr.x) return 1;
+            if (STATS) h.cells++;
+        }
     }
     if (st == 2) return tl_seek_n<STATS, OCC, K>(q, s, g, o, d, h);
     return 0;
