@@ -28,6 +28,9 @@
 #ifndef HR_AO_PRIMARY_REFILL_MIN
 #define HR_AO_PRIMARY_REFILL_MIN 32   // idle lanes that make k_ao_primary_tl refill (> 32: k_ao_primary)
 #endif
+#ifndef HR_AO_LEAF_STEPS
+#define HR_AO_LEAF_STEPS 4   // AO camera and sample rays: empty leaves stepped over per warp step
+#endif
 #ifndef HR_TRACE_MIN_BLOCKS
 #define HR_TRACE_MIN_BLOCKS 8   // blocks of kTT per SM the ray kernels' register budget must allow (8: 64 registers)
 #endif
@@ -305,7 +308,7 @@ __global__ __launch_bounds__(kTT, HR_TRACE_MIN_BLOCKS) void k_ao_primary_tl(Scen
             if (STATS) h.cells++;
         }
         const bool done = test_lists<kHitClosest, STATS>(s, o, d, b, e, false, h);
-        if (active) active = !done && tl_advance<STATS>(q, s, g, o, d, h);
+        if (active) active = !done && tl_advance<STATS, false, HR_AO_LEAF_STEPS>(q, s, g, o, d, h);
         const bool fin = has && !active;
         const bool hit = fin && valid && h.hit;
         if (hit) {
@@ -406,7 +409,7 @@ __global__ __launch_bounds__(kTT, HR_TRACE_MIN_BLOCKS) void k_ao_samples_tl(Scen
             if (STATS) h.cells++;
         }
         const bool done = test_lists<kHitAny, STATS>(s, o, w, b, e, true, h);
-        if (active) active = !done && tl_advance<STATS>(q, s, g, o, w, h);
+        if (active) active = !done && tl_advance<STATS, false, HR_AO_LEAF_STEPS>(q, s, g, o, w, h);
         const bool fin = has && !active;
         const uint32_t peers = __match_any_sync(kFullMask, fin ? pix : 0xffffffffu);
         const uint32_t nfree = __popc(__ballot_sync(kFullMask, fin && !h.hit) & peers);

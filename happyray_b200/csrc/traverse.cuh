@@ -344,14 +344,20 @@ __device__ __forceinline__ uint32_t tl_leaf(const TL& q) {
 
 // Inner step (TLGridTraverser.h:225-290): stop when the hit lies before the leaf's exit,
 // else step; leaving the sub-grid continues in the top grid.  False when the ray is done.
-template <bool STATS, bool OCC = false>
+// KL > 1: an empty next leaf (no list to test) is stepped over at once, up to KL leaves.
+template <bool STATS, bool OCC = false, int KL = 1>
 __device__ __forceinline__ bool tl_advance(TL& q, const Scene& s, const G& g, f3 o, f3 d, Hit& h) {
     const int32_t lres[3] = {(int32_t)q.lres[0], (int32_t)q.lres[1], (int32_t)q.lres[2]};
-    float tk;
-    const bool inside = dda_step(q.tm2, q.c2, q.rcp, q.scs, lres, &tk);
-    if (h.t < tk) return false;
-    if (inside) return true;
-    return tl_outer_step(q, g, h) && tl_seek<STATS, OCC>(q, s, g, o, d, h);
+    for (int j = 1;; ++j) {
+        float tk;
+        const bool inside = dda_step(q.tm2, q.c2, q.rcp, q.scs, lres, &tk);
+        if (h.t < tk) return false;
+        if (!inside) return tl_outer_step(q, g, h) && tl_seek<STATS, OCC>(q, s, g, o, d, h);
+        if (j >= KL) return true;
+        const uint2 lr = __ldg(s.leaves + tl_leaf(q));
+        if (lr.y > lr.x) return true;
+        if (STATS) h.cells++;
+    }
 }
 
 // Entry of a ray into the two-level grid (TLGridTraverser.h:79-143): clip to the grid
@@ -379,6 +385,9 @@ __device__ __forceinline__ bool tl_setup(TL& q, const Scene& s, const G& g, f3 o
 }
 
 // a15: two-level DDA, warp-synchronous
+#ifndef HR_RAY_LEAF_STEPS
+#define HR_RAY_LEAF_STEPS 1   // camera and query rays of trace_tl: empty leaves stepped over per warp step
+#endif
 template <int HM, bool STATS, bool OCC = false>
 __device__ void trace_tl(const Scene& s, const G& g, f3 o, f3 d, bool any, Hit& h, bool active) {
     TL q;
@@ -391,7 +400,7 @@ __device__ void trace_tl(const Scene& s, const G& g, f3 o, f3 d, bool any, Hit& 
             if (STATS) h.cells++;
         }
         const bool done = test_lists<HM, STATS>(s, o, d, b, e, any, h);
-        if (active) active = !done && tl_advance<STATS, OCC>(q, s, g, o, d, h);
+        if (active) active = !done && tl_advance<STATS, OCC, HR_RAY_LEAF_STEPS>(q, s, g, o, d, h);
     }
 }
 
