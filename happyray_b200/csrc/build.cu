@@ -340,6 +340,15 @@ void drop_build_graph(hr_ctx* c) {
 // Host orchestration of one build.  With wait, syncs and reports the overflow bits in
 // *ovf_out; without, only enqueues (the descriptor lands in c->desc_pinned when the stream
 // has passed the build).  Returns HR status code (0 = ok).
+// status of a built descriptor whose error word is set
+static int desc_error(hr_ctx* c) {
+    if (c->host_desc.error & kDescErrBarrier) {
+        c->small_build_max_tris = 0;   // the pipeline from now on
+        return set_error(c, 1, "grid build: a barrier of the single-launch build gave up waiting");
+    }
+    return set_error(c, 1, "triangle index out of range of the uploaded vertices");
+}
+
 static int build_once_impl(hr_ctx* c, int32_t kind, int32_t exact, uint32_t* ovf_out, bool wait) {
     cudaStream_t s = c->stream;
     GridBuffers& B = c->g;
@@ -505,8 +514,11 @@ static int build_once_impl(hr_ctx* c, int32_t kind, int32_t exact, uint32_t* ovf
         }
     }
     bool enqueued = false;
+    // a small uniform build: one cooperative launch instead of the pipeline (build_small.cu)
+    if (kind == kUniform && (rc = build_small_uniform(c, exact, key_bits, &enqueued))) return rc;
+    if (enqueued) c->nstages = 0;
     std::vector<uint8_t> key;
-    if (HR_BUILD_GRAPH && wait && c->build_graph_ok) key = build_graph_key(c, kind, exact, dens);
+    if (!enqueued && HR_BUILD_GRAPH && wait && c->build_graph_ok) key = build_graph_key(c, kind, exact, dens);
     if (!key.empty() && (key == c->build_key || key == c->last_build_key)) {
         if (c->build_exec && key == c->build_key) {
             if (cudaGraphLaunch(c->build_exec, s) == cudaSuccess) {
@@ -569,7 +581,7 @@ static int build_once_impl(hr_ctx* c, int32_t kind, int32_t exact, uint32_t* ovf
     if ((rc = cuda_check(c, cudaStreamSynchronize(s), "build"))) return rc;
     if (c->timing)
         for (int i = 0; i + 1 < c->nstages; ++i) cudaEventElapsedTime(&c->stage_ms[i], c->ev[i], c->ev[i + 1]);
-    if (c->host_desc.error) return set_error(c, 1, "triangle index out of range of the uploaded vertices");
+    if (c->host_desc.error) return desc_error(c);
     *ovf_out = c->host_desc.overflow;
     return 0;
 }
@@ -650,7 +662,7 @@ int build_async_result(hr_ctx* c, bool* fit) {
     if (!c->async_pending) return 0;
     c->async_pending = false;
     c->host_desc = *c->desc_pinned;
-    if (c->host_desc.error) return set_error(c, 1, "triangle index out of range of the uploaded vertices");
+    if (c->host_desc.error) return desc_error(c);
     const uint32_t ovf = c->host_desc.overflow;
     if (ovf) {
         *fit = false;

@@ -9,6 +9,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <vector>
@@ -230,6 +231,7 @@ hr_status hr_create(hr_ctx** out, int32_t device, void* stream) {
     c->device = device;
     if (cudaSetDevice(device) != cudaSuccess) { delete c; return HR_ERR_DEVICE; }
     cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
+    if (const char* e = std::getenv("HAPPYRAY_SMALL_BUILD_MAX_TRIS")) c->small_build_max_tris = (uint32_t)std::strtoul(e, nullptr, 10);
     if (stream) {
         c->stream = (cudaStream_t)stream;
     } else {
@@ -260,7 +262,7 @@ void hr_destroy(hr_ctx* c) {
                       &c->g.tile_hist, &c->g.row_total, &c->g.leaf_cnt, &c->g.occ,
                       &c->g.lkeys_a, &c->g.lvals_a, &c->g.lkeys_b, &c->g.lvals_b, &c->g.scan_partials,
                       &c->g.tri_ranges, &c->g.ref_ranges, &c->lights_dev, &c->tri_nrm, &c->tri_alb,
-                      &c->hit_t, &c->hit_tri, &c->unocc, &c->queue};
+                      &c->hit_t, &c->hit_tri, &c->unocc, &c->queue, &c->build_bar};
     for (DevBuf* b : bufs) free_buf(c, *b);
     cudaStreamSynchronize(c->stream);
     for (auto& e : c->ev) if (e) cudaEventDestroy(e);

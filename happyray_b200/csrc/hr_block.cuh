@@ -67,9 +67,9 @@ struct PairRun { uint32_t key0, ex, ey, sx, sxy, val; };
 // cells costs its block a few strides instead of one thread a serial loop, and consecutive
 // threads store consecutive slots.  n is this thread's run length, run is read when n > 0.
 // Every thread of the block calls it.
-// With `counts`, also adds every written key to counts[key] (a histogram of the keys; the
-// lanes of a warp holding the same key add once, so a crowded cell costs few atomics).
-template <int NT>
+// With `counts`, also adds every written key to counts[key * CS] (a histogram of the keys;
+// the lanes of a warp holding the same key add once, so a crowded cell costs few atomics).
+template <int NT, int CS = 1>
 __device__ __forceinline__ void block_write_runs(uint32_t n, const PairRun& run, uint32_t out0,
                                                  uint32_t* __restrict__ keys, uint32_t* __restrict__ vals,
                                                  uint32_t* __restrict__ counts = nullptr) {
@@ -99,7 +99,7 @@ __device__ __forceinline__ void block_write_runs(uint32_t n, const PairRun& run,
         }
         if (counts) {
             const uint32_t peers = __match_any_sync(0xffffffffu, key);
-            if (valid && lane == (uint32_t)(__ffs(peers) - 1)) atomicAdd(counts + key, (uint32_t)__popc(peers));
+            if (valid && lane == (uint32_t)(__ffs(peers) - 1)) atomicAdd(counts + (size_t)key * CS, (uint32_t)__popc(peers));
         }
     }
 }

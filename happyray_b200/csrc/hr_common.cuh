@@ -24,6 +24,9 @@ enum GridKind : int32_t { kUniform = 0, kTwoLevel = 1 };
 enum : uint32_t {
     kOvfCells = 1u, kOvfPairs = 2u, kOvfTopPairs = 4u, kOvfLeaves = 8u, kOvfLeafPairs = 16u
 };
+// bits of GridDesc::error: a triangle index beyond the uploaded vertices (set from the
+// upload's index check), a grid barrier of the single-launch build that gave up waiting
+enum : uint32_t { kDescErrIndex = 1u, kDescErrBarrier = 2u };
 
 // Grid descriptor kept in device memory and written by the build kernels, so no host
 // round trip is needed between build stages.  Mirrors UniformGrid (UniformGrid.h:37-138)

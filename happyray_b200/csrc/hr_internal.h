@@ -103,6 +103,11 @@ struct hr_ctx {
     int build_graph_stages = 0;
     bool build_graph_ok = true;      // false once a capture failed: build directly
     bool build_capturing = false;
+    // uniform builds of at most this many triangles run as one cooperative launch
+    // (build_small.cu); HAPPYRAY_SMALL_BUILD_MAX_TRIS at context creation, 0: never
+    uint32_t small_build_max_tris = 131072;
+    int small_build_bps = -1;        // resident blocks per SM of that kernel (-1: not queried)
+    hr::DevBuf build_bar;            // its grid barrier words
     uint64_t launches = 0;       // kernels enqueued by this context (host-side count)
     bool collect_stats = false;  // render kernels accumulate cells visited / triangle tests
     cudaEvent_t ev[16] = {};
@@ -162,6 +167,10 @@ int build_grid(hr_ctx* c, int32_t kind, int32_t exact);
 int build_grid_async(hr_ctx* c, int32_t kind, int32_t exact);
 void drop_build_graph(hr_ctx* c);   // frees the captured rebuild (hr_destroy)
 int build_async_result(hr_ctx* c, bool* fit);
+
+// build_small.cu: the uniform build of a small scene as one cooperative launch.  Returns
+// 0 with *done = false when the scene does not qualify (the caller runs the pipeline).
+int build_small_uniform(hr_ctx* c, int32_t exact, int key_bits, bool* done);
 
 // sort.cu
 int radix_sort_pairs(hr_ctx* c, const uint32_t* keys_in, const uint32_t* vals_in,

@@ -11,16 +11,12 @@
 // host-side capacity and surplus CTAs exit at once.
 #include "hr_internal.h"
 #include "hr_block.cuh"
+#include "radix_tile.cuh"
 
 namespace hr {
 
 namespace {
 
-constexpr int kThreads = 256;
-constexpr int kItems = 8;
-constexpr int kTile = kThreads * kItems;   // 2048 keys per tile
-constexpr int kRadix = 512;                // max digit width 9 bits (two digits per thread below)
-constexpr int kWarps = kThreads / 32;
 // ----------------------------------------------------------------------------------
 // generic exclusive scan: reduce -> scan partials -> apply
 
@@ -121,130 +117,20 @@ __global__ __launch_bounds__(kThreads) void k_scan_apply(T* data, const uint32_t
 __global__ __launch_bounds__(kThreads) void k_radix_upsweep(const uint32_t* __restrict__ keys, const uint32_t* d_count,
                                                             int shift, uint32_t mask, uint32_t* tile_hist,
                                                             uint32_t ntiles_cap) {
-    __shared__ uint32_t h[kRadix];
-    for (int d = threadIdx.x; d < kRadix; d += kThreads) h[d] = 0u;
-    __syncthreads();
-    const uint32_t n = *d_count;
-    const size_t base = (size_t)blockIdx.x * kTile;
-    const int lane = threadIdx.x & 31;
-    if (base >= n) {   // a tile past the count: an empty histogram column
-        for (uint32_t d = threadIdx.x; d <= mask; d += kThreads) tile_hist[(size_t)d * ntiles_cap + blockIdx.x] = 0u;
-        return;
-    }
-#pragma unroll
-    for (int k = 0; k < kItems; ++k) {
-        size_t i = base + threadIdx.x + (size_t)k * kThreads;
-        uint32_t dig = i < n ? (__ldg(keys + i) >> shift) & mask : 0xffffffffu;
-        uint32_t peers = __match_any_sync(kFullMask, dig);
-        if (dig != 0xffffffffu && lane == __ffs(peers) - 1) atomicAdd(&h[dig], __popc(peers));
-    }
-    __syncthreads();
-    for (uint32_t d = threadIdx.x; d <= mask; d += kThreads) tile_hist[(size_t)d * ntiles_cap + blockIdx.x] = h[d];
+    radix_upsweep_tile<false>(keys, *d_count, shift, mask, tile_hist, ntiles_cap, blockIdx.x);
 }
 
 // one CTA per digit: exclusive scan of its row of tile counts, row total out
 __global__ __launch_bounds__(1024) void k_radix_scan(uint32_t* tile_hist, uint32_t ntiles_cap, uint32_t* row_total) {
-    uint32_t* row = tile_hist + (size_t)blockIdx.x * ntiles_cap;
-    uint32_t carry = 0;
-    for (uint32_t b = 0; b < ntiles_cap; b += 1024) {
-        uint32_t i = b + threadIdx.x;
-        uint32_t x = i < ntiles_cap ? row[i] : 0u;
-        uint32_t tot;
-        uint32_t ex = block_excl_scan<uint32_t, 1024>(x, &tot);
-        if (i < ntiles_cap) row[i] = carry + ex;
-        carry += tot;
-    }
-    if (threadIdx.x == 0) row_total[blockIdx.x] = carry;
+    radix_scan_row<1024>(tile_hist + (size_t)blockIdx.x * ntiles_cap, ntiles_cap, row_total + blockIdx.x);
 }
 
 __global__ __launch_bounds__(kThreads) void k_radix_downsweep(
     const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in, uint32_t* __restrict__ keys_out,
     uint32_t* __restrict__ vals_out, const uint32_t* d_count, int shift, uint32_t mask,
     const uint32_t* __restrict__ tile_hist, uint32_t ntiles_cap, const uint32_t* __restrict__ row_total) {
-    __shared__ uint32_t s_whist[kWarps][kRadix];
-    __shared__ uint32_t s_goff[kRadix];
-    __shared__ uint32_t s_loff[kRadix];
-    __shared__ uint32_t s_keys[kTile];
-    __shared__ uint32_t s_vals[kTile];
-
-    const uint32_t n = *d_count;
-    const size_t base = (size_t)blockIdx.x * kTile;
-    if (base >= n) return;
-    const uint32_t nvalid = (uint32_t)min((size_t)kTile, n - base);
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const uint32_t lt_mask = (1u << lane) - 1u;
-
-    for (int i = threadIdx.x; i < kWarps * kRadix; i += kThreads) (&s_whist[0][0])[i] = 0u;
-    // digit start = exclusive scan of the digit totals (digits 2t and 2t + 1 on thread t)
-    {
-        const uint32_t d0 = 2u * threadIdx.x, d1 = d0 + 1u;
-        const uint32_t t0 = d0 <= mask ? row_total[d0] : 0u, t1 = d1 <= mask ? row_total[d1] : 0u;
-        uint32_t all;
-        const uint32_t ex = block_excl_scan<uint32_t, kThreads>(t0 + t1, &all);
-        if (d0 <= mask) s_goff[d0] = ex + tile_hist[(size_t)d0 * ntiles_cap + blockIdx.x];
-        if (d1 <= mask) s_goff[d1] = ex + t0 + tile_hist[(size_t)d1 * ntiles_cap + blockIdx.x];
-    }
-    __syncthreads();
-
-    uint32_t key[kItems], val[kItems], rank[kItems], dig[kItems];
-#pragma unroll
-    for (int r = 0; r < kItems; ++r) {
-        const uint32_t li = (uint32_t)w * 32u * kItems + (uint32_t)r * 32u + (uint32_t)lane;
-        const bool valid = li < nvalid;
-        key[r] = valid ? __ldg(keys_in + base + li) : 0u;
-        val[r] = valid ? __ldg(vals_in + base + li) : 0u;
-        dig[r] = valid ? (key[r] >> shift) & mask : 0xffffffffu;
-        const uint32_t peers = __match_any_sync(kFullMask, dig[r]);
-        const int leader = __ffs(peers) - 1;
-        uint32_t b = 0;
-        if (valid && lane == leader) {
-            b = s_whist[w][dig[r]];
-            s_whist[w][dig[r]] = b + __popc(peers);
-        }
-        b = __shfl_sync(kFullMask, b, leader);
-        rank[r] = b + __popc(peers & lt_mask);
-        __syncwarp();
-    }
-    __syncthreads();
-    // per digit: exclusive prefix over warps, tile-local digit totals (digits 2t, 2t + 1)
-    uint32_t tcount[2] = {0u, 0u};
-#pragma unroll
-    for (int j = 0; j < 2; ++j) {
-        const uint32_t d = 2u * threadIdx.x + (uint32_t)j;
-        if (d <= mask) {
-            uint32_t run = 0;
-#pragma unroll
-            for (int ww = 0; ww < kWarps; ++ww) {
-                uint32_t cnt = s_whist[ww][d];
-                s_whist[ww][d] = run;
-                run += cnt;
-            }
-            tcount[j] = run;
-        }
-    }
-    {
-        uint32_t all;
-        const uint32_t ex = block_excl_scan<uint32_t, kThreads>(tcount[0] + tcount[1], &all);
-        if (2u * threadIdx.x <= mask) s_loff[2u * threadIdx.x] = ex;
-        if (2u * threadIdx.x + 1u <= mask) s_loff[2u * threadIdx.x + 1u] = ex + tcount[0];
-    }
-    __syncthreads();
-#pragma unroll
-    for (int r = 0; r < kItems; ++r) {
-        if (dig[r] != 0xffffffffu) {
-            uint32_t lp = s_loff[dig[r]] + s_whist[w][dig[r]] + rank[r];
-            s_keys[lp] = key[r];
-            s_vals[lp] = val[r];
-        }
-    }
-    __syncthreads();
-    for (uint32_t j = threadIdx.x; j < nvalid; j += kThreads) {
-        uint32_t k = s_keys[j];
-        uint32_t d = (k >> shift) & mask;
-        uint32_t g = s_goff[d] + (j - s_loff[d]);
-        keys_out[g] = k;
-        vals_out[g] = s_vals[j];
-    }
+    radix_downsweep_tile<false>(keys_in, vals_in, keys_out, vals_out, *d_count, shift, mask, tile_hist, ntiles_cap,
+                                row_total, blockIdx.x);
 }
 
 }  // namespace
