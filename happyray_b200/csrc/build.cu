@@ -337,9 +337,6 @@ void drop_build_graph(hr_ctx* c) {
     c->build_key.clear();
 }
 
-// Host orchestration of one build.  With wait, syncs and reports the overflow bits in
-// *ovf_out; without, only enqueues (the descriptor lands in c->desc_pinned when the stream
-// has passed the build).  Returns HR status code (0 = ok).
 // status of a built descriptor whose error word is set
 static int desc_error(hr_ctx* c) {
     if (c->host_desc.error & kDescErrBarrier) {
@@ -349,6 +346,9 @@ static int desc_error(hr_ctx* c) {
     return set_error(c, 1, "triangle index out of range of the uploaded vertices");
 }
 
+// Host orchestration of one build.  With wait, syncs and reports the overflow bits in
+// *ovf_out; without, only enqueues (the descriptor lands in c->desc_pinned when the stream
+// has passed the build).  Returns HR status code (0 = ok).
 static int build_once_impl(hr_ctx* c, int32_t kind, int32_t exact, uint32_t* ovf_out, bool wait) {
     cudaStream_t s = c->stream;
     GridBuffers& B = c->g;
@@ -497,7 +497,9 @@ static int build_once_impl(hr_ctx* c, int32_t kind, int32_t exact, uint32_t* ovf
     // settings: a mesh rebuilt every frame) is captured once as a CUDA graph and then
     // replayed: one launch instead of about 35, so small builds are not paced by the host's
     // launch rate.  An animated mesh replays the same graph for every frame time: the frame
-    // pair and weight go to frame_sel first, outside the graph.
+    // pair and weight go to frame_sel first, outside the graph.  Asynchronous builds (the
+    // server's rebuilds) replay it too; a stream wait enqueued before the capture stays
+    // outside the graph and orders its launch.
     // (only when the word does not hold this selection already: a static mesh whose frame
     // time is set every frame launches nothing extra)
     if (c->lerp_pending) {
@@ -513,12 +515,15 @@ static int build_once_impl(hr_ctx* c, int32_t kind, int32_t exact, uint32_t* ovf
             c->frame_sel_valid = true;
         }
     }
-    bool enqueued = false;
+    bool enqueued = false, single = false;
     // a small uniform build: one cooperative launch instead of the pipeline (build_small.cu)
-    if (kind == kUniform && (rc = build_small_uniform(c, exact, key_bits, &enqueued))) return rc;
-    if (enqueued) c->nstages = 0;
+    if (kind == kUniform && wait && (rc = build_small_uniform(c, exact, key_bits, &single))) return rc;
+    if (single) {
+        enqueued = true;
+        c->nstages = 0;
+    }
     std::vector<uint8_t> key;
-    if (!enqueued && HR_BUILD_GRAPH && wait && c->build_graph_ok) key = build_graph_key(c, kind, exact, dens);
+    if (!enqueued && HR_BUILD_GRAPH && c->build_graph_ok) key = build_graph_key(c, kind, exact, dens);
     if (!key.empty() && (key == c->build_key || key == c->last_build_key)) {
         if (c->build_exec && key == c->build_key) {
             if (cudaGraphLaunch(c->build_exec, s) == cudaSuccess) {
@@ -579,6 +584,11 @@ static int build_once_impl(hr_ctx* c, int32_t kind, int32_t exact, uint32_t* ovf
                          "descriptor download")))
         return rc;
     if ((rc = cuda_check(c, cudaStreamSynchronize(s), "build"))) return rc;
+    if (single && (c->host_desc.error & kDescErrBarrier)) {
+        // the single launch gave up at a barrier: the pipeline builds it, from now on too
+        c->small_build_max_tris = 0;
+        return build_once_impl(c, kind, exact, ovf_out, wait);
+    }
     if (c->timing)
         for (int i = 0; i + 1 < c->nstages; ++i) cudaEventElapsedTime(&c->stage_ms[i], c->ev[i], c->ev[i + 1]);
     if (c->host_desc.error) return desc_error(c);

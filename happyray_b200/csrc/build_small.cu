@@ -27,7 +27,8 @@
 // Every block meets every barrier or leaves at the same point: a block returns early only
 // on conditions all blocks compute identically (overflow, bad index, the ordering choice).
 // The barrier's wait is bounded: a block that gives up sets kDescErrBarrier in the
-// descriptor's error word and returns, and the host reports the build as failed.
+// descriptor's error word and returns, and the host builds the grid again through the
+// pipeline (and keeps the context on it).
 #include "build_dev.cuh"
 #include "radix_tile.cuh"
 
@@ -508,9 +509,11 @@ int build_small_uniform(hr_ctx* c, int32_t exact, int key_bits, bool* done) {
         }
         c->small_build_bps = bps;
     }
-    // one block per SM at least (the sort phases), one per 256 triangles (phases 2-3)
+    // one block per SM at least (the sort phases), one per 256 triangles (phases 2-3), and
+    // at most half the blocks the GPU holds at once, so that two such builds on different
+    // streams always fit side by side
     const uint32_t G = std::max((ntri + kBT - 1) / kBT, (uint32_t)c->num_sms);
-    if (c->small_build_bps <= 0 || G > (uint32_t)c->small_build_bps * (uint32_t)c->num_sms) return 0;
+    if (c->small_build_bps <= 0 || 2 * G > (uint32_t)c->small_build_bps * (uint32_t)c->num_sms) return 0;
     const size_t bar_words = 4, bytes = sizeof(uint32_t) * (bar_words + 10 * (size_t)G);
     const void* before = c->build_bar.p;
     const size_t before_bytes = c->build_bar.bytes;
