@@ -226,7 +226,14 @@ __device__ __forceinline__ bool clip(const G& g, f3 o, const float* rcp, float* 
     return *t1 > *t0 && *t1 >= 0.0f;
 }
 
-// a14: uniform grid DDA (UGridTraverser.h:76-172), warp-synchronous
+// a14: uniform grid DDA (UGridTraverser.h:76-172), warp-synchronous.  After a lane's list
+// test it steps on over up to HR_UG_CELL_STEPS - 1 empty cells within the same warp step
+// (an empty cell has no list to test) and keeps the range of the non-empty cell it stops
+// at for the next step; each lane visits the same cells in the same order as one cell per
+// step would.
+#ifndef HR_UG_CELL_STEPS
+#define HR_UG_CELL_STEPS 4
+#endif
 template <int HM, bool STATS>
 __device__ void trace_ug(const Scene& s, const G& g, f3 o, f3 d, bool any, Hit& h, bool active) {
     float rcp[3] = {0.0f, 0.0f, 0.0f}, tmax[3] = {0.0f, 0.0f, 0.0f};
@@ -254,21 +261,37 @@ __device__ void trace_ug(const Scene& s, const G& g, f3 o, f3 d, bool any, Hit& 
         }
     }
     const uint32_t rx = (uint32_t)g.res[0], rxy = (uint32_t)g.res[0] * (uint32_t)g.res[1];
+    uint2 cr_next = make_uint2(0u, 0u);
+    bool have_next = false;
     while (__any_sync(kFullMask, active)) {
         uint32_t b = 0, e = 0;
         if (active) {
-            const uint2 cr = __ldg(s.cells + ((uint32_t)cell[0] + (uint32_t)cell[1] * rx + (uint32_t)cell[2] * rxy));
+            const uint2 cr = have_next ? cr_next
+                                       : __ldg(s.cells + ((uint32_t)cell[0] + (uint32_t)cell[1] * rx +
+                                                          (uint32_t)cell[2] * rxy));
             b = cr.x; e = cr.y;
             if (STATS) h.cells++;
         }
         const bool done = test_lists<HM, STATS>(s, o, d, b, e, any, h);
+        have_next = false;
         if (active) {
             if (done) {
                 active = false;
             } else {
-                float tk;
-                const bool inside = dda_step(tmax, cell, rcp, g.cs, g.res, &tk);
-                active = h.t > tk && inside;
+                for (int j = 1;; ++j) {
+                    float tk;
+                    const bool inside = dda_step(tmax, cell, rcp, g.cs, g.res, &tk);
+                    active = h.t > tk && inside;
+                    if (!active || j >= HR_UG_CELL_STEPS) break;
+                    const uint2 nx =
+                        __ldg(s.cells + ((uint32_t)cell[0] + (uint32_t)cell[1] * rx + (uint32_t)cell[2] * rxy));
+                    if (nx.y > nx.x) {
+                        cr_next = nx;
+                        have_next = true;
+                        break;
+                    }
+                    if (STATS) h.cells++;
+                }
             }
         }
     }
