@@ -92,13 +92,20 @@ class Hierarchy:
         self._check(self._lib.hr_hier_download(self._h, _p(objs), _p(oc), _p(tri), _p(tc), _p(ii)), "download")
         return objs, oc, tri, tc, ii
 
-    def trace_rays(self, org, dirs):
-        """Closest hits: (instance id, triangle id, t, u, v), -1 ids on a miss."""
+    def trace_rays(self, org, dirs, out=None):
+        """Closest hits: (instance id, triangle id, t, u, v), -1 ids on a miss.  out: five
+        caller arrays of n elements (int32, int32, float32 x 3) to fill instead of new ones,
+        e.g. page-locked ones, whose copies run at the full host link rate."""
         org = np.ascontiguousarray(org, np.float32)
         dirs = np.ascontiguousarray(dirs, np.float32)
         n = org.shape[0]
-        out = [np.empty(n, np.int32), np.empty(n, np.int32), np.empty(n, np.float32), np.empty(n, np.float32),
-               np.empty(n, np.float32)]
+        if out is None:
+            out = [np.empty(n, np.int32), np.empty(n, np.int32), np.empty(n, np.float32), np.empty(n, np.float32),
+                   np.empty(n, np.float32)]
+        else:
+            want = (np.int32, np.int32, np.float32, np.float32, np.float32)
+            if len(out) != 5 or any(a.dtype != w or a.size != n or not a.flags.c_contiguous for a, w in zip(out, want)):
+                raise ValueError("trace_rays: out must be five contiguous arrays of n int32, int32, float32 x 3")
         self._check(self._lib.hr_hier_trace_rays(self._h, _p(org), _p(dirs), n, *[_p(a) for a in out]), "trace_rays")
         return tuple(out)
 

@@ -43,6 +43,12 @@ def check_hits(h, ob, oracle, org, d):
     want = oracle.hier_trace(ob, org, d)
     for g, w in zip(got, want):
         assert np.array_equal(g, w)
+    # the same query into caller arrays (filled in place, returned as given)
+    n = org.shape[0]
+    out = [np.full(n, 7, np.int32), np.full(n, 7, np.int32)] + [np.full(n, 7.0, np.float32) for _ in range(3)]
+    again = h.trace_rays(org, d, out=out)
+    for a, o, g in zip(again, out, got):
+        assert a is o and np.array_equal(a, g)
     return got
 
 
