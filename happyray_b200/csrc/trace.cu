@@ -29,7 +29,7 @@
 #define HR_AO_PRIMARY_REFILL_MIN 32   // idle lanes that make k_ao_primary_tl refill (> 32: k_ao_primary)
 #endif
 #ifndef HR_AO_LEAF_STEPS
-#define HR_AO_LEAF_STEPS 4   // AO camera and sample rays: empty leaves stepped over per warp step
+#define HR_AO_LEAF_STEPS 6   // AO camera and sample rays: empty leaves stepped over per warp step
 #endif
 #ifndef HR_TRACE_MIN_BLOCKS
 #define HR_TRACE_MIN_BLOCKS 8   // blocks of kTT per SM the ray kernels' register budget must allow (8: 64 registers)
