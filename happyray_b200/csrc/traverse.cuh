@@ -434,7 +434,7 @@ __device__ void trace_tl(const Scene& s, const G& g, f3 o, f3 d, bool any, Hit& 
 // done, 1 in a leaf, 2 walking empty top cells.  (Camera, AO and query rays keep the
 // unbounded walk of trace_tl: paced, they measured slower.)
 #ifndef HR_PT_SEEK_STEPS
-#define HR_PT_SEEK_STEPS 2   // path and shadow rays: empty top cells per warp step (0: unbounded)
+#define HR_PT_SEEK_STEPS 3   // path and shadow rays: empty top cells per warp step (0: unbounded)
 #endif
 #ifndef HR_PT_LEAF_STEPS
 #define HR_PT_LEAF_STEPS 4   // path and shadow rays: leaves stepped per warp step while they are empty
