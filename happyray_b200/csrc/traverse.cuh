@@ -541,15 +541,16 @@ __device__ __forceinline__ void trace_one(const Scene& s, const G& g, f3 o, f3 d
 }
 
 // As trace_one, with the hit mode chosen per lane: any hit where `any` is set, closest
-// hit elsewhere (one traversal for the path and the shadow rays of a warp's lanes).
-template <int KIND, bool STATS>
+// hit elsewhere (one traversal for the path and the shadow rays of a warp's lanes).  SEEK:
+// empty top cells a lane walks per warp step (0: unbounded).
+template <int KIND, bool STATS, int SEEK = HR_PT_SEEK_STEPS>
 __device__ __forceinline__ void trace_mixed(const Scene& s, const G& g, f3 o, f3 d, float tmax, bool any, Hit& h,
                                             bool active) {
     h.t = tmax; h.u = 0.0f; h.v = 0.0f; h.tri = 0; h.hit = false; h.cells = 0; h.tests = 0;
     if (s.ntri == 0) return;
     if (KIND == kUniform) trace_ug<kHitMixed, STATS>(s, g, o, d, any, h, active);
     // path rays: occupancy bits
-    else if constexpr (HR_PT_SEEK_STEPS > 0) trace_tl_paced<kHitMixed, STATS, true, HR_PT_SEEK_STEPS>(s, g, o, d, any, h, active);
+    else if constexpr (SEEK > 0) trace_tl_paced<kHitMixed, STATS, true, SEEK>(s, g, o, d, any, h, active);
     else trace_tl<kHitMixed, STATS, true>(s, g, o, d, any, h, active);
 }
 
@@ -789,13 +790,13 @@ __device__ __forceinline__ void path_begin(PathState& p, const Cam& cam, uint32_
 // radiance, formed with the throughput before the albedo factor, is added when its shadow
 // ray comes back free.  Returns true while the path goes on (it ends on a miss, on hitting
 // the light, or after k.bounces bounces); p.L is then its radiance.  Warp-synchronous: all
-// lanes call it, lanes without a path pass alive = false.
-template <int KIND, bool STATS>
+// lanes call it, lanes without a path pass alive = false.  SEEK as in trace_mixed.
+template <int KIND, bool STATS, int SEEK = HR_PT_SEEK_STEPS>
 __device__ __forceinline__ bool path_step(const Scene& s, const G& g, const PtConsts& k, PathState& p, bool alive,
                                           PtCounts& n) {
     if (k.bounces <= 0) return false;   // no bounce: radiance 0 (uniform over the warp)
     Hit h;
-    trace_mixed<KIND, STATS>(s, g, p.o, p.d, p.tmax, p.shadow, h, alive);
+    trace_mixed<KIND, STATS, SEEK>(s, g, p.o, p.d, p.tmax, p.shadow, h, alive);
     if (!alive) return false;
     if (p.shadow) {
         n.srays += 1;
